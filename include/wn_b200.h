@@ -1,0 +1,91 @@
+/* libwn_b200 — C ABI of the B200 (sm_100a) exact generalized winding number.
+ *
+ * Drop-in for the winding-number entry points of lee101/mojo-libigl's
+ * `libmojo-libigl.so` (exported from src/capi.mojo:923-1007, bound by
+ * python/igl/_lib.py:18-32 with every argument an int64). Plain C types only:
+ * pointers, int64_t sizes and int status codes; no torch or CUDA types.
+ *
+ * Conventions
+ *   tri   triangle soup, structure of arrays: 9 rows of nf doubles, row
+ *         3*corner+axis (corner a,b,c; axis x,y,z), i.e. tri[(3c+x)*nf + f].
+ *         This is python/igl/__init__.py:248-250's
+ *         `vertices[faces].transpose(1, 2, 0).reshape(9, nf)`.
+ *   q     queries, nq x 3 row-major doubles.
+ *   w     nq doubles, W(q) = sum_f atan2(det_f, denom_f) / (2*pi).
+ *   "host" entry points take host pointers, copy in, compute, copy out and
+ *   synchronise. "device" entry points take device pointers and a cudaStream_t
+ *   passed as void*; they are asynchronous: call wn_stream_check() to
+ *   synchronise and collect device-side errors.
+ *   Return value: 0 = success, otherwise a WN_E* code; wn_last_error() gives
+ *   the message (per calling thread). The mli_* names keep the reference's
+ *   own return conventions.
+ */
+#ifndef WN_B200_H
+#define WN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  WN_OK = 0,
+  WN_EINVAL = 1,   /* bad sizes, pointers or alignment */
+  WN_ENODEV = 2,   /* no CUDA device / driver */
+  WN_ECUDA = 3,    /* a CUDA runtime call failed */
+  WN_EDEVICE = 4,  /* a kernel reported an error (e.g. a bounded wait ran out) */
+  WN_ENOMEM = 5    /* device allocation failed */
+};
+
+/* FP64 accumulation modes of the plain kernel. */
+enum {
+  WN_FP64_ARGPROD = 0, /* bit-exact pair terms, argument-of-product sum (default) */
+  WN_FP64_DIRECT = 1   /* bit-exact pair terms, one atan2 per pair */
+};
+
+/* ---- reference-compatible entry points --------------------------------- */
+
+/* Replaces src/capi.mojo:938-942 `mli_winding(tri, q, dst, nf, nq, q0, q1)`:
+ * CPU evaluation of queries [q0, q1) into dst[q0:q1). Reentrant over disjoint
+ * spans (python/igl/_lib.py:72-95 fans spans out over threads). */
+void mli_winding(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t nq, int64_t q0,
+                 int64_t q1);
+
+/* Replaces src/capi.mojo:945-947 `mli_winding_gpu(tri, q, dst, nf, nq) -> Int`
+ * (host addresses; 1 = success, 0 = failure, python/igl/__init__.py:253-263).
+ * Runs the plain FP64 kernel on the current CUDA device. */
+int64_t mli_winding_gpu(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t nq);
+
+/* The reference's other eleven exports (src/capi.mojo:923-937, 950-1007) are
+ * exported under the same names so the reference shim's loader
+ * (python/igl/_lib.py:122-130) resolves every symbol; they are outside this
+ * library's scope and abort the process with a message if called. */
+
+/* ---- runtime ------------------------------------------------------------ */
+
+int wn_version(void);                 /* 100 * major + minor */
+const char* wn_last_error(void);      /* message of this thread's last failure */
+int wn_device_count(void);            /* CUDA devices visible (0 if none) */
+int wn_device_memory(int64_t* free_bytes, int64_t* total_bytes); /* current device */
+/* Synchronise `stream` and report (then clear) device-side errors raised by
+ * device entry points launched on it since the last check. */
+int wn_stream_check(void* stream);
+
+/* ---- plain FP64 forward (no reference counterpart beyond mli_winding_gpu) */
+
+/* Host pointers; mode = WN_FP64_ARGPROD or WN_FP64_DIRECT. */
+int wn_forward_fp64_host(const double* tri, const double* q, double* w, int64_t nf, int64_t nq,
+                         int mode);
+
+/* Device pointers. tri: 9 rows with row stride ld doubles (ld even, ld >= nf),
+ * 16-byte aligned. Scratch (for face splits when nq is small) comes from the
+ * library's per-device workspace. */
+int wn_forward_fp64_device(const double* tri, int64_t ld, const double* q, double* w, int64_t nf,
+                           int64_t nq, int mode, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WN_B200_H */

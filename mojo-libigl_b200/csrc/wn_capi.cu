@@ -1,0 +1,275 @@
+// C ABI of libwn_b200 (declared in include/wn_b200.h) and its small runtime:
+// one context per CUDA device (stream, SM count, device error word) and a
+// grow-only workspace for the host-pointer entry points, all behind one mutex
+// so the library is safe to call from the reference shim's worker threads.
+//
+// The reference creates a DeviceContext, four allocations and a synchronise on
+// every call (src/capi.mojo:366-398); here the context and buffers persist and
+// only grow.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+#include <string>
+
+#include "../../include/wn_b200.h"
+#include "wn_internal.h"
+
+namespace wn {
+namespace {
+
+constexpr int kMaxDevices = 64;
+
+thread_local std::string t_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  t_last_error = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(e == cudaErrorMemoryAllocation ? WN_ENOMEM : WN_ECUDA, "%s: %s (%s)", what,
+              cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+struct Buffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t need) {
+    if (need <= bytes) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    size_t grow = need + need / 4;
+    cudaError_t e = cudaMalloc(&ptr, grow);
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      return e;
+    }
+    bytes = grow;
+    return cudaSuccess;
+  }
+};
+
+struct DeviceCtx {
+  bool ready = false;
+  int sms = 0;
+  cudaStream_t stream = nullptr;
+  int* err = nullptr;  // device error word
+  Buffer tri, q, w, scratch;
+};
+
+std::mutex g_mutex;
+DeviceCtx g_ctx[kMaxDevices];
+
+// Returns the current device's context (initialising it), or null with the
+// error recorded.
+DeviceCtx* context(int* code) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    *code = fail(WN_ENODEV, "no usable CUDA device: %s", cudaGetErrorString(e));
+    return nullptr;
+  }
+  DeviceCtx& c = g_ctx[dev];
+  if (c.ready) return &c;
+  if ((e = cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaMalloc(&c.err, sizeof(int))) != cudaSuccess ||
+      (e = cudaMemset(c.err, 0, sizeof(int))) != cudaSuccess) {
+    *code = cuda_fail(e, "device context setup");
+    return nullptr;
+  }
+  c.ready = true;
+  return &c;
+}
+
+// Reads and clears the device error word after `stream` has drained.
+int collect_device_error(DeviceCtx* c, cudaStream_t stream) {
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, c->err, sizeof(int), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel execution");
+  if (h != 0) {
+    cudaMemsetAsync(c->err, 0, sizeof(int), stream);
+    cudaStreamSynchronize(stream);
+    return fail(WN_EDEVICE, "device error word 0x%x (1 = bounded wait ran out, 2 = bad launch)",
+                h);
+  }
+  return WN_OK;
+}
+
+int64_t even_ld(int64_t nf) { return ((nf > 0 ? nf : 1) + 1) & ~int64_t(1); }
+
+int forward_fp64_host(const double* tri, const double* q, double* w, int64_t nf, int64_t nq,
+                      int mode) {
+  if (nf < 0 || nq < 0) return fail(WN_EINVAL, "negative size (nf=%lld, nq=%lld)",
+                                    (long long)nf, (long long)nq);
+  if (mode != kFp64ArgProd && mode != kFp64Direct) return fail(WN_EINVAL, "bad mode %d", mode);
+  if (nq == 0) return WN_OK;
+  if ((nf > 0 && !tri) || !q || !w) return fail(WN_EINVAL, "null pointer");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  const int64_t ld = even_ld(nf);
+  const Fp64Plan plan = plan_fp64(nf, nq, c->sms);
+  cudaError_t e;
+  if ((e = c->tri.ensure(sizeof(double) * 9 * ld)) != cudaSuccess ||
+      (e = c->q.ensure(sizeof(double) * 3 * nq)) != cudaSuccess ||
+      (e = c->w.ensure(sizeof(double) * nq)) != cudaSuccess ||
+      (e = c->scratch.ensure(sizeof(double) * (plan.scratch_doubles + 1))) != cudaSuccess)
+    return cuda_fail(e, "device allocation");
+  double* tri_d = static_cast<double*>(c->tri.ptr);
+  double* q_d = static_cast<double*>(c->q.ptr);
+  double* w_d = static_cast<double*>(c->w.ptr);
+  if (nf > 0 && (e = cudaMemcpy2DAsync(tri_d, sizeof(double) * ld, tri, sizeof(double) * nf,
+                                       sizeof(double) * nf, 9, cudaMemcpyHostToDevice,
+                                       c->stream)) != cudaSuccess)
+    return cuda_fail(e, "copy of the triangle soup");
+  if ((e = cudaMemcpyAsync(q_d, q, sizeof(double) * 3 * nq, cudaMemcpyHostToDevice, c->stream)) !=
+      cudaSuccess)
+    return cuda_fail(e, "copy of the queries");
+  if ((e = launch_fp64(plan, mode, tri_d, ld, nf, q_d, nq, w_d,
+                       static_cast<double*>(c->scratch.ptr), c->err, c->stream)) != cudaSuccess)
+    return cuda_fail(e, "FP64 winding-number launch");
+  if ((e = cudaMemcpyAsync(w, w_d, sizeof(double) * nq, cudaMemcpyDeviceToHost, c->stream)) !=
+      cudaSuccess)
+    return cuda_fail(e, "copy of the result");
+  return collect_device_error(c, c->stream);
+}
+
+[[noreturn]] void out_of_scope(const char* name) {
+  std::fprintf(stderr,
+               "libwn_b200: %s is not provided: this library implements only the "
+               "winding-number path (mli_winding, mli_winding_gpu)\n",
+               name);
+  std::abort();
+}
+
+}  // namespace
+}  // namespace wn
+
+using namespace wn;
+
+extern "C" {
+
+int wn_version(void) { return 100; }
+
+const char* wn_last_error(void) { return t_last_error.c_str(); }
+
+int wn_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int wn_device_memory(int64_t* free_bytes, int64_t* total_bytes) {
+  size_t f = 0, t = 0;
+  cudaError_t e = cudaMemGetInfo(&f, &t);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(WN_ENODEV, "cudaMemGetInfo: %s", cudaGetErrorString(e));
+  }
+  if (free_bytes) *free_bytes = static_cast<int64_t>(f);
+  if (total_bytes) *total_bytes = static_cast<int64_t>(t);
+  return WN_OK;
+}
+
+int wn_stream_check(void* stream) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  return collect_device_error(c, static_cast<cudaStream_t>(stream));
+}
+
+int wn_forward_fp64_host(const double* tri, const double* q, double* w, int64_t nf, int64_t nq,
+                         int mode) {
+  return forward_fp64_host(tri, q, w, nf, nq, mode);
+}
+
+int wn_forward_fp64_device(const double* tri, int64_t ld, const double* q, double* w, int64_t nf,
+                           int64_t nq, int mode, void* stream) {
+  if (nf < 0 || nq < 0 || (ld & 1) || ld < nf)
+    return fail(WN_EINVAL, "bad sizes (nf=%lld, nq=%lld, ld=%lld; ld must be even and >= nf)",
+                (long long)nf, (long long)nq, (long long)ld);
+  if (reinterpret_cast<uintptr_t>(tri) & 15) return fail(WN_EINVAL, "tri must be 16-byte aligned");
+  if (mode != kFp64ArgProd && mode != kFp64Direct) return fail(WN_EINVAL, "bad mode %d", mode);
+  if (nq == 0) return WN_OK;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  const Fp64Plan plan = plan_fp64(nf, nq, c->sms);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // Stream-ordered scratch: calls on different streams never share it.
+  double* scratch = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (plan.scratch_doubles > 0 &&
+      (e = cudaMallocAsync(reinterpret_cast<void**>(&scratch),
+                           sizeof(double) * plan.scratch_doubles, st)) != cudaSuccess)
+    return cuda_fail(e, "device allocation");
+  e = launch_fp64(plan, mode, tri, ld, nf, q, nq, w, scratch, c->err, st);
+  if (scratch) cudaFreeAsync(scratch, st);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "FP64 winding-number launch");
+}
+
+// src/capi.mojo:945-947: 1 on success, 0 on failure (the shim raises).
+int64_t mli_winding_gpu(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t nq) {
+  return forward_fp64_host(reinterpret_cast<const double*>(tri),
+                           reinterpret_cast<const double*>(q), reinterpret_cast<double*>(dst), nf,
+                           nq, kFp64ArgProd) == WN_OK
+             ? 1
+             : 0;
+}
+
+// Out-of-scope reference exports (src/capi.mojo:923-937, 950-1007).
+void mli_cot_entries(int64_t, int64_t, int64_t, int64_t, int64_t) {
+  out_of_scope("mli_cot_entries");
+}
+void mli_mass_contributions(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
+  out_of_scope("mli_mass_contributions");
+}
+void mli_vertex_normals(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
+  out_of_scope("mli_vertex_normals");
+}
+void mli_aabb_squared_distance(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t,
+                               int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
+  out_of_scope("mli_aabb_squared_distance");
+}
+void mli_heat_vector_divergence(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
+  out_of_scope("mli_heat_vector_divergence");
+}
+void mli_heat_precompute(int64_t, int64_t, int64_t, int64_t) {
+  out_of_scope("mli_heat_precompute");
+}
+void mli_arap_covariance(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t,
+                         int64_t) {
+  out_of_scope("mli_arap_covariance");
+}
+void mli_arap_rhs(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
+  out_of_scope("mli_arap_rhs");
+}
+void mli_arap_covariance_rims(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t,
+                              int64_t) {
+  out_of_scope("mli_arap_covariance_rims");
+}
+void mli_arap_rhs_rims(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
+  out_of_scope("mli_arap_rhs_rims");
+}
+void mli_arap_rotations(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
+  out_of_scope("mli_arap_rotations");
+}
+
+}  // extern "C"

@@ -1,0 +1,37 @@
+// Internal (non-exported) interfaces between the kernel files and the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace wn {
+
+// ---- plain FP64 forward (wn_fp64.cu) ---------------------------------------
+enum Fp64Mode : int {
+  kFp64ArgProd = 0,  // bit-exact pair terms, argument-of-product accumulation
+  kFp64Direct = 1,   // bit-exact pair terms, one atan2 per pair
+};
+
+struct Fp64Plan {
+  int threads = 128;      // threads per CTA
+  int qpt = 2;            // queries held per thread
+  int tile_faces = 128;   // faces per shared-memory tile
+  int stages = 3;         // bulk-copy ring depth
+  int64_t nsplit = 1;     // face-range splits (grid.y)
+  int64_t f_chunk = 0;    // faces per split (multiple of tile_faces)
+  int64_t qblocks = 0;    // grid.x
+  int64_t scratch_doubles = 0;  // nsplit * nq when nsplit > 1
+};
+
+// Chooses the launch shape for nf faces x nq queries on a device with `sms` SMs.
+// force_nsplit > 0 pins the number of face splits (tests use it).
+Fp64Plan plan_fp64(int64_t nf, int64_t nq, int sms, int force_nsplit = 0);
+
+// tri: 9 rows of `ld` doubles (row 3*corner+axis, ld even, ld >= nf), 16-byte
+// aligned; q: nq x 3; w: nq outputs (W, already divided by 2*pi); scratch:
+// plan.scratch_doubles doubles or null when that is 0; err: device error word.
+cudaError_t launch_fp64(const Fp64Plan& plan, int mode, const double* tri, int64_t ld, int64_t nf,
+                        const double* q, int64_t nq, double* w, double* scratch, int* err,
+                        cudaStream_t stream);
+
+}  // namespace wn

@@ -1,0 +1,44 @@
+"""The C-ABI library loads and exports every symbol include/*.h declares (CPU)."""
+
+import ctypes
+import glob
+import os
+import re
+
+from igl import _lib
+from conftest import ROOT
+
+
+def _declared_functions():
+    names = set()
+    for header in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(header).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for match in re.finditer(r"^\s*[A-Za-z_][\w\s\*]*?\b([A-Za-z_]\w*)\s*\(", text, re.M):
+            name = match.group(1)
+            if name not in ("if", "sizeof", "defined"):
+                names.add(name)
+    return names
+
+
+def test_header_declares_the_reference_entry_points():
+    names = _declared_functions()
+    assert {"mli_winding", "mli_winding_gpu", "wn_last_error"} <= names
+
+
+def test_library_exports_every_declared_symbol():
+    handle = ctypes.CDLL(_lib.build())
+    missing = [n for n in sorted(_declared_functions()) if not hasattr(handle, n)]
+    assert not missing, missing
+
+
+def test_library_exports_all_thirteen_reference_names():
+    handle = _lib.lib()
+    for name in _lib._SIGNATURES:
+        assert hasattr(handle, name)
+
+
+def test_runtime_queries_do_not_need_a_gpu():
+    handle = _lib.lib()
+    assert handle.wn_version() >= 100
+    assert handle.wn_device_count() >= 0

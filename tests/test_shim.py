@@ -1,0 +1,147 @@
+"""The drop-in Python API (CPU side): contracts of python/igl/__init__.py:232-283
+and python/igl/_lib.py, mirrored from the reference's tests/test_parity.py."""
+
+import numpy as np
+import pytest
+
+import igl
+from igl import _lib
+from conftest import GOLDEN_CASES, grid, load_golden, tetrahedron
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_cpu_path_matches_reference_golden(name):
+    g = load_golden(name)
+    W = igl.winding_number(g["V"], g["F"], g["O"])
+    assert np.abs(W - g["W"]).max() < 1e-12
+
+
+def test_published_solid_angle_invariant():
+    V, F = tetrahedron()
+    Q = np.array([[0.1, 0.1, 0.1], [2.0, 2.0, 2.0], [-1.0, 0.2, 0.2]])
+    W = igl.winding_number(V, F, Q)
+    assert W[0] == pytest.approx(1.0, abs=1e-14)
+    assert np.abs(W[1:]).max() < 1e-14
+    assert isinstance(igl.winding_number(V, F, Q[0]), float)
+    assert igl.winding_number(V, F, Q[0]) == pytest.approx(1.0, abs=1e-14)
+    assert igl.winding_number_for_point(V, F, Q[0]) == pytest.approx(1.0, abs=1e-14)
+
+
+def test_cpu_path_matches_oracle_on_degenerate_queries(oracle_mod):
+    V, F = tetrahedron()
+    Q = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.3, 0.3, 0.0], [0.0, 0.5, 0.0],
+                  [2.0, 0.0, 0.0], [1e6, 1e6, -1e6], [1e-300, 0.0, 0.0]])
+    assert np.abs(igl.winding_number(V, F, Q) - oracle_mod.winding_number(V, F, Q)).max() < 1e-14
+
+
+def _force_serial(monkeypatch):
+    monkeypatch.setattr(igl, "worker_count", lambda items, work, kernel: 1)
+
+
+def _force_parallel(monkeypatch, workers):
+    monkeypatch.setattr(igl, "worker_count",
+                        lambda items, work, kernel: max(1, min(items, workers)))
+
+
+def test_serial_and_parallel_output_is_identical(monkeypatch):
+    V, F = grid(20)
+    rng = np.random.default_rng(77)
+    Q = rng.uniform([0.0, 0.0, -2.0], [19.0, 19.0, 2.0], size=(512, 3))
+    _force_serial(monkeypatch)
+    serial = igl.winding_number(V, F, Q)
+    for workers in (1, 2, 4, 8):
+        _force_parallel(monkeypatch, workers)
+        assert np.array_equal(igl.winding_number(V, F, Q), serial)
+
+
+def test_input_contracts():
+    V, F = grid(3)
+    with pytest.raises(ValueError):
+        igl.winding_number(V, F, [[np.nan, 0.0, 0.0]])
+    with pytest.raises(ValueError):
+        igl.winding_number(V, F, [[np.inf, 0.0, 0.0]])
+    with pytest.raises(ValueError):
+        igl.winding_number(V[:, :2], F, [[0.0, 0.0, 0.0]])
+    with pytest.raises(ValueError):
+        igl.winding_number(V, F, [[0.0, 0.0]])
+    with pytest.raises(ValueError):
+        igl.winding_number(V, F, [0.0, 0.0])
+    with pytest.raises(ValueError):
+        igl.winding_number(V, F, [[0.0, 0.0, 0.0]], device="tpu")
+    with pytest.raises(ValueError):
+        igl.winding_number(V, F, [[0.0, 0.0, 0.0]], precision="fp16")
+    with pytest.raises(TypeError):
+        igl.winding_number(V, F.astype(np.float64), [[0.0, 0.0, 0.0]])
+    with pytest.raises(TypeError):
+        igl.winding_number(V.astype(complex), F, [[0.0, 0.0, 0.0]])
+    with pytest.raises(TypeError):
+        igl.winding_number(V, F.astype(bool), [[0.0, 0.0, 0.0]])
+    with pytest.raises(IndexError):
+        igl.winding_number(V, np.array([[0, 1, len(V)]]), [[0.0, 0.0, 0.0]])
+    with pytest.raises(IndexError):
+        igl.winding_number(V, np.array([[0, 1, -1]]), [[0.0, 0.0, 0.0]])
+    with pytest.raises(OverflowError):
+        igl.winding_number(V, np.array([[0, 1, 2**63]], dtype=np.uint64), [[0.0, 0.0, 0.0]])
+    with pytest.raises(ValueError):
+        igl.winding_number(V, F, np.array([[2**60, 0, 0]], dtype=np.int64))
+
+
+def test_empty_and_integer_inputs():
+    V, F = tetrahedron()
+    out = igl.winding_number(V, F, np.zeros((0, 3)))
+    assert out.shape == (0,) and out.dtype == np.float64
+    assert np.array_equal(igl.winding_number(V, F[:0], np.ones((2, 3))), np.zeros(2))
+    Vi = np.array([[0, 0, 0], [2, 0, 0], [0, 1, 0], [0, 0, 3]], dtype=np.int32)
+    assert igl.winding_number(Vi, F.astype(np.int32), [0.1, 0.1, 0.1]) == pytest.approx(1.0)
+    assert igl.winding_number(V, F, [[0.1, 0.1, 0.1]], device="CPU")[0] == pytest.approx(1.0)
+
+
+def test_gpu_request_without_device_raises(monkeypatch):
+    V, F = tetrahedron()
+    monkeypatch.setattr(igl, "_gpu_memory_available", lambda: False)
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        igl.winding_number(V, F, [[0.1, 0.1, 0.1]], device="gpu")
+
+
+def test_gpu_kernel_failure_is_not_swallowed(monkeypatch):
+    """Mirror of tests/test_parity.py:117-128 with a fake library."""
+    V, F = tetrahedron()
+
+    class FailedGpu:
+        @staticmethod
+        def mli_winding_gpu(*args):
+            return 0
+
+    monkeypatch.setattr(igl, "_gpu_memory_available", lambda: True)
+    monkeypatch.setattr(igl, "lib", lambda: FailedGpu())
+    with pytest.raises(RuntimeError, match="GPU"):
+        igl.winding_number(V, F, [[0.1, 0.1, 0.1]], device="gpu")
+
+
+def test_kernel_signatures_match_shim():
+    """Mirror of tests/test_parity.py:294-340 for the thirteen reference names."""
+    trailing = {
+        "mli_cot_entries": 2, "mli_mass_contributions": 3, "mli_vertex_normals": 3,
+        "mli_winding": 4, "mli_winding_gpu": 2, "mli_aabb_squared_distance": 4,
+        "mli_heat_vector_divergence": 2, "mli_heat_precompute": 1, "mli_arap_covariance": 2,
+        "mli_arap_rhs": 2, "mli_arap_covariance_rims": 3, "mli_arap_rhs_rims": 3,
+        "mli_arap_rotations": 4,
+    }
+    buffers = {
+        "mli_cot_entries": 3, "mli_mass_contributions": 3, "mli_vertex_normals": 3,
+        "mli_winding": 3, "mli_winding_gpu": 3, "mli_aabb_squared_distance": 10,
+        "mli_heat_vector_divergence": 4, "mli_heat_precompute": 3, "mli_arap_covariance": 6,
+        "mli_arap_rhs": 6, "mli_arap_covariance_rims": 5, "mli_arap_rhs_rims": 5,
+        "mli_arap_rotations": 2,
+    }
+    assert set(trailing) == set(buffers) == set(_lib._SIGNATURES)
+    for name in trailing:
+        assert len(_lib._SIGNATURES[name][0]) == buffers[name] + trailing[name]
+
+
+def test_worker_count_and_spans():
+    assert _lib.worker_count(1, 10**9, "winding") == 1
+    assert _lib.worker_count(1000, 1000, "winding") == 1
+    assert 1 <= _lib.worker_count(1000, 10**6, "winding") <= _lib.MAX_WORKERS
+    assert _lib.spans(10, 3) == [(0, 4), (4, 8), (8, 10)]
+    assert _lib.spans(2, 4) == [(0, 1), (1, 2)]

@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Benchmark of the exact generalized winding number on B200 (one JSON line).
+
+Workload (default): bumpy icosphere at subdivision 7, closed
+(163,842 V, 327,680 F); 2^20 queries per GPU, half uniform in the 1.2x
+bounding box and half within N(0, 1e-4) of the surface (seeded synthetic data;
+no dataset exists for this path). A step is one pass of the hot path over that
+batch: every (query, face) pair, 3.44e11 pairs per GPU.
+
+Legs, all on the same inputs:
+  * mixed  (headline when built): FP32 pair terms with compensated
+    accumulation and FP64 refinement of near-surface pairs;
+  * fp64:  the plain FP64 kernel, pair terms bit-identical to the reference;
+  * fwdbwd: forward + hand-written adjoint (when built).
+`value` is whole-job pairs/s of the headline leg with inputs resident in HBM;
+`e2e` is the same leg through the C ABI with pinned host buffers, the
+host->device copies, device preprocessing and device->host copy inside the
+timed region. L2 (126 MB) is flushed by a 256 MiB write before every timed
+step. `cpu_baseline` times the oracle (CPU restatement of the reference's
+Mojo kernel) on a bounded query sample on this host's cores.
+
+Multi-GPU: `python -m torch.distributed.run --nproc-per-node N bench.py --gpus N`
+shards nothing across ranks: each rank runs its own 2^20-query batch against
+the same mesh (weak scaling, no data-path collective); the timed region is
+bracketed by barriers and the slowest rank's time is reported.
+
+`--impl reference` times the reference's CPU path (the oracle port, all host
+threads) on a bounded sample of the same workload and prints the same metric.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mojo-libigl_b200", "python"))
+
+METRIC = ("query·face pairs/s fwd & fwd+bwd, 327k F×1M Q, mixed vs FP64, "
+          "≤1e-6 abs err")
+FLOPS_PER_PAIR = 62  # algorithmic flops per pair, FMA = 2 (src/capi.mojo:218-235)
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    p.add_argument("--queries", type=int, default=1 << 20, help="queries per GPU")
+    p.add_argument("--subdivisions", type=int, default=7)
+    p.add_argument("--legs", default="auto", help="comma list of mixed,fp64,fwdbwd")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def make_inputs(subdivisions: int, nq: int, rank: int):
+    from igl import synthetic
+
+    V, F = synthetic.bumpy_icosphere(subdivisions, seed=31)
+    O = synthetic.mixed_queries(V, F, nq, seed=33 + 1000 * rank, near_sigma=1e-4)
+    desc = (f"bumpy icosphere s={subdivisions} closed ({len(V)} V, {len(F)} F) x {nq} Q "
+            "per GPU: 50% uniform in 1.2x bbox, 50% within N(0,1e-4) of the surface")
+    return V, F, O, desc
+
+
+def soa(V, F):
+    return np.ascontiguousarray(V[F].transpose(1, 2, 0).reshape(9, len(F)))
+
+
+# ---- CPU legs (oracle: only here, as the baseline and the reference arm) ----
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def oracle_rate(tri, O, cores: int, target_s: float):
+    """Pairs/s of the oracle on a query sample sized for about target_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # CPU restatement of the reference kernel (baseline only)
+
+    nf = tri.shape[1]
+    probe = O[: max(cores, 8)]
+    t0 = time.perf_counter()
+    oracle.winding_soa(tri, probe, workers=cores)
+    rate = nf * len(probe) / max(time.perf_counter() - t0, 1e-6)
+    n = int(min(len(O), max(cores, rate * target_s / nf)))
+    # Same 50/50 box/near mix as the full batch: take from both halves.
+    half = len(O) // 2
+    sample = np.concatenate([O[: n // 2], O[half: half + n - n // 2]])
+    t0 = time.perf_counter()
+    oracle.winding_soa(tri, sample, workers=cores)
+    dt = time.perf_counter() - t0
+    return nf * len(sample) / dt, len(sample), dt
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    V, F, O, desc = make_inputs(args.subdivisions, args.queries, 0)
+    tri = soa(V, F)
+    cores = host_cores()
+    rates = []
+    samples = 0
+    for i in range(args.warmup + args.steps):
+        rate, n, dt = oracle_rate(tri, O, cores, target_s=4.0)
+        if i >= args.warmup:
+            rates.append(rate)
+            samples = n
+    value = float(np.median(rates))
+    ms = len(F) * args.queries / value * 1e3
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: " + desc,
+        "config": {"workload": "c3: " + desc, "precision": "fp64 (reference CPU path)"},
+        "cpu_baseline": {
+            "value": value, "unit": "pairs/s", "cores": cores, "kind": "port",
+            "sample": f"{samples} queries (50/50 box/near) x {len(F)} faces per step, "
+                      f"oracle restatement of src/capi.mojo:205-294 over {cores} threads "
+                      f"({cpu_model()}); ms_per_step extrapolates to the full batch",
+        },
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- GPU arm ----------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for row in out.strip().splitlines():
+            parts = [x.strip() for x in row.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        load = [s for s in sm if smax and s > 0.3 * smax] or sm
+        return {"sm_mhz": float(np.median(load)) if load else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_arm(args):
+    import torch
+
+    from igl import _lib
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    handle = _lib.lib()
+    V, F, O, desc = make_inputs(args.subdivisions, args.queries, rank)
+    nf, nq = len(F), len(O)
+    pairs = float(nf) * nq
+    tri = soa(V, F)
+    ld = nf + (nf & 1)
+    dev = torch.device("cuda", local)
+    tri_d = torch.zeros((9, ld), dtype=torch.float64, device=dev)
+    tri_d[:, :nf] = torch.from_numpy(tri).to(dev)
+    q_d = torch.from_numpy(O).to(dev)
+    w_d = torch.empty(nq, dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def check(rc):
+        if rc != 0:
+            raise RuntimeError(_lib.last_error(handle))
+
+    def fp64_step():
+        check(handle.wn_forward_fp64_device(tri_d.data_ptr(), ld, q_d.data_ptr(), w_d.data_ptr(),
+                                            nf, nq, 0, sp))
+
+    legs = {"fp64": fp64_step}
+    headline = "fp64"
+    wanted = list(legs) if args.legs == "auto" else args.legs.split(",")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def timed(step, k, w):
+        for _ in range(w):
+            step()
+        check(handle.wn_stream_check(sp))
+        barrier()
+        launches0 = handle.wn_launch_count()
+        events = []
+        for _ in range(k):
+            flush.fill_(1.0)  # 256 MiB write: evicts L2 between steps
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            events.append((e0, e1))
+        barrier()
+        check(handle.wn_stream_check(sp))
+        launches = handle.wn_launch_count() - launches0
+        total = sum(a.elapsed_time(b) for a, b in events) / 1e3
+        if world > 1:
+            t = torch.tensor([total], dtype=torch.float64, device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            total = float(t.item())
+        return total / k, launches
+
+    results = {}
+    clocks = ClockSampler(local)
+    for name in wanted:
+        if name not in legs:
+            continue
+        if name == headline:
+            clocks.start()
+            results[name] = timed(legs[name], args.steps, max(args.warmup, 3))
+            clock_info = clocks.stop()
+        else:
+            results[name] = timed(legs[name], args.steps, 1)
+
+    t_step, launches = results[headline]
+    value = world * pairs / t_step
+
+    # Parity spot check in the same run: fp64 GPU vs the oracle on 128 queries.
+    parity = None
+    if rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        fp64_step()
+        torch.cuda.synchronize()
+        w_gpu = w_d.cpu().numpy()
+        idx = np.concatenate([np.arange(64), nq // 2 + np.arange(64)])
+        ref = oracle.winding_soa(tri, O[idx], workers=host_cores())
+        parity = float(np.abs(w_gpu[idx] - ref).max())
+
+    # Roofline of the dominant kernel: algorithmic flops per launch / duration.
+    peak = ctypes.c_double(0.0)
+    check(handle.wn_probe_fma_tflops(64, ctypes.byref(peak)))
+    achieved = FLOPS_PER_PAIR * pairs / t_step / 1e12
+    traffic = None
+    traffic_file = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(traffic_file):
+        rec = json.load(open(traffic_file)).get("fp64_forward_kernel")
+        if rec:
+            traffic = rec["bytes_per_query"] * nq
+    roofline = {
+        "bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+        "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
+        "kernel": "fp64_forward_kernel",
+        "peak_source": "measured live: FP64 FMA-chain probe (wn_probe_fma_tflops), FMA = 2 flops",
+        "flops_per_pair": FLOPS_PER_PAIR,
+    }
+
+    # End to end through the C ABI with pinned host buffers.
+    e2e = None
+    if not args.no_e2e:
+        tri_h = torch.from_numpy(tri).pin_memory()
+        q_h = torch.from_numpy(O).pin_memory()
+        w_h = torch.empty(nq, dtype=torch.float64).pin_memory()
+        check(handle.wn_forward_fp64_host(tri_h.data_ptr(), q_h.data_ptr(), w_h.data_ptr(), nf,
+                                          nq, 0))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            check(handle.wn_forward_fp64_host(tri_h.data_ptr(), q_h.data_ptr(), w_h.data_ptr(),
+                                              nf, nq, 0))
+        dt = (time.perf_counter() - t0) / args.steps
+        if world > 1:
+            t = torch.tensor([dt], dtype=torch.float64, device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            dt = float(t.item())
+        e2e = {"value": world * pairs / dt, "unit": "pairs/s",
+               "h2d_bytes_per_step": int(tri.nbytes + O.nbytes), "d2h_bytes_per_step": int(nq * 8),
+               "path": "wn_forward_fp64_host (C ABI, pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = host_cores()
+        rate, n, dt = oracle_rate(tri, O, cores, target_s=12.0)
+        cpu = {"value": rate, "unit": "pairs/s", "cores": cores, "kind": "port",
+               "sample": f"{n} queries (50/50 box/near) x {nf} faces in {dt:.1f} s, oracle "
+                         f"restatement of src/capi.mojo:205-294 over {cores} threads "
+                         f"({cpu_model()})"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": t_step * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic: " + desc,
+            "config": {"workload": "c3: " + desc, "precision": headline, "faces": nf,
+                       "queries_per_gpu": nq, "pairs_per_gpu_step": pairs,
+                       "l2": "flushed before every timed step (256 MiB write)",
+                       "parallelism": f"query batches per GPU, {world} GPU(s)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clock_info,
+            "legs": {k: {"pairs_per_s": world * pairs / v[0], "ms_per_step": v[0] * 1e3}
+                     for k, v in results.items()},
+            "fp64_vs_oracle_max_abs_err_128q": parity,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

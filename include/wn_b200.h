@@ -71,6 +71,11 @@ int wn_device_memory(int64_t* free_bytes, int64_t* total_bytes); /* current devi
 /* Synchronise `stream` and report (then clear) device-side errors raised by
  * device entry points launched on it since the last check. */
 int wn_stream_check(void* stream);
+/* Number of kernels this library has launched since it was loaded. */
+int64_t wn_launch_count(void);
+/* Measured FMA-pipe peak of the current device in TFLOP/s (FMA = 2 flops),
+ * bits = 64 or 32: the roofline denominator of these FP64/FP32-bound kernels. */
+int wn_probe_fma_tflops(int bits, double* tflops);
 
 /* ---- plain FP64 forward (no reference counterpart beyond mli_winding_gpu) */
 

@@ -18,6 +18,9 @@
 #include "wn_internal.h"
 
 namespace wn {
+
+std::atomic<int64_t> g_launches{0};
+
 namespace {
 
 constexpr int kMaxDevices = 64;
@@ -162,6 +165,18 @@ using namespace wn;
 extern "C" {
 
 int wn_version(void) { return 100; }
+
+int64_t wn_launch_count(void) { return g_launches.load(); }
+
+int wn_probe_fma_tflops(int bits, double* tflops) {
+  if ((bits != 32 && bits != 64) || !tflops) return fail(WN_EINVAL, "bits must be 32 or 64");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  cudaError_t e = probe_fma_tflops(bits, c->sms, c->stream, tflops);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "FMA probe");
+}
 
 const char* wn_last_error(void) { return t_last_error.c_str(); }
 

@@ -181,6 +181,7 @@ cudaError_t launch_variant(const Fp64Plan& p, const Fp64Args& a, cudaStream_t st
   if (e != cudaSuccess) return e;
   dim3 grid(static_cast<unsigned>(p.qblocks), static_cast<unsigned>(p.nsplit));
   kernel<<<grid, THREADS, smem, stream>>>(a);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   return cudaGetLastError();
 }
 
@@ -227,6 +228,7 @@ cudaError_t launch_fp64(const Fp64Plan& p, int mode, const double* tri, int64_t 
   const int64_t blocks = (nq + threads - 1) / threads;
   sum_splits_kernel<<<static_cast<unsigned>(blocks), threads, 0, stream>>>(scratch, p.nsplit, nq,
                                                                           w);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   return cudaGetLastError();
 }
 

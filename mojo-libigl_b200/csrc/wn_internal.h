@@ -2,9 +2,17 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <cstdint>
 
 namespace wn {
+
+// Kernels launched by this library since load (wn_launch_count()).
+extern std::atomic<int64_t> g_launches;
+
+// FMA-pipe peak probe (wn_probe.cu): TFLOP/s for bits = 64 or 32.
+cudaError_t probe_fma_tflops(int bits, int sms, cudaStream_t stream, double* tflops);
 
 // ---- plain FP64 forward (wn_fp64.cu) ---------------------------------------
 enum Fp64Mode : int {

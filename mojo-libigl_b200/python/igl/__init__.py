@@ -20,6 +20,7 @@ import operator
 
 import numpy as np
 
+from . import synthetic
 from ._lib import addr, fan_out, last_error, lib, worker_count
 
 __all__ = [

@@ -89,6 +89,28 @@ int wn_forward_fp64_host(const double* tri, const double* q, double* w, int64_t 
 int wn_forward_fp64_device(const double* tri, int64_t ld, const double* q, double* w, int64_t nf,
                            int64_t nq, int mode, void* stream);
 
+/* ---- mixed precision forward (no reference counterpart) ----------------
+ * FP32 pair terms, FP32 two-sum accumulation across 64-face tiles, FP64
+ * refinement (bit-exact pair terms + atan2) of every pair with a vertex closer
+ * than kappa * (the face's longest edge). kappa in [3, 1e6]; 4 is the default
+ * of the Python API. Results agree with the FP64 kernel to ~1e-7 (the tests
+ * and bench report max / p99 absolute error). */
+
+/* Host pointers: prepares the mesh, sorts the queries and evaluates. */
+int wn_forward_mixed_host(const double* tri, const double* q, double* w, int64_t nf, int64_t nq,
+                          double kappa);
+
+/* Device path: prepare a mesh once (tri: device SoA, row stride ld, even,
+ * 16-byte aligned), evaluate query batches against it, destroy it. */
+int wn_mixed_mesh_create(const double* tri, int64_t ld, int64_t nf, double kappa, void* stream,
+                         void** mesh_out);
+int wn_mixed_mesh_destroy(void* mesh);
+int wn_forward_mixed_device(void* mesh, const double* q, int64_t nq, double* w, void* stream);
+
+/* Counters of the mixed path on the current device since the last reset:
+ * pairs refined in FP64, and (warp, tile) visits that ran the near test. */
+int wn_mixed_stats(int64_t* refined_pairs, int64_t* careful_visits, int reset);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,12 +10,14 @@
 
 #include <cstdarg>
 #include <cstdio>
+#include <algorithm>
 #include <cstdlib>
 #include <mutex>
 #include <string>
 
 #include "../../include/wn_b200.h"
 #include "wn_internal.h"
+#include "wn_mixed.h"
 
 namespace wn {
 
@@ -66,7 +68,9 @@ struct DeviceCtx {
   int sms = 0;
   cudaStream_t stream = nullptr;
   int* err = nullptr;  // device error word
+  unsigned long long* stats = nullptr;  // mixed-path counters (refined pairs, careful visits)
   Buffer tri, q, w, scratch;
+  Buffer mesh_tiles, mesh_tri64, mesh_face_of;  // prepared mesh of the host entry points
 };
 
 std::mutex g_mutex;
@@ -86,7 +90,9 @@ DeviceCtx* context(int* code) {
   if ((e = cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaMalloc(&c.err, sizeof(int))) != cudaSuccess ||
-      (e = cudaMemset(c.err, 0, sizeof(int))) != cudaSuccess) {
+      (e = cudaMemset(c.err, 0, sizeof(int))) != cudaSuccess ||
+      (e = cudaMalloc(&c.stats, 2 * sizeof(unsigned long long))) != cudaSuccess ||
+      (e = cudaMemset(c.stats, 0, 2 * sizeof(unsigned long long))) != cudaSuccess) {
     *code = cuda_fail(e, "device context setup");
     return nullptr;
   }
@@ -145,6 +151,67 @@ int forward_fp64_host(const double* tri, const double* q, double* w, int64_t nf,
     return cuda_fail(e, "FP64 winding-number launch");
   if ((e = cudaMemcpyAsync(w, w_d, sizeof(double) * nq, cudaMemcpyDeviceToHost, c->stream)) !=
       cudaSuccess)
+    return cuda_fail(e, "copy of the result");
+  return collect_device_error(c, c->stream);
+}
+
+constexpr double kMinKappa = 3.0;  // the 64-face tile angle bound needs kappa >= 3
+
+struct MeshHandle {
+  MixedMesh m;
+  int device = -1;
+};
+
+int check_kappa(double kappa) {
+  if (!(kappa >= kMinKappa) || !(kappa <= 1e6))
+    return fail(WN_EINVAL, "kappa must lie in [3, 1e6] (got %g)", kappa);
+  return WN_OK;
+}
+
+int forward_mixed_host(const double* tri, const double* q, double* w, int64_t nf, int64_t nq,
+                       double kappa) {
+  if (nf < 0 || nq < 0)
+    return fail(WN_EINVAL, "negative size (nf=%lld, nq=%lld)", (long long)nf, (long long)nq);
+  if (nf > 0x7fffffffLL || nq > 0x7fffffffLL) return fail(WN_EINVAL, "more than 2^31-1 items");
+  if (int code = check_kappa(kappa)) return code;
+  if (nq == 0) return WN_OK;
+  if ((nf > 0 && !tri) || !q || !w) return fail(WN_EINVAL, "null pointer");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  const int64_t ld = even_ld(nf);
+  const size_t scratch = std::max(mixed_sort_scratch_bytes(nf), mixed_sort_scratch_bytes(nq));
+  cudaError_t e;
+  if ((e = c->tri.ensure(sizeof(double) * 9 * ld)) != cudaSuccess ||
+      (e = c->q.ensure(sizeof(double) * 3 * nq)) != cudaSuccess ||
+      (e = c->w.ensure(sizeof(double) * nq)) != cudaSuccess ||
+      (e = c->scratch.ensure(scratch)) != cudaSuccess ||
+      (e = c->mesh_tiles.ensure(mixed_tiles_bytes(nf))) != cudaSuccess ||
+      (e = c->mesh_tri64.ensure(mixed_tri64_bytes(nf))) != cudaSuccess ||
+      (e = c->mesh_face_of.ensure(mixed_face_of_bytes(nf))) != cudaSuccess)
+    return cuda_fail(e, "device allocation");
+  double* tri_d = static_cast<double*>(c->tri.ptr);
+  if (nf > 0 && (e = cudaMemcpy2DAsync(tri_d, sizeof(double) * ld, tri, sizeof(double) * nf,
+                                       sizeof(double) * nf, 9, cudaMemcpyHostToDevice,
+                                       c->stream)) != cudaSuccess)
+    return cuda_fail(e, "copy of the triangle soup");
+  if ((e = cudaMemcpyAsync(c->q.ptr, q, sizeof(double) * 3 * nq, cudaMemcpyHostToDevice,
+                           c->stream)) != cudaSuccess)
+    return cuda_fail(e, "copy of the queries");
+  MixedMesh m;
+  m.tiles = static_cast<unsigned char*>(c->mesh_tiles.ptr);
+  m.tri64 = static_cast<double*>(c->mesh_tri64.ptr);
+  m.face_of = static_cast<uint32_t*>(c->mesh_face_of.ptr);
+  if ((e = mixed_prepare_mesh(tri_d, ld, nf, kappa, &m, c->scratch.ptr, c->scratch.bytes,
+                              c->stream)) != cudaSuccess)
+    return cuda_fail(e, "mesh preparation");
+  if ((e = mixed_forward(m, static_cast<const double*>(c->q.ptr), nq,
+                         static_cast<double*>(c->w.ptr), c->scratch.ptr, c->scratch.bytes,
+                         c->stats, c->err, c->stream)) != cudaSuccess)
+    return cuda_fail(e, "mixed winding-number launch");
+  if ((e = cudaMemcpyAsync(w, c->w.ptr, sizeof(double) * nq, cudaMemcpyDeviceToHost,
+                           c->stream)) != cudaSuccess)
     return cuda_fail(e, "copy of the result");
   return collect_device_error(c, c->stream);
 }
@@ -238,6 +305,105 @@ int wn_forward_fp64_device(const double* tri, int64_t ld, const double* q, doubl
   e = launch_fp64(plan, mode, tri, ld, nf, q, nq, w, scratch, c->err, st);
   if (scratch) cudaFreeAsync(scratch, st);
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "FP64 winding-number launch");
+}
+
+int wn_forward_mixed_host(const double* tri, const double* q, double* w, int64_t nf, int64_t nq,
+                          double kappa) {
+  return forward_mixed_host(tri, q, w, nf, nq, kappa);
+}
+
+int wn_mixed_mesh_create(const double* tri, int64_t ld, int64_t nf, double kappa, void* stream,
+                         void** mesh_out) {
+  if (!mesh_out) return fail(WN_EINVAL, "null mesh_out");
+  *mesh_out = nullptr;
+  if (nf < 0 || nf > 0x7fffffffLL || (ld & 1) || ld < nf)
+    return fail(WN_EINVAL, "bad sizes (nf=%lld, ld=%lld; ld must be even and >= nf)",
+                (long long)nf, (long long)ld);
+  if (int code = check_kappa(kappa)) return code;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  MeshHandle* h = new MeshHandle();
+  cudaGetDevice(&h->device);
+  cudaError_t e;
+  void* scratch = nullptr;
+  const size_t sb = mixed_sort_scratch_bytes(nf);
+  if ((e = cudaMalloc(reinterpret_cast<void**>(&h->m.tiles), mixed_tiles_bytes(nf))) !=
+          cudaSuccess ||
+      (e = cudaMalloc(reinterpret_cast<void**>(&h->m.tri64), mixed_tri64_bytes(nf))) !=
+          cudaSuccess ||
+      (e = cudaMalloc(reinterpret_cast<void**>(&h->m.face_of), mixed_face_of_bytes(nf))) !=
+          cudaSuccess ||
+      (e = cudaMallocAsync(&scratch, sb, st)) != cudaSuccess) {
+    cudaFree(h->m.tiles);
+    cudaFree(h->m.tri64);
+    cudaFree(h->m.face_of);
+    delete h;
+    return cuda_fail(e, "device allocation");
+  }
+  e = mixed_prepare_mesh(tri, ld, nf, kappa, &h->m, scratch, sb, st);
+  cudaFreeAsync(scratch, st);
+  if (e != cudaSuccess) {
+    cudaStreamSynchronize(st);
+    cudaFree(h->m.tiles);
+    cudaFree(h->m.tri64);
+    cudaFree(h->m.face_of);
+    delete h;
+    return cuda_fail(e, "mesh preparation");
+  }
+  *mesh_out = h;
+  return WN_OK;
+}
+
+int wn_mixed_mesh_destroy(void* mesh) {
+  if (!mesh) return WN_OK;
+  MeshHandle* h = static_cast<MeshHandle*>(mesh);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(h->device);
+  cudaDeviceSynchronize();
+  cudaFree(h->m.tiles);
+  cudaFree(h->m.tri64);
+  cudaFree(h->m.face_of);
+  cudaSetDevice(prev);
+  delete h;
+  return WN_OK;
+}
+
+int wn_forward_mixed_device(void* mesh, const double* q, int64_t nq, double* w, void* stream) {
+  if (!mesh) return fail(WN_EINVAL, "null mesh");
+  if (nq < 0 || nq > 0x7fffffffLL) return fail(WN_EINVAL, "bad nq=%lld", (long long)nq);
+  if (nq == 0) return WN_OK;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  const MeshHandle* h = static_cast<const MeshHandle*>(mesh);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t sb = mixed_sort_scratch_bytes(nq);
+  void* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, sb, st);
+  if (e != cudaSuccess) return cuda_fail(e, "device allocation");
+  e = mixed_forward(h->m, q, nq, w, scratch, sb, c->stats, c->err, st);
+  cudaFreeAsync(scratch, st);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "mixed winding-number launch");
+}
+
+int wn_mixed_stats(int64_t* refined_pairs, int64_t* careful_visits, int reset) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  unsigned long long h[2] = {0, 0};
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(h, c->stats, sizeof(h), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && reset) e = cudaMemset(c->stats, 0, sizeof(h));
+  if (e != cudaSuccess) return cuda_fail(e, "reading mixed-path counters");
+  if (refined_pairs) *refined_pairs = static_cast<int64_t>(h[0]);
+  if (careful_visits) *careful_visits = static_cast<int64_t>(h[1]);
+  return WN_OK;
 }
 
 // src/capi.mojo:945-947: 1 on success, 0 on failure (the shim raises).

@@ -1,0 +1,565 @@
+// Mixed-precision forward: FP32 pair terms, compensated FP32 accumulation
+// across face tiles, FP64 refinement of near-surface pairs.
+//
+// Same sum as the plain kernel (lee101/mojo-libigl, src/capi.mojo:205-286):
+// W(o) = sum_f atan2(det_f, denom_f) / (2*pi). Built in three parts.
+//
+// 1. Mesh preparation (once per mesh). Faces are ordered along a Morton curve
+//    of their centroids and cut into tiles of T = 64 consecutive faces. Per
+//    tile: an FP64 centre c, a power-of-two scale s ~ 1/radius, and the squared
+//    "far" radius (r + kappa*h_tile)^2, where r bounds |v - c| over the tile's
+//    vertices and h_tile is its longest edge. Per face, in FP32 tile-local
+//    scaled coordinates: A, B, C, the normal n = (B-A) x (C-A) (formed in FP64,
+//    then rounded), and thr = (kappa*h_face*s)^2. An FP64 copy of the sorted
+//    soup serves the refinement.
+// 2. Query preparation (once per batch). Queries are ordered along a Morton
+//    curve so that a warp's 32 queries are spatial neighbours.
+// 3. The kernel. A CTA holds THREADS*QPT sorted queries, QPT per thread, and
+//    streams tile records through a shared-memory ring filled by 1-D bulk
+//    copies. Per (query, tile), in FP64: o - c, the far test, and o_local =
+//    float((o - c)*s). Per pair, in FP32, with a = A - o_local etc.:
+//       ra = rsqrt(|a|^2) ...,  denom' = 1 + (a.b) ra rb + (b.c) rb rc + (c.a) rc ra
+//       det' = (a . n) ra rb rc      [det = a.(b x c) = a.((B-A) x (C-A))]
+//    so z' = denom' + i det' = z / (la lb lc) has the pair's angle and a
+//    magnitude in [3.8, 4.01] (see below). The tile's angles are added by
+//    multiplying the z' (the argument of a product is the sum of arguments),
+//    then one atan2f per (query, tile); tile angles are summed in an FP32
+//    two-sum (hi, lo) pair.
+//
+// Why this is safe. A pair is "near" when some vertex is closer than
+// kappa*h_face (h_face = the face's longest edge); near pairs are evaluated in
+// FP64 with the bit-exact pair terms and atan2, into an FP64 sum. For every
+// other pair the triangle lies at distance >= (kappa - 1/sqrt(3)) h_face, so
+// its solid angle is <= (sqrt(3)/4)/(kappa - 0.577)^2 and each side subtends
+// <= 2 asin(1/(2 kappa)): with kappa >= 3, |atan2| <= 0.037 per pair (sum over
+// a 64-face tile < pi, so atan2f of the product needs no turn counting) and
+// denom' >= 3.8. The running product starts at 2^-100 and after 64 factors in
+// [1, 4.01] stays within [2^-100, 2^28.1]: no rescaling. A tile whose ball
+// B(c, r + kappa*h_tile) excludes every query of a warp has no near pair: the
+// warp then runs the loop without the near test (the fast path).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+
+#include "wn_common.cuh"
+#include "wn_internal.h"
+#include "wn_mixed.h"
+#include "wn_pair.cuh"
+
+namespace wn {
+namespace {
+
+constexpr float kZ0 = 7.8886090522101181e-31f;  // 2^-100, start of each tile product
+
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Order-preserving map double -> uint64 (for atomic min/max of coordinates).
+__device__ __forceinline__ unsigned long long ordered_key(double x) {
+  const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(x));
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double from_ordered_key(unsigned long long k) {
+  const unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double(static_cast<long long>(b));
+}
+
+__global__ void bbox_init_kernel(unsigned long long* box) {
+  if (threadIdx.x < 3) box[threadIdx.x] = ~0ull;      // minima
+  else if (threadIdx.x < 6) box[threadIdx.x] = 0ull;  // maxima
+}
+
+// Bounding box of face centroids (tri SoA) or of points (AoS xyz).
+template <bool CENTROIDS>
+__global__ void bbox_kernel(const double* __restrict__ data, int64_t ld, int64_t n,
+                            unsigned long long* box) {
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      const double v = CENTROIDS ? (data[x * ld + i] + data[(3 + x) * ld + i] +
+                                    data[(6 + x) * ld + i]) * (1.0 / 3.0)
+                                 : data[3 * i + x];
+      lo[x] = fmin(lo[x], v);
+      hi[x] = fmax(hi[x], v);
+    }
+  }
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    for (int off = 16; off; off >>= 1) {
+      lo[x] = fmin(lo[x], __shfl_xor_sync(0xffffffffu, lo[x], off));
+      hi[x] = fmax(hi[x], __shfl_xor_sync(0xffffffffu, hi[x], off));
+    }
+  }
+  if ((threadIdx.x & 31) == 0 && isfinite(lo[0])) {
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      atomicMin(&box[x], ordered_key(lo[x]));
+      atomicMax(&box[3 + x], ordered_key(hi[x]));
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__device__ __forceinline__ uint32_t morton30(const double p[3], const unsigned long long* box) {
+  uint32_t code = 0;
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    const double lo = from_ordered_key(box[x]), hi = from_ordered_key(box[3 + x]);
+    const double ext = hi - lo;
+    double u = ext > 0 ? (p[x] - lo) / ext : 0.0;
+    u = fmin(fmax(u, 0.0), 1.0);
+    const uint32_t c = min(static_cast<uint32_t>(u * 1024.0), 1023u);
+    code |= spread10(c) << x;
+  }
+  return code;
+}
+
+template <bool CENTROIDS>
+__global__ void morton_kernel(const double* __restrict__ data, int64_t ld, int64_t n,
+                              const unsigned long long* __restrict__ box, uint32_t* keys,
+                              uint32_t* vals) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double p[3];
+#pragma unroll
+  for (int x = 0; x < 3; ++x)
+    p[x] = CENTROIDS ? (data[x * ld + i] + data[(3 + x) * ld + i] + data[(6 + x) * ld + i]) *
+                           (1.0 / 3.0)
+                     : data[3 * i + x];
+  keys[i] = morton30(p, box);
+  vals[i] = static_cast<uint32_t>(i);
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+  for (int off = 16; off; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+  for (int off = 16; off; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off));
+  return v;
+}
+
+// One CTA of kTileFaces threads per tile: gathers the tile's faces in Morton
+// order, writes the FP64 sorted copy, the tile header and the FP32 records.
+__global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
+    const double* __restrict__ tri, int64_t ld, int64_t nf, const uint32_t* __restrict__ order,
+    double kappa, unsigned char* __restrict__ tiles, double* __restrict__ tri64, int64_t ld64,
+    uint32_t* __restrict__ face_of) {
+  __shared__ double red[6][kTileFaces / 32];
+  const int j = threadIdx.x, warp = j >> 5, lane = j & 31;
+  const int64_t tile = blockIdx.x;
+  const int64_t slot = tile * kTileFaces + j;
+  const bool valid = slot < nf;
+  double v[9];
+  const int64_t f = valid ? order[slot] : 0;
+#pragma unroll
+  for (int r = 0; r < 9; ++r) v[r] = valid ? tri[r * ld + f] : 0.0;
+#pragma unroll
+  for (int r = 0; r < 9; ++r) tri64[r * ld64 + slot] = v[r];
+  face_of[slot] = valid ? static_cast<uint32_t>(f) : 0xffffffffu;
+
+  // Tile bounding box -> centre.
+  double lo[3], hi[3];
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    lo[x] = valid ? fmin(v[x], fmin(v[3 + x], v[6 + x])) : INFINITY;
+    hi[x] = valid ? fmax(v[x], fmax(v[3 + x], v[6 + x])) : -INFINITY;
+    lo[x] = warp_min(lo[x]);
+    hi[x] = warp_max(hi[x]);
+  }
+  if (lane == 0)
+    for (int x = 0; x < 3; ++x) {
+      red[x][warp] = lo[x];
+      red[3 + x][warp] = hi[x];
+    }
+  __syncthreads();
+  double c[3];
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    double l = red[x][0], h = red[3 + x][0];
+    for (int w = 1; w < kTileFaces / 32; ++w) {
+      l = fmin(l, red[x][w]);
+      h = fmax(h, red[3 + x][w]);
+    }
+    c[x] = 0.5 * (l + h);
+  }
+  __syncthreads();
+  // Radius (max vertex distance to c) and longest edge, over the tile.
+  double r2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double dx = v[3 * k] - c[0], dy = v[3 * k + 1] - c[1], dz = v[3 * k + 2] - c[2];
+    r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
+  }
+  double h2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int k2 = (k + 1) % 3;
+    const double dx = v[3 * k2] - v[3 * k], dy = v[3 * k2 + 1] - v[3 * k + 1],
+                 dz = v[3 * k2 + 2] - v[3 * k + 2];
+    h2 = fmax(h2, dx * dx + dy * dy + dz * dz);
+  }
+  if (!valid) r2 = h2 = 0.0;
+  const double h_face = sqrt(h2);
+  double rt = warp_max(sqrt(r2)), ht = warp_max(h_face);
+  if (lane == 0) {
+    red[0][warp] = rt;
+    red[1][warp] = ht;
+  }
+  __syncthreads();
+  rt = red[0][0];
+  ht = red[1][0];
+  for (int w = 1; w < kTileFaces / 32; ++w) {
+    rt = fmax(rt, red[0][w]);
+    ht = fmax(ht, red[1][w]);
+  }
+  // Power-of-two scale bringing the tile radius near 1 (exact in FP64).
+  int e = 0;
+  if (rt > 0.0) frexp(rt, &e);
+  const double scale = ldexp(1.0, -e);
+
+  unsigned char* rec = tiles + tile * kTileBytes;
+  if (j == 0) {
+    TileHeader* th = reinterpret_cast<TileHeader*>(rec);
+    th->cx = c[0];
+    th->cy = c[1];
+    th->cz = c[2];
+    const double far = rt + kappa * ht;
+    th->far_r2 = far * far;
+    th->scale = scale;
+    {
+      const int64_t left = nf - tile * kTileFaces;
+      th->n = static_cast<int32_t>(left < kTileFaces ? (left > 0 ? left : 0) : kTileFaces);
+    }
+    th->first = 0;
+    th->r = static_cast<float>(rt);
+    th->h = static_cast<float>(ht);
+  }
+  FaceRec fr;
+  const double ax = (v[0] - c[0]) * scale, ay = (v[1] - c[1]) * scale, az = (v[2] - c[2]) * scale;
+  const double bx = (v[3] - c[0]) * scale, by = (v[4] - c[1]) * scale, bz = (v[5] - c[2]) * scale;
+  const double cx = (v[6] - c[0]) * scale, cy = (v[7] - c[1]) * scale, cz = (v[8] - c[2]) * scale;
+  const double e1x = bx - ax, e1y = by - ay, e1z = bz - az;
+  const double e2x = cx - ax, e2y = cy - ay, e2z = cz - az;
+  fr.ax = static_cast<float>(ax);
+  fr.ay = static_cast<float>(ay);
+  fr.az = static_cast<float>(az);
+  fr.bx = static_cast<float>(bx);
+  fr.by = static_cast<float>(by);
+  fr.bz = static_cast<float>(bz);
+  fr.cx = static_cast<float>(cx);
+  fr.cy = static_cast<float>(cy);
+  fr.cz = static_cast<float>(cz);
+  fr.nx = static_cast<float>(e1y * e2z - e1z * e2y);
+  fr.ny = static_cast<float>(e1z * e2x - e1x * e2z);
+  fr.nz = static_cast<float>(e1x * e2y - e1y * e2x);
+  // A collapsed face (h = 0) is always refined: in FP64 it contributes
+  // atan2(0, denom >= 0) = 0 exactly, and it never reaches rsqrt(0).
+  const double thr = kappa * h_face * scale;
+  fr.thr = (valid && h_face == 0.0) ? INFINITY : static_cast<float>(thr * thr);
+  fr.pad0 = fr.pad1 = fr.pad2 = 0.f;
+  reinterpret_cast<FaceRec*>(rec + sizeof(TileHeader))[j] = fr;
+}
+
+struct MixedArgs {
+  const unsigned char* tiles;  // ntiles * kTileBytes
+  int64_t ntiles;
+  const double* tri64;  // sorted FP64 soup, 9 rows x ld64
+  int64_t ld64;
+  const double* q;         // nq x 3
+  const uint32_t* perm;    // sorted position -> query index
+  int64_t nq;
+  double* w;
+  unsigned long long* stats;  // [0] refined pairs, [1] careful (query-warp, tile) visits
+  int* err;
+};
+
+template <int THREADS, int QPT, int STAGES>
+__global__ void __launch_bounds__(THREADS) mixed_forward_kernel(const MixedArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* ring = smem_raw;  // [STAGES][kTileBytes]
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + STAGES * kTileBytes);
+  const int tid = threadIdx.x;
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * (THREADS * QPT);
+
+  double ox[QPT], oy[QPT], oz[QPT];
+  int64_t qidx[QPT];
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    const int64_t s = base + k * THREADS + tid;
+    qidx[k] = s < a.nq ? static_cast<int64_t>(a.perm[s]) : -1;
+    const int64_t i = qidx[k] >= 0 ? qidx[k] : 0;
+    ox[k] = a.nq > 0 ? a.q[3 * i] : 0.0;
+    oy[k] = a.nq > 0 ? a.q[3 * i + 1] : 0.0;
+    oz[k] = a.nq > 0 ? a.q[3 * i + 2] : 0.0;
+  }
+
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  const int ntiles = static_cast<int>(a.ntiles);
+  auto issue = [&](int t) {
+    const int slot = t % STAGES;
+    mbar_arrive_expect_tx(&full[slot], kTileBytes);
+    bulk_g2s(ring + slot * kTileBytes, a.tiles + static_cast<int64_t>(t) * kTileBytes, kTileBytes,
+             &full[slot]);
+  };
+  int issued = 0;
+  if (tid == 0)
+    for (; issued < min(STAGES, ntiles); ++issued) issue(issued);
+
+  float hi[QPT], lo[QPT];
+  double s64[QPT];
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    hi[k] = lo[k] = 0.f;
+    s64[k] = 0.0;
+  }
+  unsigned refined = 0, careful_tiles = 0;
+
+  bool failed = false;
+  int t = 0;
+  for (; t < ntiles; ++t) {
+    const int slot = t % STAGES;
+    const bool landed = mbar_wait(&full[slot], (t / STAGES) & 1, a.err);
+    if (!__syncthreads_and(landed)) {
+      failed = true;
+      break;
+    }
+    if (tid == 0 && t >= 1 && issued < ntiles) issue(issued++);
+    const unsigned char* rec = ring + slot * kTileBytes;
+    const TileHeader& th = *reinterpret_cast<const TileHeader*>(rec);
+    const float4* fr = reinterpret_cast<const float4*>(rec + sizeof(TileHeader));
+    const int n = th.n;
+
+    float lx[QPT], ly[QPT], lz[QPT];
+    bool all_far = true;
+    bool skip[QPT];
+#pragma unroll
+    for (int k = 0; k < QPT; ++k) {
+      const double dx = ox[k] - th.cx, dy = oy[k] - th.cy, dz = oz[k] - th.cz;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      all_far &= (d2 >= th.far_r2) || qidx[k] < 0;
+      lx[k] = static_cast<float>(dx * th.scale);
+      ly[k] = static_cast<float>(dy * th.scale);
+      lz[k] = static_cast<float>(dz * th.scale);
+      // Beyond 2^40 tile radii the tile's solid angle is below 2^-80: it
+      // cannot change an FP32 sum, and squared distances could overflow.
+      skip[k] = d2 * th.scale * th.scale > 1.2089258196146292e24;
+    }
+    all_far = __all_sync(0xffffffffu, all_far);
+
+    float zr[QPT], zi[QPT];
+#pragma unroll
+    for (int k = 0; k < QPT; ++k) {
+      zr[k] = kZ0;
+      zi[k] = 0.f;
+    }
+
+    if (all_far) {
+#pragma unroll 2
+      for (int j = 0; j < n; ++j) {
+        const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2];
+#pragma unroll
+        for (int k = 0; k < QPT; ++k) {
+          const float ax = r0.x - lx[k], ay = r0.y - ly[k], az = r0.z - lz[k];
+          const float bx = r0.w - lx[k], by = r1.x - ly[k], bz = r1.y - lz[k];
+          const float cx = r1.z - lx[k], cy = r1.w - ly[k], cz = r2.x - lz[k];
+          const float ra = rsqrt_approx(fmaf(ax, ax, fmaf(ay, ay, az * az)));
+          const float rb = rsqrt_approx(fmaf(bx, bx, fmaf(by, by, bz * bz)));
+          const float rc = rsqrt_approx(fmaf(cx, cx, fmaf(cy, cy, cz * cz)));
+          const float ab = fmaf(ax, bx, fmaf(ay, by, az * bz));
+          const float bc = fmaf(bx, cx, fmaf(by, cy, bz * cz));
+          const float ca = fmaf(cx, ax, fmaf(cy, ay, cz * az));
+          const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
+          const float dn = fmaf(ab, rab, fmaf(bc, rbc, fmaf(ca, rca, 1.f)));
+          const float dt = fmaf(ax, r2.y, fmaf(ay, r2.z, az * r2.w)) * (rab * rc);
+          const float nr = fmaf(zr[k], dn, -zi[k] * dt);
+          const float ni = fmaf(zr[k], dt, zi[k] * dn);
+          zr[k] = skip[k] ? zr[k] : nr;
+          zi[k] = skip[k] ? zi[k] : ni;
+        }
+      }
+    } else {
+      ++careful_tiles;
+      const int64_t first = static_cast<int64_t>(t) * kTileFaces;
+#pragma unroll 1
+      for (int j = 0; j < n; ++j) {
+        const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2], r3 = fr[4 * j + 3];
+#pragma unroll
+        for (int k = 0; k < QPT; ++k) {
+          const float ax = r0.x - lx[k], ay = r0.y - ly[k], az = r0.z - lz[k];
+          const float bx = r0.w - lx[k], by = r1.x - ly[k], bz = r1.y - lz[k];
+          const float cx = r1.z - lx[k], cy = r1.w - ly[k], cz = r2.x - lz[k];
+          const float aa = fmaf(ax, ax, fmaf(ay, ay, az * az));
+          const float bb = fmaf(bx, bx, fmaf(by, by, bz * bz));
+          const float cc = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+          const bool near = fminf(aa, fminf(bb, cc)) < r3.x && qidx[k] >= 0;
+          if (near) {
+            const double* f64 = a.tri64 + first + j;
+            const int64_t L = a.ld64;
+            double det, denom;
+            pair_terms_exact(ox[k], oy[k], oz[k], f64[0], f64[L], f64[2 * L], f64[3 * L],
+                             f64[4 * L], f64[5 * L], f64[6 * L], f64[7 * L], f64[8 * L], det,
+                             denom);
+            s64[k] += atan2(det, denom);
+            ++refined;
+          } else if (!skip[k]) {
+            const float ra = rsqrt_approx(aa), rb = rsqrt_approx(bb), rc = rsqrt_approx(cc);
+            const float ab = fmaf(ax, bx, fmaf(ay, by, az * bz));
+            const float bc = fmaf(bx, cx, fmaf(by, cy, bz * cz));
+            const float ca = fmaf(cx, ax, fmaf(cy, ay, cz * az));
+            const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
+            const float dn = fmaf(ab, rab, fmaf(bc, rbc, fmaf(ca, rca, 1.f)));
+            const float dt = fmaf(ax, r2.y, fmaf(ay, r2.z, az * r2.w)) * (rab * rc);
+            const float nr = fmaf(zr[k], dn, -zi[k] * dt);
+            const float ni = fmaf(zr[k], dt, zi[k] * dn);
+            zr[k] = nr;
+            zi[k] = ni;
+          }
+        }
+      }
+    }
+    // Tile angle, added with an FP32 two-sum (Knuth).
+#pragma unroll
+    for (int k = 0; k < QPT; ++k) {
+      const float ang = atan2f(zi[k], zr[k]);
+      const float s = hi[k] + ang;
+      const float bp = s - hi[k];
+      const float err = (hi[k] - (s - bp)) + (ang - bp);
+      hi[k] = s;
+      lo[k] += err;
+    }
+  }
+
+  if (failed) {
+    if (tid == 0)
+      for (int u = t; u < issued; ++u) mbar_wait(&full[u % STAGES], (u / STAGES) & 1, nullptr);
+    __syncthreads();
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    if (qidx[k] < 0) continue;
+    const double total = static_cast<double>(hi[k]) + static_cast<double>(lo[k]) + s64[k];
+    a.w[qidx[k]] = total / kTwoPi;
+  }
+  if (a.stats) {
+    unsigned r = refined;
+    for (int off = 16; off; off >>= 1) r += __shfl_xor_sync(0xffffffffu, r, off);
+    if ((tid & 31) == 0) {
+      atomicAdd(&a.stats[0], static_cast<unsigned long long>(r));
+      atomicAdd(&a.stats[1], static_cast<unsigned long long>(careful_tiles));
+    }
+  }
+}
+
+template <int THREADS, int QPT, int STAGES>
+cudaError_t launch_mixed_variant(const MixedArgs& a, cudaStream_t stream) {
+  auto kernel = mixed_forward_kernel<THREADS, QPT, STAGES>;
+  const size_t smem = static_cast<size_t>(STAGES) * kTileBytes + sizeof(uint64_t) * STAGES;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  const int64_t per = static_cast<int64_t>(THREADS) * QPT;
+  const int64_t blocks = (a.nq + per - 1) / per;
+  kernel<<<static_cast<unsigned>(blocks), THREADS, smem, stream>>>(a);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+
+int64_t blocks_for(int64_t n, int threads) { return std::max<int64_t>(1, (n + threads - 1) / threads); }
+
+}  // namespace
+
+size_t mixed_sort_scratch_bytes(int64_t n) {
+  size_t temp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, temp, static_cast<uint32_t*>(nullptr),
+                                  static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
+                                  static_cast<uint32_t*>(nullptr),
+                                  static_cast<int>(std::max<int64_t>(n, 1)), 0, 30);
+  const size_t n4 = ((static_cast<size_t>(std::max<int64_t>(n, 1)) * 4 + 255) / 256) * 256;
+  return 256 + 4 * n4 + temp;
+}
+
+cudaError_t mixed_prepare_mesh(const double* tri, int64_t ld, int64_t nf, double kappa,
+                               MixedMesh* m, void* scratch, size_t scratch_bytes,
+                               cudaStream_t stream) {
+  // scratch layout: box (6 u64) | keys_in | keys_out | vals_in | vals_out | cub temp
+  if (scratch_bytes < mixed_sort_scratch_bytes(nf)) return cudaErrorInvalidValue;
+  const int64_t ntiles = mixed_tiles(nf);
+  m->nf = nf;
+  m->ntiles = ntiles;
+  m->ld64 = ntiles * kTileFaces;
+  m->kappa = kappa;
+  const size_t n4 = ((static_cast<size_t>(std::max<int64_t>(nf, 1)) * 4 + 255) / 256) * 256;
+  unsigned char* s = static_cast<unsigned char*>(scratch);
+  unsigned long long* box = reinterpret_cast<unsigned long long*>(s);
+  uint32_t* keys_in = reinterpret_cast<uint32_t*>(s + 256);
+  uint32_t* keys_out = reinterpret_cast<uint32_t*>(s + 256 + n4);
+  uint32_t* vals_in = reinterpret_cast<uint32_t*>(s + 256 + 2 * n4);
+  uint32_t* vals_out = reinterpret_cast<uint32_t*>(s + 256 + 3 * n4);
+  void* temp = s + 256 + 4 * n4;
+  size_t temp_bytes = scratch_bytes - (256 + 4 * n4);
+  const int th = 256;
+  if (nf > 0) {
+    bbox_init_kernel<<<1, 32, 0, stream>>>(box);
+    bbox_kernel<true><<<static_cast<unsigned>(std::min<int64_t>(blocks_for(nf, th), 1184)), th, 0,
+                        stream>>>(tri, ld, nf, box);
+    morton_kernel<true><<<static_cast<unsigned>(blocks_for(nf, th)), th, 0, stream>>>(
+        tri, ld, nf, box, keys_in, vals_in);
+    g_launches.fetch_add(3, std::memory_order_relaxed);
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, vals_in,
+                                                    vals_out, static_cast<int>(nf), 0, 30, stream);
+    if (e != cudaSuccess) return e;
+  }
+  build_tiles_kernel<<<static_cast<unsigned>(ntiles), kTileFaces, 0, stream>>>(
+      tri, ld, nf, vals_out, kappa, m->tiles, m->tri64, m->ld64, m->face_of);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+
+cudaError_t mixed_forward(const MixedMesh& m, const double* q, int64_t nq, double* w,
+                          void* scratch, size_t scratch_bytes, unsigned long long* stats, int* err,
+                          cudaStream_t stream) {
+  if (nq <= 0) return cudaSuccess;
+  if (scratch_bytes < mixed_sort_scratch_bytes(nq)) return cudaErrorInvalidValue;
+  const size_t n4 = ((static_cast<size_t>(nq) * 4 + 255) / 256) * 256;
+  unsigned char* s = static_cast<unsigned char*>(scratch);
+  unsigned long long* box = reinterpret_cast<unsigned long long*>(s);
+  uint32_t* keys_in = reinterpret_cast<uint32_t*>(s + 256);
+  uint32_t* keys_out = reinterpret_cast<uint32_t*>(s + 256 + n4);
+  uint32_t* vals_in = reinterpret_cast<uint32_t*>(s + 256 + 2 * n4);
+  uint32_t* vals_out = reinterpret_cast<uint32_t*>(s + 256 + 3 * n4);
+  void* temp = s + 256 + 4 * n4;
+  size_t temp_bytes = scratch_bytes - (256 + 4 * n4);
+  const int th = 256;
+  bbox_init_kernel<<<1, 32, 0, stream>>>(box);
+  bbox_kernel<false><<<static_cast<unsigned>(std::min<int64_t>(blocks_for(nq, th), 1184)), th, 0,
+                       stream>>>(q, 0, nq, box);
+  morton_kernel<false><<<static_cast<unsigned>(blocks_for(nq, th)), th, 0, stream>>>(
+      q, 0, nq, box, keys_in, vals_in);
+  g_launches.fetch_add(3, std::memory_order_relaxed);
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, vals_in,
+                                                  vals_out, static_cast<int>(nq), 0, 30, stream);
+  if (e != cudaSuccess) return e;
+  MixedArgs a{m.tiles, m.ntiles, m.tri64, m.ld64, q, vals_out, nq, w, stats, err};
+  return launch_mixed_variant<128, 2, 4>(a, stream);
+}
+
+}  // namespace wn

@@ -1,0 +1,71 @@
+// Data layout of the mixed-precision path (see wn_mixed.cu for the method).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace wn {
+
+constexpr int kTileFaces = 64;  // faces per tile (the angle bound needs <= 64 at kappa >= 3)
+
+// 64-byte tile header, FP64 geometry of the tile.
+struct TileHeader {
+  double cx, cy, cz;  // centre of the tile's vertex bounding box
+  double far_r2;      // (r + kappa*h_tile)^2: queries at least this far need no refinement
+  double scale;       // power of two ~ 1/r applied to the FP32 local coordinates
+  int32_t n;          // faces in the tile (the last tile may be partial)
+  int32_t first;      // reserved
+  float r, h;         // tile radius and longest edge (diagnostics)
+  int32_t pad[2];
+};
+static_assert(sizeof(TileHeader) == 64, "tile header is 64 bytes");
+
+// 64-byte face record, FP32 tile-local scaled coordinates.
+struct FaceRec {
+  float ax, ay, az, bx, by, bz, cx, cy, cz;  // corners minus centre, times scale
+  float nx, ny, nz;                          // (B-A) x (C-A), formed in FP64
+  float thr;                                 // (kappa*h_face*scale)^2; +inf for collapsed faces
+  float pad0, pad1, pad2;
+};
+static_assert(sizeof(FaceRec) == 64, "face record is 64 bytes");
+
+constexpr int kTileBytes = static_cast<int>(sizeof(TileHeader) + kTileFaces * sizeof(FaceRec));
+static_assert(kTileBytes % 16 == 0, "bulk copies move multiples of 16 bytes");
+
+// A prepared mesh. All pointers are device memory owned by the caller.
+struct MixedMesh {
+  int64_t nf = 0, ntiles = 0, ld64 = 0;
+  double kappa = 4.0;
+  unsigned char* tiles = nullptr;  // ntiles * kTileBytes, 16-byte aligned
+  double* tri64 = nullptr;         // 9 x ld64 sorted FP64 soup (ld64 = ntiles*kTileFaces)
+  uint32_t* face_of = nullptr;     // ld64: sorted slot -> input face (0xffffffff = padding)
+};
+
+inline int64_t mixed_tiles(int64_t nf) { return nf > 0 ? (nf + kTileFaces - 1) / kTileFaces : 1; }
+
+// Device bytes of the prepared mesh arrays.
+inline size_t mixed_tiles_bytes(int64_t nf) {
+  return static_cast<size_t>(mixed_tiles(nf)) * kTileBytes;
+}
+inline size_t mixed_tri64_bytes(int64_t nf) {
+  return static_cast<size_t>(mixed_tiles(nf)) * kTileFaces * 9 * sizeof(double);
+}
+inline size_t mixed_face_of_bytes(int64_t nf) {
+  return static_cast<size_t>(mixed_tiles(nf)) * kTileFaces * sizeof(uint32_t);
+}
+
+// Scratch needed by mixed_prepare_mesh (nf faces) and by mixed_forward (nq queries).
+size_t mixed_sort_scratch_bytes(int64_t n);
+
+cudaError_t mixed_prepare_mesh(const double* tri, int64_t ld, int64_t nf, double kappa,
+                               MixedMesh* m, void* scratch, size_t scratch_bytes,
+                               cudaStream_t stream);
+
+// stats (nullable): [0] += pairs refined in FP64, [1] += careful (warp, tile) visits.
+cudaError_t mixed_forward(const MixedMesh& m, const double* q, int64_t nq, double* w,
+                          void* scratch, size_t scratch_bytes, unsigned long long* stats, int* err,
+                          cudaStream_t stream);
+
+}  // namespace wn

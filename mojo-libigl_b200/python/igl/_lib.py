@@ -56,6 +56,11 @@ _WN_SIGNATURES = {
     "wn_probe_fma_tflops": ([C_INT, ctypes.POINTER(ctypes.c_double)], C_INT),
     "wn_forward_fp64_host": ([P, P, P, I, I, C_INT], C_INT),
     "wn_forward_fp64_device": ([P, I, P, P, I, I, C_INT, P], C_INT),
+    "wn_forward_mixed_host": ([P, P, P, I, I, ctypes.c_double], C_INT),
+    "wn_mixed_mesh_create": ([P, I, I, ctypes.c_double, P, ctypes.POINTER(P)], C_INT),
+    "wn_mixed_mesh_destroy": ([P], C_INT),
+    "wn_forward_mixed_device": ([P, P, I, P, P], C_INT),
+    "wn_mixed_stats": ([ctypes.POINTER(I), ctypes.POINTER(I), C_INT], C_INT),
 }
 
 # The reference caps its pool at four workers on a shared host (_lib.py:34-37).

@@ -1,0 +1,168 @@
+"""Mixed-precision GPU kernel: FP32 pairs + FP64 refinement (needs a B200).
+
+Bar: max |W_mixed - W_oracle| <= 1e-6 per query (the target error of the
+mixed form), on the reference's cases, seeded open and closed meshes, edge
+cases (queries on vertices, edges and inside faces; collapsed faces; tiny and
+huge coordinate scales; queries very far away), and the FP64 refinement must
+actually run for near-surface queries.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+import igl
+from igl import _lib
+from conftest import GOLDEN_CASES, load_golden, tetrahedron
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+
+
+def mixed_host(tri, O, kappa=4.0):
+    tri = np.ascontiguousarray(tri, dtype=np.float64)
+    O = np.ascontiguousarray(O, dtype=np.float64).reshape(-1, 3)
+    out = np.full(len(O), np.nan)
+    rc = _lib.lib().wn_forward_mixed_host(tri.ctypes.data, O.ctypes.data, out.ctypes.data,
+                                          tri.shape[1], len(O), kappa)
+    assert rc == 0, _lib.last_error()
+    return out
+
+
+def stats(reset=True):
+    r, c = ctypes.c_int64(0), ctypes.c_int64(0)
+    assert _lib.lib().wn_mixed_stats(ctypes.byref(r), ctypes.byref(c), int(reset)) == 0
+    return r.value, c.value
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_golden_cases(gpu_required, name):
+    g = load_golden(name)
+    W = mixed_host(igl._triangle_soa(g["V"], g["F"]), g["O"])
+    assert np.abs(W - g["W"]).max() <= TOL
+
+
+def test_public_api_mixed(gpu_required):
+    V, F = tetrahedron()
+    Q = np.array([[0.1, 0.1, 0.1], [2.0, 2.0, 2.0]])
+    W = igl.winding_number(V, F, Q, device="gpu", precision="mixed")
+    assert abs(W[0] - 1.0) <= TOL and abs(W[1]) <= TOL
+
+
+@pytest.mark.parametrize("kappa", [3.0, 4.0, 8.0])
+def test_open_mesh_c2_subset(gpu_required, oracle_mod, kappa):
+    V, F, O, _ = igl.synthetic.workload("c2_open", n_queries=4096)
+    tri = igl._triangle_soa(V, F)
+    ref = oracle_mod.winding_soa(tri, O, workers=8)
+    stats()
+    W = mixed_host(tri, O, kappa)
+    refined, careful = stats()
+    err = np.abs(W - ref)
+    assert err.max() <= TOL, (kappa, err.max())
+    assert refined > 0 and careful > 0
+
+
+def test_closed_mesh_c1(gpu_required, oracle_mod):
+    V, F, O, _ = igl.synthetic.workload("c1_cpu")
+    tri = igl._triangle_soa(V, F)
+    W = mixed_host(tri, O)
+    assert np.abs(W - oracle_mod.winding_soa(tri, O, workers=8)).max() <= TOL
+    assert np.abs(W - np.round(W)).max() <= TOL
+
+
+def test_near_surface_c3_mesh_sample(gpu_required, oracle_mod):
+    V, F = igl.synthetic.bumpy_icosphere(7, seed=31)
+    O = igl.synthetic.mixed_queries(V, F, 256, seed=99, near_sigma=1e-4)
+    tri = igl._triangle_soa(V, F)
+    W = mixed_host(tri, O)
+    assert np.abs(W - oracle_mod.winding_soa(tri, O, workers=8)).max() <= TOL
+
+
+def test_degenerate_queries(gpu_required, oracle_mod):
+    V, F = igl.synthetic.bumpy_icosphere(3, seed=9)
+    tri = igl._triangle_soa(V, F)
+    t = V[F]
+    Q = np.concatenate([V[:50], 0.5 * (t[:50, 0] + t[:50, 1]),
+                        (t[:50, 0] + t[:50, 1] + t[:50, 2]) / 3,
+                        [[0.0, 0.0, 0.0], [1e3, 1e3, 1e3], [1e25, -1e25, 3e24]]])
+    W = mixed_host(tri, Q)
+    assert np.abs(W - oracle_mod.winding_soa(tri, Q)).max() <= TOL
+
+
+def test_collapsed_and_sliver_faces(gpu_required, oracle_mod):
+    rng = np.random.default_rng(5)
+    tri = rng.normal(size=(9, 300))
+    tri[:, :50] = 0.0
+    tri[3:6, 50:100] = tri[0:3, 50:100]
+    tri[6:9, 100:150] = 2 * tri[3:6, 100:150] - tri[0:3, 100:150]
+    O = rng.normal(size=(300, 3))
+    O[0] = 0.0
+    O[1] = tri[0:3, 60]
+    W = mixed_host(tri, O)
+    assert np.abs(W - oracle_mod.winding_soa(tri, O)).max() <= TOL
+
+
+@pytest.mark.parametrize("scale", [1e-12, 1e-3, 1e3, 1e12])
+def test_scale_invariance(gpu_required, oracle_mod, scale):
+    V, F = igl.synthetic.bumpy_icosphere(3, seed=4)
+    O = igl.synthetic.mixed_queries(V, F, 512, seed=5, near_sigma=1e-3)
+    tri = igl._triangle_soa(V * scale, F)
+    W = mixed_host(tri, O * scale)
+    assert np.abs(W - oracle_mod.winding_soa(tri, O * scale)).max() <= TOL
+
+
+@pytest.mark.parametrize("nf,nq", [(1, 1), (63, 5), (64, 64), (65, 257), (1000, 1)])
+def test_odd_sizes(gpu_required, oracle_mod, nf, nq):
+    rng = np.random.default_rng(nf + 31 * nq)
+    tri = rng.normal(size=(9, nf))
+    O = rng.normal(size=(nq, 3))
+    W = mixed_host(tri, O)
+    assert np.abs(W - oracle_mod.winding_soa(tri, O)).max() <= TOL
+
+
+def test_empty_faces_and_queries(gpu_required):
+    assert np.array_equal(mixed_host(np.zeros((9, 0)), np.ones((4, 3))), np.zeros(4))
+    assert mixed_host(np.zeros((9, 3)), np.zeros((0, 3))).shape == (0,)
+
+
+def test_kappa_below_bound_is_rejected(gpu_required):
+    tri = np.zeros((9, 3))
+    O = np.zeros((1, 3))
+    out = np.zeros(1)
+    rc = _lib.lib().wn_forward_mixed_host(tri.ctypes.data, O.ctypes.data, out.ctypes.data, 3, 1,
+                                          2.0)
+    assert rc != 0 and "kappa" in _lib.last_error()
+
+
+def test_device_path_with_prepared_mesh(gpu_required, oracle_mod):
+    import torch
+
+    V, F, O, _ = igl.synthetic.workload("c2_open", n_queries=3000)
+    tri = igl._triangle_soa(V, F)
+    nf = tri.shape[1]
+    ld = nf + (nf & 1)
+    tri_d = torch.zeros((9, ld), dtype=torch.float64, device="cuda")
+    tri_d[:, :nf] = torch.from_numpy(tri)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    h = _lib.lib()
+    mesh = ctypes.c_void_p()
+    assert h.wn_mixed_mesh_create(tri_d.data_ptr(), ld, nf, 4.0, stream, ctypes.byref(mesh)) == 0
+    try:
+        ref = oracle_mod.winding_soa(tri, O, workers=8)
+        for chunk in (O[:1000], O):
+            q_d = torch.from_numpy(np.ascontiguousarray(chunk)).cuda()
+            w_d = torch.empty(len(chunk), dtype=torch.float64, device="cuda")
+            assert h.wn_forward_mixed_device(mesh, q_d.data_ptr(), len(chunk), w_d.data_ptr(),
+                                             stream) == 0, _lib.last_error()
+            assert h.wn_stream_check(stream) == 0
+            assert np.abs(w_d.cpu().numpy() - ref[: len(chunk)]).max() <= TOL
+    finally:
+        h.wn_mixed_mesh_destroy(mesh)
+
+
+def test_deterministic_repeat(gpu_required):
+    V, F, O, _ = igl.synthetic.workload("c2_open", n_queries=2048)
+    tri = igl._triangle_soa(V, F)
+    a = mixed_host(tri, O)
+    assert np.array_equal(mixed_host(tri, O), a)

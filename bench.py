@@ -47,6 +47,7 @@ METRIC = ("query·face pairs/s fwd & fwd+bwd, 327k F×1M Q, mixed vs FP64, "
           "≤1e-6 abs err")
 FLOPS_PER_PAIR = 62  # algorithmic flops per pair, FMA = 2 (src/capi.mojo:218-235)
 L2_FLUSH_BYTES = 256 << 20
+KAPPA = 4.0  # refinement radius of the mixed leg, in face longest-edge units
 
 
 def parse_args():
@@ -233,13 +234,39 @@ def gpu_arm(args):
         if rc != 0:
             raise RuntimeError(_lib.last_error(handle))
 
-    def fp64_step():
-        check(handle.wn_forward_fp64_device(tri_d.data_ptr(), ld, q_d.data_ptr(), w_d.data_ptr(),
-                                            nf, nq, 0, sp))
+    kernel_events = []  # (start, end) around the dominant kernel of each timed step
+    refined_per_step = [0.0]
 
-    legs = {"fp64": fp64_step}
-    headline = "fp64"
+    def kernel_timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        kernel_events.append((e0, e1))
+
+    def fp64_step():
+        kernel_timed(lambda: check(handle.wn_forward_fp64_device(
+            tri_d.data_ptr(), ld, q_d.data_ptr(), w_d.data_ptr(), nf, nq, 0, sp)))
+
+    # Mixed: the mesh is re-prepared from the FP64 soup and the queries are
+    # re-sorted inside every step; the roofline times the pair kernel alone.
+    mesh = ctypes.c_void_p()
+    check(handle.wn_mixed_mesh_create(tri_d.data_ptr(), ld, nf, KAPPA, sp, ctypes.byref(mesh)))
+    perm_d = torch.empty(nq, dtype=torch.int32, device=dev)
+    wm_d = torch.empty(nq, dtype=torch.float64, device=dev)
+
+    def mixed_step():
+        check(handle.wn_mixed_mesh_update(mesh, tri_d.data_ptr(), ld, sp))
+        check(handle.wn_mixed_sort_queries(q_d.data_ptr(), nq, perm_d.data_ptr(), sp))
+        kernel_timed(lambda: check(handle.wn_forward_mixed_sorted_device(
+            mesh, q_d.data_ptr(), perm_d.data_ptr(), nq, wm_d.data_ptr(), sp)))
+
+    legs = {"mixed": mixed_step, "fp64": fp64_step}
+    headline = "mixed"
     wanted = list(legs) if args.legs == "auto" else args.legs.split(",")
+    if headline not in wanted:
+        headline = wanted[0]
 
     def barrier():
         if world > 1:
@@ -251,6 +278,8 @@ def gpu_arm(args):
             step()
         check(handle.wn_stream_check(sp))
         barrier()
+        kernel_events.clear()
+        handle.wn_mixed_stats(None, None, 1)  # reset the refinement counters
         launches0 = handle.wn_launch_count()
         events = []
         for _ in range(k):
@@ -264,12 +293,16 @@ def gpu_arm(args):
         barrier()
         check(handle.wn_stream_check(sp))
         launches = handle.wn_launch_count() - launches0
+        refined = ctypes.c_int64(0)
+        handle.wn_mixed_stats(ctypes.byref(refined), None, 1)
+        refined_per_step[0] = refined.value / k
         total = sum(a.elapsed_time(b) for a, b in events) / 1e3
+        kern = sum(a.elapsed_time(b) for a, b in kernel_events) / 1e3 / max(len(kernel_events), 1)
         if world > 1:
-            t = torch.tensor([total], dtype=torch.float64, device=dev)
+            t = torch.tensor([total, kern], dtype=torch.float64, device=dev)
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            total = float(t.item())
-        return total / k, launches
+            total, kern = float(t[0]), float(t[1])
+        return total / k, launches, kern
 
     results = {}
     clocks = ClockSampler(local)
@@ -280,11 +313,20 @@ def gpu_arm(args):
             clocks.start()
             results[name] = timed(legs[name], args.steps, max(args.warmup, 3))
             clock_info = clocks.stop()
+            headline_refined = refined_per_step[0]
         else:
             results[name] = timed(legs[name], args.steps, 1)
 
-    t_step, launches = results[headline]
+    t_step, launches, t_kernel = results[headline]
     value = world * pairs / t_step
+
+    # Accuracy of the mixed leg against the FP64 kernel on every query.
+    accuracy = None
+    if "mixed" in results and "fp64" in results:
+        err = (wm_d - w_d).abs()
+        accuracy = {"max_abs_err_vs_fp64": float(err.max()),
+                    "p99_abs_err_vs_fp64": float(torch.quantile(err.float(), 0.99)),
+                    "queries_compared": nq}
 
     # Parity spot check in the same run: fp64 GPU vs the oracle on 128 queries.
     parity = None
@@ -300,36 +342,46 @@ def gpu_arm(args):
         parity = float(np.abs(w_gpu[idx] - ref).max())
 
     # Roofline of the dominant kernel: algorithmic flops per launch / duration.
+    bits = 32 if headline == "mixed" else 64
     peak = ctypes.c_double(0.0)
-    check(handle.wn_probe_fma_tflops(64, ctypes.byref(peak)))
-    achieved = FLOPS_PER_PAIR * pairs / t_step / 1e12
+    check(handle.wn_probe_fma_tflops(bits, ctypes.byref(peak)))
+    achieved = FLOPS_PER_PAIR * pairs / t_kernel / 1e12
+    kname = "mixed_forward_kernel" if headline == "mixed" else "fp64_forward_kernel"
     traffic = None
     traffic_file = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(traffic_file):
-        rec = json.load(open(traffic_file)).get("fp64_forward_kernel")
+        rec = json.load(open(traffic_file)).get(kname)
         if rec:
-            traffic = rec["bytes_per_query"] * nq
+            traffic = rec["bytes_per_launch_full"]
     roofline = {
-        "bound": "fp64", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+        "bound": f"fp{bits}", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
         "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
-        "kernel": "fp64_forward_kernel",
-        "peak_source": "measured live: FP64 FMA-chain probe (wn_probe_fma_tflops), FMA = 2 flops",
+        "kernel": kname, "kernel_ms": t_kernel * 1e3,
+        "peak_source": f"measured live on this GPU: FP{bits} FMA-chain probe "
+                       "(wn_probe_fma_tflops), FMA = 2 flops",
         "flops_per_pair": FLOPS_PER_PAIR,
     }
 
-    # End to end through the C ABI with pinned host buffers.
+    # End to end through the C ABI with pinned host buffers: H2D of the soup
+    # and the queries, mesh preparation, query sort, kernel, D2H of W.
     e2e = None
     if not args.no_e2e:
         tri_h = torch.from_numpy(tri).pin_memory()
         q_h = torch.from_numpy(O).pin_memory()
         w_h = torch.empty(nq, dtype=torch.float64).pin_memory()
-        check(handle.wn_forward_fp64_host(tri_h.data_ptr(), q_h.data_ptr(), w_h.data_ptr(), nf,
-                                          nq, 0))
+        if headline == "mixed":
+            call = lambda: check(handle.wn_forward_mixed_host(  # noqa: E731
+                tri_h.data_ptr(), q_h.data_ptr(), w_h.data_ptr(), nf, nq, KAPPA))
+            path = "wn_forward_mixed_host (C ABI, pinned host buffers)"
+        else:
+            call = lambda: check(handle.wn_forward_fp64_host(  # noqa: E731
+                tri_h.data_ptr(), q_h.data_ptr(), w_h.data_ptr(), nf, nq, 0))
+            path = "wn_forward_fp64_host (C ABI, pinned host buffers)"
+        call()
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            check(handle.wn_forward_fp64_host(tri_h.data_ptr(), q_h.data_ptr(), w_h.data_ptr(),
-                                              nf, nq, 0))
+            call()
         dt = (time.perf_counter() - t0) / args.steps
         if world > 1:
             t = torch.tensor([dt], dtype=torch.float64, device=dev)
@@ -337,7 +389,7 @@ def gpu_arm(args):
             dt = float(t.item())
         e2e = {"value": world * pairs / dt, "unit": "pairs/s",
                "h2d_bytes_per_step": int(tri.nbytes + O.nbytes), "d2h_bytes_per_step": int(nq * 8),
-               "path": "wn_forward_fp64_host (C ABI, pinned host buffers)"}
+               "path": path}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -353,18 +405,26 @@ def gpu_arm(args):
             "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": t_step * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic: " + desc,
+            "dtype": "f32+f64" if headline == "mixed" else "f64", "data": "synthetic: " + desc,
             "config": {"workload": "c3: " + desc, "precision": headline, "faces": nf,
+                       "kappa": KAPPA if headline == "mixed" else None,
                        "queries_per_gpu": nq, "pairs_per_gpu_step": pairs,
                        "l2": "flushed before every timed step (256 MiB write)",
                        "parallelism": f"query batches per GPU, {world} GPU(s)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clock_info,
-            "legs": {k: {"pairs_per_s": world * pairs / v[0], "ms_per_step": v[0] * 1e3}
-                     for k, v in results.items()},
+            "legs": {k: {"pairs_per_s": world * pairs / v[0], "ms_per_step": v[0] * 1e3,
+                         "kernel_ms": v[2] * 1e3} for k, v in results.items()},
+            "mixed_over_fp64": (results["fp64"][0] / results["mixed"][0]
+                                if "mixed" in results and "fp64" in results else None),
+            "accuracy": accuracy,
+            "refinement": ({"pairs_refined_fp64_per_step": headline_refined,
+                            "fraction": headline_refined / pairs}
+                           if headline == "mixed" else None),
             "fp64_vs_oracle_max_abs_err_128q": parity,
         }
         print(json.dumps(line), flush=True)
+    handle.wn_mixed_mesh_destroy(mesh)
     if world > 1:
         torch.distributed.destroy_process_group()
 

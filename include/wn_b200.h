@@ -106,6 +106,14 @@ int wn_mixed_mesh_create(const double* tri, int64_t ld, int64_t nf, double kappa
                          void** mesh_out);
 int wn_mixed_mesh_destroy(void* mesh);
 int wn_forward_mixed_device(void* mesh, const double* q, int64_t nq, double* w, void* stream);
+/* Re-prepare an existing mesh in place from new vertex positions (same face
+ * count), e.g. once per step of a shape optimisation. */
+int wn_mixed_mesh_update(void* mesh, const double* tri, int64_t ld, void* stream);
+/* The two halves of wn_forward_mixed_device: Morton-order the queries into
+ * perm (nq uint32, device), then evaluate the queries in that order. */
+int wn_mixed_sort_queries(const double* q, int64_t nq, uint32_t* perm, void* stream);
+int wn_forward_mixed_sorted_device(void* mesh, const double* q, const uint32_t* perm, int64_t nq,
+                                   double* w, void* stream);
 
 /* Counters of the mixed path on the current device since the last reset:
  * pairs refined in FP64, and (warp, tile) visits that ran the near test. */

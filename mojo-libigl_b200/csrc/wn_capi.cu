@@ -181,7 +181,8 @@ int forward_mixed_host(const double* tri, const double* q, double* w, int64_t nf
   DeviceCtx* c = context(&code);
   if (!c) return code;
   const int64_t ld = even_ld(nf);
-  const size_t scratch = std::max(mixed_sort_scratch_bytes(nf), mixed_sort_scratch_bytes(nq));
+  const size_t scratch = std::max(mixed_sort_scratch_bytes(nf),
+                                  mixed_forward_scratch_bytes(mixed_tiles(nf), nq, c->sms));
   cudaError_t e;
   if ((e = c->tri.ensure(sizeof(double) * 9 * ld)) != cudaSuccess ||
       (e = c->q.ensure(sizeof(double) * 3 * nq)) != cudaSuccess ||
@@ -208,7 +209,7 @@ int forward_mixed_host(const double* tri, const double* q, double* w, int64_t nf
     return cuda_fail(e, "mesh preparation");
   if ((e = mixed_forward(m, static_cast<const double*>(c->q.ptr), nq,
                          static_cast<double*>(c->w.ptr), c->scratch.ptr, c->scratch.bytes,
-                         c->stats, c->err, c->stream)) != cudaSuccess)
+                         c->sms, c->stats, c->err, c->stream)) != cudaSuccess)
     return cuda_fail(e, "mixed winding-number launch");
   if ((e = cudaMemcpyAsync(w, c->w.ptr, sizeof(double) * nq, cudaMemcpyDeviceToHost,
                            c->stream)) != cudaSuccess)
@@ -382,13 +383,71 @@ int wn_forward_mixed_device(void* mesh, const double* q, int64_t nq, double* w, 
   if (!c) return code;
   const MeshHandle* h = static_cast<const MeshHandle*>(mesh);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t sb = mixed_forward_scratch_bytes(h->m.ntiles, nq, c->sms);
+  void* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, sb, st);
+  if (e != cudaSuccess) return cuda_fail(e, "device allocation");
+  e = mixed_forward(h->m, q, nq, w, scratch, sb, c->sms, c->stats, c->err, st);
+  cudaFreeAsync(scratch, st);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "mixed winding-number launch");
+}
+
+int wn_mixed_sort_queries(const double* q, int64_t nq, uint32_t* perm, void* stream) {
+  if (nq < 0 || nq > 0x7fffffffLL) return fail(WN_EINVAL, "bad nq=%lld", (long long)nq);
+  if (nq == 0) return WN_OK;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  if (!context(&code)) return code;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t sb = mixed_sort_scratch_bytes(nq);
   void* scratch = nullptr;
   cudaError_t e = cudaMallocAsync(&scratch, sb, st);
   if (e != cudaSuccess) return cuda_fail(e, "device allocation");
-  e = mixed_forward(h->m, q, nq, w, scratch, sb, c->stats, c->err, st);
+  e = mixed_sort_queries(q, nq, perm, scratch, sb, st);
   cudaFreeAsync(scratch, st);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "query sort");
+}
+
+int wn_forward_mixed_sorted_device(void* mesh, const double* q, const uint32_t* perm, int64_t nq,
+                                   double* w, void* stream) {
+  if (!mesh) return fail(WN_EINVAL, "null mesh");
+  if (nq < 0 || nq > 0x7fffffffLL) return fail(WN_EINVAL, "bad nq=%lld", (long long)nq);
+  if (nq == 0) return WN_OK;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  const MeshHandle* h = static_cast<const MeshHandle*>(mesh);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const MixedSplit p = plan_mixed(h->m.ntiles, nq, c->sms);
+  double* partial = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (p.partial_doubles > 0 &&
+      (e = cudaMallocAsync(reinterpret_cast<void**>(&partial), sizeof(double) * p.partial_doubles,
+                           st)) != cudaSuccess)
+    return cuda_fail(e, "device allocation");
+  e = mixed_forward_sorted(h->m, q, perm, nq, w, p, partial, c->stats, c->err, st);
+  if (partial) cudaFreeAsync(partial, st);
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "mixed winding-number launch");
+}
+
+int wn_mixed_mesh_update(void* mesh, const double* tri, int64_t ld, void* stream) {
+  if (!mesh) return fail(WN_EINVAL, "null mesh");
+  MeshHandle* h = static_cast<MeshHandle*>(mesh);
+  if ((ld & 1) || ld < h->m.nf)
+    return fail(WN_EINVAL, "bad ld=%lld for a mesh of %lld faces", (long long)ld,
+                (long long)h->m.nf);
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  if (!context(&code)) return code;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t sb = mixed_sort_scratch_bytes(h->m.nf);
+  void* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, sb, st);
+  if (e != cudaSuccess) return cuda_fail(e, "device allocation");
+  e = mixed_prepare_mesh(tri, ld, h->m.nf, h->m.kappa, &h->m, scratch, sb, st);
+  cudaFreeAsync(scratch, st);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "mesh preparation");
 }
 
 int wn_mixed_stats(int64_t* refined_pairs, int64_t* careful_visits, int reset) {

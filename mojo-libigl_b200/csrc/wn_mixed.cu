@@ -282,7 +282,9 @@ struct MixedArgs {
   const double* q;         // nq x 3
   const uint32_t* perm;    // sorted position -> query index
   int64_t nq;
-  double* w;
+  double* w;                  // output when gridDim.y == 1
+  double* partial;            // [gridDim.y][nq] angle sums when gridDim.y > 1
+  int64_t tiles_per_split;    // tiles handled by one grid.y slice
   unsigned long long* stats;  // [0] refined pairs, [1] careful (query-warp, tile) visits
   int* err;
 };
@@ -312,11 +314,13 @@ __global__ void __launch_bounds__(THREADS) mixed_forward_kernel(const MixedArgs 
     fence_barrier_init();
   }
   __syncthreads();
-  const int ntiles = static_cast<int>(a.ntiles);
+  const int64_t t_begin = static_cast<int64_t>(blockIdx.y) * a.tiles_per_split;
+  const int64_t t_left = a.ntiles - t_begin < a.tiles_per_split ? a.ntiles - t_begin : a.tiles_per_split;
+  const int ntiles = static_cast<int>(t_left > 0 ? t_left : 0);
   auto issue = [&](int t) {
     const int slot = t % STAGES;
     mbar_arrive_expect_tx(&full[slot], kTileBytes);
-    bulk_g2s(ring + slot * kTileBytes, a.tiles + static_cast<int64_t>(t) * kTileBytes, kTileBytes,
+    bulk_g2s(ring + slot * kTileBytes, a.tiles + (t_begin + t) * kTileBytes, kTileBytes,
              &full[slot]);
   };
   int issued = 0;
@@ -397,7 +401,7 @@ __global__ void __launch_bounds__(THREADS) mixed_forward_kernel(const MixedArgs 
       }
     } else {
       ++careful_tiles;
-      const int64_t first = static_cast<int64_t>(t) * kTileFaces;
+      const int64_t first = (t_begin + t) * kTileFaces;
 #pragma unroll 1
       for (int j = 0; j < n; ++j) {
         const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2], r3 = fr[4 * j + 3];
@@ -457,7 +461,10 @@ __global__ void __launch_bounds__(THREADS) mixed_forward_kernel(const MixedArgs 
   for (int k = 0; k < QPT; ++k) {
     if (qidx[k] < 0) continue;
     const double total = static_cast<double>(hi[k]) + static_cast<double>(lo[k]) + s64[k];
-    a.w[qidx[k]] = total / kTwoPi;
+    if (gridDim.y == 1)
+      a.w[qidx[k]] = total / kTwoPi;
+    else
+      a.partial[static_cast<int64_t>(blockIdx.y) * a.nq + qidx[k]] = total;
   }
   if (a.stats) {
     unsigned r = refined;
@@ -469,8 +476,19 @@ __global__ void __launch_bounds__(THREADS) mixed_forward_kernel(const MixedArgs 
   }
 }
 
+__global__ void sum_partials_kernel(const double* __restrict__ partial, int64_t nsplit, int64_t nq,
+                                    double* __restrict__ w) {
+  const int64_t qi = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (qi >= nq) return;
+  double s = 0.0;
+  for (int64_t y = 0; y < nsplit; ++y) s += partial[y * nq + qi];
+  w[qi] = s / kTwoPi;
+}
+
+constexpr int kMixedThreads = 128, kMixedQpt = 2, kMixedStages = 4;
+
 template <int THREADS, int QPT, int STAGES>
-cudaError_t launch_mixed_variant(const MixedArgs& a, cudaStream_t stream) {
+cudaError_t launch_mixed_variant(const MixedArgs& a, int64_t nsplit, cudaStream_t stream) {
   auto kernel = mixed_forward_kernel<THREADS, QPT, STAGES>;
   const size_t smem = static_cast<size_t>(STAGES) * kTileBytes + sizeof(uint64_t) * STAGES;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -478,7 +496,8 @@ cudaError_t launch_mixed_variant(const MixedArgs& a, cudaStream_t stream) {
   if (e != cudaSuccess) return e;
   const int64_t per = static_cast<int64_t>(THREADS) * QPT;
   const int64_t blocks = (a.nq + per - 1) / per;
-  kernel<<<static_cast<unsigned>(blocks), THREADS, smem, stream>>>(a);
+  kernel<<<dim3(static_cast<unsigned>(blocks), static_cast<unsigned>(nsplit)), THREADS, smem,
+           stream>>>(a);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return cudaGetLastError();
 }
@@ -534,9 +553,21 @@ cudaError_t mixed_prepare_mesh(const double* tri, int64_t ld, int64_t nf, double
   return cudaGetLastError();
 }
 
-cudaError_t mixed_forward(const MixedMesh& m, const double* q, int64_t nq, double* w,
-                          void* scratch, size_t scratch_bytes, unsigned long long* stats, int* err,
-                          cudaStream_t stream) {
+MixedSplit plan_mixed(int64_t ntiles, int64_t nq, int sms) {
+  MixedSplit p;
+  const int64_t per = static_cast<int64_t>(kMixedThreads) * kMixedQpt;
+  const int64_t qblocks = std::max<int64_t>(1, (nq + per - 1) / per);
+  const int64_t target = static_cast<int64_t>(std::max(sms, 1)) * 8;
+  int64_t nsplit = qblocks < target ? (target + qblocks - 1) / qblocks : 1;
+  nsplit = std::max<int64_t>(1, std::min(nsplit, ntiles));
+  p.tiles_per_split = (ntiles + nsplit - 1) / nsplit;
+  p.nsplit = std::max<int64_t>(1, (ntiles + p.tiles_per_split - 1) / p.tiles_per_split);
+  p.partial_doubles = p.nsplit > 1 ? p.nsplit * nq : 0;
+  return p;
+}
+
+cudaError_t mixed_sort_queries(const double* q, int64_t nq, uint32_t* perm, void* scratch,
+                               size_t scratch_bytes, cudaStream_t stream) {
   if (nq <= 0) return cudaSuccess;
   if (scratch_bytes < mixed_sort_scratch_bytes(nq)) return cudaErrorInvalidValue;
   const size_t n4 = ((static_cast<size_t>(nq) * 4 + 255) / 256) * 256;
@@ -545,7 +576,6 @@ cudaError_t mixed_forward(const MixedMesh& m, const double* q, int64_t nq, doubl
   uint32_t* keys_in = reinterpret_cast<uint32_t*>(s + 256);
   uint32_t* keys_out = reinterpret_cast<uint32_t*>(s + 256 + n4);
   uint32_t* vals_in = reinterpret_cast<uint32_t*>(s + 256 + 2 * n4);
-  uint32_t* vals_out = reinterpret_cast<uint32_t*>(s + 256 + 3 * n4);
   void* temp = s + 256 + 4 * n4;
   size_t temp_bytes = scratch_bytes - (256 + 4 * n4);
   const int th = 256;
@@ -555,11 +585,50 @@ cudaError_t mixed_forward(const MixedMesh& m, const double* q, int64_t nq, doubl
   morton_kernel<false><<<static_cast<unsigned>(blocks_for(nq, th)), th, 0, stream>>>(
       q, 0, nq, box, keys_in, vals_in);
   g_launches.fetch_add(3, std::memory_order_relaxed);
-  cudaError_t e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, vals_in,
-                                                  vals_out, static_cast<int>(nq), 0, 30, stream);
+  return cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, vals_in, perm,
+                                         static_cast<int>(nq), 0, 30, stream);
+}
+
+cudaError_t mixed_forward_sorted(const MixedMesh& m, const double* q, const uint32_t* perm,
+                                 int64_t nq, double* w, const MixedSplit& split, double* partial,
+                                 unsigned long long* stats, int* err, cudaStream_t stream) {
+  if (nq <= 0) return cudaSuccess;
+  if (split.nsplit > 1 && !partial) return cudaErrorInvalidValue;
+  if (split.nsplit > 65535) return cudaErrorInvalidConfiguration;
+  MixedArgs a{m.tiles, m.ntiles, m.tri64, m.ld64, q, perm, nq, w, partial,
+              split.tiles_per_split, stats, err};
+  cudaError_t e =
+      launch_mixed_variant<kMixedThreads, kMixedQpt, kMixedStages>(a, split.nsplit, stream);
+  if (e != cudaSuccess || split.nsplit == 1) return e;
+  sum_partials_kernel<<<static_cast<unsigned>(blocks_for(nq, 256)), 256, 0, stream>>>(
+      partial, split.nsplit, nq, w);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+
+size_t mixed_forward_scratch_bytes(int64_t ntiles, int64_t nq, int sms) {
+  const MixedSplit p = plan_mixed(ntiles, nq, sms);
+  const size_t perm = ((static_cast<size_t>(std::max<int64_t>(nq, 1)) * 4 + 255) / 256) * 256;
+  return perm + sizeof(double) * p.partial_doubles + mixed_sort_scratch_bytes(nq);
+}
+
+cudaError_t mixed_forward(const MixedMesh& m, const double* q, int64_t nq, double* w,
+                          void* scratch, size_t scratch_bytes, int sms,
+                          unsigned long long* stats, int* err, cudaStream_t stream) {
+  if (nq <= 0) return cudaSuccess;
+  if (scratch_bytes < mixed_forward_scratch_bytes(m.ntiles, nq, sms))
+    return cudaErrorInvalidValue;
+  const MixedSplit p = plan_mixed(m.ntiles, nq, sms);
+  unsigned char* s = static_cast<unsigned char*>(scratch);
+  uint32_t* perm = reinterpret_cast<uint32_t*>(s);
+  const size_t perm_bytes = ((static_cast<size_t>(nq) * 4 + 255) / 256) * 256;
+  double* partial = reinterpret_cast<double*>(s + perm_bytes);
+  unsigned char* sort_scratch = s + perm_bytes + sizeof(double) * p.partial_doubles;
+  cudaError_t e = mixed_sort_queries(q, nq, perm, sort_scratch, mixed_sort_scratch_bytes(nq),
+                                     stream);
   if (e != cudaSuccess) return e;
-  MixedArgs a{m.tiles, m.ntiles, m.tri64, m.ld64, q, vals_out, nq, w, stats, err};
-  return launch_mixed_variant<128, 2, 4>(a, stream);
+  return mixed_forward_sorted(m, q, perm, nq, w, p, p.nsplit > 1 ? partial : nullptr, stats, err,
+                              stream);
 }
 
 }  // namespace wn

@@ -63,9 +63,29 @@ cudaError_t mixed_prepare_mesh(const double* tri, int64_t ld, int64_t nf, double
                                MixedMesh* m, void* scratch, size_t scratch_bytes,
                                cudaStream_t stream);
 
-// stats (nullable): [0] += pairs refined in FP64, [1] += careful (warp, tile) visits.
+// Face-range split of the kernel over grid.y when there are too few queries
+// to fill the GPU; partial sums are added per query in split order.
+struct MixedSplit {
+  int64_t nsplit = 1;
+  int64_t tiles_per_split = 0;
+  int64_t partial_doubles = 0;  // nsplit * nq when nsplit > 1
+};
+MixedSplit plan_mixed(int64_t ntiles, int64_t nq, int sms);
+
+// Morton order of the queries: perm[sorted position] = query index.
+cudaError_t mixed_sort_queries(const double* q, int64_t nq, uint32_t* perm, void* scratch,
+                               size_t scratch_bytes, cudaStream_t stream);
+
+// The kernel on queries already ordered by perm. stats (nullable):
+// [0] += pairs refined in FP64, [1] += careful (warp, tile) visits.
+cudaError_t mixed_forward_sorted(const MixedMesh& m, const double* q, const uint32_t* perm,
+                                 int64_t nq, double* w, const MixedSplit& split, double* partial,
+                                 unsigned long long* stats, int* err, cudaStream_t stream);
+
+// Sort + kernel with one scratch block of mixed_forward_scratch_bytes().
+size_t mixed_forward_scratch_bytes(int64_t ntiles, int64_t nq, int sms);
 cudaError_t mixed_forward(const MixedMesh& m, const double* q, int64_t nq, double* w,
-                          void* scratch, size_t scratch_bytes, unsigned long long* stats, int* err,
-                          cudaStream_t stream);
+                          void* scratch, size_t scratch_bytes, int sms,
+                          unsigned long long* stats, int* err, cudaStream_t stream);
 
 }  // namespace wn

@@ -60,6 +60,9 @@ _WN_SIGNATURES = {
     "wn_mixed_mesh_create": ([P, I, I, ctypes.c_double, P, ctypes.POINTER(P)], C_INT),
     "wn_mixed_mesh_destroy": ([P], C_INT),
     "wn_forward_mixed_device": ([P, P, I, P, P], C_INT),
+    "wn_mixed_mesh_update": ([P, P, I, P], C_INT),
+    "wn_mixed_sort_queries": ([P, I, P, P], C_INT),
+    "wn_forward_mixed_sorted_device": ([P, P, P, I, P, P], C_INT),
     "wn_mixed_stats": ([ctypes.POINTER(I), ctypes.POINTER(I), C_INT], C_INT),
 }
 

@@ -89,6 +89,19 @@ int wn_forward_fp64_host(const double* tri, const double* q, double* w, int64_t 
 int wn_forward_fp64_device(const double* tri, int64_t ld, const double* q, double* w, int64_t nf,
                            int64_t nq, int mode, void* stream);
 
+/* No counterpart in the reference: the plain FP64 forward for callers that
+ * must not allocate GPU memory, such as host applications and plugins that own
+ * all device memory through their own pool or a fixed budget and forbid
+ * libraries from calling cudaMalloc. Same arguments and results as
+ * wn_forward_fp64_device, but its face-split scratch is a fixed 4 MiB array
+ * inside the library (held on every GPU that loads it until exit) instead of an
+ * allocation. Limit: nq <= 524288 (2^19) queries, else WN_EINVAL. The first call
+ * on each device looks up the array's device address and should come before
+ * any stream capture. All calls share the array: calls that overlap on the GPU
+ * race. Returns after the caller's stream has finished the work. */
+int wn_forward_fp64_device_noalloc(const double* tri, int64_t ld, const double* q, double* w,
+                                   int64_t nf, int64_t nq, int mode, void* stream);
+
 /* ---- mixed precision forward (no reference counterpart) ----------------
  * FP32 pair terms, FP32 two-sum accumulation across 64-face tiles, FP64
  * refinement (bit-exact pair terms + atan2) of every pair with a vertex closer

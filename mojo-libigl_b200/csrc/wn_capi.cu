@@ -226,6 +226,9 @@ int forward_mixed_host(const double* tri, const double* q, double* w, int64_t nf
 }
 
 }  // namespace
+
+void record_error(const char* message) { t_last_error = message; }
+
 }  // namespace wn
 
 using namespace wn;

@@ -8,6 +8,9 @@
 
 namespace wn {
 
+// Stores `message` as the calling thread's wn_last_error().
+void record_error(const char* message);
+
 // Kernels launched by this library since load (wn_launch_count()).
 extern std::atomic<int64_t> g_launches;
 

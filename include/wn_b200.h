@@ -132,6 +132,21 @@ int wn_forward_mixed_sorted_device(void* mesh, const double* q, const uint32_t* 
  * pairs refined in FP64, and (warp, tile) visits that ran the near test. */
 int wn_mixed_stats(int64_t* refined_pairs, int64_t* careful_visits, int reset);
 
+/* ---- adjoint (no reference counterpart) ---------------------------------
+ * gw: dL/dW per query (nq). Outputs dq (nq x 3) = dL/do and dtri (9 rows of
+ * stride ld, the soup's layout) = dL/d(corner) per face; every pair term is
+ * recomputed (nothing nf x nq is stored) and the reductions over faces and
+ * over queries are deterministic (fixed order, no floating-point atomics).
+ * Pairs with the query on a vertex or on a side contribute zero. */
+int wn_backward_fp64_device(const double* tri, int64_t ld, int64_t nf, const double* q,
+                            int64_t nq, const double* gw, double* dq, double* dtri, void* stream);
+
+/* dV (nv x 3) = sum of dtri over each vertex's (face, corner) uses; indptr (nv+1)
+ * and entries (3*face + corner, grouped by vertex) form a CSR list; the sum runs
+ * in list order (deterministic). */
+int wn_gather_vertex_grad_device(const double* dtri, int64_t ld, const int64_t* indptr,
+                                 const int64_t* entries, int64_t nv, double* dV, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

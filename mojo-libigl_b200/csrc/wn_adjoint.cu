@@ -1,0 +1,270 @@
+// Hand-written adjoint of the exact generalized winding number.
+//
+// Forward (lee101/mojo-libigl, src/capi.mojo:205-286): W(o) = sum_f Omega_f(o) / (4 pi) with
+// Omega_f = 2 atan2(det, denom). For one face with a = A - o, b = B - o, c = C - o,
+// la = |a| etc., and D_ab = la lb + a.b (likewise D_bc, D_ca), the solid angle's
+// derivatives are (the boundary-variation formula of a flat triangle, each side
+// integrated in closed form):
+//   dOmega/dA = -[ (a x b) / (la D_ab) + (c x a) / (la D_ca) ]
+//   dOmega/dB = -[ (a x b) / (lb D_ab) + (b x c) / (lb D_bc) ]
+//   dOmega/dC = -[ (b x c) / (lc D_bc) + (c x a) / (lc D_ca) ]
+//   dOmega/do = -(dOmega/dA + dOmega/dB + dOmega/dC)          (translation invariance)
+// With ra = 1/la and W_ab = ra rb / (1 + (a.b) ra rb): 1/(la D_ab) = ra W_ab, 1/(lb D_ab) = rb W_ab.
+// At a query on a vertex or on a side (la = 0 or D = 0) the derivative does not exist; such
+// pairs contribute zero.
+//
+// Given dL/dW per query (g), the kernel returns dL/do per query and dL/d(corner) per face
+// (9 values, the soup's SoA layout); a gather through a vertex -> (face, corner) list turns
+// the latter into dL/dV. Nothing Q x F-sized is stored: every pair term is recomputed.
+//
+// Work split, deterministic, no floating-point atomics. Faces are cut into blocks of
+// THREADS*FPT (each thread keeps FPT faces and their 9 gradient sums in registers), queries
+// into groups. A CTA owns (face range r, query group g): it walks the face blocks of r; for
+// each, it streams the queries of g through shared memory in chunks, every thread adds its
+// faces' terms, and each query's dL/do share is reduced over the CTA in a fixed order (warp
+// butterfly, then warps in index order) and added into dO_part[r][q], a row only this CTA
+// touches. After the last chunk a block's face sums go to dF_part[g][corner][face]. Two
+// finishing kernels add the partials over r and over g in index order.
+#include <algorithm>
+
+#include "wn_adjoint.h"
+#include "wn_common.cuh"
+#include "wn_internal.h"
+
+namespace wn {
+namespace {
+
+constexpr double kInv4Pi = 0.079577471545947667884441881686257181;  // 1 / (4 pi)
+
+struct AdjointArgs {
+  const double* tri;  // 9 x ld
+  int64_t ld, nf;
+  const double* q;   // nq x 3
+  const double* gw;  // nq
+  int64_t nq;
+  int64_t blocks_per_range;  // face blocks per face range (grid.x)
+  int64_t queries_per_group;  // queries per group (grid.y)
+  double* dO_part;  // [nranges][nq][3], zeroed before the launch
+  double* dF_part;  // [ngroups][9][ld]
+};
+
+template <int THREADS, int FPT, int QC>
+__global__ void __launch_bounds__(THREADS, 2) adjoint_fp64_kernel(const AdjointArgs a) {
+  __shared__ double sq[QC][4];                 // x, y, z, g of the chunk's queries
+  __shared__ double red[THREADS / 32][QC][3];  // per-warp dL/do shares
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int kBlockFaces = THREADS * FPT;
+  const int64_t range = blockIdx.x, group = blockIdx.y;
+  const int64_t nblocks = (a.nf + kBlockFaces - 1) / kBlockFaces;
+  const int64_t b_begin = range * a.blocks_per_range;
+  const int64_t b_end = min(nblocks, b_begin + a.blocks_per_range);
+  const int64_t q_begin = group * a.queries_per_group;
+  const int64_t q_end = min(a.nq, q_begin + a.queries_per_group);
+  double* dO_row = a.dO_part + range * a.nq * 3;
+
+  for (int64_t blk = b_begin; blk < b_end; ++blk) {
+    double fv[FPT][9], acc[FPT][9];
+    bool fvalid[FPT];
+#pragma unroll
+    for (int k = 0; k < FPT; ++k) {
+      const int64_t f = blk * kBlockFaces + k * THREADS + tid;
+      fvalid[k] = f < a.nf;
+#pragma unroll
+      for (int r = 0; r < 9; ++r) {
+        fv[k][r] = fvalid[k] ? a.tri[r * a.ld + f] : 0.0;
+        acc[k][r] = 0.0;
+      }
+    }
+    for (int64_t c0 = q_begin; c0 < q_end; c0 += QC) {
+      const int nc = static_cast<int>(q_end - c0 < QC ? q_end - c0 : QC);
+      __syncthreads();  // previous chunk fully consumed
+      if (tid < nc) {
+        const int64_t qi = c0 + tid;
+        sq[tid][0] = a.q[3 * qi];
+        sq[tid][1] = a.q[3 * qi + 1];
+        sq[tid][2] = a.q[3 * qi + 2];
+        sq[tid][3] = a.gw[qi];
+      }
+      __syncthreads();
+#pragma unroll 1
+      for (int j = 0; j < nc; ++j) {
+        const double ox = sq[j][0], oy = sq[j][1], oz = sq[j][2], g = sq[j][3];
+        double dox = 0.0, doy = 0.0, doz = 0.0;
+#pragma unroll
+        for (int k = 0; k < FPT; ++k) {
+          const double ax = fv[k][0] - ox, ay = fv[k][1] - oy, az = fv[k][2] - oz;
+          const double bx = fv[k][3] - ox, by = fv[k][4] - oy, bz = fv[k][5] - oz;
+          const double cx = fv[k][6] - ox, cy = fv[k][7] - oy, cz = fv[k][8] - oz;
+          const double aa = ax * ax + ay * ay + az * az;
+          const double bb = bx * bx + by * by + bz * bz;
+          const double cc = cx * cx + cy * cy + cz * cz;
+          const double ra = rsqrt(aa), rb = rsqrt(bb), rc = rsqrt(cc);
+          const double rab = ra * rb, rbc = rb * rc, rca = rc * ra;
+          const double dab = 1.0 + (ax * bx + ay * by + az * bz) * rab;
+          const double dbc = 1.0 + (bx * cx + by * cy + bz * cz) * rbc;
+          const double dca = 1.0 + (cx * ax + cy * ay + cz * az) * rca;
+          // Zero for padding faces and for the pairs where the derivative does not
+          // exist; every factor is selected so that no inf * 0 can appear.
+          const bool ok = fvalid[k] && aa > 0.0 && bb > 0.0 && cc > 0.0 && dab > 0.0 &&
+                          dbc > 0.0 && dca > 0.0;
+          const double inv = ok ? g / (dab * dbc * dca) : 0.0;
+          const double wab = ok ? rab * dbc * dca * inv : 0.0;
+          const double wbc = ok ? rbc * dab * dca * inv : 0.0;
+          const double wca = ok ? rca * dab * dbc * inv : 0.0;
+          const double sa = ok ? ra : 0.0, sb = ok ? rb : 0.0, sc = ok ? rc : 0.0;
+          // a x b, b x c, c x a
+          const double xab0 = ay * bz - az * by, xab1 = az * bx - ax * bz, xab2 = ax * by - ay * bx;
+          const double xbc0 = by * cz - bz * cy, xbc1 = bz * cx - bx * cz, xbc2 = bx * cy - by * cx;
+          const double xca0 = cy * az - cz * ay, xca1 = cz * ax - cx * az, xca2 = cx * ay - cy * ax;
+          const double kA1 = sa * wab, kA2 = sa * wca, kB1 = sb * wab, kB2 = sb * wbc;
+          const double kC1 = sc * wbc, kC2 = sc * wca;
+          acc[k][0] -= kA1 * xab0 + kA2 * xca0;
+          acc[k][1] -= kA1 * xab1 + kA2 * xca1;
+          acc[k][2] -= kA1 * xab2 + kA2 * xca2;
+          acc[k][3] -= kB1 * xab0 + kB2 * xbc0;
+          acc[k][4] -= kB1 * xab1 + kB2 * xbc1;
+          acc[k][5] -= kB1 * xab2 + kB2 * xbc2;
+          acc[k][6] -= kC1 * xbc0 + kC2 * xca0;
+          acc[k][7] -= kC1 * xbc1 + kC2 * xca1;
+          acc[k][8] -= kC1 * xbc2 + kC2 * xca2;
+          const double sab = kA1 + kB1, sbc = kB2 + kC1, sca = kC2 + kA2;
+          dox += sab * xab0 + sbc * xbc0 + sca * xca0;
+          doy += sab * xab1 + sbc * xbc1 + sca * xca1;
+          doz += sab * xab2 + sbc * xbc2 + sca * xca2;
+        }
+        for (int off = 16; off; off >>= 1) {
+          dox += __shfl_xor_sync(0xffffffffu, dox, off);
+          doy += __shfl_xor_sync(0xffffffffu, doy, off);
+          doz += __shfl_xor_sync(0xffffffffu, doz, off);
+        }
+        if (lane == 0) {
+          red[warp][j][0] = dox;
+          red[warp][j][1] = doy;
+          red[warp][j][2] = doz;
+        }
+      }
+      __syncthreads();
+      for (int e = tid; e < nc * 3; e += THREADS) {
+        const int j = e / 3, x = e % 3;
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < THREADS / 32; ++w) s += red[w][j][x];
+        dO_row[(c0 + j) * 3 + x] += s;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < FPT; ++k) {
+      const int64_t f = blk * kBlockFaces + k * THREADS + tid;
+      if (!fvalid[k]) continue;
+#pragma unroll
+      for (int r = 0; r < 9; ++r) a.dF_part[(group * 9 + r) * a.ld + f] = acc[k][r];
+    }
+  }
+}
+
+// dq[q] = (1/4pi) sum_r dO_part[r][q] (r in index order).
+__global__ void finish_dq_kernel(const double* __restrict__ part, int64_t nranges, int64_t nq,
+                                 double* __restrict__ dq) {
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= nq * 3) return;
+  double s = 0.0;
+  for (int64_t r = 0; r < nranges; ++r) s += part[r * nq * 3 + e];
+  dq[e] = s * kInv4Pi;
+}
+
+// dtri[row][f] = (1/4pi) sum_g dF_part[g][row][f] (g in index order).
+__global__ void finish_dtri_kernel(const double* __restrict__ part, int64_t ngroups, int64_t ld,
+                                   int64_t nf, double* __restrict__ dtri) {
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= 9 * nf) return;
+  const int64_t r = e / nf, f = e % nf;
+  double s = 0.0;
+  for (int64_t g = 0; g < ngroups; ++g) s += part[(g * 9 + r) * ld + f];
+  dtri[r * ld + f] = s * kInv4Pi;
+}
+
+// dV[v][x] = sum over the vertex's (face, corner) entries, in list order.
+__global__ void gather_vertex_kernel(const double* __restrict__ dtri, int64_t ld,
+                                     const int64_t* __restrict__ indptr,
+                                     const int64_t* __restrict__ entries, int64_t nv,
+                                     double* __restrict__ dV) {
+  const int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int64_t e = indptr[v]; e < indptr[v + 1]; ++e) {
+    const int64_t f = entries[e] / 3, c = entries[e] % 3;
+    s0 += dtri[(3 * c) * ld + f];
+    s1 += dtri[(3 * c + 1) * ld + f];
+    s2 += dtri[(3 * c + 2) * ld + f];
+  }
+  dV[3 * v] = s0;
+  dV[3 * v + 1] = s1;
+  dV[3 * v + 2] = s2;
+}
+
+constexpr int kAdjThreads = 128, kAdjFpt = 2, kAdjQc = 64;
+
+int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+}  // namespace
+
+AdjointPlan plan_adjoint(int64_t nf, int64_t nq, int sms) {
+  AdjointPlan p;
+  const int64_t block_faces = kAdjThreads * kAdjFpt;
+  const int64_t nblocks = std::max<int64_t>(1, cdiv(nf, block_faces));
+  const int64_t target = static_cast<int64_t>(std::max(sms, 1)) * 4;
+  const int64_t nranges = std::min<int64_t>(nblocks, 16);
+  p.blocks_per_range = cdiv(nblocks, nranges);
+  p.nranges = cdiv(nblocks, p.blocks_per_range);
+  int64_t ngroups = std::max<int64_t>(1, cdiv(target, p.nranges));
+  ngroups = std::min(ngroups, std::max<int64_t>(1, cdiv(nq, kAdjQc)));
+  ngroups = std::min<int64_t>(ngroups, 65535);
+  p.queries_per_group = cdiv(std::max<int64_t>(nq, 1), ngroups);
+  p.ngroups = cdiv(std::max<int64_t>(nq, 1), p.queries_per_group);
+  return p;
+}
+
+size_t adjoint_scratch_bytes(const AdjointPlan& p, int64_t ld, int64_t nq) {
+  return sizeof(double) * (static_cast<size_t>(p.nranges) * nq * 3 +
+                           static_cast<size_t>(p.ngroups) * 9 * ld) +
+         256;
+}
+
+cudaError_t adjoint_fp64(const AdjointPlan& p, const double* tri, int64_t ld, int64_t nf,
+                         const double* q, int64_t nq, const double* gw, double* dq, double* dtri,
+                         void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+  if (nq <= 0 || nf <= 0) {
+    cudaError_t e = cudaSuccess;
+    if (nq > 0) e = cudaMemsetAsync(dq, 0, sizeof(double) * 3 * nq, stream);
+    if (e == cudaSuccess && nf > 0) e = cudaMemsetAsync(dtri, 0, sizeof(double) * 9 * ld, stream);
+    return e;
+  }
+  if (scratch_bytes < adjoint_scratch_bytes(p, ld, nq)) return cudaErrorInvalidValue;
+  double* dO_part = static_cast<double*>(scratch);
+  double* dF_part = dO_part + static_cast<size_t>(p.nranges) * nq * 3;
+  cudaError_t e =
+      cudaMemsetAsync(dO_part, 0, sizeof(double) * static_cast<size_t>(p.nranges) * nq * 3, stream);
+  if (e != cudaSuccess) return e;
+  AdjointArgs a{tri, ld, nf, q, gw, nq, p.blocks_per_range, p.queries_per_group, dO_part, dF_part};
+  adjoint_fp64_kernel<kAdjThreads, kAdjFpt, kAdjQc>
+      <<<dim3(static_cast<unsigned>(p.nranges), static_cast<unsigned>(p.ngroups)), kAdjThreads, 0,
+         stream>>>(a);
+  finish_dq_kernel<<<static_cast<unsigned>(cdiv(nq * 3, 256)), 256, 0, stream>>>(dO_part, p.nranges,
+                                                                               nq, dq);
+  finish_dtri_kernel<<<static_cast<unsigned>(cdiv(9 * nf, 256)), 256, 0, stream>>>(
+      dF_part, p.ngroups, ld, nf, dtri);
+  g_launches.fetch_add(3, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+
+cudaError_t gather_vertex_grad(const double* dtri, int64_t ld, const int64_t* indptr,
+                               const int64_t* entries, int64_t nv, double* dV,
+                               cudaStream_t stream) {
+  if (nv <= 0) return cudaSuccess;
+  gather_vertex_kernel<<<static_cast<unsigned>(cdiv(nv, 256)), 256, 0, stream>>>(
+      dtri, ld, indptr, entries, nv, dV);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+
+}  // namespace wn

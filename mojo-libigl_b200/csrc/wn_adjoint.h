@@ -1,0 +1,31 @@
+// Adjoint (backward) of the winding number: interfaces (see wn_adjoint.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace wn {
+
+struct AdjointPlan {
+  int64_t nranges = 1, blocks_per_range = 1;   // face ranges (grid.x) of 256-face blocks
+  int64_t ngroups = 1, queries_per_group = 1;  // query groups (grid.y)
+};
+
+AdjointPlan plan_adjoint(int64_t nf, int64_t nq, int sms);
+
+// Scratch for the partial sums: nranges*nq*3 + ngroups*9*ld doubles.
+size_t adjoint_scratch_bytes(const AdjointPlan& p, int64_t ld, int64_t nq);
+
+// FP64 adjoint: gw (nq) = dL/dW; outputs dq (nq x 3) = dL/do and dtri (9 x ld) = dL/d(corner).
+cudaError_t adjoint_fp64(const AdjointPlan& p, const double* tri, int64_t ld, int64_t nf,
+                         const double* q, int64_t nq, const double* gw, double* dq, double* dtri,
+                         void* scratch, size_t scratch_bytes, cudaStream_t stream);
+
+// dV (nv x 3) from dtri through the vertex -> (3*face + corner) list (CSR indptr, entries).
+cudaError_t gather_vertex_grad(const double* dtri, int64_t ld, const int64_t* indptr,
+                               const int64_t* entries, int64_t nv, double* dV,
+                               cudaStream_t stream);
+
+}  // namespace wn

@@ -16,6 +16,7 @@
 #include <string>
 
 #include "../../include/wn_b200.h"
+#include "wn_adjoint.h"
 #include "wn_internal.h"
 #include "wn_mixed.h"
 
@@ -466,6 +467,34 @@ int wn_mixed_stats(int64_t* refined_pairs, int64_t* careful_visits, int reset) {
   if (refined_pairs) *refined_pairs = static_cast<int64_t>(h[0]);
   if (careful_visits) *careful_visits = static_cast<int64_t>(h[1]);
   return WN_OK;
+}
+
+int wn_backward_fp64_device(const double* tri, int64_t ld, int64_t nf, const double* q,
+                            int64_t nq, const double* gw, double* dq, double* dtri, void* stream) {
+  if (nf < 0 || nq < 0 || (ld & 1) || ld < nf)
+    return fail(WN_EINVAL, "bad sizes (nf=%lld, nq=%lld, ld=%lld; ld must be even and >= nf)",
+                (long long)nf, (long long)nq, (long long)ld);
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const AdjointPlan p = plan_adjoint(nf, nq, c->sms);
+  const size_t sb = adjoint_scratch_bytes(p, ld, nq);
+  void* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, sb, st);
+  if (e != cudaSuccess) return cuda_fail(e, "device allocation");
+  e = adjoint_fp64(p, tri, ld, nf, q, nq, gw, dq, dtri, scratch, sb, st);
+  cudaFreeAsync(scratch, st);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "FP64 adjoint launch");
+}
+
+int wn_gather_vertex_grad_device(const double* dtri, int64_t ld, const int64_t* indptr,
+                                 const int64_t* entries, int64_t nv, double* dV, void* stream) {
+  if (nv < 0) return fail(WN_EINVAL, "bad nv=%lld", (long long)nv);
+  cudaError_t e = gather_vertex_grad(dtri, ld, indptr, entries, nv, dV,
+                                     static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "vertex gradient gather");
 }
 
 // src/capi.mojo:945-947: 1 on success, 0 on failure (the shim raises).

@@ -1,0 +1,126 @@
+"""Differentiable winding number for PyTorch tensors on a CUDA device.
+
+``winding_number_torch(V, F, O)`` returns W (nq,) and backpropagates dL/dV and
+dL/dO through the library's hand-written adjoint (``wn_backward_fp64_device``):
+pair terms are recomputed (nothing nq x nf is stored), per-face sums over the
+queries and per-query sums over the faces are deterministic, and dL/dV is
+gathered from the per-corner face gradients through a vertex -> (face, corner)
+list in a fixed order. Tensors are plumbing here: the forward and the adjoint
+run in libwn_b200's kernels on the tensors' memory and current stream.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError("libwn_b200: " + _lib.last_error())
+
+
+def _stream() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def triangle_soa(V: torch.Tensor, F: torch.Tensor) -> tuple[torch.Tensor, int, int]:
+    """(9, ld) float64 SoA, row 3*corner+axis, ld even (the C ABI's layout)."""
+    nf = F.shape[0]
+    ld = nf + (nf & 1)
+    tri = torch.zeros((9, max(ld, 2)), dtype=torch.float64, device=V.device)
+    if nf:
+        tri[:, :nf] = V.to(torch.float64)[F].permute(1, 2, 0).reshape(9, nf)
+    return tri, ld, nf
+
+
+def vertex_csr(F: torch.Tensor, nv: int) -> tuple[torch.Tensor, torch.Tensor]:
+    """Vertex -> entries 3*face+corner, grouped by vertex in a fixed order."""
+    flat = F.reshape(-1).to(torch.int64)
+    order = torch.argsort(flat, stable=True)
+    counts = torch.bincount(flat, minlength=nv)
+    indptr = torch.zeros(nv + 1, dtype=torch.int64, device=F.device)
+    indptr[1:] = torch.cumsum(counts, 0)
+    return indptr, order.contiguous()
+
+
+def forward_fp64(tri: torch.Tensor, ld: int, nf: int, O: torch.Tensor) -> torch.Tensor:
+    q = O.to(torch.float64).contiguous()
+    w = torch.empty(q.shape[0], dtype=torch.float64, device=q.device)
+    if q.shape[0]:
+        _check(_lib.lib().wn_forward_fp64_device(tri.data_ptr(), ld, q.data_ptr(), w.data_ptr(),
+                                                 nf, q.shape[0], 0, _stream()))
+    return w
+
+
+def forward_mixed(tri: torch.Tensor, ld: int, nf: int, O: torch.Tensor,
+                  kappa: float = 4.0) -> torch.Tensor:
+    handle = _lib.lib()
+    q = O.to(torch.float64).contiguous()
+    w = torch.empty(q.shape[0], dtype=torch.float64, device=q.device)
+    if not q.shape[0]:
+        return w
+    mesh = ctypes.c_void_p()
+    _check(handle.wn_mixed_mesh_create(tri.data_ptr(), ld, nf, kappa, _stream(),
+                                       ctypes.byref(mesh)))
+    try:
+        _check(handle.wn_forward_mixed_device(mesh, q.data_ptr(), q.shape[0], w.data_ptr(),
+                                              _stream()))
+    finally:
+        torch.cuda.current_stream().synchronize()
+        handle.wn_mixed_mesh_destroy(mesh)
+    return w
+
+
+def backward_fp64(tri, ld, nf, O, gW, F, nv):
+    """(dL/dV, dL/dO) for L with dL/dW = gW."""
+    handle = _lib.lib()
+    q = O.to(torch.float64).contiguous()
+    gw = gW.to(torch.float64).contiguous()
+    nq = q.shape[0]
+    dq = torch.empty((nq, 3), dtype=torch.float64, device=q.device)
+    dtri = torch.empty_like(tri)
+    _check(handle.wn_backward_fp64_device(tri.data_ptr(), ld, nf, q.data_ptr(), nq,
+                                          gw.data_ptr(), dq.data_ptr(), dtri.data_ptr(),
+                                          _stream()))
+    dV = torch.zeros((nv, 3), dtype=torch.float64, device=q.device)
+    if nf and nv:
+        indptr, entries = vertex_csr(F, nv)
+        _check(handle.wn_gather_vertex_grad_device(dtri.data_ptr(), ld, indptr.data_ptr(),
+                                                   entries.data_ptr(), nv, dV.data_ptr(),
+                                                   _stream()))
+    return dV, dq
+
+
+class WindingNumberFunction(torch.autograd.Function):
+    """W = winding_number(V, F, O) with the library's adjoint as backward."""
+
+    @staticmethod
+    def forward(ctx, V, F, O, precision="fp64"):
+        tri, ld, nf = triangle_soa(V, F)
+        if precision == "mixed":
+            w = forward_mixed(tri, ld, nf, O)
+        else:
+            w = forward_fp64(tri, ld, nf, O)
+        ctx.save_for_backward(V, F, O)
+        ctx.tri, ctx.ld, ctx.nf = tri, ld, nf
+        return w.to(O.dtype)
+
+    @staticmethod
+    def backward(ctx, gW):
+        V, F, O = ctx.saved_tensors
+        dV, dq = backward_fp64(ctx.tri, ctx.ld, ctx.nf, O, gW, F, V.shape[0])
+        return dV.to(V.dtype), None, dq.to(O.dtype), None
+
+
+def winding_number_torch(V: torch.Tensor, F: torch.Tensor, O: torch.Tensor,
+                         precision: str = "fp64") -> torch.Tensor:
+    """Differentiable W for CUDA tensors V (nv,3), F (nf,3) int, O (nq,3)."""
+    if not (V.is_cuda and F.is_cuda and O.is_cuda):
+        raise RuntimeError("winding_number_torch needs CUDA tensors (no CPU fallback)")
+    if precision not in ("fp64", "mixed"):
+        raise ValueError("precision must be 'fp64' or 'mixed'")
+    return WindingNumberFunction.apply(V, F, O, precision)

@@ -141,6 +141,13 @@ int wn_mixed_stats(int64_t* refined_pairs, int64_t* careful_visits, int reset);
 int wn_backward_fp64_device(const double* tri, int64_t ld, int64_t nf, const double* q,
                             int64_t nq, const double* gw, double* dq, double* dtri, void* stream);
 
+/* Mixed-precision adjoint over a mesh prepared by wn_mixed_mesh_create: FP32
+ * pair terms for pairs with every vertex at least kappa * (longest edge) away,
+ * FP64 for the others, FP64 sums across query chunks and over faces. dtri has
+ * row stride ld (even, >= nf) and is indexed by the input face order. */
+int wn_backward_mixed_device(void* mesh, const double* q, int64_t nq, const double* gw,
+                             double* dq, double* dtri, int64_t ld, void* stream);
+
 /* dV (nv x 3) = sum of dtri over each vertex's (face, corner) uses; indptr (nv+1)
  * and entries (3*face + corner, grouped by vertex) form a CSR list; the sum runs
  * in list order (deterministic). */

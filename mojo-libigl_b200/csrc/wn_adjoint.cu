@@ -30,11 +30,56 @@
 #include "wn_adjoint.h"
 #include "wn_common.cuh"
 #include "wn_internal.h"
+#include "wn_mixed.h"
 
 namespace wn {
 namespace {
 
 constexpr double kInv4Pi = 0.079577471545947667884441881686257181;  // 1 / (4 pi)
+
+// g * dOmega/d(A, B, C) of one pair in FP64 (see the file comment), added into gv[9]
+// (corners A, B, C), and g * dOmega/do added into go[3]. Zero for padding faces and for
+// pairs where the derivative does not exist; every factor is selected so that no
+// inf * 0 can appear.
+__device__ __forceinline__ void pair_grad_fp64(double ox, double oy, double oz, const double* v,
+                                               double g, bool valid, double* gv, double* go) {
+  const double ax = v[0] - ox, ay = v[1] - oy, az = v[2] - oz;
+  const double bx = v[3] - ox, by = v[4] - oy, bz = v[5] - oz;
+  const double cx = v[6] - ox, cy = v[7] - oy, cz = v[8] - oz;
+  const double aa = ax * ax + ay * ay + az * az;
+  const double bb = bx * bx + by * by + bz * bz;
+  const double cc = cx * cx + cy * cy + cz * cz;
+  const double ra = rsqrt(aa), rb = rsqrt(bb), rc = rsqrt(cc);
+  const double rab = ra * rb, rbc = rb * rc, rca = rc * ra;
+  const double dab = 1.0 + (ax * bx + ay * by + az * bz) * rab;
+  const double dbc = 1.0 + (bx * cx + by * cy + bz * cz) * rbc;
+  const double dca = 1.0 + (cx * ax + cy * ay + cz * az) * rca;
+  const bool ok = valid && aa > 0.0 && bb > 0.0 && cc > 0.0 && dab > 0.0 && dbc > 0.0 &&
+                  dca > 0.0;
+  const double inv = ok ? g / (dab * dbc * dca) : 0.0;
+  const double wab = ok ? rab * dbc * dca * inv : 0.0;
+  const double wbc = ok ? rbc * dab * dca * inv : 0.0;
+  const double wca = ok ? rca * dab * dbc * inv : 0.0;
+  const double sa = ok ? ra : 0.0, sb = ok ? rb : 0.0, sc = ok ? rc : 0.0;
+  const double xab0 = ay * bz - az * by, xab1 = az * bx - ax * bz, xab2 = ax * by - ay * bx;
+  const double xbc0 = by * cz - bz * cy, xbc1 = bz * cx - bx * cz, xbc2 = bx * cy - by * cx;
+  const double xca0 = cy * az - cz * ay, xca1 = cz * ax - cx * az, xca2 = cx * ay - cy * ax;
+  const double kA1 = sa * wab, kA2 = sa * wca, kB1 = sb * wab, kB2 = sb * wbc;
+  const double kC1 = sc * wbc, kC2 = sc * wca;
+  gv[0] -= kA1 * xab0 + kA2 * xca0;
+  gv[1] -= kA1 * xab1 + kA2 * xca1;
+  gv[2] -= kA1 * xab2 + kA2 * xca2;
+  gv[3] -= kB1 * xab0 + kB2 * xbc0;
+  gv[4] -= kB1 * xab1 + kB2 * xbc1;
+  gv[5] -= kB1 * xab2 + kB2 * xbc2;
+  gv[6] -= kC1 * xbc0 + kC2 * xca0;
+  gv[7] -= kC1 * xbc1 + kC2 * xca1;
+  gv[8] -= kC1 * xbc2 + kC2 * xca2;
+  const double sab = kA1 + kB1, sbc = kB2 + kC1, sca = kC2 + kA2;
+  go[0] += sab * xab0 + sbc * xbc0 + sca * xca0;
+  go[1] += sab * xab1 + sbc * xbc1 + sca * xca1;
+  go[2] += sab * xab2 + sbc * xbc2 + sca * xca2;
+}
 
 struct AdjointArgs {
   const double* tri;  // 9 x ld
@@ -89,49 +134,10 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_fp64_kernel(const AdjointA
 #pragma unroll 1
       for (int j = 0; j < nc; ++j) {
         const double ox = sq[j][0], oy = sq[j][1], oz = sq[j][2], g = sq[j][3];
-        double dox = 0.0, doy = 0.0, doz = 0.0;
+        double go[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-        for (int k = 0; k < FPT; ++k) {
-          const double ax = fv[k][0] - ox, ay = fv[k][1] - oy, az = fv[k][2] - oz;
-          const double bx = fv[k][3] - ox, by = fv[k][4] - oy, bz = fv[k][5] - oz;
-          const double cx = fv[k][6] - ox, cy = fv[k][7] - oy, cz = fv[k][8] - oz;
-          const double aa = ax * ax + ay * ay + az * az;
-          const double bb = bx * bx + by * by + bz * bz;
-          const double cc = cx * cx + cy * cy + cz * cz;
-          const double ra = rsqrt(aa), rb = rsqrt(bb), rc = rsqrt(cc);
-          const double rab = ra * rb, rbc = rb * rc, rca = rc * ra;
-          const double dab = 1.0 + (ax * bx + ay * by + az * bz) * rab;
-          const double dbc = 1.0 + (bx * cx + by * cy + bz * cz) * rbc;
-          const double dca = 1.0 + (cx * ax + cy * ay + cz * az) * rca;
-          // Zero for padding faces and for the pairs where the derivative does not
-          // exist; every factor is selected so that no inf * 0 can appear.
-          const bool ok = fvalid[k] && aa > 0.0 && bb > 0.0 && cc > 0.0 && dab > 0.0 &&
-                          dbc > 0.0 && dca > 0.0;
-          const double inv = ok ? g / (dab * dbc * dca) : 0.0;
-          const double wab = ok ? rab * dbc * dca * inv : 0.0;
-          const double wbc = ok ? rbc * dab * dca * inv : 0.0;
-          const double wca = ok ? rca * dab * dbc * inv : 0.0;
-          const double sa = ok ? ra : 0.0, sb = ok ? rb : 0.0, sc = ok ? rc : 0.0;
-          // a x b, b x c, c x a
-          const double xab0 = ay * bz - az * by, xab1 = az * bx - ax * bz, xab2 = ax * by - ay * bx;
-          const double xbc0 = by * cz - bz * cy, xbc1 = bz * cx - bx * cz, xbc2 = bx * cy - by * cx;
-          const double xca0 = cy * az - cz * ay, xca1 = cz * ax - cx * az, xca2 = cx * ay - cy * ax;
-          const double kA1 = sa * wab, kA2 = sa * wca, kB1 = sb * wab, kB2 = sb * wbc;
-          const double kC1 = sc * wbc, kC2 = sc * wca;
-          acc[k][0] -= kA1 * xab0 + kA2 * xca0;
-          acc[k][1] -= kA1 * xab1 + kA2 * xca1;
-          acc[k][2] -= kA1 * xab2 + kA2 * xca2;
-          acc[k][3] -= kB1 * xab0 + kB2 * xbc0;
-          acc[k][4] -= kB1 * xab1 + kB2 * xbc1;
-          acc[k][5] -= kB1 * xab2 + kB2 * xbc2;
-          acc[k][6] -= kC1 * xbc0 + kC2 * xca0;
-          acc[k][7] -= kC1 * xbc1 + kC2 * xca1;
-          acc[k][8] -= kC1 * xbc2 + kC2 * xca2;
-          const double sab = kA1 + kB1, sbc = kB2 + kC1, sca = kC2 + kA2;
-          dox += sab * xab0 + sbc * xbc0 + sca * xca0;
-          doy += sab * xab1 + sbc * xbc1 + sca * xca1;
-          doz += sab * xab2 + sbc * xbc2 + sca * xca2;
-        }
+        for (int k = 0; k < FPT; ++k) pair_grad_fp64(ox, oy, oz, fv[k], g, fvalid[k], acc[k], go);
+        double dox = go[0], doy = go[1], doz = go[2];
         for (int off = 16; off; off >>= 1) {
           dox += __shfl_xor_sync(0xffffffffu, dox, off);
           doy += __shfl_xor_sync(0xffffffffu, doy, off);
@@ -160,6 +166,220 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_fp64_kernel(const AdjointA
       for (int r = 0; r < 9; ++r) a.dF_part[(group * 9 + r) * a.ld + f] = acc[k][r];
     }
   }
+}
+
+// ---- mixed precision adjoint ---------------------------------------------
+// Same decomposition over the prepared mesh of the mixed forward (wn_mixed.cu):
+// 64-face tiles in Morton order with FP32 tile-local scaled coordinates, queries in
+// Morton order. A face block is 4 tiles; thread t keeps face (t mod 64) of tiles
+// 4b + (t/64) and 4b + 2 + (t/64), so each warp's 32 faces share one tile and a
+// query's far test against that tile is uniform over the warp. Far pairs are
+// evaluated in FP32 in the tile's scaled frame (derivatives scale as 1/length: the
+// tile's scale factor multiplies them back); a pair with a vertex closer than
+// kappa * h_face is evaluated in FP64 from the sorted FP64 soup. Per-face sums are
+// kept in FP32 within a query chunk and in FP64 across chunks; per-query sums over
+// faces are reduced in FP64 (large near-surface terms cancel there).
+struct MixedAdjointArgs {
+  const unsigned char* tiles;
+  int64_t ntiles;
+  const double* tri64;  // sorted FP64 soup, 9 x ld64
+  int64_t ld64;
+  const double* q;        // nq x 3, input order
+  const uint32_t* perm;   // sorted position -> query index
+  const double* gw;       // nq, input order
+  int64_t nq;
+  int64_t blocks_per_range;   // 4-tile blocks per range (grid.x)
+  int64_t queries_per_group;  // sorted query positions per group (grid.y)
+  double* dO_part;  // [nranges][nq][3] by sorted position, zeroed before the launch
+  double* dF_part;  // [ngroups][9][ld64] by sorted slot
+};
+
+template <int THREADS, int QC>
+__global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAdjointArgs a) {
+  static_assert(THREADS == 2 * kTileFaces, "one thread per face of two tiles");
+  constexpr int kTilesPerBlock = 4;
+  __shared__ float4 sl[QC][kTilesPerBlock];   // local scaled query, w = 1 if far from the tile
+  __shared__ double sq[QC][4];                // FP64 query and g
+  __shared__ double red[THREADS / 32][QC][3];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int j = tid & (kTileFaces - 1), half = tid >> 6;
+  const int64_t nblocks = (a.ntiles + kTilesPerBlock - 1) / kTilesPerBlock;
+  const int64_t range = blockIdx.x, group = blockIdx.y;
+  const int64_t b_begin = range * a.blocks_per_range;
+  const int64_t b_end = min(nblocks, b_begin + a.blocks_per_range);
+  const int64_t q_begin = group * a.queries_per_group;
+  const int64_t q_end = min(a.nq, q_begin + a.queries_per_group);
+  double* dO_row = a.dO_part + range * a.nq * 3;
+
+  for (int64_t blk = b_begin; blk < b_end; ++blk) {
+    float fv[2][10];  // A, B, C (scaled local), thr
+    double scale[2];
+    int64_t slot[2];
+    bool valid[2];
+    float acc32[2][9];
+    double acc64[2][9];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int64_t t = blk * kTilesPerBlock + 2 * k + half;
+      const bool tile_ok = t < a.ntiles;
+      const TileHeader* th =
+          reinterpret_cast<const TileHeader*>(a.tiles + (tile_ok ? t : 0) * kTileBytes);
+      valid[k] = tile_ok && j < th->n;
+      scale[k] = tile_ok ? th->scale : 0.0;
+      slot[k] = (tile_ok ? t : 0) * kTileFaces + j;
+      const float* fr = reinterpret_cast<const float*>(a.tiles + (tile_ok ? t : 0) * kTileBytes +
+                                                       sizeof(TileHeader)) + 16 * j;
+#pragma unroll
+      for (int r = 0; r < 9; ++r) fv[k][r] = valid[k] ? fr[r] : 0.f;
+      fv[k][9] = valid[k] ? fr[12] : 0.f;
+#pragma unroll
+      for (int r = 0; r < 9; ++r) {
+        acc32[k][r] = 0.f;
+        acc64[k][r] = 0.0;
+      }
+    }
+    for (int64_t c0 = q_begin; c0 < q_end; c0 += QC) {
+      const int nc = static_cast<int>(q_end - c0 < QC ? q_end - c0 : QC);
+      __syncthreads();
+      for (int item = tid; item < nc * kTilesPerBlock; item += THREADS) {
+        const int jq = item / kTilesPerBlock, tt = item % kTilesPerBlock;
+        const int64_t qi = a.perm[c0 + jq];
+        const double ox = a.q[3 * qi], oy = a.q[3 * qi + 1], oz = a.q[3 * qi + 2];
+        const int64_t t = blk * kTilesPerBlock + tt;
+        float4 l = make_float4(0.f, 0.f, 0.f, 1.f);
+        if (t < a.ntiles) {
+          const TileHeader* th = reinterpret_cast<const TileHeader*>(a.tiles + t * kTileBytes);
+          const double dx = ox - th->cx, dy = oy - th->cy, dz = oz - th->cz;
+          const double d2 = dx * dx + dy * dy + dz * dz;
+          l = make_float4(static_cast<float>(dx * th->scale), static_cast<float>(dy * th->scale),
+                          static_cast<float>(dz * th->scale), d2 >= th->far_r2 ? 1.f : 0.f);
+        }
+        sl[jq][tt] = l;
+        if (tt == 0) {
+          sq[jq][0] = ox;
+          sq[jq][1] = oy;
+          sq[jq][2] = oz;
+          sq[jq][3] = a.gw[qi];
+        }
+      }
+      __syncthreads();
+#pragma unroll 1
+      for (int jq = 0; jq < nc; ++jq) {
+        const float g = static_cast<float>(sq[jq][3]);
+        float dof[3] = {0.f, 0.f, 0.f};
+        double go[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const float4 l = sl[jq][2 * k + half];
+          const float ax = fv[k][0] - l.x, ay = fv[k][1] - l.y, az = fv[k][2] - l.z;
+          const float bx = fv[k][3] - l.x, by = fv[k][4] - l.y, bz = fv[k][5] - l.z;
+          const float cx = fv[k][6] - l.x, cy = fv[k][7] - l.y, cz = fv[k][8] - l.z;
+          const float aa = fmaf(ax, ax, fmaf(ay, ay, az * az));
+          const float bb = fmaf(bx, bx, fmaf(by, by, bz * bz));
+          const float cc = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+          const bool near = l.w == 0.f && fminf(aa, fminf(bb, cc)) < fv[k][9];
+          if (near) {
+            if (valid[k]) {
+              double v[9];
+#pragma unroll
+              for (int r = 0; r < 9; ++r) v[r] = a.tri64[r * a.ld64 + slot[k]];
+              pair_grad_fp64(sq[jq][0], sq[jq][1], sq[jq][2], v, sq[jq][3], true, acc64[k], go);
+            }
+          } else if (valid[k]) {
+            float ra, rb, rc;
+            asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(ra) : "f"(aa));
+            asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rb) : "f"(bb));
+            asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(cc));
+            const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
+            const float dab = fmaf(fmaf(ax, bx, fmaf(ay, by, az * bz)), rab, 1.f);
+            const float dbc = fmaf(fmaf(bx, cx, fmaf(by, cy, bz * cz)), rbc, 1.f);
+            const float dca = fmaf(fmaf(cx, ax, fmaf(cy, ay, cz * az)), rca, 1.f);
+            float iab, ibc, ica;
+            asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(iab) : "f"(dab));
+            asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ibc) : "f"(dbc));
+            asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ica) : "f"(dca));
+            const float wab = g * rab * iab, wbc = g * rbc * ibc, wca = g * rca * ica;
+            const float xab0 = ay * bz - az * by, xab1 = az * bx - ax * bz, xab2 = ax * by - ay * bx;
+            const float xbc0 = by * cz - bz * cy, xbc1 = bz * cx - bx * cz, xbc2 = bx * cy - by * cx;
+            const float xca0 = cy * az - cz * ay, xca1 = cz * ax - cx * az, xca2 = cx * ay - cy * ax;
+            const float kA1 = ra * wab, kA2 = ra * wca, kB1 = rb * wab, kB2 = rb * wbc;
+            const float kC1 = rc * wbc, kC2 = rc * wca;
+            acc32[k][0] -= fmaf(kA1, xab0, kA2 * xca0);
+            acc32[k][1] -= fmaf(kA1, xab1, kA2 * xca1);
+            acc32[k][2] -= fmaf(kA1, xab2, kA2 * xca2);
+            acc32[k][3] -= fmaf(kB1, xab0, kB2 * xbc0);
+            acc32[k][4] -= fmaf(kB1, xab1, kB2 * xbc1);
+            acc32[k][5] -= fmaf(kB1, xab2, kB2 * xbc2);
+            acc32[k][6] -= fmaf(kC1, xbc0, kC2 * xca0);
+            acc32[k][7] -= fmaf(kC1, xbc1, kC2 * xca1);
+            acc32[k][8] -= fmaf(kC1, xbc2, kC2 * xca2);
+            const float sc = static_cast<float>(scale[k]);
+            const float sab = (kA1 + kB1) * sc, sbc = (kB2 + kC1) * sc, sca = (kC2 + kA2) * sc;
+            dof[0] = fmaf(sab, xab0, fmaf(sbc, xbc0, fmaf(sca, xca0, dof[0])));
+            dof[1] = fmaf(sab, xab1, fmaf(sbc, xbc1, fmaf(sca, xca1, dof[1])));
+            dof[2] = fmaf(sab, xab2, fmaf(sbc, xbc2, fmaf(sca, xca2, dof[2])));
+          }
+        }
+        double dox = go[0] + dof[0], doy = go[1] + dof[1], doz = go[2] + dof[2];
+        for (int off = 16; off; off >>= 1) {
+          dox += __shfl_xor_sync(0xffffffffu, dox, off);
+          doy += __shfl_xor_sync(0xffffffffu, doy, off);
+          doz += __shfl_xor_sync(0xffffffffu, doz, off);
+        }
+        if (lane == 0) {
+          red[warp][jq][0] = dox;
+          red[warp][jq][1] = doy;
+          red[warp][jq][2] = doz;
+        }
+      }
+      __syncthreads();
+      for (int e = tid; e < nc * 3; e += THREADS) {
+        const int jq = e / 3, x = e % 3;
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < THREADS / 32; ++w) s += red[w][jq][x];
+        dO_row[(c0 + jq) * 3 + x] += s;
+      }
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int r = 0; r < 9; ++r) {
+          acc64[k][r] += scale[k] * static_cast<double>(acc32[k][r]);
+          acc32[k][r] = 0.f;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      if (!valid[k]) continue;
+#pragma unroll
+      for (int r = 0; r < 9; ++r) a.dF_part[(group * 9 + r) * a.ld64 + slot[k]] = acc64[k][r];
+    }
+  }
+}
+
+// dq[perm[s]] = (1/4pi) sum_r dO_part[r][s] (sorted positions back to input order).
+__global__ void finish_dq_sorted_kernel(const double* __restrict__ part, int64_t nranges,
+                                        int64_t nq, const uint32_t* __restrict__ perm,
+                                        double* __restrict__ dq) {
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= nq * 3) return;
+  double s = 0.0;
+  for (int64_t r = 0; r < nranges; ++r) s += part[r * nq * 3 + e];
+  dq[3 * static_cast<int64_t>(perm[e / 3]) + e % 3] = s * kInv4Pi;
+}
+
+// dtri[row][face_of[slot]] = (1/4pi) sum_g dF_part[g][row][slot] (sorted slots to input faces).
+__global__ void finish_dtri_sorted_kernel(const double* __restrict__ part, int64_t ngroups,
+                                          int64_t ld64, const uint32_t* __restrict__ face_of,
+                                          int64_t ld, double* __restrict__ dtri) {
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= 9 * ld64) return;
+  const int64_t r = e / ld64, sl = e % ld64;
+  const uint32_t f = face_of[sl];
+  if (f == 0xffffffffu) return;
+  double s = 0.0;
+  for (int64_t g = 0; g < ngroups; ++g) s += part[(g * 9 + r) * ld64 + sl];
+  dtri[r * ld + f] = s * kInv4Pi;
 }
 
 // dq[q] = (1/4pi) sum_r dO_part[r][q] (r in index order).
@@ -253,6 +473,48 @@ cudaError_t adjoint_fp64(const AdjointPlan& p, const double* tri, int64_t ld, in
                                                                                nq, dq);
   finish_dtri_kernel<<<static_cast<unsigned>(cdiv(9 * nf, 256)), 256, 0, stream>>>(
       dF_part, p.ngroups, ld, nf, dtri);
+  g_launches.fetch_add(3, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+
+AdjointPlan plan_adjoint_mixed(int64_t ntiles, int64_t nq, int sms) {
+  AdjointPlan p;
+  const int64_t nblocks = std::max<int64_t>(1, cdiv(ntiles, 4));
+  const int64_t target = static_cast<int64_t>(std::max(sms, 1)) * 4;
+  const int64_t nranges = std::min<int64_t>(nblocks, 16);
+  p.blocks_per_range = cdiv(nblocks, nranges);
+  p.nranges = cdiv(nblocks, p.blocks_per_range);
+  int64_t ngroups = std::max<int64_t>(1, cdiv(target, p.nranges));
+  ngroups = std::min(ngroups, std::max<int64_t>(1, cdiv(nq, kAdjQc)));
+  ngroups = std::min<int64_t>(ngroups, 65535);
+  p.queries_per_group = cdiv(std::max<int64_t>(nq, 1), ngroups);
+  p.ngroups = cdiv(std::max<int64_t>(nq, 1), p.queries_per_group);
+  return p;
+}
+
+cudaError_t adjoint_mixed(const AdjointPlan& p, const MixedMesh& m, const double* q,
+                          const uint32_t* perm, int64_t nq, const double* gw, double* dq,
+                          double* dtri, int64_t ld, void* scratch, size_t scratch_bytes,
+                          cudaStream_t stream) {
+  cudaError_t e = cudaSuccess;
+  if (nq > 0) e = cudaMemsetAsync(dq, 0, sizeof(double) * 3 * nq, stream);
+  if (e == cudaSuccess && m.nf > 0) e = cudaMemsetAsync(dtri, 0, sizeof(double) * 9 * ld, stream);
+  if (e != cudaSuccess || nq <= 0 || m.nf <= 0) return e;
+  if (scratch_bytes < adjoint_scratch_bytes(p, m.ld64, nq)) return cudaErrorInvalidValue;
+  double* dO_part = static_cast<double*>(scratch);
+  double* dF_part = dO_part + static_cast<size_t>(p.nranges) * nq * 3;
+  e = cudaMemsetAsync(dO_part, 0, sizeof(double) * static_cast<size_t>(p.nranges) * nq * 3,
+                      stream);
+  if (e != cudaSuccess) return e;
+  MixedAdjointArgs a{m.tiles, m.ntiles, m.tri64, m.ld64, q, perm, gw, nq,
+                     p.blocks_per_range, p.queries_per_group, dO_part, dF_part};
+  adjoint_mixed_kernel<2 * kTileFaces, kAdjQc>
+      <<<dim3(static_cast<unsigned>(p.nranges), static_cast<unsigned>(p.ngroups)), 2 * kTileFaces,
+         0, stream>>>(a);
+  finish_dq_sorted_kernel<<<static_cast<unsigned>(cdiv(nq * 3, 256)), 256, 0, stream>>>(
+      dO_part, p.nranges, nq, perm, dq);
+  finish_dtri_sorted_kernel<<<static_cast<unsigned>(cdiv(9 * m.ld64, 256)), 256, 0, stream>>>(
+      dF_part, p.ngroups, m.ld64, m.face_of, ld, dtri);
   g_launches.fetch_add(3, std::memory_order_relaxed);
   return cudaGetLastError();
 }

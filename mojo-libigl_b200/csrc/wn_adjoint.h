@@ -23,6 +23,16 @@ cudaError_t adjoint_fp64(const AdjointPlan& p, const double* tri, int64_t ld, in
                          const double* q, int64_t nq, const double* gw, double* dq, double* dtri,
                          void* scratch, size_t scratch_bytes, cudaStream_t stream);
 
+// Mixed-precision adjoint over a prepared mesh (wn_mixed.h) with Morton-ordered queries
+// (perm from mixed_sort_queries). Same outputs as adjoint_fp64, in input order; dtri has
+// row stride ld >= nf. Scratch: adjoint_scratch_bytes(p, m.ld64, nq).
+AdjointPlan plan_adjoint_mixed(int64_t ntiles, int64_t nq, int sms);
+struct MixedMesh;
+cudaError_t adjoint_mixed(const AdjointPlan& p, const MixedMesh& m, const double* q,
+                          const uint32_t* perm, int64_t nq, const double* gw, double* dq,
+                          double* dtri, int64_t ld, void* scratch, size_t scratch_bytes,
+                          cudaStream_t stream);
+
 // dV (nv x 3) from dtri through the vertex -> (3*face + corner) list (CSR indptr, entries).
 cudaError_t gather_vertex_grad(const double* dtri, int64_t ld, const int64_t* indptr,
                                const int64_t* entries, int64_t nv, double* dV,

@@ -489,6 +489,35 @@ int wn_backward_fp64_device(const double* tri, int64_t ld, int64_t nf, const dou
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "FP64 adjoint launch");
 }
 
+int wn_backward_mixed_device(void* mesh, const double* q, int64_t nq, const double* gw,
+                             double* dq, double* dtri, int64_t ld, void* stream) {
+  if (!mesh) return fail(WN_EINVAL, "null mesh");
+  const MeshHandle* h = static_cast<const MeshHandle*>(mesh);
+  if (nq < 0 || nq > 0x7fffffffLL || (ld & 1) || ld < h->m.nf)
+    return fail(WN_EINVAL, "bad sizes (nq=%lld, ld=%lld for %lld faces)", (long long)nq,
+                (long long)ld, (long long)h->m.nf);
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const AdjointPlan p = plan_adjoint_mixed(h->m.ntiles, nq, c->sms);
+  const size_t perm_bytes = ((static_cast<size_t>(std::max<int64_t>(nq, 1)) * 4 + 255) / 256) * 256;
+  const size_t sort_bytes = mixed_sort_scratch_bytes(nq);
+  const size_t adj_bytes = adjoint_scratch_bytes(p, h->m.ld64, nq);
+  unsigned char* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&scratch),
+                                  perm_bytes + std::max(sort_bytes, adj_bytes), st);
+  if (e != cudaSuccess) return cuda_fail(e, "device allocation");
+  uint32_t* perm = reinterpret_cast<uint32_t*>(scratch);
+  e = mixed_sort_queries(q, nq, perm, scratch + perm_bytes, sort_bytes, st);
+  if (e == cudaSuccess)
+    e = adjoint_mixed(p, h->m, q, perm, nq, gw, dq, dtri, ld, scratch + perm_bytes, adj_bytes,
+                      st);
+  cudaFreeAsync(scratch, st);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "mixed adjoint launch");
+}
+
 int wn_gather_vertex_grad_device(const double* dtri, int64_t ld, const int64_t* indptr,
                                  const int64_t* entries, int64_t nv, double* dV, void* stream) {
   if (nv < 0) return fail(WN_EINVAL, "bad nv=%lld", (long long)nv);

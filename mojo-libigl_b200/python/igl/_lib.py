@@ -66,6 +66,7 @@ _WN_SIGNATURES = {
     "wn_mixed_stats": ([ctypes.POINTER(I), ctypes.POINTER(I), C_INT], C_INT),
     "wn_backward_fp64_device": ([P, I, I, P, I, P, P, P, P], C_INT),
     "wn_gather_vertex_grad_device": ([P, I, P, P, I, P, P], C_INT),
+    "wn_backward_mixed_device": ([P, P, I, P, P, P, I, P], C_INT),
 }
 
 # The reference caps its pool at four workers on a shared host (_lib.py:34-37).

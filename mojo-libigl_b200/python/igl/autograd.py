@@ -56,23 +56,65 @@ def forward_fp64(tri: torch.Tensor, ld: int, nf: int, O: torch.Tensor) -> torch.
     return w
 
 
+class PreparedMesh:
+    """A mesh prepared for the mixed-precision kernels (Morton-ordered tiles)."""
+
+    def __init__(self, tri: torch.Tensor, ld: int, nf: int, kappa: float = 4.0):
+        self.handle = _lib.lib()
+        self.tri, self.ld, self.nf = tri, ld, nf
+        self.mesh = ctypes.c_void_p()
+        _check(self.handle.wn_mixed_mesh_create(tri.data_ptr(), ld, nf, kappa, _stream(),
+                                                ctypes.byref(self.mesh)))
+
+    def forward(self, O: torch.Tensor) -> torch.Tensor:
+        q = O.to(torch.float64).contiguous()
+        w = torch.empty(q.shape[0], dtype=torch.float64, device=q.device)
+        if q.shape[0]:
+            _check(self.handle.wn_forward_mixed_device(self.mesh, q.data_ptr(), q.shape[0],
+                                                       w.data_ptr(), _stream()))
+        return w
+
+    def backward(self, O: torch.Tensor, gW: torch.Tensor):
+        """(dq, dtri): dL/do (nq, 3) and dL/d(corner) (9, ld) for dL/dW = gW."""
+        q = O.to(torch.float64).contiguous()
+        gw = gW.to(torch.float64).contiguous()
+        dq = torch.empty((q.shape[0], 3), dtype=torch.float64, device=q.device)
+        dtri = torch.zeros_like(self.tri)
+        _check(self.handle.wn_backward_mixed_device(self.mesh, q.data_ptr(), q.shape[0],
+                                                    gw.data_ptr(), dq.data_ptr(),
+                                                    dtri.data_ptr(), self.ld, _stream()))
+        return dq, dtri
+
+    def close(self):
+        if self.mesh:
+            torch.cuda.current_stream().synchronize()
+            self.handle.wn_mixed_mesh_destroy(self.mesh)
+            self.mesh = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown
+            pass
+
+
 def forward_mixed(tri: torch.Tensor, ld: int, nf: int, O: torch.Tensor,
                   kappa: float = 4.0) -> torch.Tensor:
-    handle = _lib.lib()
-    q = O.to(torch.float64).contiguous()
-    w = torch.empty(q.shape[0], dtype=torch.float64, device=q.device)
-    if not q.shape[0]:
-        return w
-    mesh = ctypes.c_void_p()
-    _check(handle.wn_mixed_mesh_create(tri.data_ptr(), ld, nf, kappa, _stream(),
-                                       ctypes.byref(mesh)))
+    mesh = PreparedMesh(tri, ld, nf, kappa)
     try:
-        _check(handle.wn_forward_mixed_device(mesh, q.data_ptr(), q.shape[0], w.data_ptr(),
-                                              _stream()))
+        return mesh.forward(O)
     finally:
-        torch.cuda.current_stream().synchronize()
-        handle.wn_mixed_mesh_destroy(mesh)
-    return w
+        mesh.close()
+
+
+def gather_vertices(dtri, ld, nf, F, nv):
+    dV = torch.zeros((nv, 3), dtype=torch.float64, device=dtri.device)
+    if nf and nv:
+        indptr, entries = vertex_csr(F, nv)
+        _check(_lib.lib().wn_gather_vertex_grad_device(dtri.data_ptr(), ld, indptr.data_ptr(),
+                                                       entries.data_ptr(), nv, dV.data_ptr(),
+                                                       _stream()))
+    return dV
 
 
 def backward_fp64(tri, ld, nf, O, gW, F, nv):
@@ -86,13 +128,7 @@ def backward_fp64(tri, ld, nf, O, gW, F, nv):
     _check(handle.wn_backward_fp64_device(tri.data_ptr(), ld, nf, q.data_ptr(), nq,
                                           gw.data_ptr(), dq.data_ptr(), dtri.data_ptr(),
                                           _stream()))
-    dV = torch.zeros((nv, 3), dtype=torch.float64, device=q.device)
-    if nf and nv:
-        indptr, entries = vertex_csr(F, nv)
-        _check(handle.wn_gather_vertex_grad_device(dtri.data_ptr(), ld, indptr.data_ptr(),
-                                                   entries.data_ptr(), nv, dV.data_ptr(),
-                                                   _stream()))
-    return dV, dq
+    return gather_vertices(dtri, ld, nf, F, nv), dq
 
 
 class WindingNumberFunction(torch.autograd.Function):
@@ -101,8 +137,10 @@ class WindingNumberFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, V, F, O, precision="fp64"):
         tri, ld, nf = triangle_soa(V, F)
+        ctx.mesh = None
         if precision == "mixed":
-            w = forward_mixed(tri, ld, nf, O)
+            ctx.mesh = PreparedMesh(tri, ld, nf)
+            w = ctx.mesh.forward(O)
         else:
             w = forward_fp64(tri, ld, nf, O)
         ctx.save_for_backward(V, F, O)
@@ -112,13 +150,25 @@ class WindingNumberFunction(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gW):
         V, F, O = ctx.saved_tensors
-        dV, dq = backward_fp64(ctx.tri, ctx.ld, ctx.nf, O, gW, F, V.shape[0])
+        if ctx.mesh is not None:
+            dq, dtri = ctx.mesh.backward(O, gW)
+            dV = gather_vertices(dtri, ctx.ld, ctx.nf, F, V.shape[0])
+            ctx.mesh.close()
+        else:
+            dV, dq = backward_fp64(ctx.tri, ctx.ld, ctx.nf, O, gW, F, V.shape[0])
         return dV.to(V.dtype), None, dq.to(O.dtype), None
 
 
 def winding_number_torch(V: torch.Tensor, F: torch.Tensor, O: torch.Tensor,
-                         precision: str = "fp64") -> torch.Tensor:
-    """Differentiable W for CUDA tensors V (nv,3), F (nf,3) int, O (nq,3)."""
+                         precision: str | None = None) -> torch.Tensor:
+    """Differentiable W for CUDA tensors V (nv,3), F (nf,3) int, O (nq,3).
+
+    precision: "fp64" (plain FP64 forward and adjoint) or "mixed" (FP32 pairs with
+    FP64 refinement of near-surface pairs, forward and adjoint); by default
+    "mixed" for float32 queries and "fp64" otherwise. W has the dtype of O.
+    """
+    if precision is None:
+        precision = "mixed" if O.dtype == torch.float32 else "fp64"
     if not (V.is_cuda and F.is_cuda and O.is_cuda):
         raise RuntimeError("winding_number_torch needs CUDA tensors (no CPU fallback)")
     if precision not in ("fp64", "mixed"):

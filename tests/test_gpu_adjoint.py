@@ -143,3 +143,39 @@ def test_empty_faces(gpu_required):
     W.sum().backward()
     assert float(W.abs().max()) == 0.0
     assert float(Vt.grad.abs().max()) == 0.0 and float(Ot.grad.abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_mixed_adjoint_matches_fp64_adjoint(gpu_required, dtype):
+    """Mixed-precision adjoint (FP32 far pairs, FP64 near pairs) vs the FP64 adjoint."""
+    import torch
+
+    V, F, O, _ = igl.synthetic.workload("c4_grad", n_queries=8192)
+    g = np.random.default_rng(45).normal(size=len(O))
+    out = {}
+    for precision in ("fp64", "mixed"):
+        Vt = _cuda(V).requires_grad_(True)
+        Ot = _cuda(O, getattr(torch, dtype) if precision == "mixed" else None)
+        Ot.requires_grad_(True)
+        W = wa.winding_number_torch(Vt, _cuda(F), Ot, precision=precision)
+        (W * _cuda(g, W.dtype)).sum().backward()
+        out[precision] = (W.detach().double().cpu().numpy(), Vt.grad.cpu().numpy(),
+                          Ot.grad.double().cpu().numpy())
+    w64, dV64, dO64 = out["fp64"]
+    wm, dVm, dOm = out["mixed"]
+    tol_w = 1e-6 if dtype == "float64" else 1e-5  # float32 queries are rounded on input
+    if dtype == "float64":
+        assert np.abs(wm - w64).max() <= tol_w
+        assert np.abs(dVm - dV64).max() <= 1e-4 * np.abs(dV64).max()
+        assert np.abs(dOm - dO64).max() <= 1e-4 * np.abs(dO64).max()
+    else:
+        # float32 queries move each point by up to ~6e-8: compare the FP64 adjoint
+        # evaluated at the rounded points instead.
+        O32 = O.astype(np.float32).astype(np.float64)
+        Vt = _cuda(V).requires_grad_(True)
+        Ot = _cuda(O32).requires_grad_(True)
+        W = wa.winding_number_torch(Vt, _cuda(F), Ot, precision="fp64")
+        (W * _cuda(g)).sum().backward()
+        assert np.abs(wm - W.detach().cpu().numpy()).max() <= 1e-6
+        assert np.abs(dVm - Vt.grad.cpu().numpy()).max() <= 1e-4 * np.abs(dV64).max()
+        assert np.abs(dOm - Ot.grad.cpu().numpy()).max() <= 1e-3 * np.abs(dO64).max()

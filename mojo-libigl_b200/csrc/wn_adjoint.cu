@@ -184,9 +184,7 @@ struct MixedAdjointArgs {
   int64_t ntiles;
   const double* tri64;  // sorted FP64 soup, 9 x ld64
   int64_t ld64;
-  const double* q;        // nq x 3, input order
-  const uint32_t* perm;   // sorted position -> query index
-  const double* gw;       // nq, input order
+  const double4* qs;      // nq queries in Morton order: x, y, z, g
   int64_t nq;
   int64_t blocks_per_range;   // 4-tile blocks per range (grid.x)
   int64_t queries_per_group;  // sorted query positions per group (grid.y)
@@ -194,13 +192,33 @@ struct MixedAdjointArgs {
   double* dF_part;  // [ngroups][9][ld64] by sorted slot
 };
 
+// Queries in Morton order with their upstream gradient: xyz and g as one double4.
+__global__ void gather_sorted_queries_kernel(const double* __restrict__ q,
+                                             const double* __restrict__ gw,
+                                             const uint32_t* __restrict__ perm, int64_t nq,
+                                             double4* __restrict__ qs) {
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= nq) return;
+  const int64_t i = perm[s];
+  qs[s] = make_double4(q[3 * i], q[3 * i + 1], q[3 * i + 2], gw[i]);
+}
+
+// Shared-memory layout of adjoint_mixed_kernel (dynamic, QC queries per chunk).
+template <int THREADS, int QC>
+struct MixedAdjointSmem {
+  float dO32[QC][3][THREADS];  // per-thread FP32 dL/do shares of far pairs (transposed)
+  double red64[THREADS / 32][QC][3];  // per-warp FP64 shares of refined pairs
+  double4 sq[QC];                     // FP64 query + g
+  float4 sl[QC][4];                   // local scaled query per tile, w = 1 if far
+  TileHeader th[4];
+};
+
 template <int THREADS, int QC>
 __global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAdjointArgs a) {
   static_assert(THREADS == 2 * kTileFaces, "one thread per face of two tiles");
   constexpr int kTilesPerBlock = 4;
-  __shared__ float4 sl[QC][kTilesPerBlock];   // local scaled query, w = 1 if far from the tile
-  __shared__ double sq[QC][4];                // FP64 query and g
-  __shared__ double red[THREADS / 32][QC][3];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto& sm = *reinterpret_cast<MixedAdjointSmem<THREADS, QC>*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int j = tid & (kTileFaces - 1), half = tid >> 6;
   const int64_t nblocks = (a.ntiles + kTilesPerBlock - 1) / kTilesPerBlock;
@@ -212,6 +230,17 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAd
   double* dO_row = a.dO_part + range * a.nq * 3;
 
   for (int64_t blk = b_begin; blk < b_end; ++blk) {
+    __syncthreads();  // previous block's shared data fully consumed
+    if (tid < kTilesPerBlock) {
+      const int64_t t = blk * kTilesPerBlock + tid;
+      if (t < a.ntiles) {
+        sm.th[tid] = *reinterpret_cast<const TileHeader*>(a.tiles + t * kTileBytes);
+      } else {
+        TileHeader empty{};
+        empty.far_r2 = 0.0;  // every query is "far" from a missing tile
+        sm.th[tid] = empty;
+      }
+    }
     float fv[2][10];  // A, B, C (scaled local), thr
     double scale[2];
     int64_t slot[2];
@@ -243,34 +272,28 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAd
       __syncthreads();
       for (int item = tid; item < nc * kTilesPerBlock; item += THREADS) {
         const int jq = item / kTilesPerBlock, tt = item % kTilesPerBlock;
-        const int64_t qi = a.perm[c0 + jq];
-        const double ox = a.q[3 * qi], oy = a.q[3 * qi + 1], oz = a.q[3 * qi + 2];
-        const int64_t t = blk * kTilesPerBlock + tt;
-        float4 l = make_float4(0.f, 0.f, 0.f, 1.f);
-        if (t < a.ntiles) {
-          const TileHeader* th = reinterpret_cast<const TileHeader*>(a.tiles + t * kTileBytes);
-          const double dx = ox - th->cx, dy = oy - th->cy, dz = oz - th->cz;
-          const double d2 = dx * dx + dy * dy + dz * dz;
-          l = make_float4(static_cast<float>(dx * th->scale), static_cast<float>(dy * th->scale),
-                          static_cast<float>(dz * th->scale), d2 >= th->far_r2 ? 1.f : 0.f);
-        }
-        sl[jq][tt] = l;
-        if (tt == 0) {
-          sq[jq][0] = ox;
-          sq[jq][1] = oy;
-          sq[jq][2] = oz;
-          sq[jq][3] = a.gw[qi];
-        }
+        const double4 o = a.qs[c0 + jq];
+        const TileHeader& th = sm.th[tt];
+        const double dx = o.x - th.cx, dy = o.y - th.cy, dz = o.z - th.cz;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        sm.sl[jq][tt] = make_float4(static_cast<float>(dx * th.scale),
+                                    static_cast<float>(dy * th.scale),
+                                    static_cast<float>(dz * th.scale), d2 >= th.far_r2 ? 1.f : 0.f);
+        if (tt == 0) sm.sq[jq] = o;
       }
+      for (int e = tid; e < (THREADS / 32) * QC * 3; e += THREADS)
+        (&sm.red64[0][0][0])[e] = 0.0;
       __syncthreads();
 #pragma unroll 1
       for (int jq = 0; jq < nc; ++jq) {
-        const float g = static_cast<float>(sq[jq][3]);
+        const double4 o = sm.sq[jq];
+        const float g = static_cast<float>(o.w);
         float dof[3] = {0.f, 0.f, 0.f};
         double go[3] = {0.0, 0.0, 0.0};
+        bool refined = false;
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-          const float4 l = sl[jq][2 * k + half];
+          const float4 l = sm.sl[jq][2 * k + half];
           const float ax = fv[k][0] - l.x, ay = fv[k][1] - l.y, az = fv[k][2] - l.z;
           const float bx = fv[k][3] - l.x, by = fv[k][4] - l.y, bz = fv[k][5] - l.z;
           const float cx = fv[k][6] - l.x, cy = fv[k][7] - l.y, cz = fv[k][8] - l.z;
@@ -283,7 +306,8 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAd
               double v[9];
 #pragma unroll
               for (int r = 0; r < 9; ++r) v[r] = a.tri64[r * a.ld64 + slot[k]];
-              pair_grad_fp64(sq[jq][0], sq[jq][1], sq[jq][2], v, sq[jq][3], true, acc64[k], go);
+              pair_grad_fp64(o.x, o.y, o.z, v, o.w, true, acc64[k], go);
+              refined = true;
             }
           } else if (valid[k]) {
             float ra, rb, rc;
@@ -320,25 +344,37 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAd
             dof[2] = fmaf(sab, xab2, fmaf(sbc, xbc2, fmaf(sca, xca2, dof[2])));
           }
         }
-        double dox = go[0] + dof[0], doy = go[1] + dof[1], doz = go[2] + dof[2];
-        for (int off = 16; off; off >>= 1) {
-          dox += __shfl_xor_sync(0xffffffffu, dox, off);
-          doy += __shfl_xor_sync(0xffffffffu, doy, off);
-          doz += __shfl_xor_sync(0xffffffffu, doz, off);
-        }
-        if (lane == 0) {
-          red[warp][jq][0] = dox;
-          red[warp][jq][1] = doy;
-          red[warp][jq][2] = doz;
+        sm.dO32[jq][0][tid] = dof[0];
+        sm.dO32[jq][1][tid] = dof[1];
+        sm.dO32[jq][2][tid] = dof[2];
+        // Refined pairs carry large, cancelling terms: reduce them in FP64.
+        if (__any_sync(0xffffffffu, refined)) {
+          for (int off = 16; off; off >>= 1) {
+            go[0] += __shfl_xor_sync(0xffffffffu, go[0], off);
+            go[1] += __shfl_xor_sync(0xffffffffu, go[1], off);
+            go[2] += __shfl_xor_sync(0xffffffffu, go[2], off);
+          }
+          if (lane == 0) {
+            sm.red64[warp][jq][0] = go[0];
+            sm.red64[warp][jq][1] = go[1];
+            sm.red64[warp][jq][2] = go[2];
+          }
         }
       }
       __syncthreads();
-      for (int e = tid; e < nc * 3; e += THREADS) {
+      // One warp per (query, component): FP32 shares summed in lane order, then the
+      // FP64 shares in warp order; the sum is added into this CTA's row.
+      for (int e = warp; e < nc * 3; e += THREADS / 32) {
         const int jq = e / 3, x = e % 3;
-        double s = 0.0;
+        const float4 v4 = reinterpret_cast<const float4*>(&sm.dO32[jq][x][0])[lane];
+        float v = (v4.x + v4.y) + (v4.z + v4.w);
+        for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == 0) {
+          double s = static_cast<double>(v);
 #pragma unroll
-        for (int w = 0; w < THREADS / 32; ++w) s += red[w][jq][x];
-        dO_row[(c0 + jq) * 3 + x] += s;
+          for (int w = 0; w < THREADS / 32; ++w) s += sm.red64[w][jq][x];
+          dO_row[(c0 + jq) * 3 + x] += s;
+        }
       }
 #pragma unroll
       for (int k = 0; k < 2; ++k)
@@ -445,9 +481,10 @@ AdjointPlan plan_adjoint(int64_t nf, int64_t nq, int sms) {
 }
 
 size_t adjoint_scratch_bytes(const AdjointPlan& p, int64_t ld, int64_t nq) {
+  // dO partials, dF partials, and the Morton-ordered (query, g) copy of the mixed path.
   return sizeof(double) * (static_cast<size_t>(p.nranges) * nq * 3 +
                            static_cast<size_t>(p.ngroups) * 9 * ld) +
-         256;
+         sizeof(double4) * static_cast<size_t>(std::max<int64_t>(nq, 1)) + 256;
 }
 
 cudaError_t adjoint_fp64(const AdjointPlan& p, const double* tri, int64_t ld, int64_t nf,
@@ -506,16 +543,25 @@ cudaError_t adjoint_mixed(const AdjointPlan& p, const MixedMesh& m, const double
   e = cudaMemsetAsync(dO_part, 0, sizeof(double) * static_cast<size_t>(p.nranges) * nq * 3,
                       stream);
   if (e != cudaSuccess) return e;
-  MixedAdjointArgs a{m.tiles, m.ntiles, m.tri64, m.ld64, q, perm, gw, nq,
+  const size_t qs_off =
+      ((reinterpret_cast<uintptr_t>(dF_part + static_cast<size_t>(p.ngroups) * 9 * m.ld64) + 255) &
+       ~static_cast<uintptr_t>(255)) - reinterpret_cast<uintptr_t>(scratch);
+  double4* qs = reinterpret_cast<double4*>(static_cast<unsigned char*>(scratch) + qs_off);
+  gather_sorted_queries_kernel<<<static_cast<unsigned>(cdiv(nq, 256)), 256, 0, stream>>>(
+      q, gw, perm, nq, qs);
+  MixedAdjointArgs a{m.tiles, m.ntiles, m.tri64, m.ld64, qs, nq,
                      p.blocks_per_range, p.queries_per_group, dO_part, dF_part};
-  adjoint_mixed_kernel<2 * kTileFaces, kAdjQc>
-      <<<dim3(static_cast<unsigned>(p.nranges), static_cast<unsigned>(p.ngroups)), 2 * kTileFaces,
-         0, stream>>>(a);
+  auto kernel = adjoint_mixed_kernel<2 * kTileFaces, kAdjQc>;
+  const int smem = static_cast<int>(sizeof(MixedAdjointSmem<2 * kTileFaces, kAdjQc>));
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  kernel<<<dim3(static_cast<unsigned>(p.nranges), static_cast<unsigned>(p.ngroups)),
+           2 * kTileFaces, smem, stream>>>(a);
   finish_dq_sorted_kernel<<<static_cast<unsigned>(cdiv(nq * 3, 256)), 256, 0, stream>>>(
       dO_part, p.nranges, nq, perm, dq);
   finish_dtri_sorted_kernel<<<static_cast<unsigned>(cdiv(9 * m.ld64, 256)), 256, 0, stream>>>(
       dF_part, p.ngroups, m.ld64, m.face_of, ld, dtri);
-  g_launches.fetch_add(3, std::memory_order_relaxed);
+  g_launches.fetch_add(4, std::memory_order_relaxed);
   return cudaGetLastError();
 }
 

@@ -209,6 +209,7 @@ struct MixedAdjointSmem {
   float dO32[QC][3][THREADS];  // per-thread FP32 dL/do shares of far pairs (transposed)
   double red64[THREADS / 32][QC][3];  // per-warp FP64 shares of refined pairs
   double4 sq[QC];                     // FP64 query + g
+  double dsum[QC * 3];                // the chunk's dL/do sums before they go to global
   float4 sl[QC][4];                   // local scaled query per tile, w = 1 if far
   TileHeader th[4];
 };
@@ -373,9 +374,11 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAd
           double s = static_cast<double>(v);
 #pragma unroll
           for (int w = 0; w < THREADS / 32; ++w) s += sm.red64[w][jq][x];
-          dO_row[(c0 + jq) * 3 + x] += s;
+          sm.dsum[e] = s;
         }
       }
+      __syncthreads();
+      for (int e = tid; e < nc * 3; e += THREADS) dO_row[c0 * 3 + e] += sm.dsum[e];
 #pragma unroll
       for (int k = 0; k < 2; ++k)
 #pragma unroll

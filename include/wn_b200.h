@@ -148,11 +148,22 @@ int wn_backward_fp64_device(const double* tri, int64_t ld, int64_t nf, const dou
 int wn_backward_mixed_device(void* mesh, const double* q, int64_t nq, const double* gw,
                              double* dq, double* dtri, int64_t ld, void* stream);
 
-/* dV (nv x 3) = sum of dtri over each vertex's (face, corner) uses; indptr (nv+1)
- * and entries (3*face + corner, grouped by vertex) form a CSR list; the sum runs
- * in list order (deterministic). */
-int wn_gather_vertex_grad_device(const double* dtri, int64_t ld, const int64_t* indptr,
-                                 const int64_t* entries, int64_t nv, double* dV, void* stream);
+/* Boundary-edge adjoint for indexed meshes (mathematically equal to the per-face
+ * adjoint summed at the vertices: the terms of a directed side and its reverse
+ * cancel, so only edges with nonzero net multiplicity m = #(u->v) - #(v->u)
+ * remain). edges: 7 rows of stride le (Px, Py, Pz, Qx, Qy, Qz, m); outputs dq
+ * (nq x 3) and dedge (6 rows of stride le: dL/dP, dL/dQ). FP64, deterministic. */
+int wn_backward_edges_device(const double* edges, int64_t le, int64_t ne, const double* q,
+                             int64_t nq, const double* gw, double* dq, double* dedge,
+                             void* stream);
+
+/* dV (nv x 3) = sum of per-element corner gradients over each vertex's uses.
+ * grad: rows 3*corner+axis with stride ld; corners = 3 (faces, dtri) or 2 (edges,
+ * dedge); indptr (nv+1) and entries (corners*element + corner, grouped by
+ * vertex) form a CSR list summed in list order (deterministic). */
+int wn_gather_vertex_grad_device(const double* grad, int64_t ld, int corners,
+                                 const int64_t* indptr, const int64_t* entries, int64_t nv,
+                                 double* dV, void* stream);
 
 #ifdef __cplusplus
 }

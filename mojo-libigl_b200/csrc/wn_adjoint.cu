@@ -421,6 +421,134 @@ __global__ void finish_dtri_sorted_kernel(const double* __restrict__ part, int64
   dtri[r * ld + f] = s * kInv4Pi;
 }
 
+// ---- boundary-edge adjoint ------------------------------------------------
+// For an indexed mesh the per-face terms above telescope. Write a face's
+// derivative as a sum over its three directed sides P -> Q (p = P - o, q = Q - o,
+// D = |p||q| + p.q):
+//   side P -> Q adds  -(p x q)/(|p| D) to dOmega/dP  and  -(p x q)/(|q| D) to dOmega/dQ.
+// The reversed side Q -> P of a neighbouring face adds exactly the negatives, so
+// at both endpoints the two cancel. Summed over the mesh only the net boundary
+// survives: every undirected edge {u, v} enters with multiplicity
+// m = #(u -> v) - #(v -> u), and edges with m = 0 drop out. This kernel evaluates
+// those edges (endpoints P, Q and m in a 7 x le SoA); its per-edge sums over the
+// queries go to dedge (6 x le: dL/dP, dL/dQ) and the per-query sums over edges to dq.
+// Same work split and fixed reduction order as adjoint_fp64_kernel.
+struct EdgeAdjointArgs {
+  const double* edges;  // 7 x le: Px, Py, Pz, Qx, Qy, Qz, m
+  int64_t le, ne;
+  const double* q;
+  const double* gw;
+  int64_t nq;
+  int64_t blocks_per_range, queries_per_group;
+  double* dO_part;  // [nranges][nq][3], zeroed
+  double* dE_part;  // [ngroups][6][le]
+};
+
+template <int THREADS, int EPT, int QC>
+__global__ void __launch_bounds__(THREADS, 2) adjoint_edges_kernel(const EdgeAdjointArgs a) {
+  __shared__ double sq[QC][4];
+  __shared__ double red[THREADS / 32][QC][3];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int kBlockEdges = THREADS * EPT;
+  const int64_t nblocks = (a.ne + kBlockEdges - 1) / kBlockEdges;
+  const int64_t range = blockIdx.x, group = blockIdx.y;
+  const int64_t b_begin = range * a.blocks_per_range;
+  const int64_t b_end = min(nblocks, b_begin + a.blocks_per_range);
+  const int64_t q_begin = group * a.queries_per_group;
+  const int64_t q_end = min(a.nq, q_begin + a.queries_per_group);
+  double* dO_row = a.dO_part + range * a.nq * 3;
+  for (int64_t blk = b_begin; blk < b_end; ++blk) {
+    double ev[EPT][7], acc[EPT][6];
+#pragma unroll
+    for (int k = 0; k < EPT; ++k) {
+      const int64_t e = blk * kBlockEdges + k * THREADS + tid;
+      const bool valid = e < a.ne;
+#pragma unroll
+      for (int r = 0; r < 7; ++r) ev[k][r] = valid ? a.edges[r * a.le + e] : 0.0;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) acc[k][r] = 0.0;
+    }
+    for (int64_t c0 = q_begin; c0 < q_end; c0 += QC) {
+      const int nc = static_cast<int>(q_end - c0 < QC ? q_end - c0 : QC);
+      __syncthreads();
+      if (tid < nc) {
+        const int64_t qi = c0 + tid;
+        sq[tid][0] = a.q[3 * qi];
+        sq[tid][1] = a.q[3 * qi + 1];
+        sq[tid][2] = a.q[3 * qi + 2];
+        sq[tid][3] = a.gw[qi];
+      }
+      __syncthreads();
+#pragma unroll 1
+      for (int j = 0; j < nc; ++j) {
+        const double ox = sq[j][0], oy = sq[j][1], oz = sq[j][2], g = sq[j][3];
+        double dox = 0.0, doy = 0.0, doz = 0.0;
+#pragma unroll
+        for (int k = 0; k < EPT; ++k) {
+          const double px = ev[k][0] - ox, py = ev[k][1] - oy, pz = ev[k][2] - oz;
+          const double qx = ev[k][3] - ox, qy = ev[k][4] - oy, qz = ev[k][5] - oz;
+          const double pp = px * px + py * py + pz * pz;
+          const double qq = qx * qx + qy * qy + qz * qz;
+          const double rp = rsqrt(pp), rq = rsqrt(qq);
+          const double rpq = rp * rq;
+          const double d = 1.0 + (px * qx + py * qy + pz * qz) * rpq;
+          // Zero for padding (m = 0) and where the derivative does not exist.
+          const bool ok = ev[k][6] != 0.0 && pp > 0.0 && qq > 0.0 && d > 0.0;
+          const double w = ok ? g * ev[k][6] * rpq / d : 0.0;
+          const double cp = ok ? rp * w : 0.0, cq = ok ? rq * w : 0.0;
+          const double x0 = py * qz - pz * qy, x1 = pz * qx - px * qz, x2 = px * qy - py * qx;
+          acc[k][0] -= cp * x0;
+          acc[k][1] -= cp * x1;
+          acc[k][2] -= cp * x2;
+          acc[k][3] -= cq * x0;
+          acc[k][4] -= cq * x1;
+          acc[k][5] -= cq * x2;
+          const double c = cp + cq;
+          dox += c * x0;
+          doy += c * x1;
+          doz += c * x2;
+        }
+        for (int off = 16; off; off >>= 1) {
+          dox += __shfl_xor_sync(0xffffffffu, dox, off);
+          doy += __shfl_xor_sync(0xffffffffu, doy, off);
+          doz += __shfl_xor_sync(0xffffffffu, doz, off);
+        }
+        if (lane == 0) {
+          red[warp][j][0] = dox;
+          red[warp][j][1] = doy;
+          red[warp][j][2] = doz;
+        }
+      }
+      __syncthreads();
+      for (int e = tid; e < nc * 3; e += THREADS) {
+        const int j = e / 3, x = e % 3;
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < THREADS / 32; ++w) s += red[w][j][x];
+        dO_row[(c0 + j) * 3 + x] += s;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < EPT; ++k) {
+      const int64_t e = blk * kBlockEdges + k * THREADS + tid;
+      if (e >= a.ne) continue;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) a.dE_part[(group * 6 + r) * a.le + e] = acc[k][r];
+    }
+  }
+}
+
+// dedge[row][e] = (1/4pi) sum_g dE_part[g][row][e].
+__global__ void finish_dedge_kernel(const double* __restrict__ part, int64_t ngroups, int64_t le,
+                                    int64_t ne, double* __restrict__ dedge) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= 6 * ne) return;
+  const int64_t r = i / ne, e = i % ne;
+  double s = 0.0;
+  for (int64_t g = 0; g < ngroups; ++g) s += part[(g * 6 + r) * le + e];
+  dedge[r * le + e] = s * kInv4Pi;
+}
+
 // dq[q] = (1/4pi) sum_r dO_part[r][q] (r in index order).
 __global__ void finish_dq_kernel(const double* __restrict__ part, int64_t nranges, int64_t nq,
                                  double* __restrict__ dq) {
@@ -443,7 +571,7 @@ __global__ void finish_dtri_kernel(const double* __restrict__ part, int64_t ngro
 }
 
 // dV[v][x] = sum over the vertex's (face, corner) entries, in list order.
-__global__ void gather_vertex_kernel(const double* __restrict__ dtri, int64_t ld,
+__global__ void gather_vertex_kernel(const double* __restrict__ dtri, int64_t ld, int corners,
                                      const int64_t* __restrict__ indptr,
                                      const int64_t* __restrict__ entries, int64_t nv,
                                      double* __restrict__ dV) {
@@ -451,7 +579,7 @@ __global__ void gather_vertex_kernel(const double* __restrict__ dtri, int64_t ld
   if (v >= nv) return;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
   for (int64_t e = indptr[v]; e < indptr[v + 1]; ++e) {
-    const int64_t f = entries[e] / 3, c = entries[e] % 3;
+    const int64_t f = entries[e] / corners, c = entries[e] % corners;
     s0 += dtri[(3 * c) * ld + f];
     s1 += dtri[(3 * c + 1) * ld + f];
     s2 += dtri[(3 * c + 2) * ld + f];
@@ -517,6 +645,53 @@ cudaError_t adjoint_fp64(const AdjointPlan& p, const double* tri, int64_t ld, in
   return cudaGetLastError();
 }
 
+AdjointPlan plan_adjoint_edges(int64_t ne, int64_t nq, int sms) {
+  AdjointPlan p;
+  const int64_t nblocks = std::max<int64_t>(1, cdiv(ne, kAdjThreads * kAdjFpt));
+  const int64_t target = static_cast<int64_t>(std::max(sms, 1)) * 4;
+  const int64_t nranges = std::min<int64_t>(nblocks, 16);
+  p.blocks_per_range = cdiv(nblocks, nranges);
+  p.nranges = cdiv(nblocks, p.blocks_per_range);
+  int64_t ngroups = std::max<int64_t>(1, cdiv(target, p.nranges));
+  ngroups = std::min(ngroups, std::max<int64_t>(1, cdiv(nq, kAdjQc)));
+  ngroups = std::min<int64_t>(ngroups, 65535);
+  p.queries_per_group = cdiv(std::max<int64_t>(nq, 1), ngroups);
+  p.ngroups = cdiv(std::max<int64_t>(nq, 1), p.queries_per_group);
+  return p;
+}
+
+size_t adjoint_edges_scratch_bytes(const AdjointPlan& p, int64_t le, int64_t nq) {
+  return sizeof(double) * (static_cast<size_t>(p.nranges) * nq * 3 +
+                           static_cast<size_t>(p.ngroups) * 6 * le) + 256;
+}
+
+cudaError_t adjoint_edges(const AdjointPlan& p, const double* edges, int64_t le, int64_t ne,
+                          const double* q, int64_t nq, const double* gw, double* dq,
+                          double* dedge, void* scratch, size_t scratch_bytes,
+                          cudaStream_t stream) {
+  cudaError_t e = cudaSuccess;
+  if (nq > 0) e = cudaMemsetAsync(dq, 0, sizeof(double) * 3 * nq, stream);
+  if (e == cudaSuccess && ne > 0) e = cudaMemsetAsync(dedge, 0, sizeof(double) * 6 * le, stream);
+  if (e != cudaSuccess || nq <= 0 || ne <= 0) return e;
+  if (scratch_bytes < adjoint_edges_scratch_bytes(p, le, nq)) return cudaErrorInvalidValue;
+  double* dO_part = static_cast<double*>(scratch);
+  double* dE_part = dO_part + static_cast<size_t>(p.nranges) * nq * 3;
+  e = cudaMemsetAsync(dO_part, 0, sizeof(double) * static_cast<size_t>(p.nranges) * nq * 3,
+                      stream);
+  if (e != cudaSuccess) return e;
+  EdgeAdjointArgs a{edges, le, ne, q, gw, nq, p.blocks_per_range, p.queries_per_group,
+                    dO_part, dE_part};
+  adjoint_edges_kernel<kAdjThreads, kAdjFpt, kAdjQc>
+      <<<dim3(static_cast<unsigned>(p.nranges), static_cast<unsigned>(p.ngroups)), kAdjThreads, 0,
+         stream>>>(a);
+  finish_dq_kernel<<<static_cast<unsigned>(cdiv(nq * 3, 256)), 256, 0, stream>>>(dO_part, p.nranges,
+                                                                               nq, dq);
+  finish_dedge_kernel<<<static_cast<unsigned>(cdiv(6 * ne, 256)), 256, 0, stream>>>(
+      dE_part, p.ngroups, le, ne, dedge);
+  g_launches.fetch_add(3, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+
 AdjointPlan plan_adjoint_mixed(int64_t ntiles, int64_t nq, int sms) {
   AdjointPlan p;
   const int64_t nblocks = std::max<int64_t>(1, cdiv(ntiles, 4));
@@ -568,12 +743,12 @@ cudaError_t adjoint_mixed(const AdjointPlan& p, const MixedMesh& m, const double
   return cudaGetLastError();
 }
 
-cudaError_t gather_vertex_grad(const double* dtri, int64_t ld, const int64_t* indptr,
-                               const int64_t* entries, int64_t nv, double* dV,
-                               cudaStream_t stream) {
+cudaError_t gather_vertex_grad(const double* dtri, int64_t ld, int corners,
+                               const int64_t* indptr, const int64_t* entries, int64_t nv,
+                               double* dV, cudaStream_t stream) {
   if (nv <= 0) return cudaSuccess;
   gather_vertex_kernel<<<static_cast<unsigned>(cdiv(nv, 256)), 256, 0, stream>>>(
-      dtri, ld, indptr, entries, nv, dV);
+      dtri, ld, corners, indptr, entries, nv, dV);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return cudaGetLastError();
 }

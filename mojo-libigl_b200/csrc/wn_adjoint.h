@@ -33,9 +33,20 @@ cudaError_t adjoint_mixed(const AdjointPlan& p, const MixedMesh& m, const double
                           double* dtri, int64_t ld, void* scratch, size_t scratch_bytes,
                           cudaStream_t stream);
 
-// dV (nv x 3) from dtri through the vertex -> (3*face + corner) list (CSR indptr, entries).
-cudaError_t gather_vertex_grad(const double* dtri, int64_t ld, const int64_t* indptr,
-                               const int64_t* entries, int64_t nv, double* dV,
-                               cudaStream_t stream);
+// Boundary-edge adjoint (indexed meshes): edges 7 x le (P, Q, net multiplicity m), outputs
+// dq (nq x 3) and dedge (6 x le: dL/dP, dL/dQ).
+AdjointPlan plan_adjoint_edges(int64_t ne, int64_t nq, int sms);
+size_t adjoint_edges_scratch_bytes(const AdjointPlan& p, int64_t le, int64_t nq);
+cudaError_t adjoint_edges(const AdjointPlan& p, const double* edges, int64_t le, int64_t ne,
+                          const double* q, int64_t nq, const double* gw, double* dq,
+                          double* dedge, void* scratch, size_t scratch_bytes,
+                          cudaStream_t stream);
+
+// dV (nv x 3) from per-element corner gradients (rows 3*corner+axis, stride ld) through the
+// vertex -> (corners*element + corner) list (CSR indptr, entries); corners = 3 (faces) or 2
+// (edges).
+cudaError_t gather_vertex_grad(const double* dtri, int64_t ld, int corners,
+                               const int64_t* indptr, const int64_t* entries, int64_t nv,
+                               double* dV, cudaStream_t stream);
 
 }  // namespace wn

@@ -518,10 +518,33 @@ int wn_backward_mixed_device(void* mesh, const double* q, int64_t nq, const doub
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "mixed adjoint launch");
 }
 
-int wn_gather_vertex_grad_device(const double* dtri, int64_t ld, const int64_t* indptr,
-                                 const int64_t* entries, int64_t nv, double* dV, void* stream) {
-  if (nv < 0) return fail(WN_EINVAL, "bad nv=%lld", (long long)nv);
-  cudaError_t e = gather_vertex_grad(dtri, ld, indptr, entries, nv, dV,
+int wn_backward_edges_device(const double* edges, int64_t le, int64_t ne, const double* q,
+                             int64_t nq, const double* gw, double* dq, double* dedge,
+                             void* stream) {
+  if (ne < 0 || nq < 0 || le < ne)
+    return fail(WN_EINVAL, "bad sizes (ne=%lld, nq=%lld, le=%lld)", (long long)ne,
+                (long long)nq, (long long)le);
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const AdjointPlan p = plan_adjoint_edges(ne, nq, c->sms);
+  const size_t sb = adjoint_edges_scratch_bytes(p, le, nq);
+  void* scratch = nullptr;
+  cudaError_t e = cudaMallocAsync(&scratch, sb, st);
+  if (e != cudaSuccess) return cuda_fail(e, "device allocation");
+  e = adjoint_edges(p, edges, le, ne, q, nq, gw, dq, dedge, scratch, sb, st);
+  cudaFreeAsync(scratch, st);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "boundary-edge adjoint launch");
+}
+
+int wn_gather_vertex_grad_device(const double* dtri, int64_t ld, int corners,
+                                 const int64_t* indptr, const int64_t* entries, int64_t nv,
+                                 double* dV, void* stream) {
+  if (nv < 0 || (corners != 2 && corners != 3))
+    return fail(WN_EINVAL, "bad nv=%lld or corners=%d", (long long)nv, corners);
+  cudaError_t e = gather_vertex_grad(dtri, ld, corners, indptr, entries, nv, dV,
                                      static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "vertex gradient gather");
 }

@@ -65,7 +65,8 @@ _WN_SIGNATURES = {
     "wn_forward_mixed_sorted_device": ([P, P, P, I, P, P], C_INT),
     "wn_mixed_stats": ([ctypes.POINTER(I), ctypes.POINTER(I), C_INT], C_INT),
     "wn_backward_fp64_device": ([P, I, I, P, I, P, P, P, P], C_INT),
-    "wn_gather_vertex_grad_device": ([P, I, P, P, I, P, P], C_INT),
+    "wn_gather_vertex_grad_device": ([P, I, C_INT, P, P, I, P, P], C_INT),
+    "wn_backward_edges_device": ([P, I, I, P, I, P, P, P, P], C_INT),
     "wn_backward_mixed_device": ([P, P, I, P, P, P, I, P], C_INT),
 }
 

@@ -1,12 +1,19 @@
 """Differentiable winding number for PyTorch tensors on a CUDA device.
 
 ``winding_number_torch(V, F, O)`` returns W (nq,) and backpropagates dL/dV and
-dL/dO through the library's hand-written adjoint (``wn_backward_fp64_device``):
-pair terms are recomputed (nothing nq x nf is stored), per-face sums over the
-queries and per-query sums over the faces are deterministic, and dL/dV is
-gathered from the per-corner face gradients through a vertex -> (face, corner)
-list in a fixed order. Tensors are plumbing here: the forward and the adjoint
-run in libwn_b200's kernels on the tensors' memory and current stream.
+dL/dO through the library's hand-written adjoints. Pair terms are recomputed
+(nothing nq x nf is stored); every reduction runs in a fixed order.
+
+adjoint="faces": per-face sums over the queries (``wn_backward_fp64_device`` or,
+for precision="mixed", ``wn_backward_mixed_device``), then dL/dV gathered from
+the per-corner face gradients through a vertex -> (face, corner) list.
+adjoint="edges" (default): the same derivative from the mesh's net boundary
+edges only (``wn_backward_edges_device``): the per-face terms of a directed side
+and of its reverse cancel at both endpoints, so interior edges contribute
+nothing (exactly zero for a closed, consistently oriented mesh).
+
+Tensors are plumbing here: the forward and the adjoints run in libwn_b200's
+kernels on the tensors' memory and current stream.
 """
 
 from __future__ import annotations
@@ -107,14 +114,59 @@ def forward_mixed(tri: torch.Tensor, ld: int, nf: int, O: torch.Tensor,
         mesh.close()
 
 
-def gather_vertices(dtri, ld, nf, F, nv):
+def gather_vertices(dtri, ld, nf, F, nv, corners=3):
+    """dL/dV from per-element corner gradients (faces: corners=3; edges: 2)."""
     dV = torch.zeros((nv, 3), dtype=torch.float64, device=dtri.device)
     if nf and nv:
         indptr, entries = vertex_csr(F, nv)
-        _check(_lib.lib().wn_gather_vertex_grad_device(dtri.data_ptr(), ld, indptr.data_ptr(),
-                                                       entries.data_ptr(), nv, dV.data_ptr(),
-                                                       _stream()))
+        _check(_lib.lib().wn_gather_vertex_grad_device(dtri.data_ptr(), ld, corners,
+                                                       indptr.data_ptr(), entries.data_ptr(),
+                                                       nv, dV.data_ptr(), _stream()))
     return dV
+
+
+def boundary_edges(V: torch.Tensor, F: torch.Tensor):
+    """Undirected edges {u < v} with net multiplicity m = #(u->v) - #(v->u) != 0.
+
+    Returns (edges (7, le) float64 SoA: V[u], V[v], m; ne; endpoints (ne, 2) int64).
+    """
+    nv = V.shape[0]
+    e = torch.cat([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]]).to(torch.int64)
+    e = e[e[:, 0] != e[:, 1]]
+    lo = torch.minimum(e[:, 0], e[:, 1])
+    hi = torch.maximum(e[:, 0], e[:, 1])
+    sign = torch.where(e[:, 0] < e[:, 1], 1, -1).to(torch.int64)
+    keys, inverse = torch.unique(lo * nv + hi, return_inverse=True)
+    m = torch.zeros(keys.shape[0], dtype=torch.int64, device=F.device)
+    m.scatter_add_(0, inverse, sign)
+    keep = m != 0
+    keys, m = keys[keep], m[keep]
+    ends = torch.stack([keys // nv, keys % nv], 1)
+    ne = ends.shape[0]
+    le = max(ne, 1)
+    edges = torch.zeros((7, le), dtype=torch.float64, device=V.device)
+    if ne:
+        Vd = V.to(torch.float64)
+        edges[0:3, :ne] = Vd[ends[:, 0]].T
+        edges[3:6, :ne] = Vd[ends[:, 1]].T
+        edges[6, :ne] = m.to(torch.float64)
+    return edges, ne, ends
+
+
+def backward_edges(V, F, O, gW):
+    """(dL/dV, dL/dO) from the net boundary edges (FP64)."""
+    handle = _lib.lib()
+    q = O.to(torch.float64).contiguous()
+    gw = gW.to(torch.float64).contiguous()
+    nq, nv = q.shape[0], V.shape[0]
+    edges, ne, ends = boundary_edges(V, F)
+    le = edges.shape[1]
+    dq = torch.empty((nq, 3), dtype=torch.float64, device=q.device)
+    dedge = torch.zeros((6, le), dtype=torch.float64, device=q.device)
+    _check(handle.wn_backward_edges_device(edges.data_ptr(), le, ne, q.data_ptr(), nq,
+                                           gw.data_ptr(), dq.data_ptr(), dedge.data_ptr(),
+                                           _stream()))
+    return gather_vertices(dedge, le, ne, ends, nv, corners=2), dq
 
 
 def backward_fp64(tri, ld, nf, O, gW, F, nv):
@@ -135,37 +187,45 @@ class WindingNumberFunction(torch.autograd.Function):
     """W = winding_number(V, F, O) with the library's adjoint as backward."""
 
     @staticmethod
-    def forward(ctx, V, F, O, precision="fp64"):
+    def forward(ctx, V, F, O, precision="fp64", adjoint="edges"):
         tri, ld, nf = triangle_soa(V, F)
         ctx.mesh = None
         if precision == "mixed":
-            ctx.mesh = PreparedMesh(tri, ld, nf)
-            w = ctx.mesh.forward(O)
+            mesh = PreparedMesh(tri, ld, nf)
+            w = mesh.forward(O)
+            if adjoint == "faces":
+                ctx.mesh = mesh
+            else:
+                mesh.close()
         else:
             w = forward_fp64(tri, ld, nf, O)
         ctx.save_for_backward(V, F, O)
-        ctx.tri, ctx.ld, ctx.nf = tri, ld, nf
+        ctx.tri, ctx.ld, ctx.nf, ctx.adjoint = tri, ld, nf, adjoint
         return w.to(O.dtype)
 
     @staticmethod
     def backward(ctx, gW):
         V, F, O = ctx.saved_tensors
-        if ctx.mesh is not None:
+        if ctx.adjoint == "edges":
+            dV, dq = backward_edges(V, F, O, gW)
+        elif ctx.mesh is not None:
             dq, dtri = ctx.mesh.backward(O, gW)
             dV = gather_vertices(dtri, ctx.ld, ctx.nf, F, V.shape[0])
             ctx.mesh.close()
         else:
             dV, dq = backward_fp64(ctx.tri, ctx.ld, ctx.nf, O, gW, F, V.shape[0])
-        return dV.to(V.dtype), None, dq.to(O.dtype), None
+        return dV.to(V.dtype), None, dq.to(O.dtype), None, None
 
 
 def winding_number_torch(V: torch.Tensor, F: torch.Tensor, O: torch.Tensor,
-                         precision: str | None = None) -> torch.Tensor:
+                         precision: str | None = None, adjoint: str = "edges") -> torch.Tensor:
     """Differentiable W for CUDA tensors V (nv,3), F (nf,3) int, O (nq,3).
 
     precision: "fp64" (plain FP64 forward and adjoint) or "mixed" (FP32 pairs with
     FP64 refinement of near-surface pairs, forward and adjoint); by default
     "mixed" for float32 queries and "fp64" otherwise. W has the dtype of O.
+    adjoint: "edges" (net boundary edges, FP64) or "faces" (per-face reduction,
+    in the forward's precision); both give the same derivative.
     """
     if precision is None:
         precision = "mixed" if O.dtype == torch.float32 else "fp64"
@@ -173,4 +233,6 @@ def winding_number_torch(V: torch.Tensor, F: torch.Tensor, O: torch.Tensor,
         raise RuntimeError("winding_number_torch needs CUDA tensors (no CPU fallback)")
     if precision not in ("fp64", "mixed"):
         raise ValueError("precision must be 'fp64' or 'mixed'")
-    return WindingNumberFunction.apply(V, F, O, precision)
+    if adjoint not in ("edges", "faces"):
+        raise ValueError("adjoint must be 'edges' or 'faces'")
+    return WindingNumberFunction.apply(V, F, O, precision, adjoint)

@@ -26,7 +26,8 @@ def _cuda(x, dtype=None):
     return t.to(dtype) if dtype is not None else t
 
 
-def test_matches_torch_autograd_fp64(gpu_required, oracle_mod):
+@pytest.mark.parametrize("adjoint", ["faces", "edges"])
+def test_matches_torch_autograd_fp64(gpu_required, oracle_mod, adjoint):
     import torch
 
     V, F = igl.synthetic.bumpy_icosphere(3, seed=11)
@@ -36,7 +37,7 @@ def test_matches_torch_autograd_fp64(gpu_required, oracle_mod):
     Vt = _cuda(V).requires_grad_(True)
     Ot = _cuda(O).requires_grad_(True)
     Ft = _cuda(F)
-    W = wa.winding_number_torch(Vt, Ft, Ot)
+    W = wa.winding_number_torch(Vt, Ft, Ot, adjoint=adjoint)
     (W * _cuda(g)).sum().backward()
     dV, dO = Vt.grad.cpu().numpy(), Ot.grad.cpu().numpy()
 
@@ -51,7 +52,8 @@ def test_matches_torch_autograd_fp64(gpu_required, oracle_mod):
     del torch
 
 
-def test_central_differences_c4(gpu_required):
+@pytest.mark.parametrize("adjoint", ["faces", "edges"])
+def test_central_differences_c4(gpu_required, adjoint):
     import torch
 
     V, F, O, _ = igl.synthetic.workload("c4_grad")
@@ -61,7 +63,7 @@ def test_central_differences_c4(gpu_required):
     Ot = _cuda(O).requires_grad_(True)
     Ft = _cuda(F)
     gt = _cuda(g)
-    W = wa.winding_number_torch(Vt, Ft, Ot)
+    W = wa.winding_number_torch(Vt, Ft, Ot, adjoint=adjoint)
     (W * gt).sum().backward()
     dV, dO = Vt.grad.cpu().numpy(), Ot.grad.cpu().numpy()
 
@@ -104,20 +106,22 @@ def test_central_differences_c4(gpu_required):
     del torch
 
 
-def test_closed_mesh_gradients_cancel(gpu_required):
+@pytest.mark.parametrize("adjoint", ["faces", "edges"])
+def test_closed_mesh_gradients_cancel(gpu_required, adjoint):
     V, F = igl.synthetic.bumpy_icosphere(3, seed=21)
     rng = np.random.default_rng(22)
     O = np.concatenate([rng.uniform(-0.4, 0.4, size=(64, 3)), rng.normal(size=(64, 3)) * 3])
     Vt = _cuda(V).requires_grad_(True)
     Ot = _cuda(O).requires_grad_(True)
-    W = wa.winding_number_torch(Vt, _cuda(F), Ot)
+    W = wa.winding_number_torch(Vt, _cuda(F), Ot, adjoint=adjoint)
     W.sum().backward()
     # Off the surface W of a closed mesh is locally constant: every derivative cancels.
     assert float(Vt.grad.abs().max()) < 1e-9
     assert float(Ot.grad.abs().max()) < 1e-9
 
 
-def test_deterministic_and_finite_on_degenerate_queries(gpu_required):
+@pytest.mark.parametrize("adjoint", ["faces", "edges"])
+def test_deterministic_and_finite_on_degenerate_queries(gpu_required, adjoint):
     V, F = igl.synthetic.bumpy_icosphere(2, seed=31)
     O = np.concatenate([V[:20], 0.5 * (V[F[:20, 0]] + V[F[:20, 1]]),
                         np.random.default_rng(32).normal(size=(200, 3))])
@@ -125,7 +129,7 @@ def test_deterministic_and_finite_on_degenerate_queries(gpu_required):
     for _ in range(2):
         Vt = _cuda(V).requires_grad_(True)
         Ot = _cuda(O).requires_grad_(True)
-        W = wa.winding_number_torch(Vt, _cuda(F), Ot)
+        W = wa.winding_number_torch(Vt, _cuda(F), Ot, adjoint=adjoint)
         (W * _cuda(np.linspace(-1, 1, len(O)))).sum().backward()
         grads.append((Vt.grad.cpu().numpy(), Ot.grad.cpu().numpy()))
     assert np.isfinite(grads[0][0]).all() and np.isfinite(grads[0][1]).all()
@@ -157,7 +161,7 @@ def test_mixed_adjoint_matches_fp64_adjoint(gpu_required, dtype):
         Vt = _cuda(V).requires_grad_(True)
         Ot = _cuda(O, getattr(torch, dtype) if precision == "mixed" else None)
         Ot.requires_grad_(True)
-        W = wa.winding_number_torch(Vt, _cuda(F), Ot, precision=precision)
+        W = wa.winding_number_torch(Vt, _cuda(F), Ot, precision=precision, adjoint="faces")
         (W * _cuda(g, W.dtype)).sum().backward()
         out[precision] = (W.detach().double().cpu().numpy(), Vt.grad.cpu().numpy(),
                           Ot.grad.double().cpu().numpy())
@@ -174,8 +178,30 @@ def test_mixed_adjoint_matches_fp64_adjoint(gpu_required, dtype):
         O32 = O.astype(np.float32).astype(np.float64)
         Vt = _cuda(V).requires_grad_(True)
         Ot = _cuda(O32).requires_grad_(True)
-        W = wa.winding_number_torch(Vt, _cuda(F), Ot, precision="fp64")
+        W = wa.winding_number_torch(Vt, _cuda(F), Ot, precision="fp64", adjoint="faces")
         (W * _cuda(g)).sum().backward()
         assert np.abs(wm - W.detach().cpu().numpy()).max() <= 1e-6
         assert np.abs(dVm - Vt.grad.cpu().numpy()).max() <= 1e-4 * np.abs(dV64).max()
         assert np.abs(dOm - Ot.grad.cpu().numpy()).max() <= 1e-3 * np.abs(dO64).max()
+
+
+def test_edge_and_face_adjoints_agree_on_nonmanifold_soup(gpu_required):
+    """Inconsistent orientation and a non-manifold edge: net multiplicities still telescope."""
+    import torch
+
+    V, F = igl.synthetic.bumpy_icosphere(2, seed=61)
+    F = igl.synthetic.delete_faces(F, 0.1, seed=62).copy()
+    F[:7] = F[:7, [0, 2, 1]]                        # flipped faces
+    F = np.concatenate([F, F[20:23], [[5, 5, 9]]])  # duplicated faces, a degenerate face
+    O = igl.synthetic.mixed_queries(V, F, 1024, seed=63, near_sigma=1e-2)
+    g = np.random.default_rng(64).normal(size=len(O))
+    res = {}
+    for adjoint in ("faces", "edges"):
+        Vt = _cuda(V).requires_grad_(True)
+        Ot = _cuda(O).requires_grad_(True)
+        W = wa.winding_number_torch(Vt, _cuda(F), Ot, adjoint=adjoint)
+        (W * _cuda(g)).sum().backward()
+        res[adjoint] = (Vt.grad.cpu().numpy(), Ot.grad.cpu().numpy())
+    for a, b in zip(res["faces"], res["edges"]):
+        assert np.abs(a - b).max() <= 1e-9 * np.abs(a).max()
+    del torch

@@ -11,7 +11,10 @@ Legs, all on the same inputs:
   * mixed  (headline when built): FP32 pair terms with compensated
     accumulation and FP64 refinement of near-surface pairs;
   * fp64:  the plain FP64 kernel, pair terms bit-identical to the reference;
-  * fwdbwd: forward + hand-written adjoint (when built).
+  * fwdbwd_faces / fwdbwd_edges: mixed forward + the per-face mixed-precision
+    adjoint / the boundary-edge adjoint (both followed by the vertex gather);
+  * c4: the gradient workload (subdivision-5 mesh, 8% faces deleted, 262,144
+    near-surface queries): forward alone and forward + each adjoint.
 `value` is whole-job pairs/s of the headline leg with inputs resident in HBM;
 `e2e` is the same leg through the C ABI with pinned host buffers, the
 host->device copies, device preprocessing and device->host copy inside the
@@ -61,6 +64,7 @@ def parse_args():
     p.add_argument("--legs", default="auto", help="comma list of mixed,fp64,fwdbwd")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-c4", action="store_true", help="skip the gradient workload")
     return p.parse_args()
 
 
@@ -262,7 +266,30 @@ def gpu_arm(args):
         kernel_timed(lambda: check(handle.wn_forward_mixed_sorted_device(
             mesh, q_d.data_ptr(), perm_d.data_ptr(), nq, wm_d.data_ptr(), sp)))
 
-    legs = {"mixed": mixed_step, "fp64": fp64_step}
+    # Forward + backward on the same batch, dL/dW ~ N(0, 1). "faces": the
+    # per-face mixed-precision adjoint over the prepared mesh (queries re-sorted
+    # inside), then the vertex gather. "edges": the boundary-edge adjoint (edge
+    # list rebuilt from F inside the step), then the vertex gather.
+    from igl import autograd as wa
+
+    V_d = torch.from_numpy(V).to(dev)
+    F_d = torch.from_numpy(F).to(dev)
+    gw_d = torch.from_numpy(np.random.default_rng(7 + rank).normal(size=nq)).to(dev)
+    dq_d = torch.empty((nq, 3), dtype=torch.float64, device=dev)
+    dtri_d = torch.zeros_like(tri_d)
+
+    def fwdbwd_faces_step():
+        mixed_step()
+        check(handle.wn_backward_mixed_device(mesh, q_d.data_ptr(), nq, gw_d.data_ptr(),
+                                              dq_d.data_ptr(), dtri_d.data_ptr(), ld, sp))
+        wa.gather_vertices(dtri_d, ld, nf, F_d, len(V))
+
+    def fwdbwd_edges_step():
+        mixed_step()
+        wa.backward_edges(V_d, F_d, q_d, gw_d)
+
+    legs = {"mixed": mixed_step, "fp64": fp64_step, "fwdbwd_faces": fwdbwd_faces_step,
+            "fwdbwd_edges": fwdbwd_edges_step}
     headline = "mixed"
     wanted = list(legs) if args.legs == "auto" else args.legs.split(",")
     if headline not in wanted:
@@ -319,6 +346,49 @@ def gpu_arm(args):
 
     t_step, launches, t_kernel = results[headline]
     value = world * pairs / t_step
+    fwdbwd = {}
+    for name in ("fwdbwd_faces", "fwdbwd_edges"):
+        if name in results:
+            fwdbwd[name.split("_")[1]] = {
+                "ms_per_step": results[name][0] * 1e3,
+                "pairs_per_s": world * pairs / results[name][0],
+                "ratio_to_forward": results[name][0] / t_step,
+            }
+
+    # Gradient workload: subdivision-5 mesh with 8% faces deleted (open), 262,144
+    # near-surface queries: mixed forward alone vs forward + each adjoint.
+    c4 = None
+    if not args.no_c4:
+        from igl import synthetic
+
+        V4, F4, O4, desc4 = synthetic.workload("c4_grad")
+        V4d, F4d = torch.from_numpy(V4).to(dev), torch.from_numpy(F4).to(dev)
+        O4d = torch.from_numpy(O4).to(dev)
+        g4d = torch.from_numpy(np.random.default_rng(47).normal(size=len(O4))).to(dev)
+        tri4, ld4, nf4 = wa.triangle_soa(V4d, F4d)
+        mesh4 = wa.PreparedMesh(tri4, ld4, nf4)
+
+        def c4_fwd():
+            check(handle.wn_mixed_mesh_update(mesh4.mesh, tri4.data_ptr(), ld4, sp))
+            mesh4.forward(O4d)
+
+        def c4_faces():
+            c4_fwd()
+            dq4, dt4 = mesh4.backward(O4d, g4d)
+            wa.gather_vertices(dt4, ld4, nf4, F4d, len(V4))
+
+        def c4_edges():
+            c4_fwd()
+            wa.backward_edges(V4d, F4d, O4d, g4d)
+
+        t4 = {k: timed(fn, args.steps, 2)[0] for k, fn in
+              (("fwd", c4_fwd), ("faces", c4_faces), ("edges", c4_edges))}
+        pairs4 = float(nf4) * len(O4)
+        c4 = {"workload": desc4, "pairs": pairs4,
+              "fwd_ms": t4["fwd"] * 1e3,
+              "fwdbwd_faces_ms": t4["faces"] * 1e3, "fwdbwd_edges_ms": t4["edges"] * 1e3,
+              "ratio_faces": t4["faces"] / t4["fwd"], "ratio_edges": t4["edges"] / t4["fwd"]}
+        mesh4.close()
 
     # Accuracy of the mixed leg against the FP64 kernel on every query.
     accuracy = None
@@ -417,6 +487,8 @@ def gpu_arm(args):
                          "kernel_ms": v[2] * 1e3} for k, v in results.items()},
             "mixed_over_fp64": (results["fp64"][0] / results["mixed"][0]
                                 if "mixed" in results and "fp64" in results else None),
+            "fwd_bwd": fwdbwd,
+            "c4_fwd_bwd": c4,
             "accuracy": accuracy,
             "refinement": ({"pairs_refined_fp64_per_step": headline_refined,
                             "fraction": headline_refined / pairs}

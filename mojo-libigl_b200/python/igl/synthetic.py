@@ -106,7 +106,8 @@ def near_surface_points(V, F, n: int, seed: int, sigma: float) -> np.ndarray:
     tri = V[F[fi]]
     p = tri[:, 0] + u[:, :1] * (tri[:, 1] - tri[:, 0]) + u[:, 1:] * (tri[:, 2] - tri[:, 0])
     nrm = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
-    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    length = np.linalg.norm(nrm, axis=1, keepdims=True)
+    nrm = np.where(length > 0, nrm / np.where(length > 0, length, 1.0), 0.0)  # zero-area: no offset
     return p + nrm * rng.normal(0.0, sigma, size=(n, 1))
 
 

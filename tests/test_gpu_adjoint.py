@@ -192,8 +192,8 @@ def test_edge_and_face_adjoints_agree_on_nonmanifold_soup(gpu_required):
     V, F = igl.synthetic.bumpy_icosphere(2, seed=61)
     F = igl.synthetic.delete_faces(F, 0.1, seed=62).copy()
     F[:7] = F[:7, [0, 2, 1]]                        # flipped faces
-    F = np.concatenate([F, F[20:23], [[5, 5, 9]]])  # duplicated faces, a degenerate face
     O = igl.synthetic.mixed_queries(V, F, 1024, seed=63, near_sigma=1e-2)
+    F = np.concatenate([F, F[20:23], [[5, 5, 9]]])  # duplicated faces, a degenerate face
     g = np.random.default_rng(64).normal(size=len(O))
     res = {}
     for adjoint in ("faces", "edges"):

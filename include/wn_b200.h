@@ -132,6 +132,31 @@ int wn_forward_mixed_sorted_device(void* mesh, const double* q, const uint32_t* 
  * pairs refined in FP64, and (warp, tile) visits that ran the near test. */
 int wn_mixed_stats(int64_t* refined_pairs, int64_t* careful_visits, int reset);
 
+/* ---- batched meshes (no reference counterpart) ---------------------------
+ * Many indexed meshes with their own query sets, of uneven sizes, evaluated by
+ * one persistent launch (mixed precision). Create once per set of sizes and
+ * faces; forward is asynchronous, allocation-free and synchronisation-free, so
+ * a sequence of forwards can be captured in a CUDA graph.
+ *   nv/nf/nq: host arrays of nmesh sizes; faces: host, total_nf x 3 int64,
+ *   vertex indices local to each mesh (meshes concatenated in order).
+ *   qpt: queries per thread (1, 2 or 4); target_pairs: pairs per work item;
+ *   ctas_per_sm: persistent CTAs per SM (0 = as many as fit).
+ *   V (total_nv x 3), q (total_nq x 3), w (total_nq): device, concatenated. */
+int wn_batch_create(int64_t nmesh, const int64_t* nv, const int64_t* nf, const int64_t* nq,
+                    const int64_t* faces, double kappa, int qpt, int64_t target_pairs,
+                    int ctas_per_sm, void** batch_out);
+int wn_batch_forward(void* batch, const double* V, const double* q, double* w, void* stream);
+/* Adjoint of every mesh through its net boundary edges (FP64, persistent,
+ * deterministic): gw (total_nq) -> dq (total_nq x 3), dV (total_nv x 3). Same
+ * launch properties as wn_batch_forward. */
+int wn_batch_backward(void* batch, const double* V, const double* q, const double* gw,
+                      double* dq, double* dV, void* stream);
+/* out[0..n): nmesh, total_nv, total_nf, total_nq, total_tiles, work items,
+ * persistent grid, partial sums, qpt, target_pairs, boundary edges, adjoint
+ * work items. */
+int wn_batch_info(void* batch, int64_t* out, int64_t n);
+int wn_batch_destroy(void* batch);
+
 /* ---- adjoint (no reference counterpart) ---------------------------------
  * gw: dL/dW per query (nq). Outputs dq (nq x 3) = dL/do and dtri (9 rows of
  * stride ld, the soup's layout) = dL/d(corner) per face; every pair term is

@@ -26,8 +26,10 @@
 // touches. After the last chunk a block's face sums go to dF_part[g][corner][face]. Two
 // finishing kernels add the partials over r and over g in index order.
 #include <algorithm>
+#include <vector>
 
 #include "wn_adjoint.h"
+#include "wn_batch.h"
 #include "wn_common.cuh"
 #include "wn_internal.h"
 #include "wn_mixed.h"
@@ -750,6 +752,365 @@ cudaError_t gather_vertex_grad(const double* dtri, int64_t ld, int corners,
   gather_vertex_kernel<<<static_cast<unsigned>(cdiv(nv, 256)), 256, 0, stream>>>(
       dtri, ld, corners, indptr, entries, nv, dV);
   g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+
+// ---- batched boundary-edge adjoint ------------------------------------------
+// Every mesh's net boundary edges (computed once from the faces on the host)
+// are concatenated; work items (mesh, range of edges, group of queries) are
+// taken from an atomic counter by a persistent grid. An item owns one row of
+// the mesh's per-range dL/do partials and one row of its per-group edge
+// partials, so the schedule is dynamic but every sum is in a fixed order.
+struct BatchEdgeItem {
+  int64_t e_begin, e_end;  // global edge indices
+  int64_t q_begin, q_end;  // global query indices
+  int64_t do_row;          // dO_part offset of this item's row, in doubles, minus 3*q_off
+  int64_t de_row;          // dE_part offset of this item's group, in doubles, minus e_off
+  int64_t ne;              // edges in the mesh (row stride of the group block)
+};
+
+struct BatchEdgeMesh {
+  int64_t e_off, ne, q_off, nq, nranges, ngroups, do_off, de_off;
+};
+
+struct BatchEdges {
+  int64_t ne_total = 0, le = 1, n_items = 0, do_doubles = 0, de_doubles = 0;
+  int grid = 0;
+  int64_t* ends = nullptr;      // ne_total x 2, global vertex indices
+  double* mult = nullptr;       // ne_total
+  double* edges = nullptr;      // 7 x le SoA (positions filled per call)
+  double* dedge = nullptr;      // 6 x le
+  int64_t* indptr = nullptr;    // total_nv + 1
+  int64_t* entries = nullptr;   // 2 * ne_total
+  BatchEdgeItem* items = nullptr;
+  BatchEdgeMesh* meshes = nullptr;
+  int32_t* query_mesh = nullptr;  // total_nq
+  int32_t* edge_mesh = nullptr;   // ne_total
+  unsigned int* counter = nullptr;
+  double* dO_part = nullptr;
+  double* dE_part = nullptr;
+};
+
+namespace {
+
+constexpr int64_t kBatchEdgeRange = 2048;   // edges per item
+constexpr int64_t kBatchQueryGroup = 2048;  // queries per item
+
+__global__ void batch_edge_positions_kernel(const double* __restrict__ V,
+                                            const int64_t* __restrict__ ends,
+                                            const double* __restrict__ mult, int64_t ne,
+                                            int64_t le, double* __restrict__ edges) {
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const int64_t u = ends[2 * e], v = ends[2 * e + 1];
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    edges[x * le + e] = V[3 * u + x];
+    edges[(3 + x) * le + e] = V[3 * v + x];
+  }
+  edges[6 * le + e] = mult[e];
+}
+
+struct BatchEdgeArgs {
+  const double* edges;
+  int64_t le;
+  const double* q;
+  const double* gw;
+  const BatchEdgeItem* items;
+  int64_t n_items;
+  unsigned int* counter;
+  double* dO_part;
+  double* dE_part;
+};
+
+template <int THREADS, int EPT, int QC>
+__global__ void __launch_bounds__(THREADS, 2) batch_edges_kernel(const BatchEdgeArgs a) {
+  __shared__ double sq[QC][4];
+  __shared__ double red[THREADS / 32][QC][3];
+  __shared__ int64_t s_item;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int kBlockEdges = THREADS * EPT;
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) s_item = static_cast<int64_t>(atomicAdd(a.counter, 1u));
+    __syncthreads();
+    const int64_t item = s_item;
+    if (item >= a.n_items) break;
+    const BatchEdgeItem it = a.items[item];
+    for (int64_t b0 = it.e_begin; b0 < it.e_end; b0 += kBlockEdges) {
+      double ev[EPT][7], acc[EPT][6];
+#pragma unroll
+      for (int k = 0; k < EPT; ++k) {
+        const int64_t e = b0 + k * THREADS + tid;
+        const bool valid = e < it.e_end;
+#pragma unroll
+        for (int r = 0; r < 7; ++r) ev[k][r] = valid ? a.edges[r * a.le + e] : 0.0;
+#pragma unroll
+        for (int r = 0; r < 6; ++r) acc[k][r] = 0.0;
+      }
+      for (int64_t c0 = it.q_begin; c0 < it.q_end; c0 += QC) {
+        const int nc = static_cast<int>(it.q_end - c0 < QC ? it.q_end - c0 : QC);
+        __syncthreads();
+        if (tid < nc) {
+          const int64_t qi = c0 + tid;
+          sq[tid][0] = a.q[3 * qi];
+          sq[tid][1] = a.q[3 * qi + 1];
+          sq[tid][2] = a.q[3 * qi + 2];
+          sq[tid][3] = a.gw[qi];
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int j = 0; j < nc; ++j) {
+          const double ox = sq[j][0], oy = sq[j][1], oz = sq[j][2], g = sq[j][3];
+          double dox = 0.0, doy = 0.0, doz = 0.0;
+#pragma unroll
+          for (int k = 0; k < EPT; ++k) {
+            const double px = ev[k][0] - ox, py = ev[k][1] - oy, pz = ev[k][2] - oz;
+            const double qx = ev[k][3] - ox, qy = ev[k][4] - oy, qz = ev[k][5] - oz;
+            const double pp = px * px + py * py + pz * pz;
+            const double qq = qx * qx + qy * qy + qz * qz;
+            const double rp = rsqrt(pp), rq = rsqrt(qq);
+            const double rpq = rp * rq;
+            const double d = 1.0 + (px * qx + py * qy + pz * qz) * rpq;
+            const bool ok = ev[k][6] != 0.0 && pp > 0.0 && qq > 0.0 && d > 0.0;
+            const double w = ok ? g * ev[k][6] * rpq / d : 0.0;
+            const double cp = ok ? rp * w : 0.0, cq = ok ? rq * w : 0.0;
+            const double x0 = py * qz - pz * qy, x1 = pz * qx - px * qz, x2 = px * qy - py * qx;
+            acc[k][0] -= cp * x0;
+            acc[k][1] -= cp * x1;
+            acc[k][2] -= cp * x2;
+            acc[k][3] -= cq * x0;
+            acc[k][4] -= cq * x1;
+            acc[k][5] -= cq * x2;
+            const double c = cp + cq;
+            dox += c * x0;
+            doy += c * x1;
+            doz += c * x2;
+          }
+          for (int off = 16; off; off >>= 1) {
+            dox += __shfl_xor_sync(0xffffffffu, dox, off);
+            doy += __shfl_xor_sync(0xffffffffu, doy, off);
+            doz += __shfl_xor_sync(0xffffffffu, doz, off);
+          }
+          if (lane == 0) {
+            red[warp][j][0] = dox;
+            red[warp][j][1] = doy;
+            red[warp][j][2] = doz;
+          }
+        }
+        __syncthreads();
+        for (int e = tid; e < nc * 3; e += THREADS) {
+          const int j = e / 3, x = e % 3;
+          double sum = 0.0;
+#pragma unroll
+          for (int w = 0; w < THREADS / 32; ++w) sum += red[w][j][x];
+          a.dO_part[it.do_row + (c0 + j) * 3 + x] += sum;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < EPT; ++k) {
+        const int64_t e = b0 + k * THREADS + tid;
+        if (e >= it.e_end) continue;
+#pragma unroll
+        for (int r = 0; r < 6; ++r) a.dE_part[it.de_row + r * it.ne + e] = acc[k][r];
+      }
+    }
+  }
+}
+
+__global__ void batch_finish_dq_kernel(const double* __restrict__ dO_part,
+                                       const BatchEdgeMesh* __restrict__ meshes,
+                                       const int32_t* __restrict__ query_mesh, int64_t total_nq,
+                                       double* __restrict__ dq) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= total_nq * 3) return;
+  const int64_t qi = i / 3, x = i % 3;
+  const BatchEdgeMesh mm = meshes[query_mesh[qi]];
+  double s = 0.0;
+  for (int64_t r = 0; r < mm.nranges; ++r)
+    s += dO_part[mm.do_off + (r * mm.nq + (qi - mm.q_off)) * 3 + x];
+  dq[i] = s * kInv4Pi;
+}
+
+__global__ void batch_finish_dedge_kernel(const double* __restrict__ dE_part,
+                                          const BatchEdgeMesh* __restrict__ meshes,
+                                          const int32_t* __restrict__ edge_mesh, int64_t ne_total,
+                                          int64_t le, double* __restrict__ dedge) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= ne_total * 6) return;
+  const int64_t e = i / 6, r = i % 6;
+  const BatchEdgeMesh mm = meshes[edge_mesh[e]];
+  double s = 0.0;
+  for (int64_t g = 0; g < mm.ngroups; ++g)
+    s += dE_part[mm.de_off + (g * 6 + r) * mm.ne + (e - mm.e_off)];
+  dedge[r * le + e] = s * kInv4Pi;
+}
+
+}  // namespace
+
+cudaError_t batch_edges_create(BatchState* b, const int64_t* F) {
+  BatchEdges* E = new BatchEdges();
+  b->edges = E;
+  std::vector<int64_t> ends;
+  std::vector<double> mult;
+  std::vector<BatchEdgeMesh> meshes(b->nmesh);
+  std::vector<int32_t> edge_mesh;
+  for (int64_t m = 0; m < b->nmesh; ++m) {
+    // Net multiplicity of every undirected edge {u < v}: +1 per u -> v, -1 per v -> u.
+    std::vector<std::pair<int64_t, int>> keyed;
+    keyed.reserve(3 * b->nf[m]);
+    const int64_t nvm = std::max<int64_t>(b->nv[m], 1);
+    for (int64_t f = b->f_off[m]; f < b->f_off[m + 1]; ++f)
+      for (int c = 0; c < 3; ++c) {
+        const int64_t u = F[3 * f + c], v = F[3 * f + (c + 1) % 3];
+        if (u == v) continue;
+        keyed.emplace_back(std::min(u, v) * nvm + std::max(u, v), u < v ? 1 : -1);
+      }
+    std::sort(keyed.begin(), keyed.end());
+    const int64_t e_off = static_cast<int64_t>(mult.size());
+    for (size_t i = 0; i < keyed.size();) {
+      size_t j = i;
+      int net = 0;
+      for (; j < keyed.size() && keyed[j].first == keyed[i].first; ++j) net += keyed[j].second;
+      if (net != 0) {
+        ends.push_back(keyed[i].first / nvm + b->v_off[m]);
+        ends.push_back(keyed[i].first % nvm + b->v_off[m]);
+        mult.push_back(static_cast<double>(net));
+        edge_mesh.push_back(static_cast<int32_t>(m));
+      }
+      i = j;
+    }
+    BatchEdgeMesh& mm = meshes[m];
+    mm.e_off = e_off;
+    mm.ne = static_cast<int64_t>(mult.size()) - e_off;
+    mm.q_off = b->q_off[m];
+    mm.nq = b->nq[m];
+    mm.nranges = mm.ne > 0 ? (mm.ne + kBatchEdgeRange - 1) / kBatchEdgeRange : 0;
+    mm.ngroups = mm.nq > 0 ? (mm.nq + kBatchQueryGroup - 1) / kBatchQueryGroup : 0;
+  }
+  E->ne_total = static_cast<int64_t>(mult.size());
+  E->le = std::max<int64_t>(E->ne_total, 1);
+  std::vector<BatchEdgeItem> items;
+  int64_t do_off = 0, de_off = 0;
+  for (int64_t m = 0; m < b->nmesh; ++m) {
+    BatchEdgeMesh& mm = meshes[m];
+    mm.do_off = do_off;
+    mm.de_off = de_off;
+    if (mm.ne > 0 && mm.nq > 0) {
+      for (int64_t r = 0; r < mm.nranges; ++r)
+        for (int64_t g = 0; g < mm.ngroups; ++g) {
+          BatchEdgeItem it;
+          it.e_begin = mm.e_off + r * kBatchEdgeRange;
+          it.e_end = std::min(mm.e_off + mm.ne, it.e_begin + kBatchEdgeRange);
+          it.q_begin = mm.q_off + g * kBatchQueryGroup;
+          it.q_end = std::min(mm.q_off + mm.nq, it.q_begin + kBatchQueryGroup);
+          it.do_row = do_off + r * mm.nq * 3 - 3 * mm.q_off;
+          it.de_row = de_off + g * 6 * mm.ne - mm.e_off;
+          it.ne = mm.ne;
+          items.push_back(it);
+        }
+      do_off += mm.nranges * mm.nq * 3;
+      de_off += mm.ngroups * 6 * mm.ne;
+    }
+  }
+  std::stable_sort(items.begin(), items.end(), [](const BatchEdgeItem& x, const BatchEdgeItem& y) {
+    return (x.e_end - x.e_begin) * (x.q_end - x.q_begin) >
+           (y.e_end - y.e_begin) * (y.q_end - y.q_begin);
+  });
+  E->n_items = static_cast<int64_t>(items.size());
+  E->do_doubles = do_off;
+  E->de_doubles = de_off;
+  // Vertex -> (2*edge + end) list, grouped by global vertex id.
+  std::vector<int64_t> indptr(b->total_nv + 1, 0), entries(ends.size());
+  for (int64_t v : ends) ++indptr[v + 1];
+  for (int64_t v = 0; v < b->total_nv; ++v) indptr[v + 1] += indptr[v];
+  {
+    std::vector<int64_t> fill(indptr.begin(), indptr.end() - 1);
+    for (size_t i = 0; i < ends.size(); ++i) entries[fill[ends[i]]++] = static_cast<int64_t>(i);
+  }
+  std::vector<int32_t> query_mesh(std::max<int64_t>(b->total_nq, 1));
+  for (int64_t m = 0; m < b->nmesh; ++m)
+    for (int64_t i = b->q_off[m]; i < b->q_off[m + 1]; ++i) query_mesh[i] = static_cast<int32_t>(m);
+
+  auto up = [](auto** dst, const auto& src, size_t min_count) -> cudaError_t {
+    using T = typename std::remove_reference<decltype(src)>::type::value_type;
+    const size_t n = std::max(src.size(), min_count);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(dst), sizeof(T) * std::max<size_t>(n, 1));
+    if (e == cudaSuccess && !src.empty())
+      e = cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice);
+    return e;
+  };
+  cudaError_t e;
+  if ((e = up(&E->ends, ends, 2)) != cudaSuccess || (e = up(&E->mult, mult, 1)) != cudaSuccess ||
+      (e = up(&E->indptr, indptr, 1)) != cudaSuccess ||
+      (e = up(&E->entries, entries, 1)) != cudaSuccess ||
+      (e = up(&E->items, items, 1)) != cudaSuccess ||
+      (e = up(&E->meshes, meshes, 1)) != cudaSuccess ||
+      (e = up(&E->query_mesh, query_mesh, 1)) != cudaSuccess ||
+      (e = up(&E->edge_mesh, edge_mesh, 1)) != cudaSuccess ||
+      (e = cudaMalloc(reinterpret_cast<void**>(&E->edges), sizeof(double) * 7 * E->le)) !=
+          cudaSuccess ||
+      (e = cudaMalloc(reinterpret_cast<void**>(&E->dedge), sizeof(double) * 6 * E->le)) !=
+          cudaSuccess ||
+      (e = cudaMalloc(reinterpret_cast<void**>(&E->counter), sizeof(unsigned int))) !=
+          cudaSuccess ||
+      (e = cudaMalloc(reinterpret_cast<void**>(&E->dO_part),
+                      sizeof(double) * std::max<int64_t>(E->do_doubles, 1))) != cudaSuccess ||
+      (e = cudaMalloc(reinterpret_cast<void**>(&E->dE_part),
+                      sizeof(double) * std::max<int64_t>(E->de_doubles, 1))) != cudaSuccess)
+    return e;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, batch_edges_kernel<kAdjThreads, kAdjFpt, kAdjQc>, kAdjThreads, 0);
+  E->grid = static_cast<int>(
+      std::min<int64_t>(std::max(1, per_sm) * std::max(1, b->sms), std::max<int64_t>(E->n_items, 1)));
+  return cudaGetLastError();
+}
+
+int64_t batch_boundary_edges(const BatchState* b) { return b->edges ? b->edges->ne_total : 0; }
+int64_t batch_edge_items(const BatchState* b) { return b->edges ? b->edges->n_items : 0; }
+
+void batch_edges_destroy(BatchState* b) {
+  BatchEdges* E = b->edges;
+  if (!E) return;
+  void* ptrs[] = {E->ends,   E->mult,       E->edges,     E->dedge,   E->indptr,
+                  E->entries, E->items,     E->meshes,    E->query_mesh, E->edge_mesh,
+                  E->counter, E->dO_part,   E->dE_part};
+  for (void* p : ptrs) cudaFree(p);
+  delete E;
+  b->edges = nullptr;
+}
+
+cudaError_t batch_backward(BatchState* b, const double* V, const double* q, const double* gw,
+                           double* dq, double* dV, cudaStream_t stream) {
+  BatchEdges* E = b->edges;
+  if (!E) return cudaErrorInvalidValue;
+  cudaError_t e;
+  if (b->total_nq > 0 &&
+      (e = cudaMemsetAsync(dq, 0, sizeof(double) * 3 * b->total_nq, stream)) != cudaSuccess)
+    return e;
+  if (b->total_nv > 0 &&
+      (e = cudaMemsetAsync(dV, 0, sizeof(double) * 3 * b->total_nv, stream)) != cudaSuccess)
+    return e;
+  if (E->ne_total == 0 || b->total_nq == 0) return cudaSuccess;
+  batch_edge_positions_kernel<<<static_cast<unsigned>(cdiv(E->ne_total, 256)), 256, 0, stream>>>(
+      V, E->ends, E->mult, E->ne_total, E->le, E->edges);
+  if ((e = cudaMemsetAsync(E->dO_part, 0, sizeof(double) * std::max<int64_t>(E->do_doubles, 1),
+                           stream)) != cudaSuccess ||
+      (e = cudaMemsetAsync(E->counter, 0, sizeof(unsigned int), stream)) != cudaSuccess)
+    return e;
+  BatchEdgeArgs a{E->edges, E->le, q, gw, E->items, E->n_items, E->counter, E->dO_part,
+                  E->dE_part};
+  if (E->n_items > 0)
+    batch_edges_kernel<kAdjThreads, kAdjFpt, kAdjQc><<<E->grid, kAdjThreads, 0, stream>>>(a);
+  batch_finish_dq_kernel<<<static_cast<unsigned>(cdiv(3 * b->total_nq, 256)), 256, 0, stream>>>(
+      E->dO_part, E->meshes, E->query_mesh, b->total_nq, dq);
+  batch_finish_dedge_kernel<<<static_cast<unsigned>(cdiv(6 * E->ne_total, 256)), 256, 0,
+                              stream>>>(E->dE_part, E->meshes, E->edge_mesh, E->ne_total, E->le,
+                                        E->dedge);
+  gather_vertex_kernel<<<static_cast<unsigned>(cdiv(b->total_nv, 256)), 256, 0, stream>>>(
+      E->dedge, E->le, 2, E->indptr, E->entries, b->total_nv, dV);
+  g_launches.fetch_add(5, std::memory_order_relaxed);
   return cudaGetLastError();
 }
 

@@ -17,6 +17,7 @@
 
 #include "../../include/wn_b200.h"
 #include "wn_adjoint.h"
+#include "wn_batch.h"
 #include "wn_internal.h"
 #include "wn_mixed.h"
 
@@ -547,6 +548,101 @@ int wn_gather_vertex_grad_device(const double* dtri, int64_t ld, int corners,
   cudaError_t e = gather_vertex_grad(dtri, ld, corners, indptr, entries, nv, dV,
                                      static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "vertex gradient gather");
+}
+
+int wn_batch_create(int64_t nmesh, const int64_t* nv, const int64_t* nf, const int64_t* nq,
+                    const int64_t* faces, double kappa, int qpt, int64_t target_pairs,
+                    int ctas_per_sm, void** batch_out) {
+  if (!batch_out) return fail(WN_EINVAL, "null batch_out");
+  *batch_out = nullptr;
+  if (nmesh <= 0 || nmesh > (1 << 20) || !nv || !nf || !nq)
+    return fail(WN_EINVAL, "bad mesh count %lld or null size arrays", (long long)nmesh);
+  int64_t tf = 0, tq = 0, tv = 0;
+  for (int64_t m = 0; m < nmesh; ++m) {
+    if (nv[m] < 0 || nf[m] < 0 || nq[m] < 0) return fail(WN_EINVAL, "negative size in mesh %lld",
+                                                         (long long)m);
+    tv += nv[m];
+    tf += nf[m];
+    tq += nq[m];
+  }
+  if (tf > 0x7fffffffLL || tq > 0x7fffffffLL) return fail(WN_EINVAL, "more than 2^31-1 items");
+  if (tf > 0 && !faces) return fail(WN_EINVAL, "null faces");
+  for (int64_t m = 0, f0 = 0; m < nmesh; f0 += nf[m], ++m)
+    for (int64_t i = 3 * f0; i < 3 * (f0 + nf[m]); ++i)
+      if (faces[i] < 0 || faces[i] >= nv[m])
+        return fail(WN_EINVAL, "face index %lld outside mesh %lld's %lld vertices",
+                    (long long)faces[i], (long long)m, (long long)nv[m]);
+  if (int code = check_kappa(kappa)) return code;
+  if (qpt != 1 && qpt != 2 && qpt != 4) return fail(WN_EINVAL, "qpt must be 1, 2 or 4");
+  if (target_pairs < 1) return fail(WN_EINVAL, "target_pairs must be positive");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  BatchPlan plan;
+  plan.qpt = qpt;
+  plan.kappa = kappa;
+  plan.target_pairs = target_pairs;
+  plan.ctas_per_sm = ctas_per_sm;
+  BatchState* b = new BatchState();
+  cudaError_t e = batch_create(b, nmesh, nv, nf, nq, faces, plan, c->sms);
+  if (e == cudaSuccess) e = batch_edges_create(b, faces);
+  if (e != cudaSuccess) {
+    batch_edges_destroy(b);
+    batch_destroy(b);
+    delete b;
+    return cuda_fail(e, "batch setup");
+  }
+  *batch_out = b;
+  return WN_OK;
+}
+
+int wn_batch_forward(void* batch, const double* V, const double* q, double* w, void* stream) {
+  if (!batch) return fail(WN_EINVAL, "null batch");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  cudaError_t e = batch_forward(static_cast<BatchState*>(batch), V, q, w, c->stats, c->err,
+                                static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "batched forward launch");
+}
+
+int wn_batch_backward(void* batch, const double* V, const double* q, const double* gw,
+                      double* dq, double* dV, void* stream) {
+  if (!batch) return fail(WN_EINVAL, "null batch");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  if (!context(&code)) return code;
+  cudaError_t e = batch_backward(static_cast<BatchState*>(batch), V, q, gw, dq, dV,
+                                 static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "batched adjoint launch");
+}
+
+int wn_batch_info(void* batch, int64_t* out, int64_t n) {
+  if (!batch || !out) return fail(WN_EINVAL, "null argument");
+  const BatchState* b = static_cast<const BatchState*>(batch);
+  const int64_t vals[] = {b->nmesh,       b->total_nv,    b->total_nf, b->total_nq,
+                          b->total_tiles, b->n_items,     b->grid,     b->total_partials,
+                          b->plan.qpt,    b->plan.target_pairs,
+                          batch_boundary_edges(b), batch_edge_items(b)};
+  for (int64_t i = 0; i < n && i < static_cast<int64_t>(sizeof(vals) / sizeof(vals[0])); ++i)
+    out[i] = vals[i];
+  return WN_OK;
+}
+
+int wn_batch_destroy(void* batch) {
+  if (!batch) return WN_OK;
+  BatchState* b = static_cast<BatchState*>(batch);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(b->device);
+  cudaDeviceSynchronize();
+  batch_edges_destroy(b);
+  batch_destroy(b);
+  cudaSetDevice(prev);
+  delete b;
+  return WN_OK;
 }
 
 // src/capi.mojo:945-947: 1 on success, 0 on failure (the shim raises).

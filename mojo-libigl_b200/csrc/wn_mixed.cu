@@ -40,7 +40,10 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <numeric>
+#include <vector>
 
+#include "wn_batch.h"
 #include "wn_common.cuh"
 #include "wn_internal.h"
 #include "wn_mixed.h"
@@ -154,17 +157,29 @@ __device__ __forceinline__ double warp_min(double v) {
 
 // One CTA of kTileFaces threads per tile: gathers the tile's faces in Morton
 // order, writes the FP64 sorted copy, the tile header and the FP32 records.
+// Tile t holds the sorted faces order[first + j], j < count, where first/count
+// come from tile_first/tile_count (several meshes, each tiled on its own) or,
+// when those are null, first = 64 t and count = min(64, nf - first).
 __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
     const double* __restrict__ tri, int64_t ld, int64_t nf, const uint32_t* __restrict__ order,
     double kappa, unsigned char* __restrict__ tiles, double* __restrict__ tri64, int64_t ld64,
-    uint32_t* __restrict__ face_of) {
+    uint32_t* __restrict__ face_of, const int64_t* __restrict__ tile_first,
+    const int32_t* __restrict__ tile_count) {
   __shared__ double red[6][kTileFaces / 32];
   const int j = threadIdx.x, warp = j >> 5, lane = j & 31;
   const int64_t tile = blockIdx.x;
+  const int64_t first = tile_first ? tile_first[tile] : tile * kTileFaces;
+  int cnt = kTileFaces;
+  if (tile_count) {
+    cnt = tile_count[tile];
+  } else {
+    const int64_t left = nf - first;
+    cnt = static_cast<int>(left < kTileFaces ? (left > 0 ? left : 0) : kTileFaces);
+  }
   const int64_t slot = tile * kTileFaces + j;
-  const bool valid = slot < nf;
+  const bool valid = j < cnt;
   double v[9];
-  const int64_t f = valid ? order[slot] : 0;
+  const int64_t f = valid ? order[first + j] : 0;
 #pragma unroll
   for (int r = 0; r < 9; ++r) v[r] = valid ? tri[r * ld + f] : 0.0;
 #pragma unroll
@@ -240,10 +255,7 @@ __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
     const double far = rt + kappa * ht;
     th->far_r2 = far * far;
     th->scale = scale;
-    {
-      const int64_t left = nf - tile * kTileFaces;
-      th->n = static_cast<int32_t>(left < kTileFaces ? (left > 0 ? left : 0) : kTileFaces);
-    }
+    th->n = cnt;
     th->first = 0;
     th->r = static_cast<float>(rt);
     th->h = static_cast<float>(ht);
@@ -288,6 +300,122 @@ struct MixedArgs {
   unsigned long long* stats;  // [0] refined pairs, [1] careful (query-warp, tile) visits
   int* err;
 };
+
+// One 64-face tile against the QPT queries of this thread: FP32 argument-of-product
+// for far pairs, bit-exact FP64 terms + atan2 for near pairs, then the tile angle
+// added to the FP32 two-sum (hi, lo). `rec` is the tile record in shared memory,
+// `first` the tile's first slot in the sorted FP64 soup. Warp-collective (the fast
+// path is chosen by a vote over the warp), so every lane of the warp must call it.
+template <int QPT>
+__device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t first,
+                                           const double* __restrict__ tri64, int64_t ld64,
+                                           const double (&ox)[QPT], const double (&oy)[QPT],
+                                           const double (&oz)[QPT], const int64_t (&qidx)[QPT],
+                                           float (&hi)[QPT], float (&lo)[QPT],
+                                           double (&s64)[QPT], unsigned& refined,
+                                           unsigned& careful_tiles) {
+  const TileHeader& th = *reinterpret_cast<const TileHeader*>(rec);
+  const float4* fr = reinterpret_cast<const float4*>(rec + sizeof(TileHeader));
+  const int n = th.n;
+
+  float lx[QPT], ly[QPT], lz[QPT];
+  bool all_far = true;
+  bool skip[QPT];
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    const double dx = ox[k] - th.cx, dy = oy[k] - th.cy, dz = oz[k] - th.cz;
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    all_far &= (d2 >= th.far_r2) || qidx[k] < 0;
+    lx[k] = static_cast<float>(dx * th.scale);
+    ly[k] = static_cast<float>(dy * th.scale);
+    lz[k] = static_cast<float>(dz * th.scale);
+    // Beyond 2^40 tile radii the tile's solid angle is below 2^-80: it
+    // cannot change an FP32 sum, and squared distances could overflow.
+    skip[k] = d2 * th.scale * th.scale > 1.2089258196146292e24;
+  }
+  all_far = __all_sync(0xffffffffu, all_far);
+
+  float zr[QPT], zi[QPT];
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    zr[k] = kZ0;
+    zi[k] = 0.f;
+  }
+
+  if (all_far) {
+#pragma unroll 2
+    for (int j = 0; j < n; ++j) {
+      const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2];
+#pragma unroll
+      for (int k = 0; k < QPT; ++k) {
+        const float ax = r0.x - lx[k], ay = r0.y - ly[k], az = r0.z - lz[k];
+        const float bx = r0.w - lx[k], by = r1.x - ly[k], bz = r1.y - lz[k];
+        const float cx = r1.z - lx[k], cy = r1.w - ly[k], cz = r2.x - lz[k];
+        const float ra = rsqrt_approx(fmaf(ax, ax, fmaf(ay, ay, az * az)));
+        const float rb = rsqrt_approx(fmaf(bx, bx, fmaf(by, by, bz * bz)));
+        const float rc = rsqrt_approx(fmaf(cx, cx, fmaf(cy, cy, cz * cz)));
+        const float ab = fmaf(ax, bx, fmaf(ay, by, az * bz));
+        const float bc = fmaf(bx, cx, fmaf(by, cy, bz * cz));
+        const float ca = fmaf(cx, ax, fmaf(cy, ay, cz * az));
+        const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
+        const float dn = fmaf(ab, rab, fmaf(bc, rbc, fmaf(ca, rca, 1.f)));
+        const float dt = fmaf(ax, r2.y, fmaf(ay, r2.z, az * r2.w)) * (rab * rc);
+        const float nr = fmaf(zr[k], dn, -zi[k] * dt);
+        const float ni = fmaf(zr[k], dt, zi[k] * dn);
+        zr[k] = skip[k] ? zr[k] : nr;
+        zi[k] = skip[k] ? zi[k] : ni;
+      }
+    }
+  } else {
+    ++careful_tiles;
+#pragma unroll 1
+    for (int j = 0; j < n; ++j) {
+      const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2], r3 = fr[4 * j + 3];
+#pragma unroll
+      for (int k = 0; k < QPT; ++k) {
+        const float ax = r0.x - lx[k], ay = r0.y - ly[k], az = r0.z - lz[k];
+        const float bx = r0.w - lx[k], by = r1.x - ly[k], bz = r1.y - lz[k];
+        const float cx = r1.z - lx[k], cy = r1.w - ly[k], cz = r2.x - lz[k];
+        const float aa = fmaf(ax, ax, fmaf(ay, ay, az * az));
+        const float bb = fmaf(bx, bx, fmaf(by, by, bz * bz));
+        const float cc = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+        const bool near = fminf(aa, fminf(bb, cc)) < r3.x && qidx[k] >= 0;
+        if (near) {
+          const double* f64 = tri64 + first + j;
+          const int64_t L = ld64;
+          double det, denom;
+          pair_terms_exact(ox[k], oy[k], oz[k], f64[0], f64[L], f64[2 * L], f64[3 * L],
+                           f64[4 * L], f64[5 * L], f64[6 * L], f64[7 * L], f64[8 * L], det,
+                           denom);
+          s64[k] += atan2(det, denom);
+          ++refined;
+        } else if (!skip[k]) {
+          const float ra = rsqrt_approx(aa), rb = rsqrt_approx(bb), rc = rsqrt_approx(cc);
+          const float ab = fmaf(ax, bx, fmaf(ay, by, az * bz));
+          const float bc = fmaf(bx, cx, fmaf(by, cy, bz * cz));
+          const float ca = fmaf(cx, ax, fmaf(cy, ay, cz * az));
+          const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
+          const float dn = fmaf(ab, rab, fmaf(bc, rbc, fmaf(ca, rca, 1.f)));
+          const float dt = fmaf(ax, r2.y, fmaf(ay, r2.z, az * r2.w)) * (rab * rc);
+          const float nr = fmaf(zr[k], dn, -zi[k] * dt);
+          const float ni = fmaf(zr[k], dt, zi[k] * dn);
+          zr[k] = nr;
+          zi[k] = ni;
+        }
+      }
+    }
+  }
+  // Tile angle, added with an FP32 two-sum (Knuth).
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    const float ang = atan2f(zi[k], zr[k]);
+    const float s = hi[k] + ang;
+    const float bp = s - hi[k];
+    const float err = (hi[k] - (s - bp)) + (ang - bp);
+    hi[k] = s;
+    lo[k] += err;
+  }
+}
 
 template <int THREADS, int QPT, int STAGES>
 __global__ void __launch_bounds__(THREADS) mixed_forward_kernel(const MixedArgs a) {
@@ -346,109 +474,8 @@ __global__ void __launch_bounds__(THREADS) mixed_forward_kernel(const MixedArgs 
       break;
     }
     if (tid == 0 && t >= 1 && issued < ntiles) issue(issued++);
-    const unsigned char* rec = ring + slot * kTileBytes;
-    const TileHeader& th = *reinterpret_cast<const TileHeader*>(rec);
-    const float4* fr = reinterpret_cast<const float4*>(rec + sizeof(TileHeader));
-    const int n = th.n;
-
-    float lx[QPT], ly[QPT], lz[QPT];
-    bool all_far = true;
-    bool skip[QPT];
-#pragma unroll
-    for (int k = 0; k < QPT; ++k) {
-      const double dx = ox[k] - th.cx, dy = oy[k] - th.cy, dz = oz[k] - th.cz;
-      const double d2 = dx * dx + dy * dy + dz * dz;
-      all_far &= (d2 >= th.far_r2) || qidx[k] < 0;
-      lx[k] = static_cast<float>(dx * th.scale);
-      ly[k] = static_cast<float>(dy * th.scale);
-      lz[k] = static_cast<float>(dz * th.scale);
-      // Beyond 2^40 tile radii the tile's solid angle is below 2^-80: it
-      // cannot change an FP32 sum, and squared distances could overflow.
-      skip[k] = d2 * th.scale * th.scale > 1.2089258196146292e24;
-    }
-    all_far = __all_sync(0xffffffffu, all_far);
-
-    float zr[QPT], zi[QPT];
-#pragma unroll
-    for (int k = 0; k < QPT; ++k) {
-      zr[k] = kZ0;
-      zi[k] = 0.f;
-    }
-
-    if (all_far) {
-#pragma unroll 2
-      for (int j = 0; j < n; ++j) {
-        const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2];
-#pragma unroll
-        for (int k = 0; k < QPT; ++k) {
-          const float ax = r0.x - lx[k], ay = r0.y - ly[k], az = r0.z - lz[k];
-          const float bx = r0.w - lx[k], by = r1.x - ly[k], bz = r1.y - lz[k];
-          const float cx = r1.z - lx[k], cy = r1.w - ly[k], cz = r2.x - lz[k];
-          const float ra = rsqrt_approx(fmaf(ax, ax, fmaf(ay, ay, az * az)));
-          const float rb = rsqrt_approx(fmaf(bx, bx, fmaf(by, by, bz * bz)));
-          const float rc = rsqrt_approx(fmaf(cx, cx, fmaf(cy, cy, cz * cz)));
-          const float ab = fmaf(ax, bx, fmaf(ay, by, az * bz));
-          const float bc = fmaf(bx, cx, fmaf(by, cy, bz * cz));
-          const float ca = fmaf(cx, ax, fmaf(cy, ay, cz * az));
-          const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
-          const float dn = fmaf(ab, rab, fmaf(bc, rbc, fmaf(ca, rca, 1.f)));
-          const float dt = fmaf(ax, r2.y, fmaf(ay, r2.z, az * r2.w)) * (rab * rc);
-          const float nr = fmaf(zr[k], dn, -zi[k] * dt);
-          const float ni = fmaf(zr[k], dt, zi[k] * dn);
-          zr[k] = skip[k] ? zr[k] : nr;
-          zi[k] = skip[k] ? zi[k] : ni;
-        }
-      }
-    } else {
-      ++careful_tiles;
-      const int64_t first = (t_begin + t) * kTileFaces;
-#pragma unroll 1
-      for (int j = 0; j < n; ++j) {
-        const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2], r3 = fr[4 * j + 3];
-#pragma unroll
-        for (int k = 0; k < QPT; ++k) {
-          const float ax = r0.x - lx[k], ay = r0.y - ly[k], az = r0.z - lz[k];
-          const float bx = r0.w - lx[k], by = r1.x - ly[k], bz = r1.y - lz[k];
-          const float cx = r1.z - lx[k], cy = r1.w - ly[k], cz = r2.x - lz[k];
-          const float aa = fmaf(ax, ax, fmaf(ay, ay, az * az));
-          const float bb = fmaf(bx, bx, fmaf(by, by, bz * bz));
-          const float cc = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
-          const bool near = fminf(aa, fminf(bb, cc)) < r3.x && qidx[k] >= 0;
-          if (near) {
-            const double* f64 = a.tri64 + first + j;
-            const int64_t L = a.ld64;
-            double det, denom;
-            pair_terms_exact(ox[k], oy[k], oz[k], f64[0], f64[L], f64[2 * L], f64[3 * L],
-                             f64[4 * L], f64[5 * L], f64[6 * L], f64[7 * L], f64[8 * L], det,
-                             denom);
-            s64[k] += atan2(det, denom);
-            ++refined;
-          } else if (!skip[k]) {
-            const float ra = rsqrt_approx(aa), rb = rsqrt_approx(bb), rc = rsqrt_approx(cc);
-            const float ab = fmaf(ax, bx, fmaf(ay, by, az * bz));
-            const float bc = fmaf(bx, cx, fmaf(by, cy, bz * cz));
-            const float ca = fmaf(cx, ax, fmaf(cy, ay, cz * az));
-            const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
-            const float dn = fmaf(ab, rab, fmaf(bc, rbc, fmaf(ca, rca, 1.f)));
-            const float dt = fmaf(ax, r2.y, fmaf(ay, r2.z, az * r2.w)) * (rab * rc);
-            const float nr = fmaf(zr[k], dn, -zi[k] * dt);
-            const float ni = fmaf(zr[k], dt, zi[k] * dn);
-            zr[k] = nr;
-            zi[k] = ni;
-          }
-        }
-      }
-    }
-    // Tile angle, added with an FP32 two-sum (Knuth).
-#pragma unroll
-    for (int k = 0; k < QPT; ++k) {
-      const float ang = atan2f(zi[k], zr[k]);
-      const float s = hi[k] + ang;
-      const float bp = s - hi[k];
-      const float err = (hi[k] - (s - bp)) + (ang - bp);
-      hi[k] = s;
-      lo[k] += err;
-    }
+    mixed_tile<QPT>(ring + slot * kTileBytes, (t_begin + t) * kTileFaces, a.tri64, a.ld64, ox, oy,
+                    oz, qidx, hi, lo, s64, refined, careful_tiles);
   }
 
   if (failed) {
@@ -548,7 +575,7 @@ cudaError_t mixed_prepare_mesh(const double* tri, int64_t ld, int64_t nf, double
     if (e != cudaSuccess) return e;
   }
   build_tiles_kernel<<<static_cast<unsigned>(ntiles), kTileFaces, 0, stream>>>(
-      tri, ld, nf, vals_out, kappa, m->tiles, m->tri64, m->ld64, m->face_of);
+      tri, ld, nf, vals_out, kappa, m->tiles, m->tri64, m->ld64, m->face_of, nullptr, nullptr);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return cudaGetLastError();
 }
@@ -629,6 +656,507 @@ cudaError_t mixed_forward(const MixedMesh& m, const double* q, int64_t nq, doubl
   if (e != cudaSuccess) return e;
   return mixed_forward_sorted(m, q, perm, nq, w, p, p.nsplit > 1 ? partial : nullptr, stats, err,
                               stream);
+}
+
+// ---- batched meshes -------------------------------------------------------
+// Many meshes with their own query sets, of uneven sizes, in one persistent
+// launch. The meshes are concatenated (vertices, faces, queries); faces and
+// queries are Morton-ordered inside their own mesh by one radix sort each, on
+// 64-bit keys (mesh id << 30 | 30-bit Morton code of the point in its mesh's
+// box), so every mesh stays a contiguous segment. Each mesh is tiled on its
+// own. The work is a list of items (mesh, block of Morton-ordered queries,
+// range of that mesh's tiles) sized to ~target_pairs pairs and ordered largest
+// first; a persistent grid takes items from one atomic counter, and every item
+// writes its own slice of a partial-sum array, which a finishing kernel adds up
+// per query in chunk order. The schedule is dynamic, the result is not: no slot
+// is written twice and every sum runs in a fixed order.
+struct BatchDevice {
+  int64_t* F = nullptr;           // total_nf x 3, global vertex indices
+  int32_t* face_mesh = nullptr;   // total_nf
+  int32_t* query_mesh = nullptr;  // total_nq (original order == sorted segment order)
+  int64_t* tile_first = nullptr;  // total_tiles: sorted position of the tile's first face
+  int32_t* tile_count = nullptr;  // total_tiles
+  double* tri = nullptr;          // 9 x ldt soup built from V and F
+  unsigned long long* fbox = nullptr;  // nmesh x 6
+  unsigned long long* qbox = nullptr;  // nmesh x 6
+  uint64_t *fkeys_in = nullptr, *fkeys_out = nullptr;
+  uint32_t *fvals_in = nullptr, *fvals_out = nullptr;
+  uint64_t *qkeys_in = nullptr, *qkeys_out = nullptr;
+  uint32_t *qvals_in = nullptr, *perm = nullptr;
+  void* sort_temp = nullptr;
+  size_t sort_temp_bytes = 0;
+  MixedMesh mesh;                 // all tiles of all meshes
+  BatchItem* items = nullptr;
+  BatchMeshInfo* info = nullptr;  // nmesh
+  unsigned int* counter = nullptr;
+  double* partial = nullptr;
+};
+
+namespace {
+
+__global__ void soup_from_indexed_kernel(const double* __restrict__ V,
+                                         const int64_t* __restrict__ F, int64_t nf, int64_t ld,
+                                         double* __restrict__ tri) {
+  const int64_t f = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const int64_t v = F[3 * f + c];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) tri[(3 * c + x) * ld + f] = V[3 * v + x];
+  }
+}
+
+__global__ void batch_bbox_init_kernel(unsigned long long* box, int64_t nmesh) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < nmesh * 6) box[i] = (i % 6) < 3 ? ~0ull : 0ull;
+}
+
+__device__ __forceinline__ void point_of(const double* data, int64_t ld, int64_t i, bool centroid,
+                                         double p[3]) {
+#pragma unroll
+  for (int x = 0; x < 3; ++x)
+    p[x] = centroid ? (data[x * ld + i] + data[(3 + x) * ld + i] + data[(6 + x) * ld + i]) *
+                          (1.0 / 3.0)
+                    : data[3 * i + x];
+}
+
+// Per-mesh boxes: each thread scans 16 consecutive points (meshes are
+// contiguous, so a run rarely changes mesh), a warp whose lanes all stayed in
+// one mesh combines before its one set of atomics.
+template <bool CENTROIDS>
+__global__ void batch_bbox_kernel(const double* __restrict__ data, int64_t ld, int64_t n,
+                                  const int32_t* __restrict__ mesh_of,
+                                  unsigned long long* box) {
+  constexpr int kRun = 16;
+  const int64_t begin = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) * kRun;
+  const int64_t end = min(n, begin + kRun);
+  int cur = begin < n ? mesh_of[begin] : -1;
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  auto flush = [&](int m) {
+    if (m < 0 || !isfinite(lo[0])) return;
+    for (int x = 0; x < 3; ++x) {
+      atomicMin(&box[6 * m + x], ordered_key(lo[x]));
+      atomicMax(&box[6 * m + 3 + x], ordered_key(hi[x]));
+    }
+  };
+  for (int64_t i = begin; i < end; ++i) {
+    const int m = mesh_of[i];
+    if (m != cur) {
+      flush(cur);
+      cur = m;
+      for (int x = 0; x < 3; ++x) {
+        lo[x] = INFINITY;
+        hi[x] = -INFINITY;
+      }
+    }
+    double p[3];
+    point_of(data, ld, i, CENTROIDS, p);
+    for (int x = 0; x < 3; ++x) {
+      lo[x] = fmin(lo[x], p[x]);
+      hi[x] = fmax(hi[x], p[x]);
+    }
+  }
+  const int lead = __shfl_sync(0xffffffffu, cur, 0);
+  if (__all_sync(0xffffffffu, cur == lead)) {
+    for (int x = 0; x < 3; ++x) {
+      lo[x] = warp_min(lo[x]);
+      hi[x] = warp_max(hi[x]);
+    }
+    if ((threadIdx.x & 31) == 0) flush(cur);
+  } else {
+    flush(cur);
+  }
+}
+
+template <bool CENTROIDS>
+__global__ void batch_morton_kernel(const double* __restrict__ data, int64_t ld, int64_t n,
+                                    const int32_t* __restrict__ mesh_of,
+                                    const unsigned long long* __restrict__ box,
+                                    uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double p[3];
+  point_of(data, ld, i, CENTROIDS, p);
+  const int m = mesh_of[i];
+  keys[i] = (static_cast<uint64_t>(m) << 30) | morton30(p, box + 6 * m);
+  vals[i] = static_cast<uint32_t>(i);
+}
+
+struct BatchArgs {
+  const unsigned char* tiles;
+  const double* tri64;
+  int64_t ld64;
+  const double* q;
+  const uint32_t* perm;
+  const BatchItem* items;
+  int64_t n_items;
+  unsigned int* counter;
+  double* partial;
+  unsigned long long* stats;
+  int* err;
+};
+
+template <int THREADS, int QPT, int STAGES>
+__global__ void __launch_bounds__(THREADS) batch_forward_kernel(const BatchArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* ring = smem_raw;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + STAGES * kTileBytes);
+  __shared__ int64_t s_item;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
+    fence_barrier_init();
+  }
+  int64_t gt = 0;  // tiles consumed by this CTA so far: ring slot and phase
+  unsigned refined = 0, careful_tiles = 0;
+  bool failed = false;
+  for (;;) {
+    __syncthreads();  // everyone is done with the previous item and its tiles
+    if (tid == 0) s_item = static_cast<int64_t>(atomicAdd(a.counter, 1u));
+    __syncthreads();
+    const int64_t item = s_item;
+    if (item >= a.n_items) break;
+    const BatchItem it = a.items[item];
+    double ox[QPT], oy[QPT], oz[QPT];
+    int64_t qidx[QPT];
+#pragma unroll
+    for (int k = 0; k < QPT; ++k) {
+      const int64_t off = k * THREADS + tid;
+      qidx[k] = off < it.q_count ? static_cast<int64_t>(a.perm[it.q_begin + off]) : -1;
+      const int64_t i = qidx[k] >= 0 ? qidx[k] : static_cast<int64_t>(a.perm[it.q_begin]);
+      ox[k] = a.q[3 * i];
+      oy[k] = a.q[3 * i + 1];
+      oz[k] = a.q[3 * i + 2];
+    }
+    float hi[QPT], lo[QPT];
+    double s64[QPT];
+#pragma unroll
+    for (int k = 0; k < QPT; ++k) {
+      hi[k] = lo[k] = 0.f;
+      s64[k] = 0.0;
+    }
+    const int nt = it.t_count;
+    auto issue = [&](int u) {
+      const int slot = static_cast<int>((gt + u) % STAGES);
+      mbar_arrive_expect_tx(&full[slot], kTileBytes);
+      bulk_g2s(ring + slot * kTileBytes, a.tiles + (it.t_begin + u) * kTileBytes, kTileBytes,
+               &full[slot]);
+    };
+    int issued = 0;
+    if (tid == 0)
+      for (; issued < min(STAGES, nt); ++issued) issue(issued);
+    int u = 0;
+    for (; u < nt; ++u) {
+      const int slot = static_cast<int>((gt + u) % STAGES);
+      const bool landed =
+          mbar_wait(&full[slot], static_cast<uint32_t>(((gt + u) / STAGES) & 1), a.err);
+      if (!__syncthreads_and(landed)) {
+        failed = true;
+        break;
+      }
+      if (tid == 0 && u >= 1 && issued < nt) issue(issued++);
+      mixed_tile<QPT>(ring + slot * kTileBytes, (it.t_begin + u) * kTileFaces, a.tri64, a.ld64,
+                      ox, oy, oz, qidx, hi, lo, s64, refined, careful_tiles);
+    }
+    if (failed) {
+      if (tid == 0)
+        for (int w = u; w < issued; ++w)
+          mbar_wait(&full[(gt + w) % STAGES], static_cast<uint32_t>(((gt + w) / STAGES) & 1),
+                    nullptr);
+      break;
+    }
+    gt += nt;
+#pragma unroll
+    for (int k = 0; k < QPT; ++k) {
+      const int64_t off = k * THREADS + tid;
+      if (off >= it.q_count) continue;
+      a.partial[it.p_base + off] =
+          static_cast<double>(hi[k]) + static_cast<double>(lo[k]) + s64[k];
+    }
+  }
+  __syncthreads();
+  if (a.stats) {
+    unsigned r = refined;
+    for (int off = 16; off; off >>= 1) r += __shfl_xor_sync(0xffffffffu, r, off);
+    if ((tid & 31) == 0) {
+      atomicAdd(&a.stats[0], static_cast<unsigned long long>(r));
+      atomicAdd(&a.stats[1], static_cast<unsigned long long>(careful_tiles));
+    }
+  }
+}
+
+// W[perm[s]] = (sum over the mesh's tile chunks, in order) / (2 pi).
+__global__ void batch_finish_kernel(const double* __restrict__ partial,
+                                    const BatchMeshInfo* __restrict__ info,
+                                    const int32_t* __restrict__ query_mesh,
+                                    const uint32_t* __restrict__ perm, int64_t total_nq,
+                                    double* __restrict__ w) {
+  const int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (s >= total_nq) return;
+  const BatchMeshInfo mi = info[query_mesh[s]];
+  const int64_t local = s - mi.q_off;
+  double sum = 0.0;
+  for (int64_t c = 0; c < mi.nchunk; ++c) sum += partial[mi.p_off + c * mi.nq + local];
+  w[perm[s]] = sum / kTwoPi;
+}
+
+template <int QPT>
+cudaError_t launch_batch_variant(const BatchArgs& a, int grid, cudaStream_t stream) {
+  constexpr int kThreads = 128, kStages = 4;
+  auto kernel = batch_forward_kernel<kThreads, QPT, kStages>;
+  const size_t smem = static_cast<size_t>(kStages) * kTileBytes + sizeof(uint64_t) * kStages;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  kernel<<<grid, kThreads, smem, stream>>>(a);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+
+template <int QPT>
+int batch_grid(int sms, int ctas_per_sm) {
+  constexpr int kThreads = 128, kStages = 4;
+  const size_t smem = static_cast<size_t>(kStages) * kTileBytes + sizeof(uint64_t) * kStages;
+  int per_sm = 0;
+  cudaFuncSetAttribute(batch_forward_kernel<kThreads, QPT, kStages>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_forward_kernel<kThreads, QPT, kStages>,
+                                                kThreads, smem);
+  if (ctas_per_sm > 0) per_sm = std::min(per_sm, ctas_per_sm);
+  return std::max(1, per_sm) * std::max(1, sms);
+}
+
+template <typename T>
+cudaError_t dmalloc(T** p, size_t count) {
+  return cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * std::max<size_t>(count, 1));
+}
+
+}  // namespace
+
+cudaError_t batch_create(BatchState* b, int64_t nmesh, const int64_t* nv, const int64_t* nf,
+                         const int64_t* nq, const int64_t* F, const BatchPlan& plan, int sms) {
+  b->plan = plan;
+  b->sms = sms;
+  b->nmesh = nmesh;
+  cudaGetDevice(&b->device);
+  b->v_off.assign(nmesh + 1, 0);
+  b->f_off.assign(nmesh + 1, 0);
+  b->q_off.assign(nmesh + 1, 0);
+  b->t_off.assign(nmesh + 1, 0);
+  b->nv.assign(nv, nv + nmesh);
+  b->nf.assign(nf, nf + nmesh);
+  b->nq.assign(nq, nq + nmesh);
+  b->ntile.assign(nmesh, 0);
+  for (int64_t m = 0; m < nmesh; ++m) {
+    b->ntile[m] = nf[m] > 0 ? (nf[m] + kTileFaces - 1) / kTileFaces : 0;
+    b->v_off[m + 1] = b->v_off[m] + nv[m];
+    b->f_off[m + 1] = b->f_off[m] + nf[m];
+    b->q_off[m + 1] = b->q_off[m] + nq[m];
+    b->t_off[m + 1] = b->t_off[m] + b->ntile[m];
+  }
+  b->total_nv = b->v_off[nmesh];
+  b->total_nf = b->f_off[nmesh];
+  b->total_nq = b->q_off[nmesh];
+  b->total_tiles = b->t_off[nmesh];
+  b->ldt = ((std::max<int64_t>(b->total_nf, 1) + 1) / 2) * 2;
+  b->mesh_bits = 1;
+  while ((int64_t(1) << b->mesh_bits) < nmesh) ++b->mesh_bits;
+
+  // Work items and partial-sum layout.
+  const int64_t per_block = int64_t(128) * plan.qpt;
+  std::vector<BatchItem> items;
+  std::vector<BatchMeshInfo> info(nmesh);
+  int64_t p_off = 0;
+  for (int64_t m = 0; m < nmesh; ++m) {
+    const int64_t nt = b->ntile[m];
+    int64_t chunk = nt;
+    if (nt > 0) {
+      const int64_t want = plan.target_pairs / (per_block * kTileFaces);
+      chunk = std::max<int64_t>(1, std::min<int64_t>(nt, want));
+      chunk = (nt + ((nt + chunk - 1) / chunk) - 1) / ((nt + chunk - 1) / chunk);  // even chunks
+    }
+    const int64_t nchunk = nt > 0 ? (nt + chunk - 1) / chunk : 0;
+    info[m] = BatchMeshInfo{b->q_off[m], nq[m], p_off, nchunk};
+    for (int64_t c = 0; c < nchunk; ++c) {
+      const int64_t t0 = c * chunk, tn = std::min(chunk, nt - t0);
+      for (int64_t q0 = 0; q0 < nq[m]; q0 += per_block) {
+        BatchItem it;
+        it.q_begin = b->q_off[m] + q0;
+        it.t_begin = b->t_off[m] + t0;
+        it.p_base = p_off + c * nq[m] + q0;
+        it.q_count = static_cast<int32_t>(std::min(per_block, nq[m] - q0));
+        it.t_count = static_cast<int32_t>(tn);
+        items.push_back(it);
+      }
+    }
+    p_off += nchunk * nq[m];
+  }
+  std::stable_sort(items.begin(), items.end(), [](const BatchItem& x, const BatchItem& y) {
+    return int64_t(x.q_count) * x.t_count > int64_t(y.q_count) * y.t_count;
+  });
+  b->n_items = static_cast<int64_t>(items.size());
+  b->total_partials = p_off;
+
+  // Tile table and mesh ids.
+  std::vector<int64_t> tile_first(std::max<int64_t>(b->total_tiles, 1));
+  std::vector<int32_t> tile_count(std::max<int64_t>(b->total_tiles, 1));
+  for (int64_t m = 0; m < nmesh; ++m)
+    for (int64_t t = 0; t < b->ntile[m]; ++t) {
+      tile_first[b->t_off[m] + t] = b->f_off[m] + t * kTileFaces;
+      tile_count[b->t_off[m] + t] =
+          static_cast<int32_t>(std::min<int64_t>(kTileFaces, nf[m] - t * kTileFaces));
+    }
+  std::vector<int32_t> face_mesh(std::max<int64_t>(b->total_nf, 1)),
+      query_mesh(std::max<int64_t>(b->total_nq, 1));
+  std::vector<int64_t> Fg(std::max<int64_t>(3 * b->total_nf, 1));
+  for (int64_t m = 0; m < nmesh; ++m) {
+    for (int64_t f = b->f_off[m]; f < b->f_off[m + 1]; ++f) {
+      face_mesh[f] = static_cast<int32_t>(m);
+      for (int c = 0; c < 3; ++c) Fg[3 * f + c] = F[3 * f + c] + b->v_off[m];
+    }
+    for (int64_t i = b->q_off[m]; i < b->q_off[m + 1]; ++i) query_mesh[i] = static_cast<int32_t>(m);
+  }
+
+  BatchDevice* d = new BatchDevice();
+  b->dev = d;
+  size_t tf = 0, tq = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tf, static_cast<uint64_t*>(nullptr),
+                                  static_cast<uint64_t*>(nullptr), static_cast<uint32_t*>(nullptr),
+                                  static_cast<uint32_t*>(nullptr),
+                                  static_cast<int>(std::max<int64_t>(b->total_nf, 1)), 0,
+                                  30 + b->mesh_bits);
+  cub::DeviceRadixSort::SortPairs(nullptr, tq, static_cast<uint64_t*>(nullptr),
+                                  static_cast<uint64_t*>(nullptr), static_cast<uint32_t*>(nullptr),
+                                  static_cast<uint32_t*>(nullptr),
+                                  static_cast<int>(std::max<int64_t>(b->total_nq, 1)), 0,
+                                  30 + b->mesh_bits);
+  d->sort_temp_bytes = std::max(tf, tq);
+  const int64_t ld64 = std::max<int64_t>(b->total_tiles, 1) * kTileFaces;
+  cudaError_t e;
+  if ((e = dmalloc(&d->F, 3 * b->total_nf)) != cudaSuccess ||
+      (e = dmalloc(&d->face_mesh, b->total_nf)) != cudaSuccess ||
+      (e = dmalloc(&d->query_mesh, b->total_nq)) != cudaSuccess ||
+      (e = dmalloc(&d->tile_first, b->total_tiles)) != cudaSuccess ||
+      (e = dmalloc(&d->tile_count, b->total_tiles)) != cudaSuccess ||
+      (e = dmalloc(&d->tri, 9 * b->ldt)) != cudaSuccess ||
+      (e = dmalloc(&d->fbox, 6 * nmesh)) != cudaSuccess ||
+      (e = dmalloc(&d->qbox, 6 * nmesh)) != cudaSuccess ||
+      (e = dmalloc(&d->fkeys_in, b->total_nf)) != cudaSuccess ||
+      (e = dmalloc(&d->fkeys_out, b->total_nf)) != cudaSuccess ||
+      (e = dmalloc(&d->fvals_in, b->total_nf)) != cudaSuccess ||
+      (e = dmalloc(&d->fvals_out, b->total_nf)) != cudaSuccess ||
+      (e = dmalloc(&d->qkeys_in, b->total_nq)) != cudaSuccess ||
+      (e = dmalloc(&d->qkeys_out, b->total_nq)) != cudaSuccess ||
+      (e = dmalloc(&d->qvals_in, b->total_nq)) != cudaSuccess ||
+      (e = dmalloc(&d->perm, b->total_nq)) != cudaSuccess ||
+      (e = cudaMalloc(&d->sort_temp, std::max<size_t>(d->sort_temp_bytes, 16))) != cudaSuccess ||
+      (e = dmalloc(&d->mesh.tiles, static_cast<size_t>(std::max<int64_t>(b->total_tiles, 1)) *
+                                       kTileBytes)) != cudaSuccess ||
+      (e = dmalloc(&d->mesh.tri64, 9 * ld64)) != cudaSuccess ||
+      (e = dmalloc(&d->mesh.face_of, ld64)) != cudaSuccess ||
+      (e = dmalloc(&d->items, b->n_items)) != cudaSuccess ||
+      (e = dmalloc(&d->info, nmesh)) != cudaSuccess ||
+      (e = dmalloc(&d->counter, 1)) != cudaSuccess ||
+      (e = dmalloc(&d->partial, b->total_partials)) != cudaSuccess)
+    return e;
+  d->mesh.nf = b->total_nf;
+  d->mesh.ntiles = b->total_tiles;
+  d->mesh.ld64 = ld64;
+  d->mesh.kappa = plan.kappa;
+  if ((e = cudaMemcpy(d->F, Fg.data(), sizeof(int64_t) * Fg.size(), cudaMemcpyHostToDevice)) !=
+          cudaSuccess ||
+      (e = cudaMemcpy(d->face_mesh, face_mesh.data(), sizeof(int32_t) * face_mesh.size(),
+                      cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(d->query_mesh, query_mesh.data(), sizeof(int32_t) * query_mesh.size(),
+                      cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(d->tile_first, tile_first.data(), sizeof(int64_t) * tile_first.size(),
+                      cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(d->tile_count, tile_count.data(), sizeof(int32_t) * tile_count.size(),
+                      cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (items.size() && (e = cudaMemcpy(d->items, items.data(), sizeof(BatchItem) * items.size(),
+                                       cudaMemcpyHostToDevice)) != cudaSuccess) ||
+      (e = cudaMemcpy(d->info, info.data(), sizeof(BatchMeshInfo) * info.size(),
+                      cudaMemcpyHostToDevice)) != cudaSuccess)
+    return e;
+  switch (plan.qpt) {
+    case 1: b->grid = batch_grid<1>(sms, plan.ctas_per_sm); break;
+    case 4: b->grid = batch_grid<4>(sms, plan.ctas_per_sm); break;
+    default: b->grid = batch_grid<2>(sms, plan.ctas_per_sm); break;
+  }
+  b->grid = static_cast<int>(std::min<int64_t>(b->grid, std::max<int64_t>(b->n_items, 1)));
+  return cudaGetLastError();
+}
+
+void batch_destroy(BatchState* b) {
+  BatchDevice* d = b->dev;
+  if (!d) return;
+  void* ptrs[] = {d->F, d->face_mesh, d->query_mesh, d->tile_first, d->tile_count, d->tri,
+                  d->fbox, d->qbox, d->fkeys_in, d->fkeys_out, d->fvals_in, d->fvals_out,
+                  d->qkeys_in, d->qkeys_out, d->qvals_in, d->perm, d->sort_temp,
+                  d->mesh.tiles, d->mesh.tri64, d->mesh.face_of, d->items, d->info,
+                  d->counter, d->partial};
+  for (void* p : ptrs) cudaFree(p);
+  delete d;
+  b->dev = nullptr;
+}
+
+cudaError_t batch_forward(BatchState* b, const double* V, const double* q, double* w,
+                          unsigned long long* stats, int* err, cudaStream_t stream) {
+  BatchDevice* d = b->dev;
+  const int th = 256;
+  const int kbits = 30 + b->mesh_bits;
+  cudaError_t e;
+  if (b->total_nf > 0) {
+    soup_from_indexed_kernel<<<static_cast<unsigned>(blocks_for(b->total_nf, th)), th, 0,
+                               stream>>>(V, d->F, b->total_nf, b->ldt, d->tri);
+    batch_bbox_init_kernel<<<static_cast<unsigned>(blocks_for(6 * b->nmesh, th)), th, 0,
+                             stream>>>(d->fbox, b->nmesh);
+    batch_bbox_kernel<true><<<static_cast<unsigned>(blocks_for((b->total_nf + 15) / 16, th)), th,
+                              0, stream>>>(d->tri, b->ldt, b->total_nf, d->face_mesh, d->fbox);
+    batch_morton_kernel<true><<<static_cast<unsigned>(blocks_for(b->total_nf, th)), th, 0,
+                                stream>>>(d->tri, b->ldt, b->total_nf, d->face_mesh, d->fbox,
+                                          d->fkeys_in, d->fvals_in);
+    size_t tb = d->sort_temp_bytes;
+    if ((e = cub::DeviceRadixSort::SortPairs(d->sort_temp, tb, d->fkeys_in, d->fkeys_out,
+                                             d->fvals_in, d->fvals_out,
+                                             static_cast<int>(b->total_nf), 0, kbits, stream)) !=
+        cudaSuccess)
+      return e;
+    build_tiles_kernel<<<static_cast<unsigned>(b->total_tiles), kTileFaces, 0, stream>>>(
+        d->tri, b->ldt, b->total_nf, d->fvals_out, b->plan.kappa, d->mesh.tiles, d->mesh.tri64,
+        d->mesh.ld64, d->mesh.face_of, d->tile_first, d->tile_count);
+    g_launches.fetch_add(5, std::memory_order_relaxed);
+  }
+  if (b->total_nq == 0) return cudaGetLastError();
+  batch_bbox_init_kernel<<<static_cast<unsigned>(blocks_for(6 * b->nmesh, th)), th, 0, stream>>>(
+      d->qbox, b->nmesh);
+  batch_bbox_kernel<false><<<static_cast<unsigned>(blocks_for((b->total_nq + 15) / 16, th)), th,
+                             0, stream>>>(q, 0, b->total_nq, d->query_mesh, d->qbox);
+  batch_morton_kernel<false><<<static_cast<unsigned>(blocks_for(b->total_nq, th)), th, 0,
+                               stream>>>(q, 0, b->total_nq, d->query_mesh, d->qbox, d->qkeys_in,
+                                         d->qvals_in);
+  size_t tb = d->sort_temp_bytes;
+  if ((e = cub::DeviceRadixSort::SortPairs(d->sort_temp, tb, d->qkeys_in, d->qkeys_out,
+                                           d->qvals_in, d->perm, static_cast<int>(b->total_nq), 0,
+                                           kbits, stream)) != cudaSuccess)
+    return e;
+  g_launches.fetch_add(3, std::memory_order_relaxed);
+  if ((e = cudaMemsetAsync(d->counter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
+  BatchArgs a{d->mesh.tiles, d->mesh.tri64, d->mesh.ld64, q,     d->perm, d->items,
+              b->n_items,    d->counter,    d->partial,   stats, err};
+  if (b->n_items > 0) {
+    switch (b->plan.qpt) {
+      case 1: e = launch_batch_variant<1>(a, b->grid, stream); break;
+      case 4: e = launch_batch_variant<4>(a, b->grid, stream); break;
+      default: e = launch_batch_variant<2>(a, b->grid, stream); break;
+    }
+    if (e != cudaSuccess) return e;
+  }
+  batch_finish_kernel<<<static_cast<unsigned>(blocks_for(b->total_nq, th)), th, 0, stream>>>(
+      d->partial, d->info, d->query_mesh, d->perm, b->total_nq, w);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError();
 }
 
 }  // namespace wn

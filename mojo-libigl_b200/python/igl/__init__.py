@@ -23,6 +23,15 @@ import numpy as np
 from . import synthetic
 from ._lib import addr, fan_out, last_error, lib, worker_count
 
+def __getattr__(name):
+    # torch-dependent submodules load on first use.
+    if name in ("autograd", "batched", "autotune"):
+        import importlib
+
+        return importlib.import_module(f".{name}", __name__)
+    raise AttributeError(name)
+
+
 __all__ = [
     "winding_number",
     "winding_number_for_point",

@@ -1,0 +1,106 @@
+"""Batched persistent launch, CUDA-graph capture and the autotuner (needs a B200).
+
+The batched forward of every mesh must agree with the single-mesh mixed kernel
+and with the oracle (<= 1e-6), the batched adjoint with the single-mesh
+boundary-edge adjoint (<= 1e-12 relative), graph replays with eager runs
+bit for bit, and repeated runs with each other bit for bit.
+"""
+
+import numpy as np
+import pytest
+
+import igl
+from igl import autograd as wa
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_batch(n=7, seed=5, max_level=4, max_q=3000):
+    rng = np.random.default_rng(seed)
+    meshes, queries = [], []
+    for i in range(n):
+        level = int(rng.integers(0, max_level + 1))
+        V, F = igl.synthetic.bumpy_icosphere(level, seed=100 + i)
+        F = igl.synthetic.delete_faces(F, float(rng.uniform(0, 0.1)), seed=200 + i)
+        nq = int(rng.integers(1, max_q))
+        meshes.append((V, F))
+        queries.append(igl.synthetic.mixed_queries(V, F, nq, seed=300 + i, near_sigma=1e-3))
+    return meshes, queries
+
+
+@pytest.mark.parametrize("qpt", [1, 2, 4])
+def test_batched_forward_matches_oracle(gpu_required, oracle_mod, qpt):
+    meshes, queries = _small_batch()
+    b = igl.batched.Batch(meshes, queries, qpt=qpt, target_pairs=1 << 16)
+    try:
+        W = b.split(b.forward().clone())
+        assert b.info()["work_items"] > len(meshes)
+        for (V, F), O, w in zip(meshes, queries, W):
+            ref = oracle_mod.winding_number(V, F, O)
+            assert np.abs(w.cpu().numpy() - ref).max() <= 1e-6
+    finally:
+        b.close()
+
+
+def test_batched_backward_matches_single_mesh_adjoint(gpu_required):
+    import torch
+
+    meshes, queries = _small_batch(seed=6)
+    b = igl.batched.Batch(meshes, queries, target_pairs=1 << 16)
+    try:
+        b.gW.copy_(torch.randn(b.gW.shape, dtype=torch.float64,
+                               generator=torch.Generator().manual_seed(1)).cuda())
+        b.forward()
+        dV, dQ = b.backward()
+        dVs, dQs, gs = b.split(dV.clone(), "v"), b.split(dQ.clone()), b.split(b.gW.clone())
+        for (V, F), O, dv, dq, g in zip(meshes, queries, dVs, dQs, gs):
+            Vt, Ft, Ot = (torch.from_numpy(x).cuda() for x in (V, F, O))
+            ref_v, ref_q = wa.backward_edges(Vt, Ft, Ot, g)
+            scale = max(float(ref_v.abs().max()), float(ref_q.abs().max()), 1e-30)
+            assert float((dv - ref_v).abs().max()) <= 1e-12 * scale
+            assert float((dq - ref_q).abs().max()) <= 1e-12 * scale
+    finally:
+        b.close()
+
+
+def test_graph_replay_matches_eager_and_is_deterministic(gpu_required):
+    import torch
+
+    meshes, queries = _small_batch(seed=8)
+    b = igl.batched.Batch(meshes, queries, target_pairs=1 << 16)
+    try:
+        b.gW.normal_(generator=torch.Generator(device="cuda").manual_seed(3))
+        b.step()
+        torch.cuda.synchronize()
+        eager = (b.W.clone(), b.dV.clone(), b.dQ.clone())
+        b.step()
+        torch.cuda.synchronize()
+        assert torch.equal(b.W, eager[0]) and torch.equal(b.dV, eager[1])
+        b.capture()
+        b.W.zero_()
+        b.dV.zero_()
+        b.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(b.W, eager[0])
+        assert torch.equal(b.dV, eager[1]) and torch.equal(b.dQ, eager[2])
+        # New query positions through the same graph.
+        b.Q.add_(1e-3)
+        b.replay()
+        torch.cuda.synchronize()
+        moved = b.W.clone()
+        b.graph = None
+        b.forward()
+        torch.cuda.synchronize()
+        assert torch.equal(b.W, moved)
+    finally:
+        b.close()
+
+
+def test_autotuner_picks_and_caches(gpu_required, tmp_path, monkeypatch):
+    monkeypatch.setenv("WN_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    meshes, queries = _small_batch(n=4, seed=9)
+    space = {"qpt": (1, 2), "target_pairs": (1 << 16,), "ctas_per_sm": (0,), "kappa": (4.0,)}
+    first = igl.autotune.tune(meshes, queries, space=space, reps=1)
+    assert not first["cached"] and len(first["trials"]) == 2
+    again = igl.autotune.tune(meshes, queries, space=space, reps=1)
+    assert again["cached"] and again["config"] == first["config"]

@@ -14,7 +14,9 @@ Legs, all on the same inputs:
   * fwdbwd_faces / fwdbwd_edges: mixed forward + the per-face mixed-precision
     adjoint / the boundary-edge adjoint (both followed by the vertex gather);
   * c4: the gradient workload (subdivision-5 mesh, 8% faces deleted, 262,144
-    near-surface queries): forward alone and forward + each adjoint.
+    near-surface queries): forward alone and forward + each adjoint;
+  * c5: 64 uneven meshes in one persistent launch, forward alone and forward +
+    boundary-edge adjoint replayed from one captured CUDA graph.
 `value` is whole-job pairs/s of the headline leg with inputs resident in HBM;
 `e2e` is the same leg through the C ABI with pinned host buffers, the
 host->device copies, device preprocessing and device->host copy inside the
@@ -65,6 +67,9 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-c4", action="store_true", help="skip the gradient workload")
+    p.add_argument("--no-c5", action="store_true", help="skip the batched workload")
+    p.add_argument("--autotune", action="store_true",
+                   help="autotune the batched launch (cached per GPU and size bucket)")
     return p.parse_args()
 
 
@@ -390,6 +395,32 @@ def gpu_arm(args):
               "ratio_faces": t4["faces"] / t4["fwd"], "ratio_edges": t4["edges"] / t4["fwd"]}
         mesh4.close()
 
+    # Batched workload: 64 bumpy icospheres (subdivision U{2..7}, 0-10% faces
+    # deleted, queries log-uniform in [1024, 2^20]), forward and forward +
+    # boundary-edge adjoint as one captured CUDA graph of persistent launches.
+    c5 = None
+    if not args.no_c5:
+        from igl import autotune, batched, synthetic
+
+        work = synthetic.batched_workload(seed=51 + rank)
+        meshes = [(Vm, Fm) for Vm, Fm, _ in work]
+        queries = [Om for _, _, Om in work]
+        tuned = autotune.tune(meshes, queries) if args.autotune else None
+        cfg = tuned["config"] if tuned else {"qpt": 2, "target_pairs": 1 << 21, "kappa": 4.0}
+        bt = batched.Batch(meshes, queries, **cfg)
+        bt.gW.normal_()
+        t_f = timed(lambda: bt.forward(), args.steps, 2)[0]
+        bt.capture(backward=True)
+        t_g, launches_g, _ = timed(bt.replay, args.steps, 2)
+        c5 = {"workload": "64 bumpy icospheres, subdivision U{2..7}, 0-10% faces deleted, "
+                          "queries log-uniform in [1024, 2^20], 50/50 box/near(1e-3)",
+              "meshes": len(meshes), "pairs": bt.pairs, "config": cfg,
+              "autotuned": tuned is not None, "info": bt.info(),
+              "fwd_ms": t_f * 1e3, "fwd_pairs_per_s": world * bt.pairs / t_f,
+              "graph_fwdbwd_ms": t_g * 1e3, "graph_fwdbwd_pairs_per_s": world * bt.pairs / t_g,
+              "ratio_fwdbwd_to_fwd": t_g / t_f}
+        bt.close()
+
     # Accuracy of the mixed leg against the FP64 kernel on every query.
     accuracy = None
     if "mixed" in results and "fp64" in results:
@@ -489,6 +520,7 @@ def gpu_arm(args):
                                 if "mixed" in results and "fp64" in results else None),
             "fwd_bwd": fwdbwd,
             "c4_fwd_bwd": c4,
+            "c5_batched": c5,
             "accuracy": accuracy,
             "refinement": ({"pairs_refined_fp64_per_step": headline_refined,
                             "fraction": headline_refined / pairs}

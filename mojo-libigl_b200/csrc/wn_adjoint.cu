@@ -261,9 +261,14 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAd
       slot[k] = (tile_ok ? t : 0) * kTileFaces + j;
       const float* fr = reinterpret_cast<const float*>(a.tiles + (tile_ok ? t : 0) * kTileBytes +
                                                        sizeof(TileHeader)) + 16 * j;
+      // Corners from the record's A, e1 = B - A, e2 = C - A; the threshold last.
 #pragma unroll
-      for (int r = 0; r < 9; ++r) fv[k][r] = valid[k] ? fr[r] : 0.f;
-      fv[k][9] = valid[k] ? fr[12] : 0.f;
+      for (int r = 0; r < 3; ++r) {
+        fv[k][r] = valid[k] ? fr[r] : 0.f;
+        fv[k][3 + r] = valid[k] ? fr[r] + fr[3 + r] : 0.f;
+        fv[k][6 + r] = valid[k] ? fr[r] + fr[6 + r] : 0.f;
+      }
+      fv[k][9] = valid[k] ? fr[15] : 0.f;
 #pragma unroll
       for (int r = 0; r < 9; ++r) {
         acc32[k][r] = 0.f;

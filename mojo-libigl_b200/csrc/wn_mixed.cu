@@ -262,27 +262,29 @@ __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
   }
   FaceRec fr;
   const double ax = (v[0] - c[0]) * scale, ay = (v[1] - c[1]) * scale, az = (v[2] - c[2]) * scale;
-  const double bx = (v[3] - c[0]) * scale, by = (v[4] - c[1]) * scale, bz = (v[5] - c[2]) * scale;
-  const double cx = (v[6] - c[0]) * scale, cy = (v[7] - c[1]) * scale, cz = (v[8] - c[2]) * scale;
-  const double e1x = bx - ax, e1y = by - ay, e1z = bz - az;
-  const double e2x = cx - ax, e2y = cy - ay, e2z = cz - az;
+  const double e1x = (v[3] - v[0]) * scale, e1y = (v[4] - v[1]) * scale,
+               e1z = (v[5] - v[2]) * scale;
+  const double e2x = (v[6] - v[0]) * scale, e2y = (v[7] - v[1]) * scale,
+               e2z = (v[8] - v[2]) * scale;
   fr.ax = static_cast<float>(ax);
   fr.ay = static_cast<float>(ay);
   fr.az = static_cast<float>(az);
-  fr.bx = static_cast<float>(bx);
-  fr.by = static_cast<float>(by);
-  fr.bz = static_cast<float>(bz);
-  fr.cx = static_cast<float>(cx);
-  fr.cy = static_cast<float>(cy);
-  fr.cz = static_cast<float>(cz);
+  fr.e1x = static_cast<float>(e1x);
+  fr.e1y = static_cast<float>(e1y);
+  fr.e1z = static_cast<float>(e1z);
+  fr.e2x = static_cast<float>(e2x);
+  fr.e2y = static_cast<float>(e2y);
+  fr.e2z = static_cast<float>(e2z);
   fr.nx = static_cast<float>(e1y * e2z - e1z * e2y);
   fr.ny = static_cast<float>(e1z * e2x - e1x * e2z);
   fr.nz = static_cast<float>(e1x * e2y - e1y * e2x);
+  fr.e11 = static_cast<float>(e1x * e1x + e1y * e1y + e1z * e1z);
+  fr.e22 = static_cast<float>(e2x * e2x + e2y * e2y + e2z * e2z);
+  fr.e12 = static_cast<float>(e1x * e2x + e1y * e2y + e1z * e2z);
   // A collapsed face (h = 0) is always refined: in FP64 it contributes
   // atan2(0, denom >= 0) = 0 exactly, and it never reaches rsqrt(0).
   const double thr = kappa * h_face * scale;
   fr.thr = (valid && h_face == 0.0) ? INFINITY : static_cast<float>(thr * thr);
-  fr.pad0 = fr.pad1 = fr.pad2 = 0.f;
   reinterpret_cast<FaceRec*>(rec + sizeof(TileHeader))[j] = fr;
 }
 
@@ -300,6 +302,40 @@ struct MixedArgs {
   unsigned long long* stats;  // [0] refined pairs, [1] careful (query-warp, tile) visits
   int* err;
 };
+
+// Squared lengths and dot products of one pair from a face record (FaceRec
+// layout: r0 = A.xyz e1.x, r1 = e1.yz e2.xy, r2 = e2.z n.xyz, r3 = e11 e22 e12 thr).
+struct PairSq {
+  float aa, bb, cc, ab, bc, ca, det;
+};
+
+__device__ __forceinline__ PairSq pair_sq(const float4& r0, const float4& r1, const float4& r2,
+                                          const float4& r3, float lx, float ly, float lz) {
+  const float ax = r0.x - lx, ay = r0.y - ly, az = r0.z - lz;
+  PairSq p;
+  p.aa = fmaf(ax, ax, fmaf(ay, ay, az * az));
+  const float s1 = fmaf(ax, r0.w, fmaf(ay, r1.x, az * r1.y));  // a.e1
+  const float s2 = fmaf(ax, r1.z, fmaf(ay, r1.w, az * r2.x));  // a.e2
+  p.det = fmaf(ax, r2.y, fmaf(ay, r2.z, az * r2.w));          // a.(e1 x e2) = a.(b x c)
+  p.ab = p.aa + s1;
+  p.ca = p.aa + s2;
+  p.bb = fmaf(2.f, s1, p.aa + r3.x);
+  p.cc = fmaf(2.f, s2, p.aa + r3.y);
+  p.bc = p.ab + (s2 + r3.z);
+  return p;
+}
+
+// z' = (denom + i det) / (|a||b||c|) of a far pair, multiplied into (zr, zi).
+__device__ __forceinline__ void pair_mul(const PairSq& p, float& zr, float& zi) {
+  const float ra = rsqrt_approx(p.aa), rb = rsqrt_approx(p.bb), rc = rsqrt_approx(p.cc);
+  const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
+  const float dn = fmaf(p.ab, rab, fmaf(p.bc, rbc, fmaf(p.ca, rca, 1.f)));
+  const float dt = p.det * (rab * rc);
+  const float nr = fmaf(zr, dn, -zi * dt);
+  const float ni = fmaf(zr, dt, zi * dn);
+  zr = nr;
+  zi = ni;
+}
 
 // One 64-face tile against the QPT queries of this thread: FP32 argument-of-product
 // for far pairs, bit-exact FP64 terms + atan2 for near pairs, then the tile angle
@@ -332,7 +368,9 @@ __device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t fir
     // Beyond 2^40 tile radii the tile's solid angle is below 2^-80: it
     // cannot change an FP32 sum, and squared distances could overflow.
     skip[k] = d2 * th.scale * th.scale > 1.2089258196146292e24;
+    all_far &= !skip[k];
   }
+  // The fast path: no lane has a near pair or a skipped tile.
   all_far = __all_sync(0xffffffffu, all_far);
 
   float zr[QPT], zi[QPT];
@@ -345,26 +383,9 @@ __device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t fir
   if (all_far) {
 #pragma unroll 2
     for (int j = 0; j < n; ++j) {
-      const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2];
+      const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2], r3 = fr[4 * j + 3];
 #pragma unroll
-      for (int k = 0; k < QPT; ++k) {
-        const float ax = r0.x - lx[k], ay = r0.y - ly[k], az = r0.z - lz[k];
-        const float bx = r0.w - lx[k], by = r1.x - ly[k], bz = r1.y - lz[k];
-        const float cx = r1.z - lx[k], cy = r1.w - ly[k], cz = r2.x - lz[k];
-        const float ra = rsqrt_approx(fmaf(ax, ax, fmaf(ay, ay, az * az)));
-        const float rb = rsqrt_approx(fmaf(bx, bx, fmaf(by, by, bz * bz)));
-        const float rc = rsqrt_approx(fmaf(cx, cx, fmaf(cy, cy, cz * cz)));
-        const float ab = fmaf(ax, bx, fmaf(ay, by, az * bz));
-        const float bc = fmaf(bx, cx, fmaf(by, cy, bz * cz));
-        const float ca = fmaf(cx, ax, fmaf(cy, ay, cz * az));
-        const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
-        const float dn = fmaf(ab, rab, fmaf(bc, rbc, fmaf(ca, rca, 1.f)));
-        const float dt = fmaf(ax, r2.y, fmaf(ay, r2.z, az * r2.w)) * (rab * rc);
-        const float nr = fmaf(zr[k], dn, -zi[k] * dt);
-        const float ni = fmaf(zr[k], dt, zi[k] * dn);
-        zr[k] = skip[k] ? zr[k] : nr;
-        zi[k] = skip[k] ? zi[k] : ni;
-      }
+      for (int k = 0; k < QPT; ++k) pair_mul(pair_sq(r0, r1, r2, r3, lx[k], ly[k], lz[k]), zr[k], zi[k]);
     }
   } else {
     ++careful_tiles;
@@ -373,13 +394,8 @@ __device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t fir
       const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2], r3 = fr[4 * j + 3];
 #pragma unroll
       for (int k = 0; k < QPT; ++k) {
-        const float ax = r0.x - lx[k], ay = r0.y - ly[k], az = r0.z - lz[k];
-        const float bx = r0.w - lx[k], by = r1.x - ly[k], bz = r1.y - lz[k];
-        const float cx = r1.z - lx[k], cy = r1.w - ly[k], cz = r2.x - lz[k];
-        const float aa = fmaf(ax, ax, fmaf(ay, ay, az * az));
-        const float bb = fmaf(bx, bx, fmaf(by, by, bz * bz));
-        const float cc = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
-        const bool near = fminf(aa, fminf(bb, cc)) < r3.x && qidx[k] >= 0;
+        const PairSq p = pair_sq(r0, r1, r2, r3, lx[k], ly[k], lz[k]);
+        const bool near = fminf(p.aa, fminf(p.bb, p.cc)) < r3.w && qidx[k] >= 0;
         if (near) {
           const double* f64 = tri64 + first + j;
           const int64_t L = ld64;
@@ -390,17 +406,7 @@ __device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t fir
           s64[k] += atan2(det, denom);
           ++refined;
         } else if (!skip[k]) {
-          const float ra = rsqrt_approx(aa), rb = rsqrt_approx(bb), rc = rsqrt_approx(cc);
-          const float ab = fmaf(ax, bx, fmaf(ay, by, az * bz));
-          const float bc = fmaf(bx, cx, fmaf(by, cy, bz * cz));
-          const float ca = fmaf(cx, ax, fmaf(cy, ay, cz * az));
-          const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
-          const float dn = fmaf(ab, rab, fmaf(bc, rbc, fmaf(ca, rca, 1.f)));
-          const float dt = fmaf(ax, r2.y, fmaf(ay, r2.z, az * r2.w)) * (rab * rc);
-          const float nr = fmaf(zr[k], dn, -zi[k] * dt);
-          const float ni = fmaf(zr[k], dt, zi[k] * dn);
-          zr[k] = nr;
-          zi[k] = ni;
+          pair_mul(p, zr[k], zi[k]);
         }
       }
     }

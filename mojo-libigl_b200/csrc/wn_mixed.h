@@ -22,12 +22,16 @@ struct TileHeader {
 };
 static_assert(sizeof(TileHeader) == 64, "tile header is 64 bytes");
 
-// 64-byte face record, FP32 tile-local scaled coordinates.
+// 64-byte face record, FP32 tile-local scaled coordinates. With a = A - o the
+// pair needs |a|^2, a.e1, a.e2 and a.n only: b = a + e1 and c = a + e2 give
+// |b|^2 = |a|^2 + 2 a.e1 + |e1|^2, a.b = |a|^2 + a.e1, b.c = a.b + a.e2 + e1.e2, ...
 struct FaceRec {
-  float ax, ay, az, bx, by, bz, cx, cy, cz;  // corners minus centre, times scale
-  float nx, ny, nz;                          // (B-A) x (C-A), formed in FP64
-  float thr;                                 // (kappa*h_face*scale)^2; +inf for collapsed faces
-  float pad0, pad1, pad2;
+  float ax, ay, az;     // corner A minus centre, times scale
+  float e1x, e1y, e1z;  // B - A (formed in FP64, then rounded)
+  float e2x, e2y, e2z;  // C - A
+  float nx, ny, nz;     // e1 x e2
+  float e11, e22, e12;  // |e1|^2, |e2|^2, e1.e2
+  float thr;            // (kappa*h_face*scale)^2; +inf for collapsed faces
 };
 static_assert(sizeof(FaceRec) == 64, "face record is 64 bytes");
 

@@ -40,8 +40,10 @@ enum {
 
 /* FP64 accumulation modes of the plain kernel. */
 enum {
-  WN_FP64_ARGPROD = 0, /* bit-exact pair terms, argument-of-product sum (default) */
-  WN_FP64_DIRECT = 1   /* bit-exact pair terms, one atan2 per pair */
+  WN_FP64_ARGPROD = 0, /* bit-exact pair terms, argument-of-product sum */
+  WN_FP64_DIRECT = 1,  /* bit-exact pair terms, one atan2 per pair */
+  WN_FP64_TILED = 2    /* WN_FP64_ARGPROD over a prepared mesh (Morton tiles, faces in
+                          strips) that reuses repeated corners; host entry only */
 };
 
 /* ---- reference-compatible entry points --------------------------------- */
@@ -79,7 +81,7 @@ int wn_probe_fma_tflops(int bits, double* tflops);
 
 /* ---- plain FP64 forward (no reference counterpart beyond mli_winding_gpu) */
 
-/* Host pointers; mode = WN_FP64_ARGPROD or WN_FP64_DIRECT. */
+/* Host pointers; mode = WN_FP64_ARGPROD, WN_FP64_DIRECT or WN_FP64_TILED. */
 int wn_forward_fp64_host(const double* tri, const double* q, double* w, int64_t nf, int64_t nq,
                          int mode);
 
@@ -118,6 +120,10 @@ int wn_forward_mixed_host(const double* tri, const double* q, double* w, int64_t
 int wn_mixed_mesh_create(const double* tri, int64_t ld, int64_t nf, double kappa, void* stream,
                          void** mesh_out);
 int wn_mixed_mesh_destroy(void* mesh);
+/* The plain FP64 forward over a prepared mesh (WN_FP64_TILED): same bit-exact
+ * pair terms, corners shared by consecutive faces evaluated once. */
+int wn_forward_fp64_mesh_device(void* mesh, const double* q, int64_t nq, double* w,
+                                void* stream);
 int wn_forward_mixed_device(void* mesh, const double* q, int64_t nq, double* w, void* stream);
 /* Re-prepare an existing mesh in place from new vertex positions (same face
  * count), e.g. once per step of a shape optimisation. */

@@ -72,7 +72,7 @@ struct DeviceCtx {
   int* err = nullptr;  // device error word
   unsigned long long* stats = nullptr;  // mixed-path counters (refined pairs, careful visits)
   Buffer tri, q, w, scratch;
-  Buffer mesh_tiles, mesh_tri64, mesh_face_of;  // prepared mesh of the host entry points
+  Buffer mesh_tiles, mesh_tri64, mesh_face_of, mesh_reuse;  // prepared mesh (host entry points)
 };
 
 std::mutex g_mutex;
@@ -123,7 +123,9 @@ int forward_fp64_host(const double* tri, const double* q, double* w, int64_t nf,
                       int mode) {
   if (nf < 0 || nq < 0) return fail(WN_EINVAL, "negative size (nf=%lld, nq=%lld)",
                                     (long long)nf, (long long)nq);
-  if (mode != kFp64ArgProd && mode != kFp64Direct) return fail(WN_EINVAL, "bad mode %d", mode);
+  if (mode != kFp64ArgProd && mode != kFp64Direct && mode != kFp64Tiled)
+    return fail(WN_EINVAL, "bad mode %d", mode);
+  if (mode == kFp64Tiled && nf > 0x7fffffffLL) return fail(WN_EINVAL, "more than 2^31-1 faces");
   if (nq == 0) return WN_OK;
   if ((nf > 0 && !tri) || !q || !w) return fail(WN_EINVAL, "null pointer");
   std::lock_guard<std::mutex> lock(g_mutex);
@@ -132,11 +134,21 @@ int forward_fp64_host(const double* tri, const double* q, double* w, int64_t nf,
   if (!c) return code;
   const int64_t ld = even_ld(nf);
   const Fp64Plan plan = plan_fp64(nf, nq, c->sms);
+  const Fp64TiledPlan tplan = plan_fp64_tiled(mixed_tiles(nf), nq, c->sms);
+  size_t scratch = sizeof(double) * (plan.scratch_doubles + 1);
+  if (mode == kFp64Tiled)
+    scratch = std::max(mixed_sort_scratch_bytes(nf), sizeof(double) * (tplan.scratch_doubles + 1));
   cudaError_t e;
   if ((e = c->tri.ensure(sizeof(double) * 9 * ld)) != cudaSuccess ||
       (e = c->q.ensure(sizeof(double) * 3 * nq)) != cudaSuccess ||
       (e = c->w.ensure(sizeof(double) * nq)) != cudaSuccess ||
-      (e = c->scratch.ensure(sizeof(double) * (plan.scratch_doubles + 1))) != cudaSuccess)
+      (e = c->scratch.ensure(scratch)) != cudaSuccess)
+    return cuda_fail(e, "device allocation");
+  if (mode == kFp64Tiled &&
+      ((e = c->mesh_tiles.ensure(mixed_tiles_bytes(nf))) != cudaSuccess ||
+       (e = c->mesh_tri64.ensure(mixed_tri64_bytes(nf))) != cudaSuccess ||
+       (e = c->mesh_face_of.ensure(mixed_face_of_bytes(nf))) != cudaSuccess ||
+       (e = c->mesh_reuse.ensure(mixed_reuse_bytes(nf))) != cudaSuccess))
     return cuda_fail(e, "device allocation");
   double* tri_d = static_cast<double*>(c->tri.ptr);
   double* q_d = static_cast<double*>(c->q.ptr);
@@ -148,9 +160,23 @@ int forward_fp64_host(const double* tri, const double* q, double* w, int64_t nf,
   if ((e = cudaMemcpyAsync(q_d, q, sizeof(double) * 3 * nq, cudaMemcpyHostToDevice, c->stream)) !=
       cudaSuccess)
     return cuda_fail(e, "copy of the queries");
-  if ((e = launch_fp64(plan, mode, tri_d, ld, nf, q_d, nq, w_d,
-                       static_cast<double*>(c->scratch.ptr), c->err, c->stream)) != cudaSuccess)
+  if (mode == kFp64Tiled) {
+    MixedMesh m;
+    m.tiles = static_cast<unsigned char*>(c->mesh_tiles.ptr);
+    m.tri64 = static_cast<double*>(c->mesh_tri64.ptr);
+    m.face_of = static_cast<uint32_t*>(c->mesh_face_of.ptr);
+    m.reuse = static_cast<uint8_t*>(c->mesh_reuse.ptr);
+    if ((e = mixed_prepare_mesh(tri_d, ld, nf, 4.0, &m, c->scratch.ptr, c->scratch.bytes,
+                                c->stream)) != cudaSuccess)
+      return cuda_fail(e, "mesh preparation");
+    if ((e = launch_fp64_tiled(tplan, m, q_d, nq, w_d, static_cast<double*>(c->scratch.ptr),
+                               c->err, c->stream)) != cudaSuccess)
+      return cuda_fail(e, "FP64 winding-number launch");
+  } else if ((e = launch_fp64(plan, mode, tri_d, ld, nf, q_d, nq, w_d,
+                              static_cast<double*>(c->scratch.ptr), c->err, c->stream)) !=
+             cudaSuccess) {
     return cuda_fail(e, "FP64 winding-number launch");
+  }
   if ((e = cudaMemcpyAsync(w, w_d, sizeof(double) * nq, cudaMemcpyDeviceToHost, c->stream)) !=
       cudaSuccess)
     return cuda_fail(e, "copy of the result");
@@ -192,7 +218,8 @@ int forward_mixed_host(const double* tri, const double* q, double* w, int64_t nf
       (e = c->scratch.ensure(scratch)) != cudaSuccess ||
       (e = c->mesh_tiles.ensure(mixed_tiles_bytes(nf))) != cudaSuccess ||
       (e = c->mesh_tri64.ensure(mixed_tri64_bytes(nf))) != cudaSuccess ||
-      (e = c->mesh_face_of.ensure(mixed_face_of_bytes(nf))) != cudaSuccess)
+      (e = c->mesh_face_of.ensure(mixed_face_of_bytes(nf))) != cudaSuccess ||
+      (e = c->mesh_reuse.ensure(mixed_reuse_bytes(nf))) != cudaSuccess)
     return cuda_fail(e, "device allocation");
   double* tri_d = static_cast<double*>(c->tri.ptr);
   if (nf > 0 && (e = cudaMemcpy2DAsync(tri_d, sizeof(double) * ld, tri, sizeof(double) * nf,
@@ -206,6 +233,7 @@ int forward_mixed_host(const double* tri, const double* q, double* w, int64_t nf
   m.tiles = static_cast<unsigned char*>(c->mesh_tiles.ptr);
   m.tri64 = static_cast<double*>(c->mesh_tri64.ptr);
   m.face_of = static_cast<uint32_t*>(c->mesh_face_of.ptr);
+  m.reuse = static_cast<uint8_t*>(c->mesh_reuse.ptr);
   if ((e = mixed_prepare_mesh(tri_d, ld, nf, kappa, &m, c->scratch.ptr, c->scratch.bytes,
                               c->stream)) != cudaSuccess)
     return cuda_fail(e, "mesh preparation");
@@ -293,7 +321,8 @@ int wn_forward_fp64_device(const double* tri, int64_t ld, const double* q, doubl
     return fail(WN_EINVAL, "bad sizes (nf=%lld, nq=%lld, ld=%lld; ld must be even and >= nf)",
                 (long long)nf, (long long)nq, (long long)ld);
   if (reinterpret_cast<uintptr_t>(tri) & 15) return fail(WN_EINVAL, "tri must be 16-byte aligned");
-  if (mode != kFp64ArgProd && mode != kFp64Direct) return fail(WN_EINVAL, "bad mode %d", mode);
+  if (mode != kFp64ArgProd && mode != kFp64Direct)
+    return fail(WN_EINVAL, "bad mode %d (the prepared-mesh mode has its own entry point)", mode);
   if (nq == 0) return WN_OK;
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
@@ -342,10 +371,13 @@ int wn_mixed_mesh_create(const double* tri, int64_t ld, int64_t nf, double kappa
           cudaSuccess ||
       (e = cudaMalloc(reinterpret_cast<void**>(&h->m.face_of), mixed_face_of_bytes(nf))) !=
           cudaSuccess ||
+      (e = cudaMalloc(reinterpret_cast<void**>(&h->m.reuse), mixed_reuse_bytes(nf))) !=
+          cudaSuccess ||
       (e = cudaMallocAsync(&scratch, sb, st)) != cudaSuccess) {
     cudaFree(h->m.tiles);
     cudaFree(h->m.tri64);
     cudaFree(h->m.face_of);
+    cudaFree(h->m.reuse);
     delete h;
     return cuda_fail(e, "device allocation");
   }
@@ -356,6 +388,7 @@ int wn_mixed_mesh_create(const double* tri, int64_t ld, int64_t nf, double kappa
     cudaFree(h->m.tiles);
     cudaFree(h->m.tri64);
     cudaFree(h->m.face_of);
+    cudaFree(h->m.reuse);
     delete h;
     return cuda_fail(e, "mesh preparation");
   }
@@ -373,6 +406,7 @@ int wn_mixed_mesh_destroy(void* mesh) {
   cudaFree(h->m.tiles);
   cudaFree(h->m.tri64);
   cudaFree(h->m.face_of);
+  cudaFree(h->m.reuse);
   cudaSetDevice(prev);
   delete h;
   return WN_OK;
@@ -395,6 +429,29 @@ int wn_forward_mixed_device(void* mesh, const double* q, int64_t nq, double* w, 
   e = mixed_forward(h->m, q, nq, w, scratch, sb, c->sms, c->stats, c->err, st);
   cudaFreeAsync(scratch, st);
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "mixed winding-number launch");
+}
+
+int wn_forward_fp64_mesh_device(void* mesh, const double* q, int64_t nq, double* w,
+                                void* stream) {
+  if (!mesh) return fail(WN_EINVAL, "null mesh");
+  if (nq < 0 || nq > 0x7fffffffLL) return fail(WN_EINVAL, "bad nq=%lld", (long long)nq);
+  if (nq == 0) return WN_OK;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  const MeshHandle* h = static_cast<const MeshHandle*>(mesh);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const Fp64TiledPlan p = plan_fp64_tiled(h->m.ntiles, nq, c->sms);
+  double* scratch = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (p.scratch_doubles > 0 &&
+      (e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), sizeof(double) * p.scratch_doubles,
+                           st)) != cudaSuccess)
+    return cuda_fail(e, "device allocation");
+  e = launch_fp64_tiled(p, h->m, q, nq, w, scratch, c->err, st);
+  if (scratch) cudaFreeAsync(scratch, st);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "FP64 winding-number launch");
 }
 
 int wn_mixed_sort_queries(const double* q, int64_t nq, uint32_t* perm, void* stream) {

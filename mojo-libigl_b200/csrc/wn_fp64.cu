@@ -19,6 +19,7 @@
 
 #include "wn_common.cuh"
 #include "wn_internal.h"
+#include "wn_mixed.h"
 #include "wn_pair.cuh"
 
 namespace wn {
@@ -172,6 +173,135 @@ __global__ void sum_splits_kernel(const double* __restrict__ partial, int64_t ns
   w[qi] = s / kTwoPi;
 }
 
+// ---- FP64 over a prepared mesh, with corner reuse ---------------------------
+// Same bit-exact pair terms and argument-of-product sum, but the faces come from a
+// prepared mesh (wn_mixed.cu): Morton-ordered 64-face tiles whose faces are
+// ordered as strips, with a per-face code telling which corners equal a corner
+// of the previous face. a = v - o and |a| (three subtractions, three products,
+// two sums and a correctly rounded sqrt) depend only on the vertex and the
+// query, so a repeated corner is copied instead of recomputed: the same bits,
+// about 40% fewer FP64 instructions per pair on a typical mesh.
+struct Fp64TiledArgs {
+  const double* tri64;  // 9 x ld64, tile-major sorted soup
+  int64_t ld64;
+  const uint8_t* reuse;  // ld64 codes
+  int64_t ntiles;
+  const double* q;
+  int64_t nq;
+  int64_t tiles_per_split;
+  double* w;
+  double* partial;
+  int* err;
+};
+
+constexpr int kFp64TileBytes = 9 * kTileFaces * 8 + kTileFaces;  // coordinates + codes
+
+__device__ __forceinline__ Corner pick_corner(unsigned code, const Corner& c0, const Corner& c1,
+                                              const Corner& c2) {
+  return code == 0 ? c0 : (code == 1 ? c1 : c2);
+}
+
+template <int THREADS, int STAGES>
+__global__ void __launch_bounds__(THREADS) fp64_tiled_kernel(const Fp64TiledArgs a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* ring = smem_raw;  // [STAGES][kFp64TileBytes]
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + STAGES * kFp64TileBytes);
+  const int tid = threadIdx.x;
+  const int64_t qi = static_cast<int64_t>(blockIdx.x) * THREADS + tid;
+  const int64_t t_begin = static_cast<int64_t>(blockIdx.y) * a.tiles_per_split;
+  const int64_t t_left = a.ntiles - t_begin < a.tiles_per_split ? a.ntiles - t_begin
+                                                                 : a.tiles_per_split;
+  const int ntiles = static_cast<int>(t_left > 0 ? t_left : 0);
+  const bool valid = qi < a.nq;
+  const double ox = valid ? a.q[3 * qi] : 0.0, oy = valid ? a.q[3 * qi + 1] : 0.0,
+               oz = valid ? a.q[3 * qi + 2] : 0.0;
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  // Tile t: 9 coordinate rows of 64 doubles (512 bytes each, 16-byte aligned since
+  // ld64 is a multiple of 64) and 64 reuse codes.
+  auto issue = [&](int t) {
+    const int slot = t % STAGES;
+    unsigned char* dst = ring + slot * kFp64TileBytes;
+    const int64_t base = (t_begin + t) * kTileFaces;
+    mbar_arrive_expect_tx(&full[slot], kFp64TileBytes);
+#pragma unroll
+    for (int r = 0; r < 9; ++r)
+      bulk_g2s(dst + r * kTileFaces * 8, a.tri64 + r * a.ld64 + base, kTileFaces * 8, &full[slot]);
+    bulk_g2s(dst + 9 * kTileFaces * 8, a.reuse + base, kTileFaces, &full[slot]);
+  };
+  int issued = 0;
+  if (tid == 0)
+    for (; issued < min(STAGES, ntiles); ++issued) issue(issued);
+  ArgAcc acc;
+  argacc_init(acc);
+  Corner p0{0, 0, 0, 0}, p1{0, 0, 0, 0}, p2{0, 0, 0, 0};
+  bool failed = false;
+  int t = 0;
+  for (; t < ntiles; ++t) {
+    const int slot = t % STAGES;
+    const bool landed = mbar_wait(&full[slot], (t / STAGES) & 1, a.err);
+    if (!__syncthreads_and(landed)) {
+      failed = true;
+      break;
+    }
+    if (tid == 0 && t >= 1 && issued < ntiles) issue(issued++);
+    const double* s = reinterpret_cast<const double*>(ring + slot * kFp64TileBytes);
+    const uint8_t* codes = ring + slot * kFp64TileBytes + 9 * kTileFaces * 8;
+#pragma unroll 1
+    for (int j = 0; j < kTileFaces; ++j) {
+      const unsigned code = codes[j];
+      if (code == 0xffu) break;  // padding: the rest of the tile is empty
+      Corner c[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const unsigned ck = (code >> (2 * k)) & 3u;
+        if (ck == 3u) {
+          c[k] = corner_exact(ox, oy, oz, s[(3 * k) * kTileFaces + j], s[(3 * k + 1) * kTileFaces + j],
+                              s[(3 * k + 2) * kTileFaces + j]);
+        } else {
+          c[k] = pick_corner(ck, p0, p1, p2);
+        }
+      }
+      double det, denom;
+      face_exact(c[0], c[1], c[2], det, denom);
+      argacc_push(acc, denom, det);
+      p0 = c[0];
+      p1 = c[1];
+      p2 = c[2];
+    }
+  }
+  if (failed) {
+    if (tid == 0)
+      for (int u = t; u < issued; ++u) mbar_wait(&full[u % STAGES], (u / STAGES) & 1, nullptr);
+    __syncthreads();
+    return;
+  }
+  if (!valid) return;
+  double angle;
+  if (!acc.bad) {
+    angle = atan2(acc.zi, acc.zr) + static_cast<double>(acc.k) * kTwoPi;
+  } else {
+    // Recovery: one atan2 per pair over this slice, from global memory.
+    angle = 0.0;
+    for (int64_t f = t_begin * kTileFaces; f < (t_begin + ntiles) * kTileFaces; ++f) {
+      if (a.reuse[f] == 0xffu) continue;
+      const double* v = a.tri64 + f;
+      const int64_t L = a.ld64;
+      double det, denom;
+      pair_terms_exact(ox, oy, oz, v[0], v[L], v[2 * L], v[3 * L], v[4 * L], v[5 * L],
+                       v[6 * L], v[7 * L], v[8 * L], det, denom);
+      angle += atan2(det, denom);
+    }
+  }
+  if (gridDim.y == 1)
+    a.w[qi] = angle / kTwoPi;
+  else
+    a.partial[static_cast<int64_t>(blockIdx.y) * a.nq + qi] = angle;
+}
+
 template <int THREADS, int QPT, int TF, int STAGES, int MODE>
 cudaError_t launch_variant(const Fp64Plan& p, const Fp64Args& a, cudaStream_t stream) {
   auto kernel = fp64_forward_kernel<THREADS, QPT, TF, STAGES, MODE>;
@@ -205,6 +335,43 @@ Fp64Plan plan_fp64(int64_t nf, int64_t nq, int sms, int force_nsplit) {
   p.nsplit = std::max<int64_t>(1, (nf + p.f_chunk - 1) / p.f_chunk);
   p.scratch_doubles = p.nsplit > 1 ? p.nsplit * nq : 0;
   return p;
+}
+
+Fp64TiledPlan plan_fp64_tiled(int64_t ntiles, int64_t nq, int sms) {
+  Fp64TiledPlan p;
+  const int64_t qblocks = std::max<int64_t>(1, (nq + 127) / 128);
+  const int64_t target = static_cast<int64_t>(std::max(sms, 1)) * 8;
+  int64_t nsplit = qblocks < target ? (target + qblocks - 1) / qblocks : 1;
+  nsplit = std::max<int64_t>(1, std::min(nsplit, std::max<int64_t>(ntiles, 1)));
+  p.tiles_per_split = (std::max<int64_t>(ntiles, 1) + nsplit - 1) / nsplit;
+  p.nsplit = std::max<int64_t>(1, (std::max<int64_t>(ntiles, 1) + p.tiles_per_split - 1) /
+                                      p.tiles_per_split);
+  p.qblocks = qblocks;
+  p.scratch_doubles = p.nsplit > 1 ? p.nsplit * nq : 0;
+  return p;
+}
+
+cudaError_t launch_fp64_tiled(const Fp64TiledPlan& p, const MixedMesh& m, const double* q,
+                              int64_t nq, double* w, double* scratch, int* err,
+                              cudaStream_t stream) {
+  if (nq <= 0) return cudaSuccess;
+  if (!m.reuse || (p.nsplit > 1 && !scratch) || p.nsplit > 65535)
+    return cudaErrorInvalidValue;
+  constexpr int kThreads = 128, kStages = 3;
+  Fp64TiledArgs a{m.tri64, m.ld64, m.reuse, m.ntiles, q, nq, p.tiles_per_split, w, scratch, err};
+  auto kernel = fp64_tiled_kernel<kThreads, kStages>;
+  const size_t smem = static_cast<size_t>(kStages) * kFp64TileBytes + sizeof(uint64_t) * kStages;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  kernel<<<dim3(static_cast<unsigned>(p.qblocks), static_cast<unsigned>(p.nsplit)), kThreads,
+           smem, stream>>>(a);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if ((e = cudaGetLastError()) != cudaSuccess || p.nsplit == 1) return e;
+  sum_splits_kernel<<<static_cast<unsigned>((nq + 255) / 256), 256, 0, stream>>>(scratch,
+                                                                             p.nsplit, nq, w);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_fp64(const Fp64Plan& p, int mode, const double* tri, int64_t ld, int64_t nf,

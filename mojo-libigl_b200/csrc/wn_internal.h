@@ -21,6 +21,7 @@ cudaError_t probe_fma_tflops(int bits, int sms, cudaStream_t stream, double* tfl
 enum Fp64Mode : int {
   kFp64ArgProd = 0,  // bit-exact pair terms, argument-of-product accumulation
   kFp64Direct = 1,   // bit-exact pair terms, one atan2 per pair
+  kFp64Tiled = 2,    // kFp64ArgProd over a prepared mesh, repeated corners reused
 };
 
 struct Fp64Plan {
@@ -44,5 +45,15 @@ Fp64Plan plan_fp64(int64_t nf, int64_t nq, int sms, int force_nsplit = 0);
 cudaError_t launch_fp64(const Fp64Plan& plan, int mode, const double* tri, int64_t ld, int64_t nf,
                         const double* q, int64_t nq, double* w, double* scratch, int* err,
                         cudaStream_t stream);
+
+// ---- plain FP64 over a prepared mesh, with corner reuse (wn_fp64.cu) -------
+struct MixedMesh;
+struct Fp64TiledPlan {
+  int64_t qblocks = 1, nsplit = 1, tiles_per_split = 1, scratch_doubles = 0;
+};
+Fp64TiledPlan plan_fp64_tiled(int64_t ntiles, int64_t nq, int sms);
+cudaError_t launch_fp64_tiled(const Fp64TiledPlan& p, const MixedMesh& m, const double* q,
+                              int64_t nq, double* w, double* scratch, int* err,
+                              cudaStream_t stream);
 
 }  // namespace wn

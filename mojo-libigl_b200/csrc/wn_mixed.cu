@@ -164,8 +164,12 @@ __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
     const double* __restrict__ tri, int64_t ld, int64_t nf, const uint32_t* __restrict__ order,
     double kappa, unsigned char* __restrict__ tiles, double* __restrict__ tri64, int64_t ld64,
     uint32_t* __restrict__ face_of, const int64_t* __restrict__ tile_first,
-    const int32_t* __restrict__ tile_count) {
+    const int32_t* __restrict__ tile_count, uint8_t* __restrict__ reuse) {
   __shared__ double red[6][kTileFaces / 32];
+  __shared__ double sv[kTileFaces][9];  // the tile's faces, input order
+  __shared__ int64_t sf[kTileFaces];
+  __shared__ int sorder[kTileFaces];
+  __shared__ int sbest[kTileFaces / 32];
   const int j = threadIdx.x, warp = j >> 5, lane = j & 31;
   const int64_t tile = blockIdx.x;
   const int64_t first = tile_first ? tile_first[tile] : tile * kTileFaces;
@@ -176,15 +180,11 @@ __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
     const int64_t left = nf - first;
     cnt = static_cast<int>(left < kTileFaces ? (left > 0 ? left : 0) : kTileFaces);
   }
-  const int64_t slot = tile * kTileFaces + j;
-  const bool valid = j < cnt;
+  bool valid = j < cnt;
   double v[9];
-  const int64_t f = valid ? order[first + j] : 0;
+  int64_t f = valid ? order[first + j] : 0;
 #pragma unroll
   for (int r = 0; r < 9; ++r) v[r] = valid ? tri[r * ld + f] : 0.0;
-#pragma unroll
-  for (int r = 0; r < 9; ++r) tri64[r * ld64 + slot] = v[r];
-  face_of[slot] = valid ? static_cast<uint32_t>(f) : 0xffffffffu;
 
   // Tile bounding box -> centre.
   double lo[3], hi[3];
@@ -228,8 +228,7 @@ __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
     h2 = fmax(h2, dx * dx + dy * dy + dz * dz);
   }
   if (!valid) r2 = h2 = 0.0;
-  const double h_face = sqrt(h2);
-  double rt = warp_max(sqrt(r2)), ht = warp_max(h_face);
+  double rt = warp_max(sqrt(r2)), ht = warp_max(sqrt(h2));
   if (lane == 0) {
     red[0][warp] = rt;
     red[1][warp] = ht;
@@ -260,6 +259,77 @@ __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
     th->r = static_cast<float>(rt);
     th->h = static_cast<float>(ht);
   }
+  // Order the tile's faces as strips: each next face is the unvisited one that
+  // shares the most corners (bitwise-equal coordinates) with the current one.
+  // Consecutive faces then share corners, whose (v - o, |v - o|) the FP64 kernel
+  // reuses; reuse[slot] says, per corner, which corner of the previous face it
+  // equals (0..2) or 3 for a new one (0xff marks padding).
+#pragma unroll
+  for (int r = 0; r < 9; ++r) sv[j][r] = v[r];
+  sf[j] = f;
+  if (j == 0) sorder[0] = 0;
+  __syncthreads();
+  bool visited = (j == 0) || !valid;
+  int cur = 0;
+  for (int p = 1; p < cnt; ++p) {
+    int key = -1;
+    if (!visited) {
+      int shared = 0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+          shared += (__double_as_longlong(v[3 * k]) == __double_as_longlong(sv[cur][3 * m]) &&
+                     __double_as_longlong(v[3 * k + 1]) == __double_as_longlong(sv[cur][3 * m + 1]) &&
+                     __double_as_longlong(v[3 * k + 2]) == __double_as_longlong(sv[cur][3 * m + 2]))
+                        ? 1 : 0;
+      key = (min(shared, 3) << 7) | (127 - j);
+    }
+    for (int off = 16; off; off >>= 1) key = max(key, __shfl_xor_sync(0xffffffffu, key, off));
+    if (lane == 0) sbest[warp] = key;
+    __syncthreads();
+    int best = sbest[0];
+    for (int w = 1; w < kTileFaces / 32; ++w) best = max(best, sbest[w]);
+    cur = 127 - (best & 127);
+    if (j == cur) visited = true;
+    if (j == 0) sorder[p] = cur;
+    __syncthreads();
+  }
+  const int src = j < cnt ? sorder[j] : j;
+  const int prev = j >= 1 && j < cnt ? sorder[j - 1] : -1;
+  valid = j < cnt;
+#pragma unroll
+  for (int r = 0; r < 9; ++r) v[r] = sv[src][r];
+  f = sf[src];
+  const int64_t slot = tile * kTileFaces + j;
+#pragma unroll
+  for (int r = 0; r < 9; ++r) tri64[r * ld64 + slot] = valid ? v[r] : 0.0;
+  face_of[slot] = valid ? static_cast<uint32_t>(f) : 0xffffffffu;
+  if (reuse) {
+    unsigned code = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      unsigned match = 3;
+      if (prev >= 0)
+        for (int m = 2; m >= 0; --m)
+          if (__double_as_longlong(v[3 * k]) == __double_as_longlong(sv[prev][3 * m]) &&
+              __double_as_longlong(v[3 * k + 1]) == __double_as_longlong(sv[prev][3 * m + 1]) &&
+              __double_as_longlong(v[3 * k + 2]) == __double_as_longlong(sv[prev][3 * m + 2]))
+            match = static_cast<unsigned>(m);
+      code |= match << (2 * k);
+    }
+    reuse[slot] = valid ? static_cast<uint8_t>(code) : static_cast<uint8_t>(0xff);
+  }
+  double h2f = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int k2 = (k + 1) % 3;
+    const double dx = v[3 * k2] - v[3 * k], dy = v[3 * k2 + 1] - v[3 * k + 1],
+                 dz = v[3 * k2 + 2] - v[3 * k + 2];
+    h2f = fmax(h2f, dx * dx + dy * dy + dz * dz);
+  }
+  const double h_face = valid ? sqrt(h2f) : 0.0;
+
   FaceRec fr;
   const double ax = (v[0] - c[0]) * scale, ay = (v[1] - c[1]) * scale, az = (v[2] - c[2]) * scale;
   const double e1x = (v[3] - v[0]) * scale, e1y = (v[4] - v[1]) * scale,
@@ -581,7 +651,8 @@ cudaError_t mixed_prepare_mesh(const double* tri, int64_t ld, int64_t nf, double
     if (e != cudaSuccess) return e;
   }
   build_tiles_kernel<<<static_cast<unsigned>(ntiles), kTileFaces, 0, stream>>>(
-      tri, ld, nf, vals_out, kappa, m->tiles, m->tri64, m->ld64, m->face_of, nullptr, nullptr);
+      tri, ld, nf, vals_out, kappa, m->tiles, m->tri64, m->ld64, m->face_of, nullptr, nullptr,
+      m->reuse);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return cudaGetLastError();
 }
@@ -1061,6 +1132,7 @@ cudaError_t batch_create(BatchState* b, int64_t nmesh, const int64_t* nv, const 
                                        kTileBytes)) != cudaSuccess ||
       (e = dmalloc(&d->mesh.tri64, 9 * ld64)) != cudaSuccess ||
       (e = dmalloc(&d->mesh.face_of, ld64)) != cudaSuccess ||
+      (e = dmalloc(&d->mesh.reuse, ld64)) != cudaSuccess ||
       (e = dmalloc(&d->items, b->n_items)) != cudaSuccess ||
       (e = dmalloc(&d->info, nmesh)) != cudaSuccess ||
       (e = dmalloc(&d->counter, 1)) != cudaSuccess ||
@@ -1100,7 +1172,7 @@ void batch_destroy(BatchState* b) {
   void* ptrs[] = {d->F, d->face_mesh, d->query_mesh, d->tile_first, d->tile_count, d->tri,
                   d->fbox, d->qbox, d->fkeys_in, d->fkeys_out, d->fvals_in, d->fvals_out,
                   d->qkeys_in, d->qkeys_out, d->qvals_in, d->perm, d->sort_temp,
-                  d->mesh.tiles, d->mesh.tri64, d->mesh.face_of, d->items, d->info,
+                  d->mesh.tiles, d->mesh.tri64, d->mesh.face_of, d->mesh.reuse, d->items, d->info,
                   d->counter, d->partial};
   for (void* p : ptrs) cudaFree(p);
   delete d;
@@ -1131,7 +1203,7 @@ cudaError_t batch_forward(BatchState* b, const double* V, const double* q, doubl
       return e;
     build_tiles_kernel<<<static_cast<unsigned>(b->total_tiles), kTileFaces, 0, stream>>>(
         d->tri, b->ldt, b->total_nf, d->fvals_out, b->plan.kappa, d->mesh.tiles, d->mesh.tri64,
-        d->mesh.ld64, d->mesh.face_of, d->tile_first, d->tile_count);
+        d->mesh.ld64, d->mesh.face_of, d->tile_first, d->tile_count, d->mesh.reuse);
     g_launches.fetch_add(5, std::memory_order_relaxed);
   }
   if (b->total_nq == 0) return cudaGetLastError();

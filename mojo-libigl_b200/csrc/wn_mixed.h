@@ -45,6 +45,8 @@ struct MixedMesh {
   unsigned char* tiles = nullptr;  // ntiles * kTileBytes, 16-byte aligned
   double* tri64 = nullptr;         // 9 x ld64 sorted FP64 soup (ld64 = ntiles*kTileFaces)
   uint32_t* face_of = nullptr;     // ld64: sorted slot -> input face (0xffffffff = padding)
+  uint8_t* reuse = nullptr;        // ld64: per corner (2 bits) the previous face's equal corner
+                                   // (0..2) or 3 = new; 0xff = padding. May be null.
 };
 
 inline int64_t mixed_tiles(int64_t nf) { return nf > 0 ? (nf + kTileFaces - 1) / kTileFaces : 1; }
@@ -58,6 +60,9 @@ inline size_t mixed_tri64_bytes(int64_t nf) {
 }
 inline size_t mixed_face_of_bytes(int64_t nf) {
   return static_cast<size_t>(mixed_tiles(nf)) * kTileFaces * sizeof(uint32_t);
+}
+inline size_t mixed_reuse_bytes(int64_t nf) {
+  return static_cast<size_t>(mixed_tiles(nf)) * kTileFaces;
 }
 
 // Scratch needed by mixed_prepare_mesh (nf faces) and by mixed_forward (nq queries).

@@ -77,25 +77,42 @@ WN_HD double from_words(int32_t hi, uint32_t lo) {
 }
 #endif
 
+// One corner of a pair: a = V - o and la = |a|, bit-identical to capi.mojo:218-229.
+// These depend only on the vertex and the query, so a corner shared by consecutive
+// faces can be reused without changing any bit of the result.
+struct Corner {
+  double x, y, z, l;
+};
+
+WN_HD Corner corner_exact(double ox, double oy, double oz, double Vx, double Vy, double Vz) {
+  Corner c;
+  c.x = dsub(Vx, ox);
+  c.y = dsub(Vy, oy);
+  c.z = dsub(Vz, oz);
+  c.l = dsqrt(dadd(dadd(dmul(c.x, c.x), dmul(c.y, c.y)), dmul(c.z, c.z)));
+  return c;
+}
+
+// det and denom of a pair from its three corners, bit-identical to capi.mojo:230-234.
+WN_HD void face_exact(const Corner& a, const Corner& b, const Corner& c, double& det,
+                      double& denom) {
+  const double t0 = dmul(a.x, dsub(dmul(b.y, c.z), dmul(b.z, c.y)));
+  const double t1 = dmul(a.y, dsub(dmul(b.x, c.z), dmul(b.z, c.x)));
+  const double t2 = dmul(a.z, dsub(dmul(b.x, c.y), dmul(b.y, c.x)));
+  det = dadd(dsub(t0, t1), t2);
+  double d = dmul(dmul(a.l, b.l), c.l);
+  d = dadd(d, dmul(dadd(dadd(dmul(a.x, b.x), dmul(a.y, b.y)), dmul(a.z, b.z)), c.l));
+  d = dadd(d, dmul(dadd(dadd(dmul(b.x, c.x), dmul(b.y, c.y)), dmul(b.z, c.z)), a.l));
+  d = dadd(d, dmul(dadd(dadd(dmul(c.x, a.x), dmul(c.y, a.y)), dmul(c.z, a.z)), b.l));
+  denom = d;
+}
+
 // det and denom of one (triangle, query) pair, bit-identical to capi.mojo:218-235.
 WN_HD void pair_terms_exact(double ox, double oy, double oz, double Ax, double Ay, double Az,
                             double Bx, double By, double Bz, double Cx, double Cy, double Cz,
                             double& det, double& denom) {
-  const double ax = dsub(Ax, ox), ay = dsub(Ay, oy), az = dsub(Az, oz);
-  const double bx = dsub(Bx, ox), by = dsub(By, oy), bz = dsub(Bz, oz);
-  const double cx = dsub(Cx, ox), cy = dsub(Cy, oy), cz = dsub(Cz, oz);
-  const double la = dsqrt(dadd(dadd(dmul(ax, ax), dmul(ay, ay)), dmul(az, az)));
-  const double lb = dsqrt(dadd(dadd(dmul(bx, bx), dmul(by, by)), dmul(bz, bz)));
-  const double lc = dsqrt(dadd(dadd(dmul(cx, cx), dmul(cy, cy)), dmul(cz, cz)));
-  const double t0 = dmul(ax, dsub(dmul(by, cz), dmul(bz, cy)));
-  const double t1 = dmul(ay, dsub(dmul(bx, cz), dmul(bz, cx)));
-  const double t2 = dmul(az, dsub(dmul(bx, cy), dmul(by, cx)));
-  det = dadd(dsub(t0, t1), t2);
-  double d = dmul(dmul(la, lb), lc);
-  d = dadd(d, dmul(dadd(dadd(dmul(ax, bx), dmul(ay, by)), dmul(az, bz)), lc));
-  d = dadd(d, dmul(dadd(dadd(dmul(bx, cx), dmul(by, cy)), dmul(bz, cz)), la));
-  d = dadd(d, dmul(dadd(dadd(dmul(cx, ax), dmul(cy, ay)), dmul(cz, az)), lb));
-  denom = d;
+  face_exact(corner_exact(ox, oy, oz, Ax, Ay, Az), corner_exact(ox, oy, oz, Bx, By, Bz),
+             corner_exact(ox, oy, oz, Cx, Cy, Cz), det, denom);
 }
 
 // Running product of z_i = denom_i + i*det_i (see the file comment).

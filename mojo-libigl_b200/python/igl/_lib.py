@@ -59,6 +59,7 @@ _WN_SIGNATURES = {
     "wn_forward_mixed_host": ([P, P, P, I, I, ctypes.c_double], C_INT),
     "wn_mixed_mesh_create": ([P, I, I, ctypes.c_double, P, ctypes.POINTER(P)], C_INT),
     "wn_mixed_mesh_destroy": ([P], C_INT),
+    "wn_forward_fp64_mesh_device": ([P, P, I, P, P], C_INT),
     "wn_forward_mixed_device": ([P, P, I, P, P], C_INT),
     "wn_mixed_mesh_update": ([P, P, I, P], C_INT),
     "wn_mixed_sort_queries": ([P, I, P, P], C_INT),

@@ -17,7 +17,7 @@ from conftest import GOLDEN_CASES, load_golden, tetrahedron
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
-MODES = {"argprod": 0, "direct": 1}
+MODES = {"argprod": 0, "direct": 1, "tiled": 2}
 
 
 def gpu_host(tri, O, mode="argprod"):

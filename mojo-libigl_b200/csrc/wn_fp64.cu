@@ -201,20 +201,26 @@ __device__ __forceinline__ Corner pick_corner(unsigned code, const Corner& c0, c
   return code == 0 ? c0 : (code == 1 ? c1 : c2);
 }
 
-template <int THREADS, int STAGES>
+template <int THREADS, int QPT, int STAGES>
 __global__ void __launch_bounds__(THREADS) fp64_tiled_kernel(const Fp64TiledArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* ring = smem_raw;  // [STAGES][kFp64TileBytes]
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + STAGES * kFp64TileBytes);
   const int tid = threadIdx.x;
-  const int64_t qi = static_cast<int64_t>(blockIdx.x) * THREADS + tid;
+  const int64_t q_base = static_cast<int64_t>(blockIdx.x) * (THREADS * QPT);
   const int64_t t_begin = static_cast<int64_t>(blockIdx.y) * a.tiles_per_split;
   const int64_t t_left = a.ntiles - t_begin < a.tiles_per_split ? a.ntiles - t_begin
                                                                  : a.tiles_per_split;
   const int ntiles = static_cast<int>(t_left > 0 ? t_left : 0);
-  const bool valid = qi < a.nq;
-  const double ox = valid ? a.q[3 * qi] : 0.0, oy = valid ? a.q[3 * qi + 1] : 0.0,
-               oz = valid ? a.q[3 * qi + 2] : 0.0;
+  double ox[QPT], oy[QPT], oz[QPT];
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    const int64_t qi = q_base + k * THREADS + tid;
+    const bool valid = qi < a.nq;
+    ox[k] = valid ? a.q[3 * qi] : 0.0;
+    oy[k] = valid ? a.q[3 * qi + 1] : 0.0;
+    oz[k] = valid ? a.q[3 * qi + 2] : 0.0;
+  }
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
     fence_barrier_init();
@@ -235,9 +241,13 @@ __global__ void __launch_bounds__(THREADS) fp64_tiled_kernel(const Fp64TiledArgs
   int issued = 0;
   if (tid == 0)
     for (; issued < min(STAGES, ntiles); ++issued) issue(issued);
-  ArgAcc acc;
-  argacc_init(acc);
-  Corner p0{0, 0, 0, 0}, p1{0, 0, 0, 0}, p2{0, 0, 0, 0};
+  ArgAcc acc[QPT];
+  Corner p0[QPT], p1[QPT], p2[QPT];
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    argacc_init(acc[k]);
+    p0[k] = p1[k] = p2[k] = Corner{0, 0, 0, 0};
+  }
   bool failed = false;
   int t = 0;
   for (; t < ntiles; ++t) {
@@ -254,23 +264,25 @@ __global__ void __launch_bounds__(THREADS) fp64_tiled_kernel(const Fp64TiledArgs
     for (int j = 0; j < kTileFaces; ++j) {
       const unsigned code = codes[j];
       if (code == 0xffu) break;  // padding: the rest of the tile is empty
-      Corner c[3];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const unsigned ck = (code >> (2 * k)) & 3u;
-        if (ck == 3u) {
-          c[k] = corner_exact(ox, oy, oz, s[(3 * k) * kTileFaces + j], s[(3 * k + 1) * kTileFaces + j],
-                              s[(3 * k + 2) * kTileFaces + j]);
-        } else {
-          c[k] = pick_corner(ck, p0, p1, p2);
+      for (int k = 0; k < QPT; ++k) {
+        Corner c[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          const unsigned cm = (code >> (2 * m)) & 3u;
+          if (cm == 3u)
+            c[m] = corner_exact(ox[k], oy[k], oz[k], s[(3 * m) * kTileFaces + j],
+                                s[(3 * m + 1) * kTileFaces + j], s[(3 * m + 2) * kTileFaces + j]);
+          else
+            c[m] = pick_corner(cm, p0[k], p1[k], p2[k]);
         }
+        double det, denom;
+        face_exact(c[0], c[1], c[2], det, denom);
+        argacc_push(acc[k], denom, det);
+        p0[k] = c[0];
+        p1[k] = c[1];
+        p2[k] = c[2];
       }
-      double det, denom;
-      face_exact(c[0], c[1], c[2], det, denom);
-      argacc_push(acc, denom, det);
-      p0 = c[0];
-      p1 = c[1];
-      p2 = c[2];
     }
   }
   if (failed) {
@@ -279,27 +291,31 @@ __global__ void __launch_bounds__(THREADS) fp64_tiled_kernel(const Fp64TiledArgs
     __syncthreads();
     return;
   }
-  if (!valid) return;
-  double angle;
-  if (!acc.bad) {
-    angle = atan2(acc.zi, acc.zr) + static_cast<double>(acc.k) * kTwoPi;
-  } else {
-    // Recovery: one atan2 per pair over this slice, from global memory.
-    angle = 0.0;
-    for (int64_t f = t_begin * kTileFaces; f < (t_begin + ntiles) * kTileFaces; ++f) {
-      if (a.reuse[f] == 0xffu) continue;
-      const double* v = a.tri64 + f;
-      const int64_t L = a.ld64;
-      double det, denom;
-      pair_terms_exact(ox, oy, oz, v[0], v[L], v[2 * L], v[3 * L], v[4 * L], v[5 * L],
-                       v[6 * L], v[7 * L], v[8 * L], det, denom);
-      angle += atan2(det, denom);
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    const int64_t qi = q_base + k * THREADS + tid;
+    if (qi >= a.nq) continue;
+    double angle;
+    if (!acc[k].bad) {
+      angle = atan2(acc[k].zi, acc[k].zr) + static_cast<double>(acc[k].k) * kTwoPi;
+    } else {
+      // Recovery: one atan2 per pair over this slice, from global memory.
+      angle = 0.0;
+      for (int64_t f = t_begin * kTileFaces; f < (t_begin + ntiles) * kTileFaces; ++f) {
+        if (a.reuse[f] == 0xffu) continue;
+        const double* v = a.tri64 + f;
+        const int64_t L = a.ld64;
+        double det, denom;
+        pair_terms_exact(ox[k], oy[k], oz[k], v[0], v[L], v[2 * L], v[3 * L], v[4 * L],
+                         v[5 * L], v[6 * L], v[7 * L], v[8 * L], det, denom);
+        angle += atan2(det, denom);
+      }
     }
+    if (gridDim.y == 1)
+      a.w[qi] = angle / kTwoPi;
+    else
+      a.partial[static_cast<int64_t>(blockIdx.y) * a.nq + qi] = angle;
   }
-  if (gridDim.y == 1)
-    a.w[qi] = angle / kTwoPi;
-  else
-    a.partial[static_cast<int64_t>(blockIdx.y) * a.nq + qi] = angle;
 }
 
 template <int THREADS, int QPT, int TF, int STAGES, int MODE>
@@ -337,9 +353,12 @@ Fp64Plan plan_fp64(int64_t nf, int64_t nq, int sms, int force_nsplit) {
   return p;
 }
 
+constexpr int kTiledThreads = 128, kTiledQpt = 2, kTiledStages = 3;
+
 Fp64TiledPlan plan_fp64_tiled(int64_t ntiles, int64_t nq, int sms) {
   Fp64TiledPlan p;
-  const int64_t qblocks = std::max<int64_t>(1, (nq + 127) / 128);
+  const int64_t per = static_cast<int64_t>(kTiledThreads) * kTiledQpt;
+  const int64_t qblocks = std::max<int64_t>(1, (nq + per - 1) / per);
   const int64_t target = static_cast<int64_t>(std::max(sms, 1)) * 8;
   int64_t nsplit = qblocks < target ? (target + qblocks - 1) / qblocks : 1;
   nsplit = std::max<int64_t>(1, std::min(nsplit, std::max<int64_t>(ntiles, 1)));
@@ -357,9 +376,9 @@ cudaError_t launch_fp64_tiled(const Fp64TiledPlan& p, const MixedMesh& m, const 
   if (nq <= 0) return cudaSuccess;
   if (!m.reuse || (p.nsplit > 1 && !scratch) || p.nsplit > 65535)
     return cudaErrorInvalidValue;
-  constexpr int kThreads = 128, kStages = 3;
+  constexpr int kThreads = kTiledThreads, kStages = kTiledStages;
   Fp64TiledArgs a{m.tri64, m.ld64, m.reuse, m.ntiles, q, nq, p.tiles_per_split, w, scratch, err};
-  auto kernel = fp64_tiled_kernel<kThreads, kStages>;
+  auto kernel = fp64_tiled_kernel<kThreads, kTiledQpt, kStages>;
   const size_t smem = static_cast<size_t>(kStages) * kFp64TileBytes + sizeof(uint64_t) * kStages;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));

@@ -702,11 +702,16 @@ int wn_batch_destroy(void* batch) {
   return WN_OK;
 }
 
-// src/capi.mojo:945-947: 1 on success, 0 on failure (the shim raises).
+// src/capi.mojo:945-947: 1 on success, 0 on failure (the shim raises). Large
+// problems go through the prepared-mesh FP64 kernel (its ~2 ms preparation is
+// repaid above ~1e9 pairs), small ones through the streaming FP64 kernel; both
+// give pair terms bit-identical to the reference.
 int64_t mli_winding_gpu(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t nq) {
+  const bool large = nf >= 4096 && static_cast<double>(nf) * static_cast<double>(nq) >= 1e9 &&
+                     nf <= 0x7fffffffLL;
   return forward_fp64_host(reinterpret_cast<const double*>(tri),
                            reinterpret_cast<const double*>(q), reinterpret_cast<double*>(dst), nf,
-                           nq, kFp64ArgProd) == WN_OK
+                           nq, large ? kFp64Tiled : kFp64ArgProd) == WN_OK
              ? 1
              : 0;
 }

@@ -208,16 +208,34 @@ __global__ void gather_sorted_queries_kernel(const double* __restrict__ q,
 // Shared-memory layout of adjoint_mixed_kernel (dynamic, QC queries per chunk).
 template <int THREADS, int QC>
 struct MixedAdjointSmem {
-  float dO32[QC][3][THREADS];  // per-thread FP32 dL/do shares of far pairs (transposed)
+  float dO32[QC][3][THREADS];         // per-thread FP32 dL/do shares of far pairs (transposed)
+  double acc64[2][9][THREADS];        // per-face FP64 sums across chunks (thread-private columns)
   double red64[THREADS / 32][QC][3];  // per-warp FP64 shares of refined pairs
-  double4 sq[QC];                     // FP64 query + g
   double dsum[QC * 3];                // the chunk's dL/do sums before they go to global
+  double4 sq[QC];                     // FP64 query + g
   float4 sl[QC][4];                   // local scaled query per tile, w = 1 if far
   TileHeader th[4];
 };
 
+// One refined (near) pair in FP64: g * dOmega into the face's FP64 sums in shared
+// memory (thread-private column) and into go. Kept out of line: it is rare, and
+// inlined it would raise the register count of the whole FP32 loop.
+__device__ __noinline__ void refine_pair_grad(const double* __restrict__ tri64, int64_t ld64,
+                                              int64_t slot, double4 o, double* acc_col,
+                                              int stride, double* go) {
+  double v[9], gv[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+    v[r] = tri64[r * ld64 + slot];
+    gv[r] = 0.0;
+  }
+  pair_grad_fp64(o.x, o.y, o.z, v, o.w, true, gv, go);
+#pragma unroll
+  for (int r = 0; r < 9; ++r) acc_col[r * stride] += gv[r];
+}
+
 template <int THREADS, int QC>
-__global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAdjointArgs a) {
+__global__ void __launch_bounds__(THREADS, 3) adjoint_mixed_kernel(const MixedAdjointArgs a) {
   static_assert(THREADS == 2 * kTileFaces, "one thread per face of two tiles");
   constexpr int kTilesPerBlock = 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -244,12 +262,13 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAd
         sm.th[tid] = empty;
       }
     }
-    float fv[2][10];  // A, B, C (scaled local), thr
-    double scale[2];
+    // Face records: A, e1 = B - A, e2 = C - A, |e1|^2, |e2|^2, e1.e2 and the
+    // refinement threshold (FaceRec layout), scaled tile-local FP32.
+    float fa[2][3], fe1[2][3], fe2[2][3], fg[2][3], thr[2];
+    float sc[2];
     int64_t slot[2];
     bool valid[2];
     float acc32[2][9];
-    double acc64[2][9];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int64_t t = blk * kTilesPerBlock + 2 * k + half;
@@ -257,22 +276,22 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAd
       const TileHeader* th =
           reinterpret_cast<const TileHeader*>(a.tiles + (tile_ok ? t : 0) * kTileBytes);
       valid[k] = tile_ok && j < th->n;
-      scale[k] = tile_ok ? th->scale : 0.0;
+      sc[k] = tile_ok ? static_cast<float>(th->scale) : 0.f;
       slot[k] = (tile_ok ? t : 0) * kTileFaces + j;
       const float* fr = reinterpret_cast<const float*>(a.tiles + (tile_ok ? t : 0) * kTileBytes +
                                                        sizeof(TileHeader)) + 16 * j;
-      // Corners from the record's A, e1 = B - A, e2 = C - A; the threshold last.
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
-        fv[k][r] = valid[k] ? fr[r] : 0.f;
-        fv[k][3 + r] = valid[k] ? fr[r] + fr[3 + r] : 0.f;
-        fv[k][6 + r] = valid[k] ? fr[r] + fr[6 + r] : 0.f;
+        fa[k][r] = valid[k] ? fr[r] : 0.f;
+        fe1[k][r] = valid[k] ? fr[3 + r] : 0.f;
+        fe2[k][r] = valid[k] ? fr[6 + r] : 0.f;
+        fg[k][r] = valid[k] ? fr[12 + r] : 0.f;
       }
-      fv[k][9] = valid[k] ? fr[15] : 0.f;
+      thr[k] = valid[k] ? fr[15] : 0.f;
 #pragma unroll
       for (int r = 0; r < 9; ++r) {
         acc32[k][r] = 0.f;
-        acc64[k][r] = 0.0;
+        sm.acc64[k][r][tid] = 0.0;
       }
     }
     for (int64_t c0 = q_begin; c0 < q_end; c0 += QC) {
@@ -294,43 +313,41 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAd
       __syncthreads();
 #pragma unroll 1
       for (int jq = 0; jq < nc; ++jq) {
-        const double4 o = sm.sq[jq];
-        const float g = static_cast<float>(o.w);
-        float dof[3] = {0.f, 0.f, 0.f};
+        const float g = static_cast<float>(sm.sq[jq].w);
+        float dof0 = 0.f, dof1 = 0.f, dof2 = 0.f;
         double go[3] = {0.0, 0.0, 0.0};
         bool refined = false;
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
           const float4 l = sm.sl[jq][2 * k + half];
-          const float ax = fv[k][0] - l.x, ay = fv[k][1] - l.y, az = fv[k][2] - l.z;
-          const float bx = fv[k][3] - l.x, by = fv[k][4] - l.y, bz = fv[k][5] - l.z;
-          const float cx = fv[k][6] - l.x, cy = fv[k][7] - l.y, cz = fv[k][8] - l.z;
+          const float ax = fa[k][0] - l.x, ay = fa[k][1] - l.y, az = fa[k][2] - l.z;
           const float aa = fmaf(ax, ax, fmaf(ay, ay, az * az));
-          const float bb = fmaf(bx, bx, fmaf(by, by, bz * bz));
-          const float cc = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
-          const bool near = l.w == 0.f && fminf(aa, fminf(bb, cc)) < fv[k][9];
-          if (near) {
+          const float s1 = fmaf(ax, fe1[k][0], fmaf(ay, fe1[k][1], az * fe1[k][2]));
+          const float s2 = fmaf(ax, fe2[k][0], fmaf(ay, fe2[k][1], az * fe2[k][2]));
+          const float ab = aa + s1, ca = aa + s2;
+          const float bb = fmaf(2.f, s1, aa + fg[k][0]);
+          const float cc = fmaf(2.f, s2, aa + fg[k][1]);
+          const float bc = ab + (s2 + fg[k][2]);
+          if (l.w == 0.f && fminf(aa, fminf(bb, cc)) < thr[k]) {
             if (valid[k]) {
-              double v[9];
-#pragma unroll
-              for (int r = 0; r < 9; ++r) v[r] = a.tri64[r * a.ld64 + slot[k]];
-              pair_grad_fp64(o.x, o.y, o.z, v, o.w, true, acc64[k], go);
+              refine_pair_grad(a.tri64, a.ld64, slot[k], sm.sq[jq], &sm.acc64[k][0][tid], THREADS,
+                               go);
               refined = true;
             }
           } else if (valid[k]) {
-            float ra, rb, rc;
+            float ra, rb, rc, iab, ibc, ica;
             asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(ra) : "f"(aa));
             asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rb) : "f"(bb));
             asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(cc));
             const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
-            const float dab = fmaf(fmaf(ax, bx, fmaf(ay, by, az * bz)), rab, 1.f);
-            const float dbc = fmaf(fmaf(bx, cx, fmaf(by, cy, bz * cz)), rbc, 1.f);
-            const float dca = fmaf(fmaf(cx, ax, fmaf(cy, ay, cz * az)), rca, 1.f);
-            float iab, ibc, ica;
+            const float dab = fmaf(ab, rab, 1.f), dbc = fmaf(bc, rbc, 1.f),
+                        dca = fmaf(ca, rca, 1.f);
             asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(iab) : "f"(dab));
             asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ibc) : "f"(dbc));
             asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ica) : "f"(dca));
             const float wab = g * rab * iab, wbc = g * rbc * ibc, wca = g * rca * ica;
+            const float bx = ax + fe1[k][0], by = ay + fe1[k][1], bz = az + fe1[k][2];
+            const float cx = ax + fe2[k][0], cy = ay + fe2[k][1], cz = az + fe2[k][2];
             const float xab0 = ay * bz - az * by, xab1 = az * bx - ax * bz, xab2 = ax * by - ay * bx;
             const float xbc0 = by * cz - bz * cy, xbc1 = bz * cx - bx * cz, xbc2 = bx * cy - by * cx;
             const float xca0 = cy * az - cz * ay, xca1 = cz * ax - cx * az, xca2 = cx * ay - cy * ax;
@@ -345,16 +362,16 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAd
             acc32[k][6] -= fmaf(kC1, xbc0, kC2 * xca0);
             acc32[k][7] -= fmaf(kC1, xbc1, kC2 * xca1);
             acc32[k][8] -= fmaf(kC1, xbc2, kC2 * xca2);
-            const float sc = static_cast<float>(scale[k]);
-            const float sab = (kA1 + kB1) * sc, sbc = (kB2 + kC1) * sc, sca = (kC2 + kA2) * sc;
-            dof[0] = fmaf(sab, xab0, fmaf(sbc, xbc0, fmaf(sca, xca0, dof[0])));
-            dof[1] = fmaf(sab, xab1, fmaf(sbc, xbc1, fmaf(sca, xca1, dof[1])));
-            dof[2] = fmaf(sab, xab2, fmaf(sbc, xbc2, fmaf(sca, xca2, dof[2])));
+            const float sab = (kA1 + kB1) * sc[k], sbc = (kB2 + kC1) * sc[k],
+                        sca = (kC2 + kA2) * sc[k];
+            dof0 = fmaf(sab, xab0, fmaf(sbc, xbc0, fmaf(sca, xca0, dof0)));
+            dof1 = fmaf(sab, xab1, fmaf(sbc, xbc1, fmaf(sca, xca1, dof1)));
+            dof2 = fmaf(sab, xab2, fmaf(sbc, xbc2, fmaf(sca, xca2, dof2)));
           }
         }
-        sm.dO32[jq][0][tid] = dof[0];
-        sm.dO32[jq][1][tid] = dof[1];
-        sm.dO32[jq][2][tid] = dof[2];
+        sm.dO32[jq][0][tid] = dof0;
+        sm.dO32[jq][1][tid] = dof1;
+        sm.dO32[jq][2][tid] = dof2;
         // Refined pairs carry large, cancelling terms: reduce them in FP64.
         if (__any_sync(0xffffffffu, refined)) {
           for (int off = 16; off; off >>= 1) {
@@ -371,34 +388,35 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_mixed_kernel(const MixedAd
       }
       __syncthreads();
       // One warp per (query, component): FP32 shares summed in lane order, then the
-      // FP64 shares in warp order; the sum is added into this CTA's row.
+      // FP64 shares in warp order; then all threads add the sums into this CTA's row.
       for (int e = warp; e < nc * 3; e += THREADS / 32) {
         const int jq = e / 3, x = e % 3;
         const float4 v4 = reinterpret_cast<const float4*>(&sm.dO32[jq][x][0])[lane];
         float v = (v4.x + v4.y) + (v4.z + v4.w);
         for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
         if (lane == 0) {
-          double s = static_cast<double>(v);
+          double sum = static_cast<double>(v);
 #pragma unroll
-          for (int w = 0; w < THREADS / 32; ++w) s += sm.red64[w][jq][x];
-          sm.dsum[e] = s;
+          for (int w = 0; w < THREADS / 32; ++w) sum += sm.red64[w][jq][x];
+          sm.dsum[e] = sum;
         }
       }
-      __syncthreads();
-      for (int e = tid; e < nc * 3; e += THREADS) dO_row[c0 * 3 + e] += sm.dsum[e];
 #pragma unroll
       for (int k = 0; k < 2; ++k)
 #pragma unroll
         for (int r = 0; r < 9; ++r) {
-          acc64[k][r] += scale[k] * static_cast<double>(acc32[k][r]);
+          sm.acc64[k][r][tid] += static_cast<double>(sc[k]) * static_cast<double>(acc32[k][r]);
           acc32[k][r] = 0.f;
         }
+      __syncthreads();
+      for (int e = tid; e < nc * 3; e += THREADS) dO_row[c0 * 3 + e] += sm.dsum[e];
     }
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       if (!valid[k]) continue;
 #pragma unroll
-      for (int r = 0; r < 9; ++r) a.dF_part[(group * 9 + r) * a.ld64 + slot[k]] = acc64[k][r];
+      for (int r = 0; r < 9; ++r)
+        a.dF_part[(group * 9 + r) * a.ld64 + slot[k]] = sm.acc64[k][r][tid];
     }
   }
 }
@@ -597,6 +615,7 @@ __global__ void gather_vertex_kernel(const double* __restrict__ dtri, int64_t ld
 }
 
 constexpr int kAdjThreads = 128, kAdjFpt = 2, kAdjQc = 64;
+constexpr int kMixedAdjQc = 32;  // query chunk of the mixed adjoint (shared-memory budget)
 
 int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
@@ -736,8 +755,8 @@ cudaError_t adjoint_mixed(const AdjointPlan& p, const MixedMesh& m, const double
       q, gw, perm, nq, qs);
   MixedAdjointArgs a{m.tiles, m.ntiles, m.tri64, m.ld64, qs, nq,
                      p.blocks_per_range, p.queries_per_group, dO_part, dF_part};
-  auto kernel = adjoint_mixed_kernel<2 * kTileFaces, kAdjQc>;
-  const int smem = static_cast<int>(sizeof(MixedAdjointSmem<2 * kTileFaces, kAdjQc>));
+  auto kernel = adjoint_mixed_kernel<2 * kTileFaces, kMixedAdjQc>;
+  const int smem = static_cast<int>(sizeof(MixedAdjointSmem<2 * kTileFaces, kMixedAdjQc>));
   e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   kernel<<<dim3(static_cast<unsigned>(p.nranges), static_cast<unsigned>(p.ngroups)),

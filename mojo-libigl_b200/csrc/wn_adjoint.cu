@@ -351,19 +351,20 @@ __global__ void __launch_bounds__(THREADS, 3) adjoint_mixed_kernel(const MixedAd
             const float xab0 = ay * bz - az * by, xab1 = az * bx - ax * bz, xab2 = ax * by - ay * bx;
             const float xbc0 = by * cz - bz * cy, xbc1 = bz * cx - bx * cz, xbc2 = bx * cy - by * cx;
             const float xca0 = cy * az - cz * ay, xca1 = cz * ax - cx * az, xca2 = cx * ay - cy * ax;
-            const float kA1 = ra * wab, kA2 = ra * wca, kB1 = rb * wab, kB2 = rb * wbc;
-            const float kC1 = rc * wbc, kC2 = rc * wca;
-            acc32[k][0] -= fmaf(kA1, xab0, kA2 * xca0);
-            acc32[k][1] -= fmaf(kA1, xab1, kA2 * xca1);
-            acc32[k][2] -= fmaf(kA1, xab2, kA2 * xca2);
-            acc32[k][3] -= fmaf(kB1, xab0, kB2 * xbc0);
-            acc32[k][4] -= fmaf(kB1, xab1, kB2 * xbc1);
-            acc32[k][5] -= fmaf(kB1, xab2, kB2 * xbc2);
-            acc32[k][6] -= fmaf(kC1, xbc0, kC2 * xca0);
-            acc32[k][7] -= fmaf(kC1, xbc1, kC2 * xca1);
-            acc32[k][8] -= fmaf(kC1, xbc2, kC2 * xca2);
-            const float sab = (kA1 + kB1) * sc[k], sbc = (kB2 + kC1) * sc[k],
-                        sca = (kC2 + kA2) * sc[k];
+            // Negated coefficients: each of the 9 sums takes two FMAs.
+            const float nA1 = -ra * wab, nA2 = -ra * wca, nB1 = -rb * wab, nB2 = -rb * wbc;
+            const float nC1 = -rc * wbc, nC2 = -rc * wca;
+            acc32[k][0] = fmaf(nA1, xab0, fmaf(nA2, xca0, acc32[k][0]));
+            acc32[k][1] = fmaf(nA1, xab1, fmaf(nA2, xca1, acc32[k][1]));
+            acc32[k][2] = fmaf(nA1, xab2, fmaf(nA2, xca2, acc32[k][2]));
+            acc32[k][3] = fmaf(nB1, xab0, fmaf(nB2, xbc0, acc32[k][3]));
+            acc32[k][4] = fmaf(nB1, xab1, fmaf(nB2, xbc1, acc32[k][4]));
+            acc32[k][5] = fmaf(nB1, xab2, fmaf(nB2, xbc2, acc32[k][5]));
+            acc32[k][6] = fmaf(nC1, xbc0, fmaf(nC2, xca0, acc32[k][6]));
+            acc32[k][7] = fmaf(nC1, xbc1, fmaf(nC2, xca1, acc32[k][7]));
+            acc32[k][8] = fmaf(nC1, xbc2, fmaf(nC2, xca2, acc32[k][8]));
+            const float sab = -(nA1 + nB1) * sc[k], sbc = -(nB2 + nC1) * sc[k],
+                        sca = -(nC2 + nA2) * sc[k];
             dof0 = fmaf(sab, xab0, fmaf(sbc, xbc0, fmaf(sca, xca0, dof0)));
             dof1 = fmaf(sab, xab1, fmaf(sbc, xbc1, fmaf(sca, xca1, dof1)));
             dof2 = fmaf(sab, xab2, fmaf(sbc, xbc2, fmaf(sca, xca2, dof2)));
@@ -621,20 +622,38 @@ int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 }  // namespace
 
-AdjointPlan plan_adjoint(int64_t nf, int64_t nq, int sms) {
+// Split nblocks element blocks into ranges (grid.x) and nq queries into groups
+// (grid.y) so that the grid is a whole number of waves of `slots` resident CTAs.
+AdjointPlan plan_waves(int64_t nblocks, int64_t nq, int64_t slots, int64_t qc) {
   AdjointPlan p;
-  const int64_t block_faces = kAdjThreads * kAdjFpt;
-  const int64_t nblocks = std::max<int64_t>(1, cdiv(nf, block_faces));
-  const int64_t target = static_cast<int64_t>(std::max(sms, 1)) * 4;
+  nblocks = std::max<int64_t>(1, nblocks);
+  slots = std::max<int64_t>(1, slots);
   const int64_t nranges = std::min<int64_t>(nblocks, 16);
   p.blocks_per_range = cdiv(nblocks, nranges);
   p.nranges = cdiv(nblocks, p.blocks_per_range);
-  int64_t ngroups = std::max<int64_t>(1, cdiv(target, p.nranges));
-  ngroups = std::min(ngroups, std::max<int64_t>(1, cdiv(nq, kAdjQc)));
-  ngroups = std::min<int64_t>(ngroups, 65535);
+  const int64_t max_groups = std::max<int64_t>(1, std::min<int64_t>(cdiv(nq, qc), 65535));
+  // Two whole waves: nranges * ngroups <= 2 * slots, as close to it as possible, so
+  // that no wave runs nearly empty.
+  const int64_t ngroups = std::max<int64_t>(1, std::min(max_groups, (2 * slots) / p.nranges));
   p.queries_per_group = cdiv(std::max<int64_t>(nq, 1), ngroups);
   p.ngroups = cdiv(std::max<int64_t>(nq, 1), p.queries_per_group);
   return p;
+}
+
+int resident_ctas(const void* kernel, int threads, size_t smem, int sms) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  return per_sm * std::max(sms, 1);
+}
+
+AdjointPlan plan_adjoint(int64_t nf, int64_t nq, int sms) {
+  const int slots = resident_ctas(
+      reinterpret_cast<const void*>(adjoint_fp64_kernel<kAdjThreads, kAdjFpt, kAdjQc>),
+      kAdjThreads, 0, sms);
+  return plan_waves(cdiv(nf, kAdjThreads * kAdjFpt), nq, slots, kAdjQc);
 }
 
 size_t adjoint_scratch_bytes(const AdjointPlan& p, int64_t ld, int64_t nq) {
@@ -672,18 +691,10 @@ cudaError_t adjoint_fp64(const AdjointPlan& p, const double* tri, int64_t ld, in
 }
 
 AdjointPlan plan_adjoint_edges(int64_t ne, int64_t nq, int sms) {
-  AdjointPlan p;
-  const int64_t nblocks = std::max<int64_t>(1, cdiv(ne, kAdjThreads * kAdjFpt));
-  const int64_t target = static_cast<int64_t>(std::max(sms, 1)) * 4;
-  const int64_t nranges = std::min<int64_t>(nblocks, 16);
-  p.blocks_per_range = cdiv(nblocks, nranges);
-  p.nranges = cdiv(nblocks, p.blocks_per_range);
-  int64_t ngroups = std::max<int64_t>(1, cdiv(target, p.nranges));
-  ngroups = std::min(ngroups, std::max<int64_t>(1, cdiv(nq, kAdjQc)));
-  ngroups = std::min<int64_t>(ngroups, 65535);
-  p.queries_per_group = cdiv(std::max<int64_t>(nq, 1), ngroups);
-  p.ngroups = cdiv(std::max<int64_t>(nq, 1), p.queries_per_group);
-  return p;
+  const int slots = resident_ctas(
+      reinterpret_cast<const void*>(adjoint_edges_kernel<kAdjThreads, kAdjFpt, kAdjQc>),
+      kAdjThreads, 0, sms);
+  return plan_waves(cdiv(ne, kAdjThreads * kAdjFpt), nq, slots, kAdjQc);
 }
 
 size_t adjoint_edges_scratch_bytes(const AdjointPlan& p, int64_t le, int64_t nq) {
@@ -719,18 +730,11 @@ cudaError_t adjoint_edges(const AdjointPlan& p, const double* edges, int64_t le,
 }
 
 AdjointPlan plan_adjoint_mixed(int64_t ntiles, int64_t nq, int sms) {
-  AdjointPlan p;
-  const int64_t nblocks = std::max<int64_t>(1, cdiv(ntiles, 4));
-  const int64_t target = static_cast<int64_t>(std::max(sms, 1)) * 4;
-  const int64_t nranges = std::min<int64_t>(nblocks, 16);
-  p.blocks_per_range = cdiv(nblocks, nranges);
-  p.nranges = cdiv(nblocks, p.blocks_per_range);
-  int64_t ngroups = std::max<int64_t>(1, cdiv(target, p.nranges));
-  ngroups = std::min(ngroups, std::max<int64_t>(1, cdiv(nq, kAdjQc)));
-  ngroups = std::min<int64_t>(ngroups, 65535);
-  p.queries_per_group = cdiv(std::max<int64_t>(nq, 1), ngroups);
-  p.ngroups = cdiv(std::max<int64_t>(nq, 1), p.queries_per_group);
-  return p;
+  auto kernel = adjoint_mixed_kernel<2 * kTileFaces, kMixedAdjQc>;
+  const int smem = static_cast<int>(sizeof(MixedAdjointSmem<2 * kTileFaces, kMixedAdjQc>));
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const int slots = resident_ctas(reinterpret_cast<const void*>(kernel), 2 * kTileFaces, smem, sms);
+  return plan_waves(cdiv(ntiles, 4), nq, slots, kMixedAdjQc);
 }
 
 cudaError_t adjoint_mixed(const AdjointPlan& p, const MixedMesh& m, const double* q,

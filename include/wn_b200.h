@@ -73,6 +73,11 @@ int wn_device_memory(int64_t* free_bytes, int64_t* total_bytes); /* current devi
 /* Synchronise `stream` and report (then clear) device-side errors raised by
  * device entry points launched on it since the last check. */
 int wn_stream_check(void* stream);
+/* Failure-detection self-test: a kernel waits on a phase that nothing completes,
+ * gives up after `polls` bounded polls (1..2^24), reports it through the device
+ * error word, and returns. Expected result: WN_EDEVICE, with the context still
+ * usable. No fault, no trap, no hang. */
+int wn_selftest_bounded_wait(int64_t polls);
 /* Number of kernels this library has launched since it was loaded. */
 int64_t wn_launch_count(void);
 /* Measured FMA-pipe peak of the current device in TFLOP/s (FMA = 2 flops),

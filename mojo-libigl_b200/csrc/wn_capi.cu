@@ -98,6 +98,15 @@ DeviceCtx* context(int* code) {
     *code = cuda_fail(e, "device context setup");
     return nullptr;
   }
+  // Keep memory freed by cudaFreeAsync in the device's pool across synchronisations
+  // (the default threshold of 0 hands it back to the driver at every sync, and the
+  // next stream-ordered allocation of the same scratch maps it again).
+  cudaMemPool_t pool = nullptr;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
   c.ready = true;
   return &c;
 }
@@ -300,6 +309,17 @@ int wn_device_memory(int64_t* free_bytes, int64_t* total_bytes) {
   if (free_bytes) *free_bytes = static_cast<int64_t>(f);
   if (total_bytes) *total_bytes = static_cast<int64_t>(t);
   return WN_OK;
+}
+
+int wn_selftest_bounded_wait(int64_t polls) {
+  if (polls < 1 || polls > (int64_t(1) << 24)) return fail(WN_EINVAL, "polls must be in [1, 2^24]");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  cudaError_t e = launch_wait_selftest(static_cast<uint32_t>(polls), c->err, c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "wait self-test launch");
+  return collect_device_error(c, c->stream);
 }
 
 int wn_stream_check(void* stream) {

@@ -14,6 +14,11 @@ void record_error(const char* message);
 // Kernels launched by this library since load (wn_launch_count()).
 extern std::atomic<int64_t> g_launches;
 
+// Failure-path self-test (wn_probe.cu): one CTA waits on an mbarrier phase that no
+// copy will complete, with a `polls` limit; the wait runs out, the kernel sets the
+// timeout bit of `err` and returns.
+cudaError_t launch_wait_selftest(uint32_t polls, int* err, cudaStream_t stream);
+
 // FMA-pipe peak probe (wn_probe.cu): TFLOP/s for bits = 64 or 32.
 cudaError_t probe_fma_tflops(int bits, int sms, cudaStream_t stream, double* tflops);
 

@@ -8,6 +8,7 @@
 
 #include <cstdint>
 
+#include "wn_common.cuh"
 #include "wn_internal.h"
 
 namespace wn {
@@ -55,7 +56,27 @@ cudaError_t run_probe(int sms, int iters, cudaStream_t stream, float* ms) {
   return e;
 }
 
+// The mbarrier expects one arrival plus 16 transaction bytes; the thread arrives
+// and announces the bytes but no copy ever delivers them, so the phase never
+// completes and the bounded wait gives up after `polls` polls.
+__global__ void wait_selftest_kernel(uint32_t polls, int* err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  fence_barrier_init();
+  mbar_arrive_expect_tx(&bar, 16);
+  for (uint32_t i = 0; i < polls; ++i)
+    if (mbar_try_wait(&bar, 0)) return;  // cannot happen: nothing completes the bytes
+  atomicOr(err, kErrWaitTimeout);
+}
+
 }  // namespace
+
+cudaError_t launch_wait_selftest(uint32_t polls, int* err, cudaStream_t stream) {
+  wait_selftest_kernel<<<1, 32, 0, stream>>>(polls, err);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
 
 // FMA throughput in TFLOP/s (FMA = 2 flops) for precision 64 or 32.
 cudaError_t probe_fma_tflops(int bits, int sms, cudaStream_t stream, double* tflops) {

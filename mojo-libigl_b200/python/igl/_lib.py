@@ -52,6 +52,7 @@ _WN_SIGNATURES = {
     "wn_device_count": ([], C_INT),
     "wn_device_memory": ([ctypes.POINTER(I), ctypes.POINTER(I)], C_INT),
     "wn_stream_check": ([P], C_INT),
+    "wn_selftest_bounded_wait": ([I], C_INT),
     "wn_launch_count": ([], I),
     "wn_probe_fma_tflops": ([C_INT, ctypes.POINTER(ctypes.c_double)], C_INT),
     "wn_forward_fp64_host": ([P, P, P, I, I, C_INT], C_INT),

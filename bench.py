@@ -455,17 +455,20 @@ def gpu_arm(args):
     peak = ctypes.c_double(0.0)
     check(handle.wn_probe_fma_tflops(bits, ctypes.byref(peak)))
     achieved = FLOPS_PER_PAIR * pairs / t_kernel / 1e12
-    kname = "mixed_forward_kernel" if headline == "mixed" else "fp64_forward_kernel"
+    kname = "mixed_forward_kernel" if headline == "mixed" else "fp64_tiled_kernel"
     traffic = None
-    traffic_file = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(traffic_file):
-        rec = json.load(open(traffic_file)).get(kname)
-        if rec:
-            traffic = rec["bytes_per_launch_full"]
+    traffic_file = os.path.join(ROOT, "profiles", "dram_traffic_full_size.txt")
+    if os.path.exists(traffic_file) and nf == 327680 and nq == 1 << 20:
+        for line in open(traffic_file):
+            parts = line.split()
+            if len(parts) == 4 and parts[0] == kname:
+                traffic = int(parts[1]) + int(parts[2])
     roofline = {
         "bound": f"fp{bits}", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
         "frac": achieved / peak.value if peak.value else None, "traffic": traffic,
         "kernel": kname, "kernel_ms": t_kernel * 1e3,
+        "traffic_source": "profiles/dram_traffic_full_size.txt (one-pass ncu capture of the "
+                          "same kernel at this size)" if traffic else None,
         "peak_source": f"measured live on this GPU: FP{bits} FMA-chain probe "
                        "(wn_probe_fma_tflops), FMA = 2 flops",
         "flops_per_pair": FLOPS_PER_PAIR,

@@ -513,20 +513,8 @@ __global__ void __launch_bounds__(THREADS, 5) mixed_forward_kernel(const MixedAr
     oz[k] = a.nq > 0 ? a.q[3 * i + 2] : 0.0;
   }
 
-  // Ring slots are released per warp, not per CTA: each warp waits only for the
-  // tile it needs next, and the last warp to finish with a slot (a shared-memory
-  // counter) issues that slot's next bulk copy. Warps on the fast path never wait
-  // for warps refining near-surface pairs.
-  uint32_t* relcnt = reinterpret_cast<uint32_t*>(full + STAGES);
-  __shared__ int s_issued;
-  constexpr int kWarps = THREADS / 32;
-  const int lane = tid & 31;
   if (tid == 0) {
-    for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full[s], 1);
-      relcnt[s] = 0;
-    }
-    s_issued = 0;
+    for (int s = 0; s < STAGES; ++s) mbar_init(&full[s], 1);
     fence_barrier_init();
   }
   __syncthreads();
@@ -538,10 +526,10 @@ __global__ void __launch_bounds__(THREADS, 5) mixed_forward_kernel(const MixedAr
     mbar_arrive_expect_tx(&full[slot], kTileBytes);
     bulk_g2s(ring + slot * kTileBytes, a.tiles + (t_begin + t) * kTileBytes, kTileBytes,
              &full[slot]);
-    atomicAdd(&s_issued, 1);
   };
+  int issued = 0;
   if (tid == 0)
-    for (int u = 0; u < min(STAGES, ntiles); ++u) issue(u);
+    for (; issued < min(STAGES, ntiles); ++issued) issue(issued);
 
   float hi[QPT], lo[QPT];
   double s64[QPT];
@@ -553,36 +541,22 @@ __global__ void __launch_bounds__(THREADS, 5) mixed_forward_kernel(const MixedAr
   unsigned refined = 0, careful_tiles = 0;
 
   bool failed = false;
-  for (int t = 0; t < ntiles; ++t) {
+  int t = 0;
+  for (; t < ntiles; ++t) {
     const int slot = t % STAGES;
-    const bool landed =
-        __all_sync(0xffffffffu, mbar_wait(&full[slot], (t / STAGES) & 1, a.err));
-    if (!landed) {
+    const bool landed = mbar_wait(&full[slot], (t / STAGES) & 1, a.err);
+    if (!__syncthreads_and(landed)) {
       failed = true;
       break;
     }
+    if (tid == 0 && t >= 1 && issued < ntiles) issue(issued++);
     mixed_tile<QPT>(ring + slot * kTileBytes, (t_begin + t) * kTileFaces, a.tri64, a.ld64, ox, oy,
                     oz, qidx, hi, lo, s64, refined, careful_tiles);
-    __syncwarp();
-    if (lane == 0) {
-      __threadfence_block();  // this warp's reads of the slot precede its release
-      if (atomicAdd(&relcnt[slot], 1u) == kWarps - 1) {
-        relcnt[slot] = 0;
-        __threadfence_block();
-        if (t + STAGES < ntiles) {
-          // Every warp's reads of the slot precede this bulk copy into it.
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          issue(t + STAGES);
-        }
-      }
-    }
   }
 
-  if (__syncthreads_or(failed)) {
-    // Leave no bulk copy in flight into this CTA's shared memory.
+  if (failed) {
     if (tid == 0)
-      for (int u = max(0, s_issued - STAGES); u < s_issued; ++u)
-        mbar_wait(&full[u % STAGES], (u / STAGES) & 1, nullptr);
+      for (int u = t; u < issued; ++u) mbar_wait(&full[u % STAGES], (u / STAGES) & 1, nullptr);
     __syncthreads();
     return;
   }
@@ -619,8 +593,7 @@ constexpr int kMixedThreads = 128, kMixedQpt = 2, kMixedStages = 4;
 template <int THREADS, int QPT, int STAGES>
 cudaError_t launch_mixed_variant(const MixedArgs& a, int64_t nsplit, cudaStream_t stream) {
   auto kernel = mixed_forward_kernel<THREADS, QPT, STAGES>;
-  const size_t smem = static_cast<size_t>(STAGES) * kTileBytes + sizeof(uint64_t) * STAGES +
-                      sizeof(uint32_t) * STAGES;
+  const size_t smem = static_cast<size_t>(STAGES) * kTileBytes + sizeof(uint64_t) * STAGES;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;

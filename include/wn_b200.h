@@ -59,7 +59,19 @@ void mli_winding(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t nq, in
  * Runs the plain FP64 kernel on the current CUDA device. */
 int64_t mli_winding_gpu(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t nq);
 
-/* The reference's other eleven exports (src/capi.mojo:923-937, 950-1007) are
+/* Replaces src/capi.mojo:950-959 `mli_aabb_squared_distance(p, v, f, boxes,
+ * nodes, order, sqrd, indices, closest, stack, np, nnodes, q0, q1)` (every
+ * argument an int64 host address or size, python/igl/_lib.py:23): CPU closest
+ * point of queries [q0, q1) over the tree arrays of python/igl/__init__.py:
+ * 286-319 (boxes nnodes x 6, nodes nnodes x 4, order nf), writing sqrd[qi],
+ * indices[qi] and closest[3*qi..3*qi+2]; `stack` holds at least depth + 1
+ * int64. Reentrant over disjoint spans, each with its own stack. */
+void mli_aabb_squared_distance(int64_t p, int64_t v, int64_t f, int64_t boxes, int64_t nodes,
+                               int64_t order, int64_t sqrd, int64_t indices, int64_t closest,
+                               int64_t stack, int64_t np, int64_t nnodes, int64_t q0,
+                               int64_t q1);
+
+/* The reference's other ten exports (src/capi.mojo:923-937, 962-1007) are
  * exported under the same names so the reference shim's loader
  * (python/igl/_lib.py:122-130) resolves every symbol; they are outside this
  * library's scope and abort the process with a message if called. */
@@ -200,6 +212,56 @@ int wn_backward_edges_device(const double* edges, int64_t le, int64_t ne, const 
 int wn_gather_vertex_grad_device(const double* grad, int64_t ld, int corners,
                                  const int64_t* indptr, const int64_t* entries, int64_t nv,
                                  double* dV, void* stream);
+
+/* ---- closest points over the median-split hierarchy ---------------------
+ * V: nv x 3 doubles; F: nf x 3 int64; P: np x 3 doubles. Tree arrays as the
+ * reference's python/igl/__init__.py:286-319 `_build_aabb` returns them:
+ * boxes nnodes x 6 (lo xyz, hi xyz), nodes nnodes x 4 (left, right, start,
+ * count; count > 0 marks a leaf of order[start:start+count]), order nf, nodes
+ * in preorder. Results per point: sqrd (squared distance), index (face) and
+ * closest (3 doubles), bit-identical to mli_aabb_squared_distance; with no
+ * faces, 1e300, -1 and (0, 0, 0). */
+
+/* Nodes of the tree over nf faces with at most leaf_size faces per leaf (the
+ * reference uses 8); 0 for nf = 0. No reference counterpart. */
+int64_t wn_aabb_node_count(int64_t nf, int64_t leaf_size);
+
+/* Replaces python/igl/__init__.py:286-319 `_build_aabb(vertices, faces,
+ * leaf_size)`: fills boxes (wn_aabb_node_count x 6), nodes (x 4) and order
+ * (nf) with the same tree, and *stack_size with depth + 1 (0 for nf = 0).
+ * Host memory; builds subtrees on up to `threads` threads (<= 0: all cores). */
+int wn_aabb_build(const double* V, int64_t nv, const int64_t* F, int64_t nf, int64_t leaf_size,
+                  double* boxes, int64_t* nodes, int64_t* order, int64_t* stack_size,
+                  int threads);
+
+/* Uploads a tree (host arrays above) to the current device: *tree receives a
+ * handle. The arrays are validated (children after their parent and inside
+ * the tree, leaf ranges inside order, order a list of faces, depth + 1 <= 64).
+ * No reference counterpart (the reference has no device tree). */
+int wn_aabb_create(const double* V, int64_t nv, const int64_t* F, int64_t nf,
+                   const double* boxes, const int64_t* nodes, const int64_t* order,
+                   int64_t nnodes, void** tree);
+int wn_aabb_destroy(void* tree);
+
+/* Closest points of np device-resident points (device outputs). Asynchronous
+ * on `stream`. No reference counterpart. */
+int wn_aabb_squared_distance_device(void* tree, const double* P, int64_t np, double* sqrd,
+                                    int64_t* index, double* closest, void* stream);
+
+/* Same with host buffers: copy in, traverse, copy out, synchronise. The GPU
+ * counterpart of mli_aabb_squared_distance over all points. */
+int wn_aabb_squared_distance_host(void* tree, const double* P, int64_t np, double* sqrd,
+                                  int64_t* index, double* closest);
+
+/* Signed distance by the winding-number sign (no reference counterpart):
+ * s[i] = -sqrt(sqrd) where |W(P_i)| > 1/2, else +sqrt(sqrd); W comes from the
+ * winding-number mesh `mesh` (wn_mixed_mesh_create over the same faces) with
+ * precision 0 = FP64 (wn_forward_fp64_mesh_device) or 1 = mixed
+ * (wn_forward_mixed_device) and is written to w (np doubles). index and
+ * closest as for wn_aabb_squared_distance_device. Device buffers, async. */
+int wn_signed_distance_device(void* tree, void* mesh, int precision, const double* P,
+                              int64_t np, double* s, int64_t* index, double* closest, double* w,
+                              void* stream);
 
 #ifdef __cplusplus
 }

@@ -14,8 +14,10 @@
 #include <cstdlib>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/wn_b200.h"
+#include "wn_aabb.h"
 #include "wn_adjoint.h"
 #include "wn_batch.h"
 #include "wn_internal.h"
@@ -259,7 +261,8 @@ int forward_mixed_host(const double* tri, const double* q, double* w, int64_t nf
 [[noreturn]] void out_of_scope(const char* name) {
   std::fprintf(stderr,
                "libwn_b200: %s is not provided: this library implements only the "
-               "winding-number path (mli_winding, mli_winding_gpu)\n",
+               "winding-number and closest-point paths (mli_winding, mli_winding_gpu, "
+               "mli_aabb_squared_distance)\n",
                name);
   std::abort();
 }
@@ -722,6 +725,190 @@ int wn_batch_destroy(void* batch) {
   return WN_OK;
 }
 
+// ---- closest points -------------------------------------------------------
+namespace {
+
+struct AabbHandle {
+  AabbDeviceTree t;
+  int device = -1;
+};
+
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+// Bytes of the Morton permutation + its sort scratch for np points (0 below
+// the sorting threshold).
+size_t aabb_sort_bytes(int64_t np) {
+  return np >= kAabbSortMin ? align256(sizeof(uint32_t) * np) + mixed_sort_scratch_bytes(np) : 0;
+}
+
+// Sorts (when np is large enough) and traverses; scratch holds aabb_sort_bytes(np).
+cudaError_t aabb_run(const AabbHandle* h, const double* P, int64_t np, double* sqrd,
+                     int64_t* index, double* closest, void* scratch, int* err, cudaStream_t st) {
+  uint32_t* perm = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (np >= kAabbSortMin) {
+    perm = static_cast<uint32_t*>(scratch);
+    unsigned char* rest = static_cast<unsigned char*>(scratch) + align256(sizeof(uint32_t) * np);
+    if ((e = mixed_sort_queries(P, np, perm, rest, mixed_sort_scratch_bytes(np), st)) !=
+        cudaSuccess)
+      return e;
+  }
+  return aabb_query(h->t, P, np, perm, sqrd, index, closest, err, st);
+}
+
+int check_points(const void* tree, int64_t np) {
+  if (!tree) return fail(WN_EINVAL, "null tree");
+  if (np < 0 || np > 0x7fffffffLL) return fail(WN_EINVAL, "bad np=%lld", (long long)np);
+  return WN_OK;
+}
+
+}  // namespace
+
+int64_t wn_aabb_node_count(int64_t nf, int64_t leaf_size) {
+  return leaf_size < 1 ? -1 : aabb_node_count(nf, leaf_size);
+}
+
+int wn_aabb_build(const double* V, int64_t nv, const int64_t* F, int64_t nf, int64_t leaf_size,
+                  double* boxes, int64_t* nodes, int64_t* order, int64_t* stack_size,
+                  int threads) {
+  if (!stack_size) return fail(WN_EINVAL, "null stack_size");
+  const char* why = "";
+  const int64_t s = aabb_build(V, nv, F, nf, leaf_size, boxes, nodes, order, threads, &why);
+  if (s < 0) return fail(WN_EINVAL, "cannot build the tree: %s", why);
+  *stack_size = s;
+  return WN_OK;
+}
+
+int wn_aabb_create(const double* V, int64_t nv, const int64_t* F, int64_t nf,
+                   const double* boxes, const int64_t* nodes, const int64_t* order,
+                   int64_t nnodes, void** tree) {
+  if (!tree) return fail(WN_EINVAL, "null output handle");
+  *tree = nullptr;
+  if (nv < 0 || nf < 0 || nnodes < 0) return fail(WN_EINVAL, "negative size");
+  if (nnodes > 0 && (!V || !F || !boxes || !nodes || !order))
+    return fail(WN_EINVAL, "null pointer");
+  std::vector<AabbNodeRec> nrec(static_cast<size_t>(nnodes));
+  std::vector<AabbTriRec> trec(static_cast<size_t>(nnodes > 0 ? nf : 0));
+  const char* why = "";
+  const int64_t depth =
+      aabb_pack(V, nv, F, nf, boxes, nodes, order, nnodes, nrec.data(), trec.data(), &why);
+  if (depth < 0) return fail(WN_EINVAL, "invalid tree: %s", why);
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  if (!context(&code)) return code;
+  AabbHandle* h = new AabbHandle();
+  cudaGetDevice(&h->device);
+  h->t.nnodes = nnodes;
+  h->t.nleaf_faces = static_cast<int64_t>(trec.size());
+  h->t.depth = static_cast<int>(depth);
+  if (nnodes > 0) {
+    for (int k = 0; k < 6; ++k) h->t.root[k] = boxes[k];
+    cudaError_t e;
+    if ((e = cudaMalloc(&h->t.nodes, sizeof(AabbNodeRec) * nrec.size())) != cudaSuccess ||
+        (e = cudaMalloc(&h->t.tris, sizeof(AabbTriRec) * trec.size())) != cudaSuccess ||
+        (e = cudaMemcpy(h->t.nodes, nrec.data(), sizeof(AabbNodeRec) * nrec.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(h->t.tris, trec.data(), sizeof(AabbTriRec) * trec.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess) {
+      cudaFree(h->t.nodes);
+      cudaFree(h->t.tris);
+      delete h;
+      return cuda_fail(e, "device tree upload");
+    }
+  }
+  *tree = h;
+  return WN_OK;
+}
+
+int wn_aabb_destroy(void* tree) {
+  if (!tree) return WN_OK;
+  AabbHandle* h = static_cast<AabbHandle*>(tree);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(h->device);
+  cudaDeviceSynchronize();
+  cudaFree(h->t.nodes);
+  cudaFree(h->t.tris);
+  cudaSetDevice(prev);
+  delete h;
+  return WN_OK;
+}
+
+int wn_aabb_squared_distance_device(void* tree, const double* P, int64_t np, double* sqrd,
+                                    int64_t* index, double* closest, void* stream) {
+  if (int code = check_points(tree, np)) return code;
+  if (np == 0) return WN_OK;
+  if (!P || !sqrd || !index || !closest) return fail(WN_EINVAL, "null pointer");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t sb = aabb_sort_bytes(np);
+  void* scratch = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (sb && (e = cudaMallocAsync(&scratch, sb, st)) != cudaSuccess)
+    return cuda_fail(e, "device allocation");
+  e = aabb_run(static_cast<const AabbHandle*>(tree), P, np, sqrd, index, closest, scratch, c->err,
+               st);
+  if (scratch) cudaFreeAsync(scratch, st);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "closest-point launch");
+}
+
+int wn_aabb_squared_distance_host(void* tree, const double* P, int64_t np, double* sqrd,
+                                  int64_t* index, double* closest) {
+  if (int code = check_points(tree, np)) return code;
+  if (np == 0) return WN_OK;
+  if (!P || !sqrd || !index || !closest) return fail(WN_EINVAL, "null pointer");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  const size_t out_bytes = align256(sizeof(int64_t) * np) + align256(sizeof(double) * 3 * np);
+  cudaError_t e;
+  if ((e = c->q.ensure(sizeof(double) * 3 * np)) != cudaSuccess ||
+      (e = c->w.ensure(sizeof(double) * np)) != cudaSuccess ||
+      (e = c->scratch.ensure(out_bytes + aabb_sort_bytes(np))) != cudaSuccess)
+    return cuda_fail(e, "device allocation");
+  unsigned char* s = static_cast<unsigned char*>(c->scratch.ptr);
+  int64_t* index_d = reinterpret_cast<int64_t*>(s);
+  double* closest_d = reinterpret_cast<double*>(s + align256(sizeof(int64_t) * np));
+  double* P_d = static_cast<double*>(c->q.ptr);
+  double* sqrd_d = static_cast<double*>(c->w.ptr);
+  if ((e = cudaMemcpyAsync(P_d, P, sizeof(double) * 3 * np, cudaMemcpyHostToDevice,
+                           c->stream)) != cudaSuccess)
+    return cuda_fail(e, "copy of the points");
+  if ((e = aabb_run(static_cast<const AabbHandle*>(tree), P_d, np, sqrd_d, index_d, closest_d,
+                    s + out_bytes, c->err, c->stream)) != cudaSuccess)
+    return cuda_fail(e, "closest-point launch");
+  if ((e = cudaMemcpyAsync(sqrd, sqrd_d, sizeof(double) * np, cudaMemcpyDeviceToHost,
+                           c->stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(index, index_d, sizeof(int64_t) * np, cudaMemcpyDeviceToHost,
+                           c->stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(closest, closest_d, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost,
+                           c->stream)) != cudaSuccess)
+    return cuda_fail(e, "copy of the results");
+  return collect_device_error(c, c->stream);
+}
+
+int wn_signed_distance_device(void* tree, void* mesh, int precision, const double* P,
+                              int64_t np, double* s, int64_t* index, double* closest, double* w,
+                              void* stream) {
+  if (int code = check_points(tree, np)) return code;
+  if (!mesh) return fail(WN_EINVAL, "null mesh");
+  if (precision != 0 && precision != 1) return fail(WN_EINVAL, "bad precision %d", precision);
+  if (np == 0) return WN_OK;
+  if (!w) return fail(WN_EINVAL, "null pointer");
+  if (int code = wn_aabb_squared_distance_device(tree, P, np, s, index, closest, stream))
+    return code;
+  if (int code = precision == 0 ? wn_forward_fp64_mesh_device(mesh, P, np, w, stream)
+                                : wn_forward_mixed_device(mesh, P, np, w, stream))
+    return code;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  const cudaError_t e = signed_from_winding(w, s, np, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "signed-distance launch");
+}
+
 // src/capi.mojo:945-947: 1 on success, 0 on failure (the shim raises). Large
 // problems go through the prepared-mesh FP64 kernel (its ~2 ms preparation is
 // repaid above ~1e9 pairs), small ones through the streaming FP64 kernel; both
@@ -736,7 +923,7 @@ int64_t mli_winding_gpu(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t
              : 0;
 }
 
-// Out-of-scope reference exports (src/capi.mojo:923-937, 950-1007).
+// Out-of-scope reference exports (src/capi.mojo:923-937, 962-1007).
 void mli_cot_entries(int64_t, int64_t, int64_t, int64_t, int64_t) {
   out_of_scope("mli_cot_entries");
 }
@@ -745,10 +932,6 @@ void mli_mass_contributions(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t
 }
 void mli_vertex_normals(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
   out_of_scope("mli_vertex_normals");
-}
-void mli_aabb_squared_distance(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t,
-                               int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
-  out_of_scope("mli_aabb_squared_distance");
 }
 void mli_heat_vector_divergence(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
   out_of_scope("mli_heat_vector_divergence");

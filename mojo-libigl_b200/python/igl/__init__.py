@@ -7,6 +7,11 @@ types and error classes. ``device="gpu"`` runs hand-written sm_100a kernels in
 ``libwn_b200.so``; ``device="cpu"`` runs the library's host path over the
 reference's thread fan-out.
 
+Also the closest-point path beside it (python/igl/__init__.py:286-404):
+``AABB`` (``init``, ``squared_distance``) and ``point_mesh_squared_distance``,
+with an extra ``device`` keyword (default "cpu", the reference's behaviour),
+and ``signed_distance``, which signs the distance by the winding number.
+
 Deliberate difference: when ``device="gpu"`` is requested and no CUDA device
 is usable, the reference silently computes on the CPU
 (python/igl/__init__.py:251, 264); this package raises ``RuntimeError``
@@ -25,7 +30,7 @@ from ._lib import addr, fan_out, last_error, lib, worker_count
 
 def __getattr__(name):
     # torch-dependent submodules load on first use.
-    if name in ("autograd", "batched", "autotune"):
+    if name in ("autograd", "batched", "autotune", "distance"):
         import importlib
 
         return importlib.import_module(f".{name}", __name__)
@@ -36,6 +41,9 @@ __all__ = [
     "winding_number",
     "winding_number_for_point",
     "PRECISIONS",
+    "AABB",
+    "point_mesh_squared_distance",
+    "signed_distance",
 ]
 
 # "fp64": the plain FP64 kernel, pair terms bit-identical to the reference.
@@ -192,3 +200,174 @@ def winding_number(V, F, O, device="cpu", *, precision="fp64"):
 
 def winding_number_for_point(V, F, p):
     return float(winding_number(V, F, p))
+
+
+# ---- closest points (reference python/igl/__init__.py:286-404) --------------
+_AABB_LEAF_SIZE = 8
+
+
+def _device_name(device) -> str:
+    selected = str(device).lower()
+    if selected not in ("cpu", "gpu"):
+        raise ValueError("device must be 'cpu' or 'gpu'")
+    return selected
+
+
+def _require_gpu() -> None:
+    if not _gpu_memory_available():
+        raise RuntimeError(
+            "device='gpu' was requested but no CUDA device with "
+            f"{_MIN_FREE_MIB} MiB free is available (no CPU fallback)"
+        )
+
+
+def _build_aabb(vertices: np.ndarray, faces: np.ndarray, leaf_size: int = _AABB_LEAF_SIZE):
+    """The tree of the reference's ``_build_aabb`` (__init__.py:286-319), built natively.
+
+    Returns (boxes (nnodes, 6), nodes (nnodes, 4), order (nf,), stack_size).
+    """
+    handle = lib()
+    count = handle.wn_aabb_node_count(len(faces), leaf_size)
+    boxes = np.empty((count, 6), dtype=np.float64)
+    nodes = np.empty((count, 4), dtype=np.int64)
+    order = np.empty(len(faces), dtype=np.int64)
+    stack_size = ctypes.c_int64(0)
+    status = handle.wn_aabb_build(addr(vertices), len(vertices), addr(faces), len(faces),
+                                  leaf_size, addr(boxes), addr(nodes), addr(order),
+                                  ctypes.byref(stack_size), 0)
+    if status:
+        raise ValueError(last_error(handle) or "tree construction failed")
+    return boxes, nodes, order, stack_size.value
+
+
+class AABB:
+    """libigl-compatible AABB precomputation for squared-distance queries.
+
+    Mirrors the reference class (python/igl/__init__.py:322-399). The tree is
+    the reference's median-split hierarchy, built natively; ``squared_distance``
+    takes ``device="cpu"`` (the library's host traversal over the reference's
+    span fan-out) or ``device="gpu"`` (the sm_100a traversal kernel on a tree
+    uploaded once per ``init``). Both return bit-identical results.
+    """
+
+    def __init__(self):
+        self._tree = None
+        self._gpu_tree = None
+
+    def _release(self) -> None:
+        if getattr(self, "_gpu_tree", None):
+            lib().wn_aabb_destroy(self._gpu_tree)
+        self._gpu_tree = None
+
+    def __del__(self):
+        try:
+            self._release()
+        except Exception:  # interpreter shutdown
+            pass
+
+    def init(self, V, Ele):
+        vertices, faces = _mesh(V, Ele)
+        self._release()
+        self._vertices = vertices
+        self._faces = faces
+        self._tree = _build_aabb(vertices, faces) if len(faces) else ()
+
+    def _device_tree(self):
+        if self._gpu_tree is None:
+            boxes, nodes, order, _ = self._tree
+            handle = lib()
+            tree = ctypes.c_void_p()
+            status = handle.wn_aabb_create(addr(self._vertices), len(self._vertices),
+                                           addr(self._faces), len(self._faces), addr(boxes),
+                                           addr(nodes), addr(order), len(nodes),
+                                           ctypes.byref(tree))
+            if status:
+                raise RuntimeError("the B200 closest-point tree upload failed: "
+                                   + last_error(handle))
+            self._gpu_tree = tree.value
+        return self._gpu_tree
+
+    def squared_distance(self, V, Ele, P, device="cpu"):
+        if self._tree is None:
+            raise RuntimeError("AABB.init must be called before squared_distance")
+        vertices, faces = _mesh(V, Ele)
+        if not np.array_equal(vertices, self._vertices) or not np.array_equal(
+            faces, self._faces
+        ):
+            raise ValueError("V and Ele must match the mesh passed to AABB.init")
+        vertices, faces = self._vertices, self._faces
+        points = _float_array(P, "P")
+        if points.ndim != 2 or points.shape[1] != 3:
+            raise ValueError("P must have shape (p, 3)")
+        selected_device = _device_name(device)
+        if not len(faces):
+            return (
+                np.full(len(points), np.inf),
+                np.full(len(points), -1, dtype=np.int64),
+                np.zeros((len(points), 3)),
+            )
+        boxes, nodes, order, stack_size = self._tree
+        count = len(points)
+        sqrd = np.empty(count, dtype=np.float64)
+        indices = np.empty(count, dtype=np.int64)
+        closest = np.empty((count, 3), dtype=np.float64)
+        if not count:
+            return sqrd, indices, closest
+        if selected_device == "gpu":
+            _require_gpu()
+            handle = lib()
+            status = handle.wn_aabb_squared_distance_host(
+                self._device_tree(), addr(points), count, addr(sqrd), addr(indices),
+                addr(closest))
+            if status:
+                raise RuntimeError("the B200 closest-point kernel failed: " + last_error(handle))
+            return sqrd, indices, closest
+        # One traversal stack per span (reference __init__.py:360-380).
+        depth = 1 + max(stack_size.bit_length(), 1)
+        workers = worker_count(count, count * len(faces) * depth, "aabb")
+        stacks = np.empty((workers, stack_size), dtype=np.int64)
+        function = lib().mli_aabb_squared_distance
+        arguments = (addr(points), addr(vertices), addr(faces), addr(boxes), addr(nodes),
+                     addr(order), addr(sqrd), addr(indices), addr(closest))
+
+        def query(lo, hi, span=0):
+            function(*arguments, stacks[span].ctypes.data, count, len(nodes), lo, hi)
+
+        used = fan_out(query, (), count, workers)
+        assert used <= len(stacks), "each span needs its own traversal stack"
+        return sqrd, indices, closest
+
+    def find(self, V, Ele, q, first=False):
+        raise NotImplementedError("AABB.find is outside the covered subset")
+
+    def intersect_ray(self, V, Ele, orig, dir):
+        raise NotImplementedError("AABB ray intersection is outside the covered subset")
+
+    def intersect_ray_first(self, V, Ele, orig, dir, min_t=np.inf):
+        raise NotImplementedError("AABB ray intersection is outside the covered subset")
+
+
+def point_mesh_squared_distance(P, V, Ele, device="cpu"):
+    tree = AABB()
+    tree.init(V, Ele)
+    return tree.squared_distance(V, Ele, P, device=device)
+
+
+def signed_distance(P, V, F, device="cpu", *, precision="fp64"):
+    """Distance to the surface, negative where the winding number says inside.
+
+    Returns (S, I, C): S[i] = -sqrt(sqrd) when |W(P_i)| > 1/2, else
+    +sqrt(sqrd), with (sqrd, I, C) from ``point_mesh_squared_distance`` and W
+    from ``winding_number`` on the same device (``precision`` applies to the
+    GPU winding number). For a closed, consistently oriented surface this is
+    the usual inside-negative signed distance; open meshes get the sign of the
+    rounded winding number. With no faces S is +inf.
+    """
+    points = _float_array(P, "P")
+    if points.ndim != 2 or points.shape[1] != 3:
+        raise ValueError("P must have shape (p, 3)")
+    sqrd, indices, closest = point_mesh_squared_distance(points, V, F, device=device)
+    W = winding_number(V, F, points, device=device, precision=precision) if len(points) else \
+        np.empty(0)
+    distance = np.sqrt(sqrd)
+    return np.where(np.abs(W) > 0.5, -distance, distance), indices, closest

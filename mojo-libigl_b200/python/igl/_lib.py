@@ -27,8 +27,9 @@ P = ctypes.c_void_p
 C_INT = ctypes.c_int
 
 # Reference python/igl/_lib.py:18-32: the thirteen C-ABI names with their
-# argument counts. libwn_b200 implements the two winding entries and exports
-# the other eleven only so that loaders resolving every name succeed.
+# argument counts. libwn_b200 implements the two winding entries and the
+# closest-point query, and exports the other ten only so that loaders
+# resolving every name succeed.
 _SIGNATURES = {
     "mli_cot_entries": ([I, I, I, I, I], None),
     "mli_mass_contributions": ([I, I, I, I, I, I], None),
@@ -76,6 +77,13 @@ _WN_SIGNATURES = {
     "wn_batch_info": ([P, P, I], C_INT),
     "wn_batch_destroy": ([P], C_INT),
     "wn_backward_mixed_device": ([P, P, I, P, P, P, I, P], C_INT),
+    "wn_aabb_node_count": ([I, I], I),
+    "wn_aabb_build": ([P, I, P, I, I, P, P, P, ctypes.POINTER(I), C_INT], C_INT),
+    "wn_aabb_create": ([P, I, P, I, P, P, P, I, ctypes.POINTER(P)], C_INT),
+    "wn_aabb_destroy": ([P], C_INT),
+    "wn_aabb_squared_distance_device": ([P, P, I, P, P, P, P], C_INT),
+    "wn_aabb_squared_distance_host": ([P, P, I, P, P, P], C_INT),
+    "wn_signed_distance_device": ([P, P, C_INT, P, I, P, P, P, P, P], C_INT),
 }
 
 # The reference caps its pool at four workers on a shared host (_lib.py:34-37).

@@ -13,6 +13,10 @@ bounding box and a thin shell around the surface.
 * ``mixed_queries(V, F, n, seed, near_sigma, box_scale)``: half uniform in the
   bounding box scaled by ``box_scale``; half on a random face at a uniform
   barycentric point, offset along the face normal by N(0, near_sigma).
+* ``terrain_grid(n)``: the height-field grid of the reference's closest-point
+  benchmark (bench/bench.py:33-45 of lee101/mojo-libigl): n x n vertices at
+  integer (x, y), z = 0.1 sin(x / 8) cos(y / 11), two faces per cell;
+  n = 350 gives 243,602 faces.
 """
 
 from __future__ import annotations
@@ -125,6 +129,17 @@ def mixed_queries(V, F, n: int, seed: int = 1, near_sigma: float = 1e-3,
     box = box_points(V, nb, seed, box_scale)
     near = near_surface_points(V, F, n - nb, seed + 7919, near_sigma)
     return np.ascontiguousarray(np.concatenate([box, near]))
+
+
+def terrain_grid(n: int) -> tuple[np.ndarray, np.ndarray]:
+    y, x = np.mgrid[:n, :n]
+    z = 0.1 * np.sin(x / 8.0) * np.cos(y / 11.0)
+    V = np.ascontiguousarray(np.column_stack((x.ravel(), y.ravel(), z.ravel())), dtype=np.float64)
+    cell = (np.arange(n - 1)[:, None] * n + np.arange(n - 1)[None, :]).ravel()
+    F = np.empty((2 * len(cell), 3), dtype=np.int64)
+    F[0::2] = np.column_stack((cell, cell + 1, cell + n + 1))
+    F[1::2] = np.column_stack((cell, cell + n + 1, cell + n))
+    return V, F
 
 
 # The five workloads of this path, by name; sizes as stated in each docstring.

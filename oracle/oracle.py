@@ -13,6 +13,10 @@ checkers that pin it:
   significant digits, independent of any float64 rounding: the known-answer pin.
 * ``winding_grad_torch`` is the FP64 PyTorch-autograd expression of the
   solid-angle formula, the reference for the hand-written adjoint.
+* ``build_aabb`` restates the reference's median-split hierarchy
+  (python/igl/__init__.py:286-319) and ``aabb_squared_distance`` drives the C
+  restatement of its closest-point traversal (src/capi.mojo:401-586,
+  aabb_oracle.cpp).
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
 and ``--impl reference`` legs may import this module.
@@ -54,6 +58,10 @@ def lib() -> ctypes.CDLL:
             ctypes.c_void_p, I64, I64, ctypes.c_void_p, ctypes.c_void_p
         ]
         handle.oracle_pair_terms.restype = None
+        handle.mli_aabb_squared_distance.argtypes = [I64] * 14
+        handle.mli_aabb_squared_distance.restype = None
+        handle.oracle_closest_point.argtypes = [ctypes.c_void_p] * 3
+        handle.oracle_closest_point.restype = None
         _handle = handle
     return _handle
 
@@ -161,3 +169,88 @@ def winding_grad_torch(V, F, O, gW):
     W = winding_torch(Vt, Ft, Ot)
     (W * torch.tensor(np.asarray(gW, dtype=np.float64))).sum().backward()
     return Ot.grad.numpy(), Vt.grad.numpy()
+
+
+# ---- closest points (the reference's AABB path) -----------------------------
+def build_aabb(V, F, leaf_size: int = 8):
+    """Median-split hierarchy as python/igl/__init__.py:286-319 builds it.
+
+    Returns (boxes (nnodes, 6) f64, nodes (nnodes, 4) int64, order (nf,) int64,
+    stack_size). Nodes are numbered in preorder (a node before its left
+    subtree, the left subtree before the right one). A node with more than
+    ``leaf_size`` faces splits along the axis of the largest extent of its face
+    box centres (the first such axis), after a stable sort of its faces by that
+    centre coordinate, at len // 2. ``stack_size`` is the depth (root = 1) + 1.
+    """
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    F = np.ascontiguousarray(F, dtype=np.int64)
+    tri = V[F]
+    low, high = tri.min(axis=1), tri.max(axis=1)
+    centers = 0.5 * (low + high)
+    boxes, nodes, order = [], [], []
+    depth = 0
+    # Explicit preorder walk: (face ids, depth, slot in the parent to patch).
+    work = [(np.arange(len(F), dtype=np.int64), 1, None)]
+    while work:
+        ids, d, parent = work.pop()
+        node = len(nodes)
+        depth = max(depth, d)
+        if parent is not None:
+            nodes[parent[0]][parent[1]] = node
+        boxes.append(np.concatenate((low[ids].min(axis=0), high[ids].max(axis=0))))
+        if len(ids) <= leaf_size:
+            nodes.append([-1, -1, len(order), len(ids)])
+            order.extend(ids.tolist())
+            continue
+        nodes.append([-1, -1, 0, 0])
+        c = centers[ids]
+        axis = int(np.argmax(c.max(axis=0) - c.min(axis=0)))
+        ids = ids[np.argsort(c[:, axis], kind="stable")]
+        half = len(ids) // 2
+        work.append((ids[half:], d + 1, (node, 1)))  # right, popped after the left subtree
+        work.append((ids[:half], d + 1, (node, 0)))
+    return (np.ascontiguousarray(boxes, dtype=np.float64).reshape(-1, 6),
+            np.ascontiguousarray(nodes, dtype=np.int64).reshape(-1, 4),
+            np.asarray(order, dtype=np.int64), depth + 1)
+
+
+def aabb_squared_distance(P, V, F, tree=None, workers: int = 1):
+    """(sqrd, face index, closest point) of each point, by the C oracle.
+
+    ``tree`` is a ``build_aabb`` result (built here when omitted). Spans of
+    points run on ``workers`` threads, each with its own traversal stack.
+    """
+    P = np.ascontiguousarray(P, dtype=np.float64).reshape(-1, 3)
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    F = np.ascontiguousarray(F, dtype=np.int64)
+    n = len(P)
+    if len(F) == 0:
+        return np.full(n, np.inf), np.full(n, -1, dtype=np.int64), np.zeros((n, 3))
+    boxes, nodes, order, stack_size = build_aabb(V, F) if tree is None else tree
+    sqrd = np.empty(n, dtype=np.float64)
+    index = np.empty(n, dtype=np.int64)
+    closest = np.empty((n, 3), dtype=np.float64)
+    if n == 0:
+        return sqrd, index, closest
+    workers = max(1, min(int(workers), n))
+    stacks = np.empty((workers, stack_size), dtype=np.int64)
+    fn = lib().mli_aabb_squared_distance
+    args = (P.ctypes.data, V.ctypes.data, F.ctypes.data, boxes.ctypes.data, nodes.ctypes.data,
+            order.ctypes.data, sqrd.ctypes.data, index.ctypes.data, closest.ctypes.data)
+    parts = spans(n, workers)
+    if len(parts) == 1:
+        fn(*args, stacks[0].ctypes.data, n, len(nodes), 0, n)
+    else:
+        with ThreadPoolExecutor(max_workers=len(parts)) as pool:
+            list(pool.map(lambda item: fn(*args, stacks[item[0]].ctypes.data, n, len(nodes),
+                                          item[1][0], item[1][1]), enumerate(parts)))
+    return sqrd, index, closest
+
+
+def closest_point(p, tri9) -> tuple[float, float, float, float]:
+    """(d2, x, y, z) of one point against one triangle (9 coordinates, A B C)."""
+    p = np.ascontiguousarray(p, dtype=np.float64)
+    tri9 = np.ascontiguousarray(tri9, dtype=np.float64).reshape(9)
+    out = np.empty(4, dtype=np.float64)
+    lib().oracle_closest_point(p.ctypes.data, tri9.ctypes.data, out.ctypes.data)
+    return tuple(float(x) for x in out)

@@ -20,8 +20,10 @@
 //     product and sum is rounded separately, as plain Mojo `*`/`+` are.
 //   * atan2 and sqrt are the C library's (correctly rounded sqrt; glibc atan2).
 //
-// The library also exports the reference's other twelve `mli_*` C-ABI names
-// (capi.mojo:923-1007) as no-ops, so the reference's own Python shim
+// The closest-point query (`mli_aabb_squared_distance`) lives in
+// aabb_oracle.cpp, linked into the same library. The library also exports the
+// reference's other eleven `mli_*` C-ABI names (capi.mojo:923-1007) as no-ops,
+// so the reference's own Python shim
 // (python/igl/_lib.py:122-130, which resolves all thirteen names) can load this
 // file through MOJO_LIBIGL_LIB and drive `mli_winding` unchanged.
 #include <cmath>
@@ -113,13 +115,11 @@ void mli_winding(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t nq, in
 // The oracle has no GPU: report failure exactly as capi.mojo:397-398 does.
 int64_t mli_winding_gpu(int64_t, int64_t, int64_t, int64_t, int64_t) { return 0; }
 
-// The remaining reference exports (capi.mojo:923-937, 950-1007): out of scope,
+// The remaining reference exports (capi.mojo:923-937, 962-1007): out of scope,
 // present only so the reference shim's loader finds every name.
 void mli_cot_entries(int64_t, int64_t, int64_t, int64_t, int64_t) {}
 void mli_mass_contributions(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {}
 void mli_vertex_normals(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {}
-void mli_aabb_squared_distance(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t,
-                               int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {}
 void mli_heat_vector_divergence(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {}
 void mli_heat_precompute(int64_t, int64_t, int64_t, int64_t) {}
 void mli_arap_covariance(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t,

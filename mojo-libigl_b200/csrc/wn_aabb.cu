@@ -13,6 +13,9 @@
 // Each stack entry keeps the box distance computed when it was pushed. The
 // reference recomputes that distance from the same box when it pops the node;
 // the value is the same double, so the pop-time test `d > best` is unchanged.
+// The stored key is max(box distance, slab bound) (wn_aabb.h): a child is
+// pushed, and later expanded, only when both are <= best. The push order is
+// decided by the box distances alone, as in the reference.
 #include <cuda_runtime.h>
 
 #include "wn_aabb.cuh"
@@ -36,10 +39,21 @@ struct AabbArgs {
   int* err;
   int64_t np, nnodes;
   double root[6];
+  double scale;
 };
 
 __device__ __forceinline__ double2 ldg2(const double* p) {
   return __ldg(reinterpret_cast<const double2*>(p));
+}
+
+// Squared lower bound on the distance from p to the faces inside a slab, less
+// the rounding margin `e` (0 when the slab cannot separate them).
+__device__ __forceinline__ double slab_bound2(double px, double py, double pz, float nx, float ny,
+                                              float nz, float lo, float hi, double e) {
+  const double t = fma(static_cast<double>(nz), pz,
+                       fma(static_cast<double>(ny), py, static_cast<double>(nx) * px));
+  const double g = fmax(static_cast<double>(lo) - t, t - static_cast<double>(hi)) - e;
+  return g > 0.0 ? g * g * (1.0 - kSlabMargin) : 0.0;
 }
 
 __global__ void __launch_bounds__(kAabbThreads) aabb_query_kernel(const AabbArgs a) {
@@ -50,6 +64,9 @@ __global__ void __launch_bounds__(kAabbThreads) aabb_query_kernel(const AabbArgs
   double best = 1.0e300;
   int64_t best_face = -1;
   double bx = 0.0, by = 0.0, bz = 0.0;
+  // Slab margin for this point; no slab skips at all for huge or non-finite input.
+  double margin = kSlabMargin * (a.scale + fabs(px) + fabs(py) + fabs(pz));
+  if (!(margin < 1e100)) margin = INFINITY;
   int stack_node[kAabbStack];
   double stack_d2[kAabbStack];
   int sp = 0;
@@ -63,7 +80,7 @@ __global__ void __launch_bounds__(kAabbThreads) aabb_query_kernel(const AabbArgs
     --sp;
     if (stack_d2[sp] > best) continue;
     const AabbNodeRec* nd = a.nodes + stack_node[sp];
-    const int4 meta = __ldg(reinterpret_cast<const int4*>(&nd->left));
+    const int4 meta = __ldg(reinterpret_cast<const int4*>(nd));
     if (meta.w > 0) {
       const AabbTriRec* tr = a.tris + meta.z;
       for (int k = 0; k < meta.w; ++k, ++tr) {
@@ -82,12 +99,17 @@ __global__ void __launch_bounds__(kAabbThreads) aabb_query_kernel(const AabbArgs
     } else {
       const double2 l0 = ldg2(nd->lbox), l1 = ldg2(nd->lbox + 2), l2 = ldg2(nd->lbox + 4);
       const double2 r0 = ldg2(nd->rbox), r1 = ldg2(nd->rbox + 2), r2 = ldg2(nd->rbox + 4);
+      const float4 s0 = __ldg(reinterpret_cast<const float4*>(&nd->lslab));
+      const float4 s1 = __ldg(reinterpret_cast<const float4*>(&nd->lslab) + 1);
+      const float2 s2 = __ldg(reinterpret_cast<const float2*>(&nd->rslab.lo));
       const double dl = box_distance2(px, py, pz, l0.x, l0.y, l1.x, l1.y, l2.x, l2.y);
       const double dr = box_distance2(px, py, pz, r0.x, r0.y, r1.x, r1.y, r2.x, r2.y);
+      const double kl = fmax(dl, slab_bound2(px, py, pz, s0.x, s0.y, s0.z, s0.w, s1.x, margin));
+      const double kr = fmax(dr, slab_bound2(px, py, pz, s1.y, s1.z, s1.w, s2.x, s2.y, margin));
       // Farther child first, so the nearer one is popped next (capi.mojo:571-586).
       const bool left_near = dl < dr;
       const int first = left_near ? meta.y : meta.x, second = left_near ? meta.x : meta.y;
-      const double dfirst = left_near ? dr : dl, dsecond = left_near ? dl : dr;
+      const double dfirst = left_near ? kr : kl, dsecond = left_near ? kl : kr;
       if (sp + 2 > kAabbStack) {  // cannot happen for a validated tree
         atomicOr(a.err, kErrBadLaunch);
         best_face = -2;
@@ -127,7 +149,7 @@ cudaError_t aabb_query(const AabbDeviceTree& t, const double* P, int64_t np, con
                        cudaStream_t stream) {
   if (np <= 0) return cudaSuccess;
   if (t.depth + 1 > kAabbStack) return cudaErrorInvalidValue;
-  AabbArgs a{t.nodes, t.tris, P, perm, sqrd, index, closest, err, np, t.nnodes, {}};
+  AabbArgs a{t.nodes, t.tris, P, perm, sqrd, index, closest, err, np, t.nnodes, {}, t.scale};
   for (int k = 0; k < 6; ++k) a.root[k] = t.root[k];
   const int64_t blocks = (np + kAabbThreads - 1) / kAabbThreads;
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;

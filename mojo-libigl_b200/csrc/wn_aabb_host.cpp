@@ -188,9 +188,103 @@ int64_t aabb_build(const double* V, int64_t nv, const int64_t* F, int64_t nf, in
   return b.depth.load() + 1;
 }
 
+namespace {
+
+float round_down(double x) {
+  float f = static_cast<float>(x);
+  if (static_cast<double>(f) > x) f = std::nextafter(f, -INFINITY);
+  return f;
+}
+
+float round_up(double x) {
+  float f = static_cast<float>(x);
+  if (static_cast<double>(f) < x) f = std::nextafter(f, INFINITY);
+  return f;
+}
+
+// Slab of every node: the normalised area-weighted normal sum of its faces,
+// stored as floats scaled so that |n| <= 1 (then |n.(p - x)| <= |p - x|), and
+// the range of n.x over the vertices of its faces, widened by a margin for the
+// FP64 rounding of n.x and rounded outward to float. A node whose faces are not
+// one contiguous run of `order` (possible only in a caller-made tree) gets the
+// empty slab [-inf, +inf], which never skips anything.
+void build_slabs(const AabbTriRec* tris, const int64_t* nodes, int64_t nnodes, double scale,
+                 std::vector<AabbSlab>& slabs, int threads) {
+  std::vector<double> nsum(3 * static_cast<size_t>(nnodes), 0.0);
+  std::vector<int64_t> first(nnodes), last(nnodes);
+  std::vector<char> whole(nnodes, 1);
+  for (int64_t i = nnodes - 1; i >= 0; --i) {  // children come after their parent
+    const int64_t* nd = nodes + 4 * i;
+    double* n = &nsum[3 * i];
+    if (nd[3] > 0) {
+      first[i] = nd[2];
+      last[i] = nd[2] + nd[3];
+      for (int64_t k = first[i]; k < last[i]; ++k) {
+        const AabbTriRec& t = tris[k];
+        const double u[3] = {t.b[0] - t.a[0], t.b[1] - t.a[1], t.b[2] - t.a[2]};
+        const double w[3] = {t.c[0] - t.a[0], t.c[1] - t.a[1], t.c[2] - t.a[2]};
+        n[0] += u[1] * w[2] - u[2] * w[1];
+        n[1] += u[2] * w[0] - u[0] * w[2];
+        n[2] += u[0] * w[1] - u[1] * w[0];
+      }
+    } else {
+      const int64_t l = nd[0], r = nd[1];
+      for (int k = 0; k < 3; ++k) n[k] = nsum[3 * l + k] + nsum[3 * r + k];
+      first[i] = std::min(first[l], first[r]);
+      last[i] = std::max(last[l], last[r]);
+      whole[i] = whole[l] && whole[r] && (last[l] == first[r] || last[r] == first[l]);
+    }
+  }
+  slabs.assign(static_cast<size_t>(nnodes), AabbSlab{{0.f, 0.f, 0.f}, -INFINITY, INFINITY});
+  const double pad = 1e-13 * 3.0 * scale;  // >> the rounding of a 3-term dot product
+  auto work = [&](int64_t begin, int64_t step) {
+    for (int64_t i = begin; i < nnodes; i += step) {
+      if (!whole[i]) continue;
+      const double* s = &nsum[3 * i];
+      const double len = std::sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+      double n[3] = {1.0, 0.0, 0.0};
+      if (len > 0.0 && std::isfinite(len))
+        for (int k = 0; k < 3; ++k) n[k] = s[k] / len;
+      float nf[3];
+      for (int k = 0; k < 3; ++k) nf[k] = static_cast<float>(n[k]);
+      for (int guard = 0; guard < 8; ++guard) {  // shrink until |nf| <= 1
+        const double m = std::sqrt(static_cast<double>(nf[0]) * nf[0] +
+                                   static_cast<double>(nf[1]) * nf[1] +
+                                   static_cast<double>(nf[2]) * nf[2]);
+        if (m <= 1.0) break;
+        for (int k = 0; k < 3; ++k) nf[k] *= 1.0f - 1.0f / 8388608.0f;
+      }
+      double lo = INFINITY, hi = -INFINITY;
+      for (int64_t k = first[i]; k < last[i]; ++k) {
+        const AabbTriRec& t = tris[k];
+        for (const double* v : {t.a, t.b, t.c}) {
+          const double d = static_cast<double>(nf[0]) * v[0] + static_cast<double>(nf[1]) * v[1] +
+                           static_cast<double>(nf[2]) * v[2];
+          lo = std::min(lo, d);
+          hi = std::max(hi, d);
+        }
+      }
+      AabbSlab& out = slabs[i];
+      for (int k = 0; k < 3; ++k) out.n[k] = nf[k];
+      out.lo = round_down(lo - pad);
+      out.hi = round_up(hi + pad);
+    }
+  };
+  if (threads <= 1 || nnodes < 4096) {
+    work(0, 1);
+  } else {
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(work, t, threads);
+    for (auto& th : pool) th.join();
+  }
+}
+
+}  // namespace
+
 int64_t aabb_pack(const double* V, int64_t nv, const int64_t* F, int64_t nf, const double* boxes,
                   const int64_t* nodes, const int64_t* order, int64_t nnodes,
-                  AabbNodeRec* node_out, AabbTriRec* tri_out, const char** why) {
+                  AabbNodeRec* node_out, AabbTriRec* tri_out, double* scale, const char** why) {
+  *scale = 0.0;
   if (nnodes == 0) return 0;
   if (nnodes < 0 || nnodes > 0x7fffffffLL || nf <= 0 || nf > 0x7fffffffLL) {
     *why = "node or face count out of range";
@@ -210,7 +304,14 @@ int64_t aabb_pack(const double* V, int64_t nv, const int64_t* F, int64_t nf, con
         return -1;
       }
       double* dst = c == 0 ? r.a : (c == 1 ? r.b : r.c);
-      for (int k = 0; k < 3; ++k) dst[k] = V[3 * v + k];
+      for (int k = 0; k < 3; ++k) {
+        dst[k] = V[3 * v + k];
+        if (!std::isfinite(dst[k])) {
+          *why = "non-finite vertex coordinate";
+          return -1;
+        }
+        *scale = std::max(*scale, std::fabs(dst[k]));
+      }
     }
     r.face = f;
   }
@@ -223,7 +324,7 @@ int64_t aabb_pack(const double* V, int64_t nv, const int64_t* F, int64_t nf, con
     const int64_t* nd = nodes + 4 * i;
     AabbNodeRec& r = node_out[i];
     for (int k = 0; k < 6; ++k) r.lbox[k] = r.rbox[k] = 0.0;
-    for (int k = 0; k < 4; ++k) r.pad[k] = 0;
+    for (int k = 0; k < 2; ++k) r.pad[k] = 0;
     if (level[i] == 0) {
       *why = "node unreachable from the root";
       return -1;
@@ -258,6 +359,18 @@ int64_t aabb_pack(const double* V, int64_t nv, const int64_t* F, int64_t nf, con
   if (depth + 1 > kAabbStack) {
     *why = "tree deeper than the traversal stack";
     return -1;
+  }
+  std::vector<AabbSlab> slabs;
+  build_slabs(tri_out, nodes, nnodes, *scale, slabs,
+              static_cast<int>(std::max(1u, std::thread::hardware_concurrency())));
+  for (int64_t i = 0; i < nnodes; ++i) {
+    AabbNodeRec& r = node_out[i];
+    if (r.count > 0) {
+      r.lslab = r.rslab = AabbSlab{{0.f, 0.f, 0.f}, -INFINITY, INFINITY};
+    } else {
+      r.lslab = slabs[r.left];
+      r.rslab = slabs[r.right];
+    }
   }
   return depth;
 }

@@ -790,8 +790,9 @@ int wn_aabb_create(const double* V, int64_t nv, const int64_t* F, int64_t nf,
   std::vector<AabbNodeRec> nrec(static_cast<size_t>(nnodes));
   std::vector<AabbTriRec> trec(static_cast<size_t>(nnodes > 0 ? nf : 0));
   const char* why = "";
-  const int64_t depth =
-      aabb_pack(V, nv, F, nf, boxes, nodes, order, nnodes, nrec.data(), trec.data(), &why);
+  double scale = 0.0;
+  const int64_t depth = aabb_pack(V, nv, F, nf, boxes, nodes, order, nnodes, nrec.data(),
+                                  trec.data(), &scale, &why);
   if (depth < 0) return fail(WN_EINVAL, "invalid tree: %s", why);
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
@@ -801,6 +802,7 @@ int wn_aabb_create(const double* V, int64_t nv, const int64_t* F, int64_t nf,
   h->t.nnodes = nnodes;
   h->t.nleaf_faces = static_cast<int64_t>(trec.size());
   h->t.depth = static_cast<int>(depth);
+  h->t.scale = scale;
   if (nnodes > 0) {
     for (int k = 0; k < 6; ++k) h->t.root[k] = boxes[k];
     cudaError_t e;

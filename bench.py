@@ -16,7 +16,13 @@ Legs, all on the same inputs:
   * c4: the gradient workload (subdivision-5 mesh, 8% faces deleted, 262,144
     near-surface queries): forward alone and forward + each adjoint;
   * c5: 64 uneven meshes in one persistent launch, forward alone and forward +
-    boundary-edge adjoint replayed from one captured CUDA graph.
+    boundary-edge adjoint replayed from one captured CUDA graph;
+  * closest_point: the closest-point traversal beside the path
+    (point_mesh_squared_distance over the median-split tree, bit-identical to
+    the reference's CPU query) on the reference's own AABB benchmark shape
+    (grid(350), 243,602 F x 10,000 points), on the c3 mesh x 2^20 queries and
+    on grid(350) x 2^20 points: device time, end to end through the C ABI with
+    host buffers, the oracle on this host's cores, and an exactness check.
 `value` is whole-job pairs/s of the headline leg with inputs resident in HBM;
 `e2e` is the same leg through the C ABI with pinned host buffers, the
 host->device copies, device preprocessing and device->host copy inside the
@@ -31,6 +37,11 @@ bracketed by barriers and the slowest rank's time is reported.
 
 `--impl reference` times the reference's CPU path (the oracle port, all host
 threads) on a bounded sample of the same workload and prints the same metric.
+
+`--case NAME [--case-queries N]` runs one kernel on a small case twice and
+exits (the commands behind the ncu summaries in profiles/): fp64_c3 (streaming
+FP64 kernel), fp64_tiled_c3 (FP64 over the prepared mesh), mixed_c3, adjoint_c4
+(per-face mixed adjoint) and closest_c3 (closest-point traversal).
 """
 
 from __future__ import annotations
@@ -68,6 +79,11 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-c4", action="store_true", help="skip the gradient workload")
     p.add_argument("--no-c5", action="store_true", help="skip the batched workload")
+    p.add_argument("--no-closest", action="store_true", help="skip the closest-point workloads")
+    p.add_argument("--case", choices=("fp64_c3", "fp64_tiled_c3", "mixed_c3", "adjoint_c4",
+                                      "closest_c3"),
+                   help="run one kernel on a small case twice (for profiling) and exit")
+    p.add_argument("--case-queries", type=int, default=None)
     p.add_argument("--autotune", action="store_true",
                    help="autotune the batched launch (cached per GPU and size bucket)")
     return p.parse_args()
@@ -129,6 +145,40 @@ def oracle_rate(tri, O, cores: int, target_s: float):
     oracle.winding_soa(tri, sample, workers=cores)
     dt = time.perf_counter() - t0
     return nf * len(sample) / dt, len(sample), dt
+
+
+def oracle_aabb_rate(P, V, F, tree, cores: int, target_s: float):
+    """Points/s of the oracle's closest-point query over `cores` threads on a
+    prefix of P sized to take about target_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    n = min(len(P), 4096)
+    t0 = time.perf_counter()
+    oracle.aabb_squared_distance(P[:n], V, F, tree=tree, workers=cores)
+    dt = time.perf_counter() - t0
+    n = int(min(len(P), max(n, n * target_s / max(dt, 1e-6))))
+    t0 = time.perf_counter()
+    oracle.aabb_squared_distance(P[:n], V, F, tree=tree, workers=cores)
+    dt = time.perf_counter() - t0
+    return n / dt, n, dt
+
+
+def closest_point_workloads(nq: int):
+    from igl import synthetic
+
+    Vg, Fg = synthetic.terrain_grid(350)
+    rng = np.random.default_rng(7)
+    box = ([-10.0, -10.0, -5.0], [360.0, 360.0, 5.0])
+    V3, F3, O3, _ = synthetic.workload("c3_mixed", n_queries=nq)
+    return [
+        ("reference_bench", "grid(350) height field (122,500 V, 243,602 F) x 10,000 points "
+         "uniform in [-10,360]^2 x [-5,5] (the reference's AABB benchmark shape)",
+         Vg, Fg, rng.uniform(*box, size=(10_000, 3))),
+        ("c3", "c3 mesh (327,680 F, closed) x %d queries 50/50 box/near(1e-4)" % nq, V3, F3, O3),
+        ("grid_1M", "grid(350) x %d points uniform in [-10,360]^2 x [-5,5]" % nq,
+         Vg, Fg, rng.uniform(*box, size=(nq, 3))),
+    ]
 
 
 def reference_arm(args):
@@ -429,6 +479,76 @@ def gpu_arm(args):
               "ratio_fwdbwd_to_fwd": t_g / t_f}
         bt.close()
 
+    # Closest points (the AABB query beside the winding number).
+    closest = None
+    if not args.no_closest:
+        from igl import distance
+
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        closest = {}
+        for key, desc_c, Vc, Fc, Pc in closest_point_workloads(args.queries):
+            tree = distance.DeviceAABB(Vc, Fc)
+            P_d = torch.from_numpy(Pc).to(dev)
+            npc = len(Pc)
+            s_d = torch.empty(npc, dtype=torch.float64, device=dev)
+            i_d = torch.empty(npc, dtype=torch.int64, device=dev)
+            c_d = torch.empty((npc, 3), dtype=torch.float64, device=dev)
+
+            def aabb_step():
+                kernel_timed(lambda: check(handle.wn_aabb_squared_distance_device(
+                    tree.tree, P_d.data_ptr(), npc, s_d.data_ptr(), i_d.data_ptr(),
+                    c_d.data_ptr(), sp)))
+
+            t_c, launches_c, t_ck = timed(aabb_step, max(args.steps, 5), 3)
+            entry = {"workload": desc_c, "faces": len(Fc), "points": npc,
+                     "ms_per_step": t_c * 1e3, "kernel_ms": t_ck * 1e3,
+                     "points_per_s": world * npc / t_c, "gpu_launches_per_step": launches_c /
+                     max(args.steps, 5)}
+            # End to end: pinned host points in, host results out (C ABI).
+            P_h = torch.from_numpy(Pc).pin_memory()
+            s_h = torch.empty(npc, dtype=torch.float64).pin_memory()
+            i_h = torch.empty(npc, dtype=torch.int64).pin_memory()
+            c_h = torch.empty((npc, 3), dtype=torch.float64).pin_memory()
+
+            def host_call():
+                check(handle.wn_aabb_squared_distance_host(tree.tree, P_h.data_ptr(), npc,
+                                                           s_h.data_ptr(), i_h.data_ptr(),
+                                                           c_h.data_ptr()))
+
+            if not args.no_e2e:
+                host_call()
+                barrier()
+                reps = max(args.steps, 5)
+                t0 = time.perf_counter()
+                for _ in range(reps):
+                    host_call()
+                dt_e = (time.perf_counter() - t0) / reps
+                entry["e2e"] = {"value": world * npc / dt_e, "unit": "points/s",
+                                "ms_per_step": dt_e * 1e3, "h2d_bytes_per_step": int(Pc.nbytes),
+                                "d2h_bytes_per_step": int(npc * 40),
+                                "path": "wn_aabb_squared_distance_host (C ABI, pinned host buffers)"}
+            if rank == 0:
+                torch.cuda.synchronize()
+                idx = np.random.default_rng(3).choice(npc, min(npc, 2048), replace=False)
+                exp = oracle.aabb_squared_distance(Pc[idx], Vc, Fc, tree=tree.tree_arrays,
+                                                   workers=host_cores())
+                got = (s_d.cpu().numpy()[idx], i_d.cpu().numpy()[idx], c_d.cpu().numpy()[idx])
+                entry["exact_vs_oracle_2048_points"] = all(
+                    np.array_equal(g, e) for g, e in zip(got, exp))
+                if world == 1 and not args.no_cpu_baseline:
+                    cores = host_cores()
+                    rate, n_s, dt_s = oracle_aabb_rate(Pc, Vc, Fc, tree.tree_arrays, cores, 4.0)
+                    entry["cpu_baseline"] = {
+                        "value": rate, "unit": "points/s", "cores": cores, "kind": "port",
+                        "sample": f"first {n_s} points in {dt_s:.1f} s, oracle restatement of "
+                                  f"src/capi.mojo:401-586 over {cores} threads"}
+            closest[key] = entry
+            tree.close()
+        closest["note"] = ("reference's published AABB.squared_distance for the "
+                           "reference_bench shape: 9.12 ms (its own host, README.md:105)")
+
     # Accuracy of the mixed leg against the FP64 kernel on every query.
     accuracy = None
     if "mixed" in results and "fp64" in results:
@@ -532,6 +652,7 @@ def gpu_arm(args):
             "fwd_bwd": fwdbwd,
             "c4_fwd_bwd": c4,
             "c5_batched": c5,
+            "closest_point": closest,
             "accuracy": accuracy,
             "refinement": ({"pairs_refined_fp64_per_step": headline_refined,
                             "fraction": headline_refined / pairs}
@@ -544,9 +665,59 @@ def gpu_arm(args):
         torch.distributed.destroy_process_group()
 
 
+def run_case(args):
+    """One kernel, twice, on a reduced query batch of the c3 (or c4) workload."""
+    import torch
+
+    from igl import _lib, distance, synthetic
+    from igl import autograd as wa
+
+    handle = _lib.lib()
+    default_nq = {"fp64_c3": 16384, "fp64_tiled_c3": 32768, "mixed_c3": 65536,
+                  "adjoint_c4": 16384, "closest_c3": 1 << 20}[args.case]
+    nq = args.case_queries or default_nq
+    V, F, O, _ = synthetic.workload("c4_grad" if args.case == "adjoint_c4" else "c3_mixed",
+                                    n_queries=nq)
+    Vt, Ft, Ot = (torch.from_numpy(x).cuda() for x in (V, F, O))
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    tri, ld, nf = wa.triangle_soa(Vt, Ft)
+    w = torch.empty(nq, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        if args.case == "fp64_c3":
+            rc = handle.wn_forward_fp64_device(tri.data_ptr(), ld, Ot.data_ptr(), w.data_ptr(),
+                                               nf, nq, 0, sp)
+        elif args.case == "closest_c3":
+            tree = distance.DeviceAABB(V, F)
+            w = tree.query(Ot)[0]
+            tree.close()
+            rc = 0
+        else:
+            mesh = wa.PreparedMesh(tri, ld, nf)
+            if args.case == "fp64_tiled_c3":
+                rc = handle.wn_forward_fp64_mesh_device(mesh.mesh, Ot.data_ptr(), nq,
+                                                        w.data_ptr(), sp)
+            elif args.case == "mixed_c3":
+                w = mesh.forward(Ot)
+                rc = 0
+            else:
+                g = torch.from_numpy(np.random.default_rng(5).normal(size=nq)).cuda()
+                w = mesh.backward(Ot, g)[0]
+                rc = 0
+            torch.cuda.synchronize()
+            mesh.close()
+        if rc != 0:
+            raise RuntimeError(_lib.last_error(handle))
+    torch.cuda.synchronize()
+    if handle.wn_stream_check(sp) != 0:
+        raise RuntimeError(_lib.last_error(handle))
+    print("ok", args.case, nf, nq, float(w.double().abs().sum()))
+
+
 def main():
     args = parse_args()
-    if args.impl == "reference":
+    if args.case:
+        run_case(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         gpu_arm(args)

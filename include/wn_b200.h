@@ -253,6 +253,12 @@ int wn_aabb_squared_distance_device(void* tree, const double* P, int64_t np, dou
 int wn_aabb_squared_distance_host(void* tree, const double* P, int64_t np, double* sqrd,
                                   int64_t* index, double* closest);
 
+/* Diagnostic: closest point on one triangle (tri9 = A, B, C) from p on the
+ * host; out4 = (squared distance, x, y, z), by the arithmetic the host
+ * traversal and the GPU kernel share, bit-identical to src/capi.mojo:401-495.
+ * Returns 0, or 1 for a null argument. No reference counterpart. */
+int wn_closest_point(const double* p, const double* tri9, double* out4);
+
 /* Signed distance by the winding-number sign (no reference counterpart):
  * s[i] = -sqrt(sqrd) where |W(P_i)| > 1/2, else +sqrt(sqrd); W comes from the
  * winding-number mesh `mesh` (wn_mixed_mesh_create over the same faces) with

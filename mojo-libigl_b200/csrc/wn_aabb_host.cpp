@@ -450,4 +450,20 @@ void mli_aabb_squared_distance(int64_t p, int64_t v, int64_t f, int64_t boxes, i
               qi);
 }
 
+// Diagnostic (no reference counterpart): the closest point on one triangle
+// (A, B, C as 9 doubles) from p, out4 = (d2, x, y, z), by the function the
+// host traversal and the GPU kernel share (wn_aabb.cuh). Lets tests pin that
+// arithmetic against the reference's on arbitrary triangles.
+int wn_closest_point(const double* p, const double* tri9, double* out4) {
+  if (!p || !tri9 || !out4) return 1;
+  const wn::ClosestHit h =
+      wn::closest_on_triangle(p[0], p[1], p[2], tri9[0], tri9[1], tri9[2], tri9[3], tri9[4],
+                              tri9[5], tri9[6], tri9[7], tri9[8]);
+  out4[0] = h.d2;
+  out4[1] = h.x;
+  out4[2] = h.y;
+  out4[3] = h.z;
+  return 0;
+}
+
 }  // extern "C"

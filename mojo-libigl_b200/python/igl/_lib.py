@@ -84,6 +84,7 @@ _WN_SIGNATURES = {
     "wn_aabb_squared_distance_device": ([P, P, I, P, P, P, P], C_INT),
     "wn_aabb_squared_distance_host": ([P, P, I, P, P, P], C_INT),
     "wn_signed_distance_device": ([P, P, C_INT, P, I, P, P, P, P, P], C_INT),
+    "wn_closest_point": ([P, P, P], C_INT),
 }
 
 # The reference caps its pool at four workers on a shared host (_lib.py:34-37).

@@ -190,3 +190,46 @@ def test_tree_upload_rejects_malformed_arrays():
     bad_order = order.copy()
     bad_order[0] = len(F)
     assert create(boxes, nodes, bad_order) == 1 and "order" in igl._lib.last_error()
+
+
+def _adversarial_triangles(rng, n):
+    """Random triangles plus the shapes that exercise every branch: slivers,
+    collinear corners (the degenerate branch), repeated corners, points, huge
+    and tiny scales, and points on vertices, edges and faces."""
+    tris, pts = [], []
+    for i in range(n):
+        kind = i % 8
+        t = rng.normal(size=(3, 3))
+        if kind == 1:
+            t[2] = t[0] + rng.uniform(-2, 3) * (t[1] - t[0])  # collinear
+        elif kind == 2:
+            t[1] = t[0]  # repeated corner
+        elif kind == 3:
+            t[:] = t[0]  # a point
+        elif kind == 4:
+            t[2] = t[1] + 1e-9 * rng.normal(size=3)  # sliver
+        elif kind == 5:
+            t *= 10.0 ** rng.integers(-8, 9)
+        p = rng.normal(size=3) * np.abs(t).max()
+        if kind == 6:
+            p = t[rng.integers(3)].copy()  # on a vertex
+        elif kind == 7:
+            u = rng.uniform(size=2)
+            p = t[0] + u[0] * (t[1] - t[0]) + u[1] * (1 - u[0]) * (t[2] - t[0]) + 0.0 * p
+        tris.append(t.ravel())
+        pts.append(p)
+    return np.array(tris), np.array(pts)
+
+
+def test_closest_point_matches_oracle_bitwise(oracle_mod):
+    """The arithmetic the host traversal and the GPU kernel share (wn_aabb.cuh)."""
+    rng = np.random.default_rng(99)
+    tris, pts = _adversarial_triangles(rng, 16000)
+    out = np.empty(4)
+    lib = igl.lib()
+    for t, p in zip(tris, pts):
+        expected = np.array(oracle_mod.closest_point(p, t))
+        assert lib.wn_closest_point(p.ctypes.data, t.ctypes.data, out.ctypes.data) == 0
+        assert out.tobytes() == expected.tobytes() or (
+            np.isnan(out).any() and np.array_equal(np.isnan(out), np.isnan(expected))), (
+            t, p, out, expected)

@@ -4,7 +4,7 @@
 // closest points are bit-identical to the reference's CPU path, ties included.
 //
 // The walk is a chain of dependent reads (node record -> child boxes -> next
-// node) over a tree that sits in L2 (a 327,680-face mesh: 16.8 MB of node
+// node) over a tree that sits in L2 (a 327,680-face mesh: 21.0 MB of node
 // records + 26 MB of face records), so the kernel is bound by load latency and
 // FP64 issue, not by HBM bandwidth. What helps is keeping a warp's 32 walks
 // alike: above kAabbSortMin queries the threads take their queries in Morton

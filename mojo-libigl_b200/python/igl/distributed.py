@@ -8,7 +8,10 @@ queries. Only the results move:
   (``gather_w``; all_gather of equal-sized padded blocks);
 * adjoint: dL/do stays with the rank that owns the query; dL/dV has a
   contribution from every query, so the ranks' per-vertex partials are summed
-  with one all_reduce (FP64, SUM) of nv x 3 values.
+  with one all_reduce (FP64, SUM) of nv x 3 values;
+* closest points / signed distance (``points_sharded``): each rank queries its
+  block of points against its own copy of the tree; the per-point results are
+  gathered like W.
 
 The per-rank compute is a callable, so the same host logic runs the CUDA
 kernels on GPUs (NCCL) and any CPU evaluator under gloo (the tests).
@@ -28,10 +31,14 @@ def shard(n: int, rank: int, world: int) -> tuple[int, int]:
 
 
 def gather_w(w_local: torch.Tensor, n: int, group=None) -> torch.Tensor:
-    """Concatenate every rank's block (ranks in order) into the full W on all ranks."""
+    """Concatenate every rank's block (ranks in order) into the full W on all ranks.
+
+    Works for any per-item tensor: the first dimension is the item axis.
+    """
     world = dist.get_world_size(group)
     width = -(-n // world)
-    padded = torch.zeros(width, dtype=w_local.dtype, device=w_local.device)
+    padded = torch.zeros((width,) + tuple(w_local.shape[1:]), dtype=w_local.dtype,
+                         device=w_local.device)
     padded[: w_local.shape[0]] = w_local
     blocks = [torch.empty_like(padded) for _ in range(world)]
     dist.all_gather(blocks, padded, group=group)
@@ -57,6 +64,18 @@ def backward_sharded(backward, V, F, O, gW, group=None):
     dV = dV.to(torch.float64).contiguous()
     dist.all_reduce(dV, op=dist.ReduceOp.SUM, group=group)
     return dV, dO, (lo, hi)
+
+
+def points_sharded(query, P, group=None):
+    """Per-point results for all of P: this rank evaluates query(P_block).
+
+    `query` returns a tuple of tensors whose first dimension is the block's
+    points, e.g. DeviceAABB.query -> (sqrd, index, closest) or
+    DeviceAABB.signed_distance -> (S, index, closest, W); each is gathered.
+    """
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    lo, hi = shard(P.shape[0], rank, world)
+    return tuple(gather_w(t, P.shape[0], group) for t in query(P[lo:hi]))
 
 
 def gpu_forward(V, F, O, precision: str = "mixed"):

@@ -77,8 +77,16 @@ def _worker(rank, world, port, out_dir):
 
         W = wd.forward_sharded(forward, Vt, Ft, Ot)
         dV, dO_block, (lo, hi) = wd.backward_sharded(backward, Vt, Ft, Ot, gt)
+        tree = oracle.build_aabb(V, F)
+
+        def closest(P_):
+            s, i, c = oracle.aabb_squared_distance(P_.numpy(), V, F, tree=tree)
+            return torch.from_numpy(s), torch.from_numpy(i), torch.from_numpy(c)
+
+        sq, idx, pt = wd.points_sharded(closest, Ot)
         np.savez(os.path.join(out_dir, f"rank{rank}.npz"), W=W.numpy(), dV=dV.numpy(),
-                 dO=dO_block.numpy(), lo=lo, hi=hi)
+                 dO=dO_block.numpy(), lo=lo, hi=hi, sqrd=sq.numpy(), index=idx.numpy(),
+                 closest=pt.numpy())
     finally:
         dist.destroy_process_group()
 
@@ -114,3 +122,9 @@ def test_two_rank_gloo_forward_gather_and_adjoint_all_reduce(tmp_path, oracle_mo
         dO_parts.append((int(r["lo"]), r["dO"]))
     dO = np.concatenate([d for _, d in sorted(dO_parts, key=lambda t: t[0])])
     assert np.abs(dO - dO_serial).max() <= 1e-12 * np.abs(dO_serial).max()
+    # Closest points: gathered blocks equal the serial query exactly, on every rank.
+    serial = oracle_mod.aabb_squared_distance(O, V, F)
+    for rank in range(world):
+        r = np.load(tmp_path / f"rank{rank}.npz")
+        for key, expected in zip(("sqrd", "index", "closest"), serial):
+            assert np.array_equal(r[key], expected)

@@ -269,6 +269,32 @@ int wn_signed_distance_device(void* tree, void* mesh, int precision, const doubl
                               int64_t np, double* s, int64_t* index, double* closest, double* w,
                               void* stream);
 
+/* ---- fast approximate winding numbers (no reference counterpart) --------
+ * The hierarchical evaluation of Barill et al., "Fast Winding Numbers for
+ * Soups and Clouds" (2018), which the reference lists as not covered
+ * (README.md:29): the faces are grouped by the median-split tree, a node whose
+ * centre p is farther than beta * r from the query (r: the radius about p
+ * holding its vertices) adds its second-order dipole expansion, nearer leaves
+ * add their faces' exact solid angles. Larger beta: more exact work, smaller
+ * error (beta >= 1; 2 is the published default). Each query sums in a fixed
+ * order, so results repeat bit for bit. */
+
+/* Builds the tree and moments on the host (no device work): *handle. */
+int wn_fast_create(const double* V, int64_t nv, const int64_t* F, int64_t nf, void** handle);
+int wn_fast_destroy(void* handle);
+/* out[0..n): faces, nodes, depth. */
+int wn_fast_info(void* handle, int64_t* out, int64_t n);
+/* Host evaluation of queries [q0, q1) of q (nq x 3) into w; reentrant over disjoint spans. */
+int wn_fast_eval_cpu(void* handle, const double* q, int64_t nq, double beta, double* w,
+                     int64_t q0, int64_t q1);
+/* GPU evaluation of device queries into device w, asynchronous on `stream`. The
+ * first GPU call uploads the tree to the current device; the handle then stays
+ * on that device. */
+int wn_fast_eval_device(void* handle, const double* q, int64_t nq, double beta, double* w,
+                        void* stream);
+/* Same with host buffers: copy in, evaluate, copy out, synchronise. */
+int wn_fast_eval_host(void* handle, const double* q, int64_t nq, double beta, double* w);
+
 #ifdef __cplusplus
 }
 #endif

@@ -19,6 +19,7 @@
 #include "../../include/wn_b200.h"
 #include "wn_aabb.h"
 #include "wn_adjoint.h"
+#include "wn_fwn.h"
 #include "wn_batch.h"
 #include "wn_internal.h"
 #include "wn_mixed.h"
@@ -909,6 +910,176 @@ int wn_signed_distance_device(void* tree, void* mesh, int precision, const doubl
   std::lock_guard<std::mutex> lock(g_mutex);
   const cudaError_t e = signed_from_winding(w, s, np, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "signed-distance launch");
+}
+
+// ---- fast (hierarchical) winding numbers ----------------------------------
+namespace {
+
+struct FwnHandle {
+  FwnHostTree host;
+  FwnDeviceTree dev;
+  int device = -1;  // device holding `dev` (-1: not uploaded yet)
+};
+
+int check_beta(double beta) {
+  if (!(beta >= 1.0) || !(beta <= 1e12))
+    return fail(WN_EINVAL, "beta must lie in [1, 1e12] (got %g)", beta);
+  return WN_OK;
+}
+
+// Uploads the tree to the current device on first use; the handle then stays
+// bound to that device.
+int fwn_upload(FwnHandle* h) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (h->device >= 0) {
+    if (h->device != dev)
+      return fail(WN_EINVAL, "fast winding-number handle lives on device %d, not %d",
+                  h->device, dev);
+    return WN_OK;
+  }
+  FwnDeviceTree& d = h->dev;
+  d.nnodes = h->host.nnodes;
+  d.depth = h->host.depth;
+  if (d.nnodes > 0) {
+    cudaError_t e;
+    if ((e = cudaMalloc(&d.nodes, sizeof(FwnNode) * d.nnodes)) != cudaSuccess ||
+        (e = cudaMalloc(&d.moments, sizeof(FwnMoments) * d.nnodes)) != cudaSuccess ||
+        (e = cudaMalloc(&d.tris, sizeof(AabbTriRec) * h->host.nf)) != cudaSuccess ||
+        (e = cudaMemcpy(d.nodes, h->host.nodes, sizeof(FwnNode) * d.nnodes,
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(d.moments, h->host.moments, sizeof(FwnMoments) * d.nnodes,
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(d.tris, h->host.tris, sizeof(AabbTriRec) * h->host.nf,
+                        cudaMemcpyHostToDevice)) != cudaSuccess) {
+      cudaFree(d.nodes);
+      cudaFree(d.moments);
+      cudaFree(d.tris);
+      d = FwnDeviceTree{};
+      return cuda_fail(e, "fast winding-number tree upload");
+    }
+  }
+  h->device = dev;
+  return WN_OK;
+}
+
+cudaError_t fwn_run(const FwnHandle* h, const double* q, int64_t nq, double beta, double* w,
+                    void* scratch, int* err, cudaStream_t st) {
+  uint32_t* perm = nullptr;
+  if (nq >= kAabbSortMin) {
+    perm = static_cast<uint32_t*>(scratch);
+    unsigned char* rest = static_cast<unsigned char*>(scratch) + align256(sizeof(uint32_t) * nq);
+    cudaError_t e = mixed_sort_queries(q, nq, perm, rest, mixed_sort_scratch_bytes(nq), st);
+    if (e != cudaSuccess) return e;
+  }
+  return fwn_eval_device(h->dev, q, nq, perm, beta, w, err, st);
+}
+
+}  // namespace
+
+int wn_fast_create(const double* V, int64_t nv, const int64_t* F, int64_t nf, void** out) {
+  if (!out) return fail(WN_EINVAL, "null output handle");
+  *out = nullptr;
+  if (nf > 0 && (!V || !F)) return fail(WN_EINVAL, "null pointer");
+  FwnHandle* h = new FwnHandle();
+  const char* why = "";
+  if (fwn_build(V, nv, F, nf, 0, &h->host, &why) != 0) {
+    delete h;
+    return fail(WN_EINVAL, "cannot build the fast winding-number tree: %s", why);
+  }
+  *out = h;
+  return WN_OK;
+}
+
+int wn_fast_destroy(void* handle) {
+  if (!handle) return WN_OK;
+  FwnHandle* h = static_cast<FwnHandle*>(handle);
+  if (h->device >= 0) {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(h->device);
+    cudaDeviceSynchronize();
+    cudaFree(h->dev.nodes);
+    cudaFree(h->dev.moments);
+    cudaFree(h->dev.tris);
+    cudaSetDevice(prev);
+  }
+  fwn_free(&h->host);
+  delete h;
+  return WN_OK;
+}
+
+int wn_fast_info(void* handle, int64_t* out, int64_t n) {
+  if (!handle || !out) return fail(WN_EINVAL, "null argument");
+  const FwnHandle* h = static_cast<const FwnHandle*>(handle);
+  const int64_t vals[] = {h->host.nf, h->host.nnodes, h->host.depth};
+  for (int64_t i = 0; i < n && i < 3; ++i) out[i] = vals[i];
+  return WN_OK;
+}
+
+int wn_fast_eval_cpu(void* handle, const double* q, int64_t nq, double beta, double* w,
+                     int64_t q0, int64_t q1) {
+  if (!handle) return fail(WN_EINVAL, "null handle");
+  if (int code = check_beta(beta)) return code;
+  if (nq < 0 || q0 < 0 || q1 > nq || q0 > q1) return fail(WN_EINVAL, "bad query range");
+  if (q1 == q0) return WN_OK;
+  if (!q || !w) return fail(WN_EINVAL, "null pointer");
+  fwn_eval_host(static_cast<const FwnHandle*>(handle)->host, q, q0, q1, beta, w);
+  return WN_OK;
+}
+
+int wn_fast_eval_device(void* handle, const double* q, int64_t nq, double beta, double* w,
+                        void* stream) {
+  if (!handle) return fail(WN_EINVAL, "null handle");
+  if (int code = check_beta(beta)) return code;
+  if (nq < 0 || nq > 0x7fffffffLL) return fail(WN_EINVAL, "bad nq=%lld", (long long)nq);
+  if (nq == 0) return WN_OK;
+  if (!q || !w) return fail(WN_EINVAL, "null pointer");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  FwnHandle* h = static_cast<FwnHandle*>(handle);
+  if ((code = fwn_upload(h)) != WN_OK) return code;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t sb = aabb_sort_bytes(nq);
+  void* scratch = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (sb && (e = cudaMallocAsync(&scratch, sb, st)) != cudaSuccess)
+    return cuda_fail(e, "device allocation");
+  e = fwn_run(h, q, nq, beta, w, scratch, c->err, st);
+  if (scratch) cudaFreeAsync(scratch, st);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "fast winding-number launch");
+}
+
+int wn_fast_eval_host(void* handle, const double* q, int64_t nq, double beta, double* w) {
+  if (!handle) return fail(WN_EINVAL, "null handle");
+  if (int code = check_beta(beta)) return code;
+  if (nq < 0 || nq > 0x7fffffffLL) return fail(WN_EINVAL, "bad nq=%lld", (long long)nq);
+  if (nq == 0) return WN_OK;
+  if (!q || !w) return fail(WN_EINVAL, "null pointer");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  FwnHandle* h = static_cast<FwnHandle*>(handle);
+  if ((code = fwn_upload(h)) != WN_OK) return code;
+  cudaError_t e;
+  if ((e = c->q.ensure(sizeof(double) * 3 * nq)) != cudaSuccess ||
+      (e = c->w.ensure(sizeof(double) * nq)) != cudaSuccess ||
+      (e = c->scratch.ensure(aabb_sort_bytes(nq) + 256)) != cudaSuccess)
+    return cuda_fail(e, "device allocation");
+  if ((e = cudaMemcpyAsync(c->q.ptr, q, sizeof(double) * 3 * nq, cudaMemcpyHostToDevice,
+                           c->stream)) != cudaSuccess)
+    return cuda_fail(e, "copy of the queries");
+  if ((e = fwn_run(h, static_cast<const double*>(c->q.ptr), nq, beta,
+                   static_cast<double*>(c->w.ptr), c->scratch.ptr, c->err, c->stream)) !=
+      cudaSuccess)
+    return cuda_fail(e, "fast winding-number launch");
+  if ((e = cudaMemcpyAsync(w, c->w.ptr, sizeof(double) * nq, cudaMemcpyDeviceToHost,
+                           c->stream)) != cudaSuccess)
+    return cuda_fail(e, "copy of the result");
+  return collect_device_error(c, c->stream);
 }
 
 // src/capi.mojo:945-947: 1 on success, 0 on failure (the shim raises). Large

@@ -85,6 +85,12 @@ _WN_SIGNATURES = {
     "wn_aabb_squared_distance_host": ([P, P, I, P, P, P], C_INT),
     "wn_signed_distance_device": ([P, P, C_INT, P, I, P, P, P, P, P], C_INT),
     "wn_closest_point": ([P, P, P], C_INT),
+    "wn_fast_create": ([P, I, P, I, ctypes.POINTER(P)], C_INT),
+    "wn_fast_destroy": ([P], C_INT),
+    "wn_fast_info": ([P, P, I], C_INT),
+    "wn_fast_eval_cpu": ([P, P, I, ctypes.c_double, P, I, I], C_INT),
+    "wn_fast_eval_device": ([P, P, I, ctypes.c_double, P, P], C_INT),
+    "wn_fast_eval_host": ([P, P, I, ctypes.c_double, P], C_INT),
 }
 
 # The reference caps its pool at four workers on a shared host (_lib.py:34-37).

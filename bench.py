@@ -22,7 +22,11 @@ Legs, all on the same inputs:
     the reference's CPU query) on the reference's own AABB benchmark shape
     (grid(350), 243,602 F x 10,000 points), on the c3 mesh x 2^20 queries and
     on grid(350) x 2^20 points: device time, end to end through the C ABI with
-    host buffers, the oracle on this host's cores, and an exactness check.
+    host buffers, the oracle on this host's cores, and an exactness check;
+  * fast_winding: the hierarchical approximation (Barill et al. 2018) on the
+    headline workload at beta = 2 and 4: device time, end to end, max / p99
+    error against the plain FP64 kernel's W, and the library's host evaluator
+    on this host's cores.
 `value` is whole-job pairs/s of the headline leg with inputs resident in HBM;
 `e2e` is the same leg through the C ABI with pinned host buffers, the
 host->device copies, device preprocessing and device->host copy inside the
@@ -41,7 +45,8 @@ threads) on a bounded sample of the same workload and prints the same metric.
 `--case NAME [--case-queries N]` runs one kernel on a small case twice and
 exits (the commands behind the ncu summaries in profiles/): fp64_c3 (streaming
 FP64 kernel), fp64_tiled_c3 (FP64 over the prepared mesh), mixed_c3, adjoint_c4
-(per-face mixed adjoint) and closest_c3 (closest-point traversal).
+(per-face mixed adjoint), closest_c3 (closest-point traversal) and fwn_c3 (fast
+winding number, beta = 2).
 """
 
 from __future__ import annotations
@@ -80,8 +85,9 @@ def parse_args():
     p.add_argument("--no-c4", action="store_true", help="skip the gradient workload")
     p.add_argument("--no-c5", action="store_true", help="skip the batched workload")
     p.add_argument("--no-closest", action="store_true", help="skip the closest-point workloads")
+    p.add_argument("--no-fast", action="store_true", help="skip the fast winding-number legs")
     p.add_argument("--case", choices=("fp64_c3", "fp64_tiled_c3", "mixed_c3", "adjoint_c4",
-                                      "closest_c3"),
+                                      "closest_c3", "fwn_c3"),
                    help="run one kernel on a small case twice (for profiling) and exit")
     p.add_argument("--case-queries", type=int, default=None)
     p.add_argument("--autotune", action="store_true",
@@ -549,6 +555,67 @@ def gpu_arm(args):
         closest["note"] = ("reference's published AABB.squared_distance for the "
                            "reference_bench shape: 9.12 ms (its own host, README.md:105)")
 
+    # Fast (hierarchical) winding numbers on the headline workload.
+    fast = None
+    if not args.no_fast:
+        import igl
+
+        fwn = igl.FastWindingNumber(V, F)
+        wf_d = torch.empty(nq, dtype=torch.float64, device=dev)
+        fast = {"workload": "c3: " + desc, "tree": fwn.info(),
+                "note": "error against the plain FP64 kernel's W on every query"}
+        have_exact = "fp64" in results
+        for beta in (2.0, 4.0):
+            def fast_step(beta=beta):
+                kernel_timed(lambda: check(handle.wn_fast_eval_device(
+                    fwn._handle, q_d.data_ptr(), nq, beta, wf_d.data_ptr(), sp)))
+
+            t_f, launches_f, t_fk = timed(fast_step, max(args.steps, 5), 3)
+            entry = {"ms_per_step": t_f * 1e3, "kernel_ms": t_fk * 1e3,
+                     "queries_per_s": world * nq / t_f,
+                     "pair_equivalent_per_s": world * pairs / t_f,
+                     "speedup_vs_exact_mixed": (results["mixed"][0] / t_f
+                                                if "mixed" in results else None)}
+            if have_exact:
+                err = (wf_d - w_d).abs()
+                entry["max_abs_err_vs_fp64"] = float(err.max())
+                entry["p99_abs_err_vs_fp64"] = float(torch.quantile(err.float(), 0.99))
+            if not args.no_e2e:
+                q_h = torch.from_numpy(O).pin_memory()
+                w_h = torch.empty(nq, dtype=torch.float64).pin_memory()
+                call = lambda beta=beta: check(handle.wn_fast_eval_host(  # noqa: E731
+                    fwn._handle, q_h.data_ptr(), nq, beta, w_h.data_ptr()))
+                call()
+                barrier()
+                t0 = time.perf_counter()
+                for _ in range(max(args.steps, 5)):
+                    call()
+                dt = (time.perf_counter() - t0) / max(args.steps, 5)
+                entry["e2e"] = {"value": world * nq / dt, "unit": "queries/s",
+                                "ms_per_step": dt * 1e3, "h2d_bytes_per_step": int(O.nbytes),
+                                "d2h_bytes_per_step": int(nq * 8),
+                                "path": "wn_fast_eval_host (C ABI, pinned host buffers)"}
+            if rank == 0 and world == 1 and not args.no_cpu_baseline:
+                cores = host_cores()
+                n_s = min(nq, 1 << 18)
+                w_s = np.empty(n_s)
+                O_s = np.ascontiguousarray(O[:n_s])
+                t0 = time.perf_counter()
+                fn = handle.wn_fast_eval_cpu
+                from concurrent.futures import ThreadPoolExecutor
+
+                parts = [(i * n_s // cores, (i + 1) * n_s // cores) for i in range(cores)]
+                with ThreadPoolExecutor(cores) as pool:
+                    list(pool.map(lambda ab, beta=beta: fn(fwn._handle, O_s.ctypes.data, n_s,
+                                                           beta, w_s.ctypes.data, ab[0], ab[1]),
+                                  parts))
+                dt = time.perf_counter() - t0
+                entry["cpu_host_evaluator"] = {
+                    "value": n_s / dt, "unit": "queries/s", "cores": cores,
+                    "sample": f"first {n_s} queries in {dt:.2f} s (wn_fast_eval_cpu spans)"}
+            fast[f"beta_{beta:g}"] = entry
+        fwn.close()
+
     # Accuracy of the mixed leg against the FP64 kernel on every query.
     accuracy = None
     if "mixed" in results and "fp64" in results:
@@ -653,6 +720,7 @@ def gpu_arm(args):
             "c4_fwd_bwd": c4,
             "c5_batched": c5,
             "closest_point": closest,
+            "fast_winding": fast,
             "accuracy": accuracy,
             "refinement": ({"pairs_refined_fp64_per_step": headline_refined,
                             "fraction": headline_refined / pairs}
@@ -674,7 +742,7 @@ def run_case(args):
 
     handle = _lib.lib()
     default_nq = {"fp64_c3": 16384, "fp64_tiled_c3": 32768, "mixed_c3": 65536,
-                  "adjoint_c4": 16384, "closest_c3": 1 << 20}[args.case]
+                  "adjoint_c4": 16384, "closest_c3": 1 << 20, "fwn_c3": 1 << 20}[args.case]
     nq = args.case_queries or default_nq
     V, F, O, _ = synthetic.workload("c4_grad" if args.case == "adjoint_c4" else "c3_mixed",
                                     n_queries=nq)
@@ -690,6 +758,14 @@ def run_case(args):
             tree = distance.DeviceAABB(V, F)
             w = tree.query(Ot)[0]
             tree.close()
+            rc = 0
+        elif args.case == "fwn_c3":
+            import igl
+
+            fwn = igl.FastWindingNumber(V, F)
+            w = fwn.evaluate_torch(Ot, beta=2.0)
+            torch.cuda.synchronize()
+            fwn.close()
             rc = 0
         else:
             mesh = wa.PreparedMesh(tri, ld, nf)

@@ -71,7 +71,14 @@ void mli_aabb_squared_distance(int64_t p, int64_t v, int64_t f, int64_t boxes, i
                                int64_t stack, int64_t np, int64_t nnodes, int64_t q0,
                                int64_t q1);
 
-/* The reference's other ten exports (src/capi.mojo:923-937, 962-1007) are
+/* Replaces src/capi.mojo:933-935 `mli_vertex_normals(v, f, dst, nv, nf,
+ * weighting)` (int64 host addresses and sizes, python/igl/_lib.py:21): CPU
+ * per-vertex normals into dst (nv x 3), weighting 0 uniform, 1 area, 2 angle,
+ * 3 default (= area), bit-identical to the reference's loop for 0, 1 and 3. */
+void mli_vertex_normals(int64_t v, int64_t f, int64_t dst, int64_t nv, int64_t nf,
+                        int64_t weighting);
+
+/* The reference's other nine exports (src/capi.mojo:923-932, 962-1007) are
  * exported under the same names so the reference shim's loader
  * (python/igl/_lib.py:122-130) resolves every symbol; they are outside this
  * library's scope and abort the process with a message if called. */
@@ -268,6 +275,22 @@ int wn_closest_point(const double* p, const double* tri9, double* out4);
 int wn_signed_distance_device(void* tree, void* mesh, int precision, const double* P,
                               int64_t np, double* s, int64_t* index, double* closest, double* w,
                               void* stream);
+
+/* ---- per-vertex normals on the GPU --------------------------------------
+ * The reference computes them only on the CPU (src/capi.mojo:146-202). Here the
+ * topology F (nf x 3 int64, indices in [0, nv)) is prepared once per mesh (a
+ * vertex -> (face, corner) list in face order, built on the device) and
+ * wn_vertex_normals_device then evaluates N (nv x 3) from V (nv x 3) in one
+ * launch, one thread per vertex, summing in the reference's order: uniform and
+ * area normals bit-identical to mli_vertex_normals, angle normals through
+ * CUDA's acos (within 1e-14). */
+int wn_normals_create(const int64_t* F, int64_t nf, int64_t nv, void* stream, void** handle);
+int wn_normals_destroy(void* handle);
+int wn_vertex_normals_device(void* handle, const double* V, int weighting, double* N,
+                             void* stream);
+/* One-shot GPU normals with host buffers (prepare, copy in, evaluate, copy out). */
+int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_t nf,
+                           int weighting, double* N);
 
 /* ---- fast approximate winding numbers (no reference counterpart) --------
  * The hierarchical evaluation of Barill et al., "Fast Winding Numbers for

@@ -20,6 +20,7 @@
 #include "wn_aabb.h"
 #include "wn_adjoint.h"
 #include "wn_fwn.h"
+#include "wn_normals.h"
 #include "wn_batch.h"
 #include "wn_internal.h"
 #include "wn_mixed.h"
@@ -262,8 +263,8 @@ int forward_mixed_host(const double* tri, const double* q, double* w, int64_t nf
 [[noreturn]] void out_of_scope(const char* name) {
   std::fprintf(stderr,
                "libwn_b200: %s is not provided: this library implements only the "
-               "winding-number and closest-point paths (mli_winding, mli_winding_gpu, "
-               "mli_aabb_squared_distance)\n",
+               "winding-number, closest-point and vertex-normal paths (mli_winding, "
+               "mli_winding_gpu, mli_aabb_squared_distance, mli_vertex_normals)\n",
                name);
   std::abort();
 }
@@ -1082,6 +1083,149 @@ int wn_fast_eval_host(void* handle, const double* q, int64_t nq, double beta, do
   return collect_device_error(c, c->stream);
 }
 
+// ---- per-vertex normals ----------------------------------------------------
+namespace {
+
+struct NormalsHandle {
+  NormalsTopology t;
+  int device = -1;
+};
+
+void normals_release(NormalsHandle* h) {
+  cudaFree(h->t.F);
+  cudaFree(h->t.indptr);
+  cudaFree(h->t.entries);
+  h->t = NormalsTopology{};
+}
+
+int check_weighting(int weighting) {
+  if (weighting < 0 || weighting > 3)
+    return fail(WN_EINVAL, "weighting must be 0 (uniform), 1 (area), 2 (angle) or 3 (default)");
+  return WN_OK;
+}
+
+// Validates F on the host, uploads it as int32 and builds the incidence lists
+// on `st` (caller holds g_mutex and a context).
+int normals_prepare(const int64_t* F, int64_t nf, int64_t nv, cudaStream_t st,
+                    NormalsHandle* h) {
+  if (nf < 0 || nv < 0) return fail(WN_EINVAL, "negative size");
+  if (nv > 0x7fffffffLL || 3 * nf > 0x7fffffffLL)
+    return fail(WN_EINVAL, "more than 2^31-1 vertices or incidences");
+  if (nf > 0 && !F) return fail(WN_EINVAL, "null pointer");
+  std::vector<int32_t> f32(static_cast<size_t>(3 * nf));
+  for (int64_t i = 0; i < 3 * nf; ++i) {
+    if (F[i] < 0 || F[i] >= nv) return fail(WN_EINVAL, "face index outside V");
+    f32[i] = static_cast<int32_t>(F[i]);
+  }
+  h->t.nf = nf;
+  h->t.nv = nv;
+  cudaGetDevice(&h->device);
+  cudaError_t e;
+  if ((e = cudaMalloc(&h->t.F, sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess ||
+      (e = cudaMalloc(&h->t.indptr, sizeof(int32_t) * (nv + 1))) != cudaSuccess ||
+      (e = cudaMalloc(&h->t.entries, sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess) {
+    normals_release(h);
+    return cuda_fail(e, "device allocation");
+  }
+  if (nf > 0 && (e = cudaMemcpyAsync(h->t.F, f32.data(), sizeof(int32_t) * 3 * nf,
+                                     cudaMemcpyHostToDevice, st)) != cudaSuccess) {
+    normals_release(h);
+    return cuda_fail(e, "copy of the faces");
+  }
+  const size_t sb = normals_scratch_bytes(nf);
+  void* scratch = nullptr;
+  if ((e = cudaMallocAsync(&scratch, sb, st)) != cudaSuccess) {
+    normals_release(h);
+    return cuda_fail(e, "device allocation");
+  }
+  e = normals_build(h->t, scratch, sb, st);
+  cudaFreeAsync(scratch, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the host copy of F goes out of scope
+  if (e != cudaSuccess) {
+    normals_release(h);
+    return cuda_fail(e, "incidence list build");
+  }
+  return WN_OK;
+}
+
+}  // namespace
+
+int wn_normals_create(const int64_t* F, int64_t nf, int64_t nv, void* stream, void** out) {
+  if (!out) return fail(WN_EINVAL, "null output handle");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  if (!context(&code)) return code;
+  NormalsHandle* h = new NormalsHandle();
+  if ((code = normals_prepare(F, nf, nv, static_cast<cudaStream_t>(stream), h)) != WN_OK) {
+    delete h;
+    return code;
+  }
+  *out = h;
+  return WN_OK;
+}
+
+int wn_normals_destroy(void* handle) {
+  if (!handle) return WN_OK;
+  NormalsHandle* h = static_cast<NormalsHandle*>(handle);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(h->device);
+  cudaDeviceSynchronize();
+  normals_release(h);
+  cudaSetDevice(prev);
+  delete h;
+  return WN_OK;
+}
+
+int wn_vertex_normals_device(void* handle, const double* V, int weighting, double* N,
+                             void* stream) {
+  if (!handle) return fail(WN_EINVAL, "null handle");
+  if (int code = check_weighting(weighting)) return code;
+  const NormalsHandle* h = static_cast<const NormalsHandle*>(handle);
+  if (h->t.nv == 0) return WN_OK;
+  if (!V || !N) return fail(WN_EINVAL, "null pointer");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  if (!context(&code)) return code;
+  const cudaError_t e = normals_eval(h->t, V, weighting == 3 ? 1 : weighting, N,
+                                     static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "vertex-normal launch");
+}
+
+int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_t nf,
+                           int weighting, double* N) {
+  if (int code = check_weighting(weighting)) return code;
+  if (nv < 0 || nf < 0) return fail(WN_EINVAL, "negative size");
+  if (nv == 0) return WN_OK;
+  if (!V || !N) return fail(WN_EINVAL, "null pointer");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  NormalsHandle h;
+  if ((code = normals_prepare(F, nf, nv, c->stream, &h)) != WN_OK) return code;
+  cudaError_t e;
+  if ((e = c->q.ensure(sizeof(double) * 3 * nv)) != cudaSuccess ||
+      (e = c->w.ensure(sizeof(double) * 3 * nv)) != cudaSuccess) {
+    normals_release(&h);
+    return cuda_fail(e, "device allocation");
+  }
+  if ((e = cudaMemcpyAsync(c->q.ptr, V, sizeof(double) * 3 * nv, cudaMemcpyHostToDevice,
+                           c->stream)) != cudaSuccess ||
+      (e = normals_eval(h.t, static_cast<const double*>(c->q.ptr), weighting == 3 ? 1 : weighting,
+                        static_cast<double*>(c->w.ptr), c->stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(N, c->w.ptr, sizeof(double) * 3 * nv, cudaMemcpyDeviceToHost,
+                           c->stream)) != cudaSuccess) {
+    cudaStreamSynchronize(c->stream);
+    normals_release(&h);
+    return cuda_fail(e, "vertex normals");
+  }
+  code = collect_device_error(c, c->stream);
+  normals_release(&h);
+  return code;
+}
+
 // src/capi.mojo:945-947: 1 on success, 0 on failure (the shim raises). Large
 // problems go through the prepared-mesh FP64 kernel (its ~2 ms preparation is
 // repaid above ~1e9 pairs), small ones through the streaming FP64 kernel; both
@@ -1096,15 +1240,12 @@ int64_t mli_winding_gpu(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t
              : 0;
 }
 
-// Out-of-scope reference exports (src/capi.mojo:923-937, 962-1007).
+// Out-of-scope reference exports (src/capi.mojo:923-932, 962-1007).
 void mli_cot_entries(int64_t, int64_t, int64_t, int64_t, int64_t) {
   out_of_scope("mli_cot_entries");
 }
 void mli_mass_contributions(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
   out_of_scope("mli_mass_contributions");
-}
-void mli_vertex_normals(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
-  out_of_scope("mli_vertex_normals");
 }
 void mli_heat_vector_divergence(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {
   out_of_scope("mli_heat_vector_divergence");

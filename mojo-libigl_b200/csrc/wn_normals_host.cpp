@@ -1,0 +1,29 @@
+// Host (device="cpu") path of the per-vertex normals: `mli_vertex_normals`,
+// the reference's C-ABI export (src/capi.mojo:933-935, kernel capi.mojo:146-202),
+// on the shared arithmetic of wn_normals.cuh (built with -ffp-contract=off).
+#include <cstdint>
+
+#include "wn_normals.cuh"
+
+extern "C" {
+
+// Every argument an int64 (host addresses, python/igl/_lib.py:21); weighting
+// 0 uniform, 1 area, 2 angle, 3 default (= area).
+void mli_vertex_normals(int64_t v_addr, int64_t f_addr, int64_t dst_addr, int64_t nv, int64_t nf,
+                        int64_t weighting) {
+  const double* v = reinterpret_cast<const double*>(v_addr);
+  const int64_t* f = reinterpret_cast<const int64_t*>(f_addr);
+  double* dst = reinterpret_cast<double*>(dst_addr);
+  for (int64_t i = 0; i < 3 * nv; ++i) dst[i] = 0.0;
+  const int mode = weighting == 3 ? wn::kNormalsArea : static_cast<int>(weighting);
+  for (int64_t fi = 0; fi < nf; ++fi) {
+    const double* A = v + 3 * f[3 * fi];
+    const double* B = v + 3 * f[3 * fi + 1];
+    const double* C = v + 3 * f[3 * fi + 2];
+    for (int corner = 0; corner < 3; ++corner)
+      wn::normal_corner_add(A, B, C, corner, mode, dst + 3 * f[3 * fi + corner]);
+  }
+  for (int64_t i = 0; i < nv; ++i) wn::normal_finish(dst + 3 * i);
+}
+
+}  // extern "C"

@@ -7,7 +7,8 @@ types and error classes. ``device="gpu"`` runs hand-written sm_100a kernels in
 ``libwn_b200.so``; ``device="cpu"`` runs the library's host path over the
 reference's thread fan-out.
 
-Also ``fast_winding_number`` / ``FastWindingNumber``: the hierarchical
+Also ``per_vertex_normals`` (python/igl/__init__.py:195-211 of the reference)
+with a ``device`` keyword, and ``fast_winding_number`` / ``FastWindingNumber``: the hierarchical
 approximation of Barill et al. 2018, which the reference lists as not covered.
 
 Also the closest-point path beside it (python/igl/__init__.py:286-404):
@@ -25,6 +26,7 @@ from __future__ import annotations
 
 import ctypes
 import operator
+from enum import IntEnum
 
 import numpy as np
 
@@ -33,7 +35,7 @@ from ._lib import addr, fan_out, last_error, lib, worker_count
 
 def __getattr__(name):
     # torch-dependent submodules load on first use.
-    if name in ("autograd", "batched", "autotune", "distance"):
+    if name in ("autograd", "batched", "autotune", "distance", "normals"):
         import importlib
 
         return importlib.import_module(f".{name}", __name__)
@@ -49,6 +51,8 @@ __all__ = [
     "signed_distance",
     "FastWindingNumber",
     "fast_winding_number",
+    "PerVertexNormalsWeightingType",
+    "per_vertex_normals",
 ]
 
 # "fp64": the plain FP64 kernel, pair terms bit-identical to the reference.
@@ -478,3 +482,55 @@ def fast_winding_number(V, F, O, device="cpu", *, beta=2.0):
         return fwn.evaluate(O, device=device, beta=beta)
     finally:
         fwn.close()
+
+
+# ---- per-vertex normals (reference python/igl/__init__.py:32-36, 52-63, 195-211) ----
+class PerVertexNormalsWeightingType(IntEnum):
+    PER_VERTEX_NORMALS_WEIGHTING_TYPE_UNIFORM = 0
+    PER_VERTEX_NORMALS_WEIGHTING_TYPE_AREA = 1
+    PER_VERTEX_NORMALS_WEIGHTING_TYPE_ANGLE = 2
+    PER_VERTEX_NORMALS_WEIGHTING_TYPE_DEFAULT = 3
+
+
+PER_VERTEX_NORMALS_WEIGHTING_TYPE_UNIFORM = (
+    PerVertexNormalsWeightingType.PER_VERTEX_NORMALS_WEIGHTING_TYPE_UNIFORM
+)
+PER_VERTEX_NORMALS_WEIGHTING_TYPE_AREA = (
+    PerVertexNormalsWeightingType.PER_VERTEX_NORMALS_WEIGHTING_TYPE_AREA
+)
+PER_VERTEX_NORMALS_WEIGHTING_TYPE_ANGLE = (
+    PerVertexNormalsWeightingType.PER_VERTEX_NORMALS_WEIGHTING_TYPE_ANGLE
+)
+PER_VERTEX_NORMALS_WEIGHTING_TYPE_DEFAULT = (
+    PerVertexNormalsWeightingType.PER_VERTEX_NORMALS_WEIGHTING_TYPE_DEFAULT
+)
+
+
+def per_vertex_normals(V, F, weighting=PER_VERTEX_NORMALS_WEIGHTING_TYPE_DEFAULT, FN=None,
+                       device="cpu"):
+    """Compute normalized uniform-, area-, or angle-weighted vertex normals.
+
+    ``device="gpu"`` evaluates them on the GPU (one thread per vertex over its
+    faces in the reference's order): the same numbers for uniform and area
+    weights, the same within 1e-14 for angle weights.
+    """
+    if FN is not None:
+        raise NotImplementedError("the precomputed-FN overload is not covered")
+    vertices, faces = _mesh(V, F)
+    mode = _integer(weighting, "weighting")
+    if mode not in (0, 1, 2, 3):
+        raise ValueError("invalid PerVertexNormalsWeightingType")
+    selected = _device_name(device)
+    result = np.zeros((len(vertices), 3), dtype=np.float64)
+    if len(faces):
+        handle = lib()
+        if selected == "gpu":
+            _require_gpu()
+            status = handle.wn_vertex_normals_host(addr(vertices), len(vertices), addr(faces),
+                                                   len(faces), mode, addr(result))
+            if status:
+                raise RuntimeError("the B200 vertex-normal kernel failed: " + last_error(handle))
+        else:
+            handle.mli_vertex_normals(addr(vertices), addr(faces), addr(result), len(vertices),
+                                      len(faces), mode)
+    return result

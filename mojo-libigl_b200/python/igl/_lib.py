@@ -27,9 +27,9 @@ P = ctypes.c_void_p
 C_INT = ctypes.c_int
 
 # Reference python/igl/_lib.py:18-32: the thirteen C-ABI names with their
-# argument counts. libwn_b200 implements the two winding entries and the
-# closest-point query, and exports the other ten only so that loaders
-# resolving every name succeed.
+# argument counts. libwn_b200 implements the two winding entries, the
+# closest-point query and the vertex normals, and exports the other nine only
+# so that loaders resolving every name succeed.
 _SIGNATURES = {
     "mli_cot_entries": ([I, I, I, I, I], None),
     "mli_mass_contributions": ([I, I, I, I, I, I], None),
@@ -85,6 +85,10 @@ _WN_SIGNATURES = {
     "wn_aabb_squared_distance_host": ([P, P, I, P, P, P], C_INT),
     "wn_signed_distance_device": ([P, P, C_INT, P, I, P, P, P, P, P], C_INT),
     "wn_closest_point": ([P, P, P], C_INT),
+    "wn_normals_create": ([P, I, I, P, ctypes.POINTER(P)], C_INT),
+    "wn_normals_destroy": ([P], C_INT),
+    "wn_vertex_normals_device": ([P, P, C_INT, P, P], C_INT),
+    "wn_vertex_normals_host": ([P, I, P, I, C_INT, P], C_INT),
     "wn_fast_create": ([P, I, P, I, ctypes.POINTER(P)], C_INT),
     "wn_fast_destroy": ([P], C_INT),
     "wn_fast_info": ([P, P, I], C_INT),

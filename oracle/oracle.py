@@ -15,6 +15,8 @@ checkers that pin it:
   solid-angle formula, the reference for the hand-written adjoint.
 * ``fast_winding_number`` restates the hierarchical winding number of Barill
   et al. 2018 (not in the reference; checked against the exact sum above).
+* ``per_vertex_normals`` drives the C restatement of the reference's vertex
+  normals (src/capi.mojo:146-202, normals_oracle.cpp).
 * ``build_aabb`` restates the reference's median-split hierarchy
   (python/igl/__init__.py:286-319) and ``aabb_squared_distance`` drives the C
   restatement of its closest-point traversal (src/capi.mojo:401-586,
@@ -62,6 +64,8 @@ def lib() -> ctypes.CDLL:
         handle.oracle_pair_terms.restype = None
         handle.mli_aabb_squared_distance.argtypes = [I64] * 14
         handle.mli_aabb_squared_distance.restype = None
+        handle.mli_vertex_normals.argtypes = [I64] * 6
+        handle.mli_vertex_normals.restype = None
         handle.oracle_closest_point.argtypes = [ctypes.c_void_p] * 3
         handle.oracle_closest_point.restype = None
         _handle = handle
@@ -324,4 +328,16 @@ def fast_winding_number(V, F, O, beta: float = 2.0, leaf_size: int = 8):
             else:
                 stack += [int(nodes[i, 1]), int(nodes[i, 0])]
         out[qi] = total
+    return out
+
+
+# ---- per-vertex normals ------------------------------------------------------
+def per_vertex_normals(V, F, weighting: int = 3) -> np.ndarray:
+    """(nv, 3) normals by the C restatement of src/capi.mojo:146-202."""
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    F = np.ascontiguousarray(F, dtype=np.int64)
+    out = np.zeros((len(V), 3))
+    if len(F):
+        lib().mli_vertex_normals(V.ctypes.data, F.ctypes.data, out.ctypes.data, len(V), len(F),
+                                 int(weighting))
     return out

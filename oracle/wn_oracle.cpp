@@ -21,8 +21,9 @@
 //   * atan2 and sqrt are the C library's (correctly rounded sqrt; glibc atan2).
 //
 // The closest-point query (`mli_aabb_squared_distance`) lives in
-// aabb_oracle.cpp, linked into the same library. The library also exports the
-// reference's other eleven `mli_*` C-ABI names (capi.mojo:923-1007) as no-ops,
+// aabb_oracle.cpp and the vertex normals (`mli_vertex_normals`) in
+// normals_oracle.cpp, linked into the same library. The library also exports
+// the reference's other nine `mli_*` C-ABI names (capi.mojo:923-1007) as no-ops,
 // so the reference's own Python shim
 // (python/igl/_lib.py:122-130, which resolves all thirteen names) can load this
 // file through MOJO_LIBIGL_LIB and drive `mli_winding` unchanged.
@@ -115,11 +116,10 @@ void mli_winding(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t nq, in
 // The oracle has no GPU: report failure exactly as capi.mojo:397-398 does.
 int64_t mli_winding_gpu(int64_t, int64_t, int64_t, int64_t, int64_t) { return 0; }
 
-// The remaining reference exports (capi.mojo:923-937, 962-1007): out of scope,
+// The remaining reference exports (capi.mojo:923-932, 962-1007): out of scope,
 // present only so the reference shim's loader finds every name.
 void mli_cot_entries(int64_t, int64_t, int64_t, int64_t, int64_t) {}
 void mli_mass_contributions(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {}
-void mli_vertex_normals(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {}
 void mli_heat_vector_divergence(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {}
 void mli_heat_precompute(int64_t, int64_t, int64_t, int64_t) {}
 void mli_arap_covariance(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t,

@@ -1,0 +1,72 @@
+"""Per-vertex normals on the B200 vs the reference-generated fixtures and the
+host path: bit-identical for uniform and area weights (the same separately
+rounded arithmetic, summed per vertex in the reference's face order), within
+1e-14 for angle weights (CUDA's acos vs the C library's)."""
+
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import igl
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+CASES = sorted(os.path.basename(p)[8:-4] for p in glob.glob(os.path.join(GOLDEN, "normals_*.npz")))
+
+
+def _same(actual, expected, weighting):
+    if weighting == 2:
+        return np.abs(actual - expected).max() <= 1e-14
+    return actual.tobytes() == expected.tobytes()
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("weighting", [0, 1, 2, 3])
+def test_golden(gpu_required, name, weighting):
+    g = np.load(os.path.join(GOLDEN, f"normals_{name}.npz"))
+    actual = igl.per_vertex_normals(g["V"], g["F"], weighting, device="gpu")
+    assert _same(actual, g[f"N{weighting}"], weighting)
+
+
+def test_large_soup_matches_host(gpu_required):
+    V, F = igl.synthetic.bumpy_icosphere(7, seed=31)
+    degenerate = [[5, 5, 9], [7, 7, 7]]
+    # Flipped copies cancel their originals exactly; bit-identical sums still agree.
+    soup = np.concatenate([F, F[:1000, [0, 2, 1]], degenerate])
+    for weighting in (0, 1):
+        host = igl.per_vertex_normals(V, soup, weighting)
+        assert _same(igl.per_vertex_normals(V, soup, weighting, device="gpu"), host, weighting)
+    # Angle weights differ in the last bit of acos, so they are compared where the
+    # sums do not cancel: normalising a cancelled sum's rounding residue would turn
+    # that last bit into an arbitrary direction.
+    closed = np.concatenate([F, degenerate])
+    host = igl.per_vertex_normals(V, closed, 2)
+    assert _same(igl.per_vertex_normals(V, closed, 2, device="gpu"), host, 2)
+
+
+def test_device_topology_reused_for_new_positions(gpu_required):
+    import torch
+
+    from igl import normals
+
+    V, F = igl.synthetic.bumpy_icosphere(5, seed=3)
+    dn = normals.DeviceNormals(F, len(V))
+    for step in range(3):
+        Vs = V * (1.0 + 0.1 * step) + 0.01 * step
+        got = dn.evaluate(torch.from_numpy(Vs).cuda(), 1)
+        torch.cuda.synchronize()
+        assert got.cpu().numpy().tobytes() == igl.per_vertex_normals(Vs, F, 1).tobytes()
+    dn.close()
+
+
+def test_unreferenced_vertices_and_empty_faces(gpu_required):
+    V, F = igl.synthetic.bumpy_icosphere(2, seed=4)
+    V = np.concatenate([V, [[9.0, 9.0, 9.0], [8.0, 8.0, 8.0]]])
+    N = igl.per_vertex_normals(V, F, device="gpu")
+    assert np.array_equal(N[-2:], np.zeros((2, 3)))
+    assert N.tobytes() == igl.per_vertex_normals(V, F).tobytes()
+    assert np.array_equal(igl.per_vertex_normals(V, np.zeros((0, 3), np.int64), device="gpu"),
+                          np.zeros_like(V))

@@ -23,6 +23,11 @@ Legs, all on the same inputs:
     (grid(350), 243,602 F x 10,000 points), on the c3 mesh x 2^20 queries and
     on grid(350) x 2^20 points: device time, end to end through the C ABI with
     host buffers, the oracle on this host's cores, and an exactness check;
+  * vertex_normals: per-vertex normals (area weights) on the reference's
+    benchmark shape (grid(350), 243,602 F) and on a subdivision-9 sphere
+    (5,242,880 F): topology preparation once, then device time per evaluation
+    with the achieved share of HBM bandwidth, end to end through the C ABI
+    (preparation included), and the reference's serial CPU loop (the oracle);
   * fast_winding: the hierarchical approximation (Barill et al. 2018) on the
     headline workload at beta = 2 and 4: device time, end to end, max / p99
     error against the plain FP64 kernel's W, and the library's host evaluator
@@ -45,8 +50,9 @@ threads) on a bounded sample of the same workload and prints the same metric.
 `--case NAME [--case-queries N]` runs one kernel on a small case twice and
 exits (the commands behind the ncu summaries in profiles/): fp64_c3 (streaming
 FP64 kernel), fp64_tiled_c3 (FP64 over the prepared mesh), mixed_c3, adjoint_c4
-(per-face mixed adjoint), closest_c3 (closest-point traversal) and fwn_c3 (fast
-winding number, beta = 2).
+(per-face mixed adjoint), closest_c3 (closest-point traversal), fwn_c3 (fast
+winding number, beta = 2) and normals_s9 (area-weighted vertex normals of the
+subdivision-9 sphere).
 """
 
 from __future__ import annotations
@@ -86,8 +92,9 @@ def parse_args():
     p.add_argument("--no-c5", action="store_true", help="skip the batched workload")
     p.add_argument("--no-closest", action="store_true", help="skip the closest-point workloads")
     p.add_argument("--no-fast", action="store_true", help="skip the fast winding-number legs")
+    p.add_argument("--no-normals", action="store_true", help="skip the vertex-normal workloads")
     p.add_argument("--case", choices=("fp64_c3", "fp64_tiled_c3", "mixed_c3", "adjoint_c4",
-                                      "closest_c3", "fwn_c3"),
+                                      "closest_c3", "fwn_c3", "normals_s9"),
                    help="run one kernel on a small case twice (for profiling) and exit")
     p.add_argument("--case-queries", type=int, default=None)
     p.add_argument("--autotune", action="store_true",
@@ -555,6 +562,88 @@ def gpu_arm(args):
         closest["note"] = ("reference's published AABB.squared_distance for the "
                            "reference_bench shape: 9.12 ms (its own host, README.md:105)")
 
+    # Per-vertex normals (area weights): prepared topology, then one launch per call.
+    normals_out = None
+    if not args.no_normals:
+        from igl import normals as wnorm
+        from igl import synthetic
+
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        normals_out = {}
+        hbm = None
+        peaks = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        if os.path.exists(peaks):
+            hbm = json.load(open(peaks)).get("hbm_gbs")
+        meshes = [("reference_bench", "grid(350) height field (122,500 V, 243,602 F), area "
+                   "weights (the reference's per_vertex_normals benchmark shape)",
+                   *synthetic.terrain_grid(350)),
+                  ("s9", "bumpy icosphere s=9 (2,621,442 V, 5,242,880 F), area weights",
+                   *synthetic.bumpy_icosphere(9, seed=91))]
+        for key, desc_n, Vn, Fn in meshes:
+            nvn, nfn = len(Vn), len(Fn)
+            t0 = time.perf_counter()
+            dn = wnorm.DeviceNormals(Fn, nvn)
+            torch.cuda.synchronize()
+            t_prep = time.perf_counter() - t0
+            Vn_d = torch.from_numpy(Vn).to(dev)
+            Nn_d = torch.empty((nvn, 3), dtype=torch.float64, device=dev)
+
+            def normals_step():
+                kernel_timed(lambda: check(handle.wn_vertex_normals_device(
+                    dn.h, Vn_d.data_ptr(), 1, Nn_d.data_ptr(), sp)))
+
+            t_n, launches_n, t_nk = timed(normals_step, max(args.steps, 5), 3)
+            # Algorithmic bytes: V and N (24 B per vertex each), int32 faces (12 B per
+            # face), the vertex -> (face, corner) lists (4 B per vertex + 12 B per face).
+            alg = 52 * nvn + 24 * nfn + 4
+            entry = {"workload": desc_n, "vertices": nvn, "faces": nfn,
+                     "prepare_topology_ms": t_prep * 1e3,
+                     "ms_per_step": t_n * 1e3, "kernel_ms": t_nk * 1e3,
+                     "vertices_per_s": world * nvn / t_n,
+                     "roofline": {"bound": "hbm", "algorithmic_bytes": alg,
+                                  "achieved": alg / t_nk / 1e9, "peak": hbm, "unit": "GB/s",
+                                  "frac": (alg / t_nk / 1e9 / hbm) if hbm else None,
+                                  "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}}
+            Nd = Nn_d.cpu().numpy()
+            host = np.zeros_like(Vn)
+            t0 = time.perf_counter()
+            handle.mli_vertex_normals(Vn.ctypes.data, Fn.ctypes.data, host.ctypes.data, nvn, nfn, 1)
+            dt_host = time.perf_counter() - t0
+            entry["bit_identical_to_host_path"] = Nd.tobytes() == host.tobytes()
+            entry["host_path_ms"] = dt_host * 1e3
+            if not args.no_e2e:
+                V_h = torch.from_numpy(Vn).pin_memory()
+                N_h = torch.empty((nvn, 3), dtype=torch.float64).pin_memory()
+                call = lambda: check(handle.wn_vertex_normals_host(  # noqa: E731
+                    V_h.data_ptr(), nvn, Fn.ctypes.data, nfn, 1, N_h.data_ptr()))
+                call()
+                reps = 3
+                t0 = time.perf_counter()
+                for _ in range(reps):
+                    call()
+                dt_e = (time.perf_counter() - t0) / reps
+                entry["e2e"] = {"value": world * nvn / dt_e, "unit": "vertices/s",
+                                "ms_per_step": dt_e * 1e3,
+                                "h2d_bytes_per_step": int(Vn.nbytes + Fn.nbytes),
+                                "d2h_bytes_per_step": int(nvn * 24),
+                                "path": "wn_vertex_normals_host (C ABI, one shot: faces "
+                                        "validated and prepared inside the timed region)"}
+            if rank == 0 and world == 1 and not args.no_cpu_baseline:
+                t0 = time.perf_counter()
+                oracle.per_vertex_normals(Vn, Fn, 1)
+                dt_o = time.perf_counter() - t0
+                entry["cpu_baseline"] = {"value": nvn / dt_o, "unit": "vertices/s", "cores": 1,
+                                         "kind": "port", "ms": dt_o * 1e3,
+                                         "sample": "whole mesh, the oracle restatement of "
+                                                   "src/capi.mojo:146-202 (serial, as the "
+                                                   "reference's loop)"}
+            normals_out[key] = entry
+            dn.close()
+        normals_out["note"] = ("reference's published per_vertex_normals (area, 243.6k F): "
+                               "6.15 ms on its own host (README.md:101)")
+
     # Fast (hierarchical) winding numbers on the headline workload.
     fast = None
     if not args.no_fast:
@@ -721,6 +810,7 @@ def gpu_arm(args):
             "c5_batched": c5,
             "closest_point": closest,
             "fast_winding": fast,
+            "vertex_normals": normals_out,
             "accuracy": accuracy,
             "refinement": ({"pairs_refined_fp64_per_step": headline_refined,
                             "fraction": headline_refined / pairs}
@@ -737,12 +827,26 @@ def run_case(args):
     """One kernel, twice, on a reduced query batch of the c3 (or c4) workload."""
     import torch
 
+    if args.case == "normals_s9":
+        from igl import normals, synthetic
+
+        V, F = synthetic.bumpy_icosphere(9, seed=91)
+        dn = normals.DeviceNormals(F, len(V))
+        Vt = torch.from_numpy(V).cuda()
+        for _ in range(2):
+            N = dn.evaluate(Vt, 1)
+        torch.cuda.synchronize()
+        dn.close()
+        print("ok", args.case, len(F), len(V), float(N.abs().sum()))
+        return
+
     from igl import _lib, distance, synthetic
     from igl import autograd as wa
 
     handle = _lib.lib()
     default_nq = {"fp64_c3": 16384, "fp64_tiled_c3": 32768, "mixed_c3": 65536,
-                  "adjoint_c4": 16384, "closest_c3": 1 << 20, "fwn_c3": 1 << 20}[args.case]
+                  "adjoint_c4": 16384, "closest_c3": 1 << 20, "fwn_c3": 1 << 20,
+                  "normals_s9": 1}[args.case]
     nq = args.case_queries or default_nq
     V, F, O, _ = synthetic.workload("c4_grad" if args.case == "adjoint_c4" else "c3_mixed",
                                     n_queries=nq)

@@ -1095,6 +1095,7 @@ void normals_release(NormalsHandle* h) {
   cudaFree(h->t.F);
   cudaFree(h->t.indptr);
   cudaFree(h->t.entries);
+  cudaFree(h->t.contrib);
   h->t = NormalsTopology{};
 }
 
@@ -1104,19 +1105,15 @@ int check_weighting(int weighting) {
   return WN_OK;
 }
 
-// Validates F on the host, uploads it as int32 and builds the incidence lists
-// on `st` (caller holds g_mutex and a context).
+// Uploads F (host, nf x 3 int64), checks and converts it on the device and
+// builds the incidence lists on `st`; returns after `st` drains (caller holds
+// g_mutex and a context).
 int normals_prepare(const int64_t* F, int64_t nf, int64_t nv, cudaStream_t st,
                     NormalsHandle* h) {
   if (nf < 0 || nv < 0) return fail(WN_EINVAL, "negative size");
   if (nv > 0x7fffffffLL || 3 * nf > 0x7fffffffLL)
     return fail(WN_EINVAL, "more than 2^31-1 vertices or incidences");
   if (nf > 0 && !F) return fail(WN_EINVAL, "null pointer");
-  std::vector<int32_t> f32(static_cast<size_t>(3 * nf));
-  for (int64_t i = 0; i < 3 * nf; ++i) {
-    if (F[i] < 0 || F[i] >= nv) return fail(WN_EINVAL, "face index outside V");
-    f32[i] = static_cast<int32_t>(F[i]);
-  }
   h->t.nf = nf;
   h->t.nv = nv;
   cudaGetDevice(&h->device);
@@ -1127,24 +1124,45 @@ int normals_prepare(const int64_t* F, int64_t nf, int64_t nv, cudaStream_t st,
     normals_release(h);
     return cuda_fail(e, "device allocation");
   }
-  if (nf > 0 && (e = cudaMemcpyAsync(h->t.F, f32.data(), sizeof(int32_t) * 3 * nf,
-                                     cudaMemcpyHostToDevice, st)) != cudaSuccess) {
-    normals_release(h);
-    return cuda_fail(e, "copy of the faces");
-  }
-  const size_t sb = normals_scratch_bytes(nf);
-  void* scratch = nullptr;
-  if ((e = cudaMallocAsync(&scratch, sb, st)) != cudaSuccess) {
+  const size_t f64_bytes = ((sizeof(int64_t) * 3 * nf + 255) / 256) * 256;
+  const size_t sb = f64_bytes + 256 + normals_scratch_bytes(nf);
+  unsigned char* scratch = nullptr;
+  if ((e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), sb, st)) != cudaSuccess) {
     normals_release(h);
     return cuda_fail(e, "device allocation");
   }
-  e = normals_build(h->t, scratch, sb, st);
+  int64_t* F64 = reinterpret_cast<int64_t*>(scratch);
+  int* bad = reinterpret_cast<int*>(scratch + f64_bytes);
+  if (nf > 0)
+    e = cudaMemcpyAsync(F64, F, sizeof(int64_t) * 3 * nf, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = normals_build(h->t, F64, bad, scratch + f64_bytes + 256, normals_scratch_bytes(nf), st);
+  int bad_h = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&bad_h, bad, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaFreeAsync(scratch, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the host copy of F goes out of scope
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     normals_release(h);
     return cuda_fail(e, "incidence list build");
   }
+  if (bad_h != 0) {
+    normals_release(h);
+    return fail(WN_EINVAL, "%d face indices outside V", bad_h);
+  }
+  return WN_OK;
+}
+
+// Grows the per-face contribution buffer for `mode` (uniform/area: 3 doubles
+// per face, angle: 9).
+int normals_contrib(NormalsHandle* h, int mode) {
+  const int64_t need = (mode == 2 ? 9 : 3) * h->t.nf;
+  if (need <= h->t.contrib_doubles) return WN_OK;
+  cudaFree(h->t.contrib);
+  h->t.contrib = nullptr;
+  h->t.contrib_doubles = 0;
+  const cudaError_t e = cudaMalloc(&h->t.contrib, sizeof(double) * (need > 0 ? need : 1));
+  if (e != cudaSuccess) return cuda_fail(e, "device allocation");
+  h->t.contrib_doubles = need;
   return WN_OK;
 }
 
@@ -1182,14 +1200,15 @@ int wn_vertex_normals_device(void* handle, const double* V, int weighting, doubl
                              void* stream) {
   if (!handle) return fail(WN_EINVAL, "null handle");
   if (int code = check_weighting(weighting)) return code;
-  const NormalsHandle* h = static_cast<const NormalsHandle*>(handle);
+  NormalsHandle* h = static_cast<NormalsHandle*>(handle);
   if (h->t.nv == 0) return WN_OK;
   if (!V || !N) return fail(WN_EINVAL, "null pointer");
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
   if (!context(&code)) return code;
-  const cudaError_t e = normals_eval(h->t, V, weighting == 3 ? 1 : weighting, N,
-                                     static_cast<cudaStream_t>(stream));
+  const int mode = weighting == 3 ? 1 : weighting;
+  if ((code = normals_contrib(h, mode)) != WN_OK) return code;
+  const cudaError_t e = normals_eval(h->t, V, mode, N, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "vertex-normal launch");
 }
 
@@ -1205,6 +1224,11 @@ int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_
   if (!c) return code;
   NormalsHandle h;
   if ((code = normals_prepare(F, nf, nv, c->stream, &h)) != WN_OK) return code;
+  const int mode = weighting == 3 ? 1 : weighting;
+  if ((code = normals_contrib(&h, mode)) != WN_OK) {
+    normals_release(&h);
+    return code;
+  }
   cudaError_t e;
   if ((e = c->q.ensure(sizeof(double) * 3 * nv)) != cudaSuccess ||
       (e = c->w.ensure(sizeof(double) * 3 * nv)) != cudaSuccess) {
@@ -1213,7 +1237,7 @@ int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_
   }
   if ((e = cudaMemcpyAsync(c->q.ptr, V, sizeof(double) * 3 * nv, cudaMemcpyHostToDevice,
                            c->stream)) != cudaSuccess ||
-      (e = normals_eval(h.t, static_cast<const double*>(c->q.ptr), weighting == 3 ? 1 : weighting,
+      (e = normals_eval(h.t, static_cast<const double*>(c->q.ptr), mode,
                         static_cast<double*>(c->w.ptr), c->stream)) != cudaSuccess ||
       (e = cudaMemcpyAsync(N, c->w.ptr, sizeof(double) * 3 * nv, cudaMemcpyDeviceToHost,
                            c->stream)) != cudaSuccess) {

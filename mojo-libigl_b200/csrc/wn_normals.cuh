@@ -27,35 +27,42 @@ WN_HD double dacos(double x) { return acos(x); }
 WN_HD double dacos(double x) { return std::acos(x); }
 #endif
 
-// Adds the contribution of corner `corner` of face (A, B, C) (the corner's own
-// vertex first in `P`, then the next two in face order) to acc.
-WN_HD void normal_corner_add(const double* A, const double* B, const double* C, int corner,
-                             int mode, double* acc) {
+// Unit normal u and |n| of face (A, B, C); false when the reference skips the
+// face (|n| <= 1e-30).
+WN_HD bool face_unit_normal(const double* A, const double* B, const double* C, double* u,
+                            double* norm_out) {
   const double abx = dsub(B[0], A[0]), aby = dsub(B[1], A[1]), abz = dsub(B[2], A[2]);
   const double acx = dsub(C[0], A[0]), acy = dsub(C[1], A[1]), acz = dsub(C[2], A[2]);
   const double nx = dsub(dmul(aby, acz), dmul(abz, acy));
   const double ny = dsub(dmul(abz, acx), dmul(abx, acz));
   const double nz = dsub(dmul(abx, acy), dmul(aby, acx));
   const double norm = dsqrt(dot3(nx, ny, nz, nx, ny, nz));
-  if (norm <= 1.0e-30) return;
-  const double ux = ddiv(nx, norm), uy = ddiv(ny, norm), uz = ddiv(nz, norm);
-  double weight = mode == kNormalsArea ? norm : 1.0;
-  if (mode == kNormalsAngle) {
-    const double* P[3] = {A, B, C};
-    const double* vi = P[corner];
-    const double* vj = P[(corner + 1) % 3];
-    const double* vk = P[(corner + 2) % 3];
-    const double e1x = dsub(vj[0], vi[0]), e1y = dsub(vj[1], vi[1]), e1z = dsub(vj[2], vi[2]);
-    const double e2x = dsub(vk[0], vi[0]), e2y = dsub(vk[1], vi[1]), e2z = dsub(vk[2], vi[2]);
-    const double l1 = dsqrt(dot3(e1x, e1y, e1z, e1x, e1y, e1z));
-    const double l2 = dsqrt(dot3(e2x, e2y, e2z, e2x, e2y, e2z));
-    double cosine = ddiv(dot3(e1x, e1y, e1z, e2x, e2y, e2z), dmul(l1, l2));
-    cosine = dmax(-1.0, dmin(1.0, cosine));
-    weight = dacos(cosine);
-  }
-  acc[0] = dadd(acc[0], dmul(ux, weight));
-  acc[1] = dadd(acc[1], dmul(uy, weight));
-  acc[2] = dadd(acc[2], dmul(uz, weight));
+  if (norm <= 1.0e-30) return false;
+  u[0] = ddiv(nx, norm);
+  u[1] = ddiv(ny, norm);
+  u[2] = ddiv(nz, norm);
+  *norm_out = norm;
+  return true;
+}
+
+// Interior angle at corner `corner` of the face whose corners are P[0..2].
+WN_HD double corner_angle(const double* const* P, int corner) {
+  const double* vi = P[corner];
+  const double* vj = P[(corner + 1) % 3];
+  const double* vk = P[(corner + 2) % 3];
+  const double e1x = dsub(vj[0], vi[0]), e1y = dsub(vj[1], vi[1]), e1z = dsub(vj[2], vi[2]);
+  const double e2x = dsub(vk[0], vi[0]), e2y = dsub(vk[1], vi[1]), e2z = dsub(vk[2], vi[2]);
+  const double l1 = dsqrt(dot3(e1x, e1y, e1z, e1x, e1y, e1z));
+  const double l2 = dsqrt(dot3(e2x, e2y, e2z, e2x, e2y, e2z));
+  double cosine = ddiv(dot3(e1x, e1y, e1z, e2x, e2y, e2z), dmul(l1, l2));
+  cosine = dmax(-1.0, dmin(1.0, cosine));
+  return dacos(cosine);
+}
+
+// Weight of a corner: 1 (uniform), |n| (area) or its angle.
+WN_HD double corner_weight(const double* const* P, int corner, int mode, double norm) {
+  if (mode == kNormalsAngle) return corner_angle(P, corner);
+  return mode == kNormalsArea ? norm : 1.0;
 }
 
 // Final division of a vertex sum by its length (when > 1e-30).

@@ -17,11 +17,14 @@ void mli_vertex_normals(int64_t v_addr, int64_t f_addr, int64_t dst_addr, int64_
   for (int64_t i = 0; i < 3 * nv; ++i) dst[i] = 0.0;
   const int mode = weighting == 3 ? wn::kNormalsArea : static_cast<int>(weighting);
   for (int64_t fi = 0; fi < nf; ++fi) {
-    const double* A = v + 3 * f[3 * fi];
-    const double* B = v + 3 * f[3 * fi + 1];
-    const double* C = v + 3 * f[3 * fi + 2];
-    for (int corner = 0; corner < 3; ++corner)
-      wn::normal_corner_add(A, B, C, corner, mode, dst + 3 * f[3 * fi + corner]);
+    const double* P[3] = {v + 3 * f[3 * fi], v + 3 * f[3 * fi + 1], v + 3 * f[3 * fi + 2]};
+    double u[3], norm;
+    if (!wn::face_unit_normal(P[0], P[1], P[2], u, &norm)) continue;
+    for (int corner = 0; corner < 3; ++corner) {
+      const double w = wn::corner_weight(P, corner, mode, norm);
+      double* d = dst + 3 * f[3 * fi + corner];
+      for (int k = 0; k < 3; ++k) d[k] = wn::dadd(d[k], wn::dmul(u[k], w));
+    }
   }
   for (int64_t i = 0; i < nv; ++i) wn::normal_finish(dst + 3 * i);
 }

@@ -70,3 +70,22 @@ def test_unreferenced_vertices_and_empty_faces(gpu_required):
     assert N.tobytes() == igl.per_vertex_normals(V, F).tobytes()
     assert np.array_equal(igl.per_vertex_normals(V, np.zeros((0, 3), np.int64), device="gpu"),
                           np.zeros_like(V))
+
+
+def test_out_of_range_faces_rejected_on_the_device(gpu_required):
+    """The C entry checks F on the device: out-of-range indices give WN_EINVAL, no access."""
+    import ctypes
+
+    V, F = igl.synthetic.bumpy_icosphere(2, seed=4)
+    bad = F.copy()
+    bad[7, 1] = len(V)
+    bad[9, 2] = -3
+    N = np.zeros_like(V)
+    lib = igl.lib()
+    assert lib.wn_vertex_normals_host(V.ctypes.data, len(V), bad.ctypes.data, len(bad), 1,
+                                      N.ctypes.data) == 1
+    assert "2 face indices outside V" in igl._lib.last_error()
+    handle = ctypes.c_void_p()
+    assert lib.wn_normals_create(bad.ctypes.data, len(bad), len(V), None, ctypes.byref(handle)) == 1
+    # The library keeps working afterwards.
+    assert igl.per_vertex_normals(V, F, device="gpu").tobytes() == igl.per_vertex_normals(V, F).tobytes()

@@ -493,11 +493,141 @@ __device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t fir
   }
 }
 
+// ---- face-pair (packed FP32x2) fast path ---------------------------------
+// sm_100 issues two FP32 operations per instruction (add/mul/fma .f32x2). The
+// fast path packs two FACES of a tile against one query: the query's
+// coordinates are the duplicated operand (set once per tile) and a face-pair
+// transposed copy of the tile records supplies both faces' fields in adjacent
+// registers. Every per-face operation is the scalar path's, rounded the same
+// way per lane; each lane keeps its own running product (even faces, odd
+// faces), both started at 2^-50, and the two are multiplied once per tile.
+// Each holds at most 32 factors of modulus in [3.8, 4.01], so both stay inside
+// [2^-50, 2^14.1] and their product inside [2^-100, 2^28.1], as the scalar
+// product does; the sum of the tile's angles is the same (< pi in magnitude).
+constexpr float kZ0Half = 8.8817841970012523e-16f;  // 2^-50
+constexpr int kPairFloats = 32;                     // one face pair, 16 fields x 2 lanes
+constexpr int kTileTransposedBytes = (kTileFaces / 2) * kPairFloats * 4;
+
+// tbuf[32 p + 2 f + lane] = field f of face 2 p + lane, for the tile at `rec`.
+__device__ __forceinline__ void transpose_tile(const unsigned char* rec, float* tbuf, int tid,
+                                               int threads) {
+  const float* src = reinterpret_cast<const float*>(rec + sizeof(TileHeader));
+  for (int i = tid; i < kTileFaces * 16; i += threads) {
+    const int j = i >> 4, f = i & 15;
+    tbuf[kPairFloats * (j >> 1) + 2 * f + (j & 1)] = src[i];
+  }
+}
+
+// pair_sq + pair_mul for two faces (lanes) against one query, (nlx, nly, nlz)
+// = minus the query's tile-local coordinates in both lanes.
+__device__ __forceinline__ void pair2_mul(const float4* v, float2 nlx, float2 nly, float2 nlz,
+                                          float2& zr, float2& zi) {
+  const float4 v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3];
+  const float4 v4 = v[4], v5 = v[5], v6 = v[6];
+  const float2 e12 = make_float2(v[7].x, v[7].y);
+  const float2 one = make_float2(1.f, 1.f), two = make_float2(2.f, 2.f);
+  const float2 ax = __fadd2_rn(make_float2(v0.x, v0.y), nlx);
+  const float2 ay = __fadd2_rn(make_float2(v0.z, v0.w), nly);
+  const float2 az = __fadd2_rn(make_float2(v1.x, v1.y), nlz);
+  const float2 aa = __ffma2_rn(ax, ax, __ffma2_rn(ay, ay, __fmul2_rn(az, az)));
+  const float2 s1 = __ffma2_rn(ax, make_float2(v1.z, v1.w),
+                               __ffma2_rn(ay, make_float2(v2.x, v2.y),
+                                          __fmul2_rn(az, make_float2(v2.z, v2.w))));
+  const float2 s2 = __ffma2_rn(ax, make_float2(v3.x, v3.y),
+                               __ffma2_rn(ay, make_float2(v3.z, v3.w),
+                                          __fmul2_rn(az, make_float2(v4.x, v4.y))));
+  const float2 det = __ffma2_rn(ax, make_float2(v4.z, v4.w),
+                                __ffma2_rn(ay, make_float2(v5.x, v5.y),
+                                           __fmul2_rn(az, make_float2(v5.z, v5.w))));
+  const float2 ab = __fadd2_rn(aa, s1), ca = __fadd2_rn(aa, s2);
+  const float2 bb = __ffma2_rn(two, s1, __fadd2_rn(aa, make_float2(v6.x, v6.y)));
+  const float2 cc = __ffma2_rn(two, s2, __fadd2_rn(aa, make_float2(v6.z, v6.w)));
+  const float2 bc = __fadd2_rn(ab, __fadd2_rn(s2, e12));
+  const float2 ra = make_float2(rsqrt_approx(aa.x), rsqrt_approx(aa.y));
+  const float2 rb = make_float2(rsqrt_approx(bb.x), rsqrt_approx(bb.y));
+  const float2 rc = make_float2(rsqrt_approx(cc.x), rsqrt_approx(cc.y));
+  const float2 rab = __fmul2_rn(ra, rb), rbc = __fmul2_rn(rb, rc), rca = __fmul2_rn(rc, ra);
+  const float2 dn = __ffma2_rn(ab, rab, __ffma2_rn(bc, rbc, __ffma2_rn(ca, rca, one)));
+  const float2 dt = __fmul2_rn(det, __fmul2_rn(rab, rc));
+  const float2 nzi = make_float2(-zi.x, -zi.y);
+  const float2 nr = __ffma2_rn(zr, dn, __fmul2_rn(nzi, dt));
+  const float2 ni = __ffma2_rn(zr, dt, __fmul2_rn(zi, dn));
+  zr = nr;
+  zi = ni;
+}
+
+// mixed_tile with the fast path on face pairs (tbuf: the transposed records
+// of the tile at `rec`); the careful path is mixed_tile's, on `rec`.
+template <int QPT>
+__device__ __forceinline__ void mixed_tile_pairs(const unsigned char* rec, const float* tbuf,
+                                                 int64_t first, const double* __restrict__ tri64,
+                                                 int64_t ld64, const double (&ox)[QPT],
+                                                 const double (&oy)[QPT], const double (&oz)[QPT],
+                                                 const int64_t (&qidx)[QPT], float (&hi)[QPT],
+                                                 float (&lo)[QPT], double (&s64)[QPT],
+                                                 unsigned& refined, unsigned& careful_tiles) {
+  const TileHeader& th = *reinterpret_cast<const TileHeader*>(rec);
+  const int n = th.n;
+  bool all_far = true;
+  float lx[QPT], ly[QPT], lz[QPT];
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    const double dx = ox[k] - th.cx, dy = oy[k] - th.cy, dz = oz[k] - th.cz;
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    all_far &= (d2 >= th.far_r2) || qidx[k] < 0;
+    lx[k] = static_cast<float>(dx * th.scale);
+    ly[k] = static_cast<float>(dy * th.scale);
+    lz[k] = static_cast<float>(dz * th.scale);
+    all_far &= !(d2 * th.scale * th.scale > 1.2089258196146292e24);
+  }
+  if (!__all_sync(0xffffffffu, all_far)) {
+    mixed_tile<QPT>(rec, first, tri64, ld64, ox, oy, oz, qidx, hi, lo, s64, refined,
+                    careful_tiles);
+    return;
+  }
+  float2 zr2[QPT], zi2[QPT], nlx[QPT], nly[QPT], nlz[QPT];
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    zr2[k] = make_float2(kZ0Half, kZ0Half);
+    zi2[k] = make_float2(0.f, 0.f);
+    nlx[k] = make_float2(-lx[k], -lx[k]);
+    nly[k] = make_float2(-ly[k], -ly[k]);
+    nlz[k] = make_float2(-lz[k], -lz[k]);
+  }
+  const int npairs = n >> 1;
+#pragma unroll 2
+  for (int p = 0; p < npairs; ++p) {
+    const float4* v = reinterpret_cast<const float4*>(tbuf + kPairFloats * p);
+#pragma unroll
+    for (int k = 0; k < QPT; ++k) pair2_mul(v, nlx[k], nly[k], nlz[k], zr2[k], zi2[k]);
+  }
+  const float4* fr = reinterpret_cast<const float4*>(rec + sizeof(TileHeader));
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    float zr = zr2[k].x * zr2[k].y - zi2[k].x * zi2[k].y;
+    float zi = zr2[k].x * zi2[k].y + zi2[k].x * zr2[k].y;
+    if (n & 1) {  // the odd last face, on the scalar path
+      const int j = n - 1;
+      pair_mul(pair_sq(fr[4 * j], fr[4 * j + 1], fr[4 * j + 2], fr[4 * j + 3], lx[k], ly[k],
+                       lz[k]),
+               zr, zi);
+    }
+    const float ang = atan2f(zi, zr);
+    const float s = hi[k] + ang;
+    const float bp = s - hi[k];
+    const float err = (hi[k] - (s - bp)) + (ang - bp);
+    hi[k] = s;
+    lo[k] += err;
+  }
+}
+
 template <int THREADS, int QPT, int STAGES>
 __global__ void __launch_bounds__(THREADS, 5) mixed_forward_kernel(const MixedArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* ring = smem_raw;  // [STAGES][kTileBytes]
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + STAGES * kTileBytes);
+  // Two face-pair transposed tiles (tile t uses tbuf[t & 1]).
+  float* tbuf = reinterpret_cast<float*>(smem_raw + STAGES * kTileBytes + 8 * STAGES);
   const int tid = threadIdx.x;
   const int64_t base = static_cast<int64_t>(blockIdx.x) * (THREADS * QPT);
 
@@ -545,13 +675,17 @@ __global__ void __launch_bounds__(THREADS, 5) mixed_forward_kernel(const MixedAr
   for (; t < ntiles; ++t) {
     const int slot = t % STAGES;
     const bool landed = mbar_wait(&full[slot], (t / STAGES) & 1, a.err);
+    float* tb = tbuf + (t & 1) * (kTileTransposedBytes / 4);
+    // tbuf[t & 1] was last read for tile t - 2, which every thread finished
+    // before the barrier of tile t - 1.
+    if (landed) transpose_tile(ring + slot * kTileBytes, tb, tid, THREADS);
     if (!__syncthreads_and(landed)) {
       failed = true;
       break;
     }
     if (tid == 0 && t >= 1 && issued < ntiles) issue(issued++);
-    mixed_tile<QPT>(ring + slot * kTileBytes, (t_begin + t) * kTileFaces, a.tri64, a.ld64, ox, oy,
-                    oz, qidx, hi, lo, s64, refined, careful_tiles);
+    mixed_tile_pairs<QPT>(ring + slot * kTileBytes, tb, (t_begin + t) * kTileFaces, a.tri64,
+                          a.ld64, ox, oy, oz, qidx, hi, lo, s64, refined, careful_tiles);
   }
 
   if (failed) {
@@ -593,7 +727,8 @@ constexpr int kMixedThreads = 128, kMixedQpt = 2, kMixedStages = 4;
 template <int THREADS, int QPT, int STAGES>
 cudaError_t launch_mixed_variant(const MixedArgs& a, int64_t nsplit, cudaStream_t stream) {
   auto kernel = mixed_forward_kernel<THREADS, QPT, STAGES>;
-  const size_t smem = static_cast<size_t>(STAGES) * kTileBytes + sizeof(uint64_t) * STAGES;
+  const size_t smem = static_cast<size_t>(STAGES) * kTileBytes + sizeof(uint64_t) * STAGES +
+                      2 * kTileTransposedBytes;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;

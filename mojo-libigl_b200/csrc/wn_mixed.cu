@@ -1010,10 +1010,13 @@ struct BatchArgs {
 };
 
 template <int THREADS, int QPT, int STAGES>
-__global__ void __launch_bounds__(THREADS) batch_forward_kernel(const BatchArgs a) {
+__global__ void __launch_bounds__(THREADS, QPT == 1 ? 6 : (QPT == 2 ? 4 : 3))
+    batch_forward_kernel(const BatchArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* ring = smem_raw;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + STAGES * kTileBytes);
+  // Two face-pair transposed tiles (this CTA's g-th tile uses tbuf[g & 1]).
+  float* tbuf = reinterpret_cast<float*>(smem_raw + STAGES * kTileBytes + 8 * STAGES);
   __shared__ int64_t s_item;
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -1063,13 +1066,17 @@ __global__ void __launch_bounds__(THREADS) batch_forward_kernel(const BatchArgs 
       const int slot = static_cast<int>((gt + u) % STAGES);
       const bool landed =
           mbar_wait(&full[slot], static_cast<uint32_t>(((gt + u) / STAGES) & 1), a.err);
+      float* tb = tbuf + ((gt + u) & 1) * (kTileTransposedBytes / 4);
+      // tbuf[g & 1] was last read for tile g - 2, finished by every thread before
+      // the barrier of tile g - 1 (or of the item boundary).
+      if (landed) transpose_tile(ring + slot * kTileBytes, tb, tid, THREADS);
       if (!__syncthreads_and(landed)) {
         failed = true;
         break;
       }
       if (tid == 0 && u >= 1 && issued < nt) issue(issued++);
-      mixed_tile<QPT>(ring + slot * kTileBytes, (it.t_begin + u) * kTileFaces, a.tri64, a.ld64,
-                      ox, oy, oz, qidx, hi, lo, s64, refined, careful_tiles);
+      mixed_tile_pairs<QPT>(ring + slot * kTileBytes, tb, (it.t_begin + u) * kTileFaces, a.tri64,
+                            a.ld64, ox, oy, oz, qidx, hi, lo, s64, refined, careful_tiles);
     }
     if (failed) {
       if (tid == 0)
@@ -1117,7 +1124,8 @@ template <int QPT>
 cudaError_t launch_batch_variant(const BatchArgs& a, int grid, cudaStream_t stream) {
   constexpr int kThreads = 128, kStages = 4;
   auto kernel = batch_forward_kernel<kThreads, QPT, kStages>;
-  const size_t smem = static_cast<size_t>(kStages) * kTileBytes + sizeof(uint64_t) * kStages;
+  const size_t smem = static_cast<size_t>(kStages) * kTileBytes + sizeof(uint64_t) * kStages +
+                      2 * kTileTransposedBytes;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
@@ -1129,7 +1137,8 @@ cudaError_t launch_batch_variant(const BatchArgs& a, int grid, cudaStream_t stre
 template <int QPT>
 int batch_grid(int sms, int ctas_per_sm) {
   constexpr int kThreads = 128, kStages = 4;
-  const size_t smem = static_cast<size_t>(kStages) * kTileBytes + sizeof(uint64_t) * kStages;
+  const size_t smem = static_cast<size_t>(kStages) * kTileBytes + sizeof(uint64_t) * kStages +
+                      2 * kTileTransposedBytes;
   int per_sm = 0;
   cudaFuncSetAttribute(batch_forward_kernel<kThreads, QPT, kStages>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));

@@ -77,6 +77,7 @@ struct DeviceCtx {
   unsigned long long* stats = nullptr;  // mixed-path counters (refined pairs, careful visits)
   Buffer tri, q, w, scratch;
   Buffer mesh_tiles, mesh_tri64, mesh_face_of, mesh_reuse;  // prepared mesh (host entry points)
+  Buffer nrm_f, nrm_indptr, nrm_entries, nrm_contrib;        // one-shot vertex normals
 };
 
 std::mutex g_mutex;
@@ -1105,15 +1106,16 @@ int check_weighting(int weighting) {
   return WN_OK;
 }
 
-// Uploads F (host, nf x 3 int64), checks and converts it on the device and
-// builds the incidence lists on `st`; returns after `st` drains (caller holds
-// g_mutex and a context).
-int normals_prepare(const int64_t* F, int64_t nf, int64_t nv, cudaStream_t st,
-                    NormalsHandle* h) {
+int normals_check_sizes(const int64_t* F, int64_t nf, int64_t nv) {
   if (nf < 0 || nv < 0) return fail(WN_EINVAL, "negative size");
   if (nv > 0x7fffffffLL || 3 * nf > 0x7fffffffLL)
     return fail(WN_EINVAL, "more than 2^31-1 vertices or incidences");
   if (nf > 0 && !F) return fail(WN_EINVAL, "null pointer");
+  return WN_OK;
+}
+
+// Own device arrays of a handle's topology.
+int normals_alloc(NormalsHandle* h, int64_t nf, int64_t nv) {
   h->t.nf = nf;
   h->t.nv = nv;
   cudaGetDevice(&h->device);
@@ -1124,13 +1126,19 @@ int normals_prepare(const int64_t* F, int64_t nf, int64_t nv, cudaStream_t st,
     normals_release(h);
     return cuda_fail(e, "device allocation");
   }
+  return WN_OK;
+}
+
+// Uploads F (host, nf x 3 int64), checks and converts it on the device and
+// builds the incidence lists into h->t's arrays on `st`; returns after `st`
+// drains (caller holds g_mutex and a context).
+int normals_prepare(const int64_t* F, int64_t nf, cudaStream_t st, NormalsHandle* h) {
+  cudaError_t e = cudaSuccess;
   const size_t f64_bytes = ((sizeof(int64_t) * 3 * nf + 255) / 256) * 256;
   const size_t sb = f64_bytes + 256 + normals_scratch_bytes(nf);
   unsigned char* scratch = nullptr;
-  if ((e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), sb, st)) != cudaSuccess) {
-    normals_release(h);
+  if ((e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), sb, st)) != cudaSuccess)
     return cuda_fail(e, "device allocation");
-  }
   int64_t* F64 = reinterpret_cast<int64_t*>(scratch);
   int* bad = reinterpret_cast<int*>(scratch + f64_bytes);
   if (nf > 0)
@@ -1141,14 +1149,8 @@ int normals_prepare(const int64_t* F, int64_t nf, int64_t nv, cudaStream_t st,
   if (e == cudaSuccess) e = cudaMemcpyAsync(&bad_h, bad, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaFreeAsync(scratch, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) {
-    normals_release(h);
-    return cuda_fail(e, "incidence list build");
-  }
-  if (bad_h != 0) {
-    normals_release(h);
-    return fail(WN_EINVAL, "%d face indices outside V", bad_h);
-  }
+  if (e != cudaSuccess) return cuda_fail(e, "incidence list build");
+  if (bad_h != 0) return fail(WN_EINVAL, "%d face indices outside V", bad_h);
   return WN_OK;
 }
 
@@ -1174,8 +1176,11 @@ int wn_normals_create(const int64_t* F, int64_t nf, int64_t nv, void* stream, vo
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
   if (!context(&code)) return code;
+  if ((code = normals_check_sizes(F, nf, nv)) != WN_OK) return code;
   NormalsHandle* h = new NormalsHandle();
-  if ((code = normals_prepare(F, nf, nv, static_cast<cudaStream_t>(stream), h)) != WN_OK) {
+  if ((code = normals_alloc(h, nf, nv)) != WN_OK ||
+      (code = normals_prepare(F, nf, static_cast<cudaStream_t>(stream), h)) != WN_OK) {
+    normals_release(h);
     delete h;
     return code;
   }
@@ -1222,19 +1227,28 @@ int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_
   int code = WN_OK;
   DeviceCtx* c = context(&code);
   if (!c) return code;
-  NormalsHandle h;
-  if ((code = normals_prepare(F, nf, nv, c->stream, &h)) != WN_OK) return code;
+  if ((code = normals_check_sizes(F, nf, nv)) != WN_OK) return code;
+  // The context's grow-only buffers hold the topology: no allocation per call
+  // once they are large enough.
   const int mode = weighting == 3 ? 1 : weighting;
-  if ((code = normals_contrib(&h, mode)) != WN_OK) {
-    normals_release(&h);
-    return code;
-  }
+  const int64_t ncontrib = (mode == 2 ? 9 : 3) * nf;
   cudaError_t e;
-  if ((e = c->q.ensure(sizeof(double) * 3 * nv)) != cudaSuccess ||
-      (e = c->w.ensure(sizeof(double) * 3 * nv)) != cudaSuccess) {
-    normals_release(&h);
+  if ((e = c->nrm_f.ensure(sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess ||
+      (e = c->nrm_indptr.ensure(sizeof(int32_t) * (nv + 1))) != cudaSuccess ||
+      (e = c->nrm_entries.ensure(sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess ||
+      (e = c->nrm_contrib.ensure(sizeof(double) * (ncontrib + 1))) != cudaSuccess ||
+      (e = c->q.ensure(sizeof(double) * 3 * nv)) != cudaSuccess ||
+      (e = c->w.ensure(sizeof(double) * 3 * nv)) != cudaSuccess)
     return cuda_fail(e, "device allocation");
-  }
+  NormalsHandle h;
+  h.t.F = static_cast<int32_t*>(c->nrm_f.ptr);
+  h.t.indptr = static_cast<int32_t*>(c->nrm_indptr.ptr);
+  h.t.entries = static_cast<int32_t*>(c->nrm_entries.ptr);
+  h.t.contrib = static_cast<double*>(c->nrm_contrib.ptr);
+  h.t.contrib_doubles = ncontrib;
+  h.t.nf = nf;
+  h.t.nv = nv;
+  if ((code = normals_prepare(F, nf, c->stream, &h)) != WN_OK) return code;
   if ((e = cudaMemcpyAsync(c->q.ptr, V, sizeof(double) * 3 * nv, cudaMemcpyHostToDevice,
                            c->stream)) != cudaSuccess ||
       (e = normals_eval(h.t, static_cast<const double*>(c->q.ptr), mode,
@@ -1242,12 +1256,9 @@ int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_
       (e = cudaMemcpyAsync(N, c->w.ptr, sizeof(double) * 3 * nv, cudaMemcpyDeviceToHost,
                            c->stream)) != cudaSuccess) {
     cudaStreamSynchronize(c->stream);
-    normals_release(&h);
     return cuda_fail(e, "vertex normals");
   }
-  code = collect_device_error(c, c->stream);
-  normals_release(&h);
-  return code;
+  return collect_device_error(c, c->stream);
 }
 
 // src/capi.mojo:945-947: 1 on success, 0 on failure (the shim raises). Large

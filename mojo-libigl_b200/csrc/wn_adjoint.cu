@@ -234,6 +234,109 @@ __device__ __noinline__ void refine_pair_grad(const double* __restrict__ tri64, 
   for (int r = 0; r < 9; ++r) acc_col[r * stride] += gv[r];
 }
 
+// Lane k of a float2 (k a compile-time constant after unrolling).
+__device__ __forceinline__ float lane_of(const float2& v, int k) { return k == 0 ? v.x : v.y; }
+__device__ __forceinline__ float& lane_ref(float2& v, int k) { return k == 0 ? v.x : v.y; }
+
+// Far-pair gradient terms of one face (lane k) against one query, FP32: adds
+// the face's corner gradients (scaled by the tile's coordinate scale later) to
+// acc[r] lane k and its share of dL/do to dof[x] lane k.
+__device__ __forceinline__ void adj_far_lane(float g, float ax, float ay, float az,
+                                             const float2 (&fe1)[3], const float2 (&fe2)[3],
+                                             float aa, float bb, float cc, float ab, float bc,
+                                             float ca, float sck, int k, float2 (&acc)[9],
+                                             float2 (&dof)[3]) {
+  float ra, rb, rc, iab, ibc, ica;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(ra) : "f"(aa));
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rb) : "f"(bb));
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(cc));
+  const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
+  const float dab = fmaf(ab, rab, 1.f), dbc = fmaf(bc, rbc, 1.f), dca = fmaf(ca, rca, 1.f);
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(iab) : "f"(dab));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ibc) : "f"(dbc));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ica) : "f"(dca));
+  const float wab = g * rab * iab, wbc = g * rbc * ibc, wca = g * rca * ica;
+  const float bx = ax + lane_of(fe1[0], k), by = ay + lane_of(fe1[1], k), bz = az + lane_of(fe1[2], k);
+  const float cx = ax + lane_of(fe2[0], k), cy = ay + lane_of(fe2[1], k), cz = az + lane_of(fe2[2], k);
+  const float xab0 = ay * bz - az * by, xab1 = az * bx - ax * bz, xab2 = ax * by - ay * bx;
+  const float xbc0 = by * cz - bz * cy, xbc1 = bz * cx - bx * cz, xbc2 = bx * cy - by * cx;
+  const float xca0 = cy * az - cz * ay, xca1 = cz * ax - cx * az, xca2 = cx * ay - cy * ax;
+  // Negated coefficients: each of the 9 sums takes two FMAs.
+  const float nA1 = -ra * wab, nA2 = -ra * wca, nB1 = -rb * wab, nB2 = -rb * wbc;
+  const float nC1 = -rc * wbc, nC2 = -rc * wca;
+  lane_ref(acc[0], k) = fmaf(nA1, xab0, fmaf(nA2, xca0, lane_of(acc[0], k)));
+  lane_ref(acc[1], k) = fmaf(nA1, xab1, fmaf(nA2, xca1, lane_of(acc[1], k)));
+  lane_ref(acc[2], k) = fmaf(nA1, xab2, fmaf(nA2, xca2, lane_of(acc[2], k)));
+  lane_ref(acc[3], k) = fmaf(nB1, xab0, fmaf(nB2, xbc0, lane_of(acc[3], k)));
+  lane_ref(acc[4], k) = fmaf(nB1, xab1, fmaf(nB2, xbc1, lane_of(acc[4], k)));
+  lane_ref(acc[5], k) = fmaf(nB1, xab2, fmaf(nB2, xbc2, lane_of(acc[5], k)));
+  lane_ref(acc[6], k) = fmaf(nC1, xbc0, fmaf(nC2, xca0, lane_of(acc[6], k)));
+  lane_ref(acc[7], k) = fmaf(nC1, xbc1, fmaf(nC2, xca1, lane_of(acc[7], k)));
+  lane_ref(acc[8], k) = fmaf(nC1, xbc2, fmaf(nC2, xca2, lane_of(acc[8], k)));
+  const float sab = -(nA1 + nB1) * sck, sbc = -(nB2 + nC1) * sck, sca = -(nC2 + nA2) * sck;
+  lane_ref(dof[0], k) = fmaf(sab, xab0, fmaf(sbc, xbc0, fmaf(sca, xca0, lane_of(dof[0], k))));
+  lane_ref(dof[1], k) = fmaf(sab, xab1, fmaf(sbc, xbc1, fmaf(sca, xca1, lane_of(dof[1], k))));
+  lane_ref(dof[2], k) = fmaf(sab, xab2, fmaf(sbc, xbc2, fmaf(sca, xca2, lane_of(dof[2], k))));
+}
+
+// adj_far_lane for both faces at once, packed; nsc = minus the two tiles' scales.
+__device__ __forceinline__ void adj_far_pair2(float g, float2 ax, float2 ay, float2 az,
+                                              const float2 (&fe1)[3], const float2 (&fe2)[3],
+                                              float2 aa, float2 bb, float2 cc, float2 ab,
+                                              float2 bc, float2 ca, float2 nsc,
+                                              float2 (&acc)[9], float2 (&dof)[3]) {
+  float2 ra, rb, rc, iab, ibc, ica;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(ra.x) : "f"(aa.x));
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(ra.y) : "f"(aa.y));
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rb.x) : "f"(bb.x));
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rb.y) : "f"(bb.y));
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rc.x) : "f"(cc.x));
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rc.y) : "f"(cc.y));
+  const float2 one = make_float2(1.f, 1.f);
+  const float2 rab = __fmul2_rn(ra, rb), rbc = __fmul2_rn(rb, rc), rca = __fmul2_rn(rc, ra);
+  const float2 dab = __ffma2_rn(ab, rab, one), dbc = __ffma2_rn(bc, rbc, one);
+  const float2 dca = __ffma2_rn(ca, rca, one);
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(iab.x) : "f"(dab.x));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(iab.y) : "f"(dab.y));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ibc.x) : "f"(dbc.x));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ibc.y) : "f"(dbc.y));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ica.x) : "f"(dca.x));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ica.y) : "f"(dca.y));
+  const float2 g2 = make_float2(g, g);
+  const float2 wab = __fmul2_rn(__fmul2_rn(g2, rab), iab);
+  const float2 wbc = __fmul2_rn(__fmul2_rn(g2, rbc), ibc);
+  const float2 wca = __fmul2_rn(__fmul2_rn(g2, rca), ica);
+  const float2 bx = __fadd2_rn(ax, fe1[0]), by = __fadd2_rn(ay, fe1[1]), bz = __fadd2_rn(az, fe1[2]);
+  const float2 cx = __fadd2_rn(ax, fe2[0]), cy = __fadd2_rn(ay, fe2[1]), cz = __fadd2_rn(az, fe2[2]);
+  auto neg = [](float2 v) { return make_float2(-v.x, -v.y); };
+  // u x v component: u1 v2 - u2 v1 as one multiply and one FMA.
+  auto cross = [&](float2 u1, float2 v2, float2 u2, float2 v1) {
+    return __ffma2_rn(u1, v2, __fmul2_rn(neg(u2), v1));
+  };
+  const float2 xab0 = cross(ay, bz, az, by), xab1 = cross(az, bx, ax, bz), xab2 = cross(ax, by, ay, bx);
+  const float2 xbc0 = cross(by, cz, bz, cy), xbc1 = cross(bz, cx, bx, cz), xbc2 = cross(bx, cy, by, cx);
+  const float2 xca0 = cross(cy, az, cz, ay), xca1 = cross(cz, ax, cx, az), xca2 = cross(cx, ay, cy, ax);
+  const float2 nra = neg(ra), nrb = neg(rb), nrc = neg(rc);
+  const float2 nA1 = __fmul2_rn(nra, wab), nA2 = __fmul2_rn(nra, wca);
+  const float2 nB1 = __fmul2_rn(nrb, wab), nB2 = __fmul2_rn(nrb, wbc);
+  const float2 nC1 = __fmul2_rn(nrc, wbc), nC2 = __fmul2_rn(nrc, wca);
+  acc[0] = __ffma2_rn(nA1, xab0, __ffma2_rn(nA2, xca0, acc[0]));
+  acc[1] = __ffma2_rn(nA1, xab1, __ffma2_rn(nA2, xca1, acc[1]));
+  acc[2] = __ffma2_rn(nA1, xab2, __ffma2_rn(nA2, xca2, acc[2]));
+  acc[3] = __ffma2_rn(nB1, xab0, __ffma2_rn(nB2, xbc0, acc[3]));
+  acc[4] = __ffma2_rn(nB1, xab1, __ffma2_rn(nB2, xbc1, acc[4]));
+  acc[5] = __ffma2_rn(nB1, xab2, __ffma2_rn(nB2, xbc2, acc[5]));
+  acc[6] = __ffma2_rn(nC1, xbc0, __ffma2_rn(nC2, xca0, acc[6]));
+  acc[7] = __ffma2_rn(nC1, xbc1, __ffma2_rn(nC2, xca1, acc[7]));
+  acc[8] = __ffma2_rn(nC1, xbc2, __ffma2_rn(nC2, xca2, acc[8]));
+  const float2 sab = __fmul2_rn(__fadd2_rn(nA1, nB1), nsc);
+  const float2 sbc = __fmul2_rn(__fadd2_rn(nB2, nC1), nsc);
+  const float2 sca = __fmul2_rn(__fadd2_rn(nC2, nA2), nsc);
+  dof[0] = __ffma2_rn(sab, xab0, __ffma2_rn(sbc, xbc0, __ffma2_rn(sca, xca0, dof[0])));
+  dof[1] = __ffma2_rn(sab, xab1, __ffma2_rn(sbc, xbc1, __ffma2_rn(sca, xca1, dof[1])));
+  dof[2] = __ffma2_rn(sab, xab2, __ffma2_rn(sbc, xbc2, __ffma2_rn(sca, xca2, dof[2])));
+}
+
 template <int THREADS, int QC>
 __global__ void __launch_bounds__(THREADS, 3) adjoint_mixed_kernel(const MixedAdjointArgs a) {
   static_assert(THREADS == 2 * kTileFaces, "one thread per face of two tiles");
@@ -263,12 +366,13 @@ __global__ void __launch_bounds__(THREADS, 3) adjoint_mixed_kernel(const MixedAd
       }
     }
     // Face records: A, e1 = B - A, e2 = C - A, |e1|^2, |e2|^2, e1.e2 and the
-    // refinement threshold (FaceRec layout), scaled tile-local FP32.
-    float fa[2][3], fe1[2][3], fe2[2][3], fg[2][3], thr[2];
-    float sc[2];
+    // refinement threshold (FaceRec layout), scaled tile-local FP32. The thread's
+    // two faces are the two lanes of every float2 (lane k = face k), so the far
+    // pairs of both run as packed FP32x2 arithmetic (sm_100 add/mul/fma .f32x2).
+    float2 fa[3], fe1[3], fe2[3], fg[3], acc[9];
+    float thr[2], sc[2];
     int64_t slot[2];
     bool valid[2];
-    float acc32[2][9];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int64_t t = blk * kTilesPerBlock + 2 * k + half;
@@ -282,18 +386,19 @@ __global__ void __launch_bounds__(THREADS, 3) adjoint_mixed_kernel(const MixedAd
                                                        sizeof(TileHeader)) + 16 * j;
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
-        fa[k][r] = valid[k] ? fr[r] : 0.f;
-        fe1[k][r] = valid[k] ? fr[3 + r] : 0.f;
-        fe2[k][r] = valid[k] ? fr[6 + r] : 0.f;
-        fg[k][r] = valid[k] ? fr[12 + r] : 0.f;
+        lane_ref(fa[r], k) = valid[k] ? fr[r] : 0.f;
+        lane_ref(fe1[r], k) = valid[k] ? fr[3 + r] : 0.f;
+        lane_ref(fe2[r], k) = valid[k] ? fr[6 + r] : 0.f;
+        lane_ref(fg[r], k) = valid[k] ? fr[12 + r] : 0.f;
       }
       thr[k] = valid[k] ? fr[15] : 0.f;
 #pragma unroll
-      for (int r = 0; r < 9; ++r) {
-        acc32[k][r] = 0.f;
-        sm.acc64[k][r][tid] = 0.0;
-      }
+      for (int r = 0; r < 9; ++r) sm.acc64[k][r][tid] = 0.0;
     }
+#pragma unroll
+    for (int r = 0; r < 9; ++r) acc[r] = make_float2(0.f, 0.f);
+    const float2 nsc = make_float2(-sc[0], -sc[1]);
+    const bool both_valid = valid[0] && valid[1];
     for (int64_t c0 = q_begin; c0 < q_end; c0 += QC) {
       const int nc = static_cast<int>(q_end - c0 < QC ? q_end - c0 : QC);
       __syncthreads();
@@ -314,62 +419,42 @@ __global__ void __launch_bounds__(THREADS, 3) adjoint_mixed_kernel(const MixedAd
 #pragma unroll 1
       for (int jq = 0; jq < nc; ++jq) {
         const float g = static_cast<float>(sm.sq[jq].w);
-        float dof0 = 0.f, dof1 = 0.f, dof2 = 0.f;
+        float2 dof[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
         double go[3] = {0.0, 0.0, 0.0};
         bool refined = false;
+        const float4 l0 = sm.sl[jq][half], l1 = sm.sl[jq][2 + half];
+        const float2 ax = __fadd2_rn(fa[0], make_float2(-l0.x, -l1.x));
+        const float2 ay = __fadd2_rn(fa[1], make_float2(-l0.y, -l1.y));
+        const float2 az = __fadd2_rn(fa[2], make_float2(-l0.z, -l1.z));
+        const float2 aa = __ffma2_rn(ax, ax, __ffma2_rn(ay, ay, __fmul2_rn(az, az)));
+        const float2 s1 = __ffma2_rn(ax, fe1[0], __ffma2_rn(ay, fe1[1], __fmul2_rn(az, fe1[2])));
+        const float2 s2 = __ffma2_rn(ax, fe2[0], __ffma2_rn(ay, fe2[1], __fmul2_rn(az, fe2[2])));
+        const float2 ab = __fadd2_rn(aa, s1), ca = __fadd2_rn(aa, s2);
+        const float2 two = make_float2(2.f, 2.f);
+        const float2 bb = __ffma2_rn(two, s1, __fadd2_rn(aa, fg[0]));
+        const float2 cc = __ffma2_rn(two, s2, __fadd2_rn(aa, fg[1]));
+        const float2 bc = __fadd2_rn(ab, __fadd2_rn(s2, fg[2]));
+        const bool near0 = l0.w == 0.f && fminf(aa.x, fminf(bb.x, cc.x)) < thr[0];
+        const bool near1 = l1.w == 0.f && fminf(aa.y, fminf(bb.y, cc.y)) < thr[1];
+        if (!near0 && !near1 && both_valid) {
+          adj_far_pair2(g, ax, ay, az, fe1, fe2, aa, bb, cc, ab, bc, ca, nsc, acc, dof);
+        } else {
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const float4 l = sm.sl[jq][2 * k + half];
-          const float ax = fa[k][0] - l.x, ay = fa[k][1] - l.y, az = fa[k][2] - l.z;
-          const float aa = fmaf(ax, ax, fmaf(ay, ay, az * az));
-          const float s1 = fmaf(ax, fe1[k][0], fmaf(ay, fe1[k][1], az * fe1[k][2]));
-          const float s2 = fmaf(ax, fe2[k][0], fmaf(ay, fe2[k][1], az * fe2[k][2]));
-          const float ab = aa + s1, ca = aa + s2;
-          const float bb = fmaf(2.f, s1, aa + fg[k][0]);
-          const float cc = fmaf(2.f, s2, aa + fg[k][1]);
-          const float bc = ab + (s2 + fg[k][2]);
-          if (l.w == 0.f && fminf(aa, fminf(bb, cc)) < thr[k]) {
-            if (valid[k]) {
+          for (int k = 0; k < 2; ++k) {
+            if (!valid[k]) continue;
+            if (k == 0 ? near0 : near1) {
               refine_pair_grad(a.tri64, a.ld64, slot[k], sm.sq[jq], &sm.acc64[k][0][tid], THREADS,
                                go);
               refined = true;
+            } else {
+              adj_far_lane(g, lane_of(ax, k), lane_of(ay, k), lane_of(az, k), fe1, fe2, lane_of(aa, k),
+                           lane_of(bb, k), lane_of(cc, k), lane_of(ab, k), lane_of(bc, k), lane_of(ca, k),
+                           sc[k], k, acc, dof);
             }
-          } else if (valid[k]) {
-            float ra, rb, rc, iab, ibc, ica;
-            asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(ra) : "f"(aa));
-            asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rb) : "f"(bb));
-            asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(cc));
-            const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
-            const float dab = fmaf(ab, rab, 1.f), dbc = fmaf(bc, rbc, 1.f),
-                        dca = fmaf(ca, rca, 1.f);
-            asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(iab) : "f"(dab));
-            asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ibc) : "f"(dbc));
-            asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ica) : "f"(dca));
-            const float wab = g * rab * iab, wbc = g * rbc * ibc, wca = g * rca * ica;
-            const float bx = ax + fe1[k][0], by = ay + fe1[k][1], bz = az + fe1[k][2];
-            const float cx = ax + fe2[k][0], cy = ay + fe2[k][1], cz = az + fe2[k][2];
-            const float xab0 = ay * bz - az * by, xab1 = az * bx - ax * bz, xab2 = ax * by - ay * bx;
-            const float xbc0 = by * cz - bz * cy, xbc1 = bz * cx - bx * cz, xbc2 = bx * cy - by * cx;
-            const float xca0 = cy * az - cz * ay, xca1 = cz * ax - cx * az, xca2 = cx * ay - cy * ax;
-            // Negated coefficients: each of the 9 sums takes two FMAs.
-            const float nA1 = -ra * wab, nA2 = -ra * wca, nB1 = -rb * wab, nB2 = -rb * wbc;
-            const float nC1 = -rc * wbc, nC2 = -rc * wca;
-            acc32[k][0] = fmaf(nA1, xab0, fmaf(nA2, xca0, acc32[k][0]));
-            acc32[k][1] = fmaf(nA1, xab1, fmaf(nA2, xca1, acc32[k][1]));
-            acc32[k][2] = fmaf(nA1, xab2, fmaf(nA2, xca2, acc32[k][2]));
-            acc32[k][3] = fmaf(nB1, xab0, fmaf(nB2, xbc0, acc32[k][3]));
-            acc32[k][4] = fmaf(nB1, xab1, fmaf(nB2, xbc1, acc32[k][4]));
-            acc32[k][5] = fmaf(nB1, xab2, fmaf(nB2, xbc2, acc32[k][5]));
-            acc32[k][6] = fmaf(nC1, xbc0, fmaf(nC2, xca0, acc32[k][6]));
-            acc32[k][7] = fmaf(nC1, xbc1, fmaf(nC2, xca1, acc32[k][7]));
-            acc32[k][8] = fmaf(nC1, xbc2, fmaf(nC2, xca2, acc32[k][8]));
-            const float sab = -(nA1 + nB1) * sc[k], sbc = -(nB2 + nC1) * sc[k],
-                        sca = -(nC2 + nA2) * sc[k];
-            dof0 = fmaf(sab, xab0, fmaf(sbc, xbc0, fmaf(sca, xca0, dof0)));
-            dof1 = fmaf(sab, xab1, fmaf(sbc, xbc1, fmaf(sca, xca1, dof1)));
-            dof2 = fmaf(sab, xab2, fmaf(sbc, xbc2, fmaf(sca, xca2, dof2)));
           }
         }
+        const float dof0 = dof[0].x + dof[0].y, dof1 = dof[1].x + dof[1].y;
+        const float dof2 = dof[2].x + dof[2].y;
         sm.dO32[jq][0][tid] = dof0;
         sm.dO32[jq][1][tid] = dof1;
         sm.dO32[jq][2][tid] = dof2;
@@ -403,12 +488,11 @@ __global__ void __launch_bounds__(THREADS, 3) adjoint_mixed_kernel(const MixedAd
         }
       }
 #pragma unroll
-      for (int k = 0; k < 2; ++k)
-#pragma unroll
-        for (int r = 0; r < 9; ++r) {
-          sm.acc64[k][r][tid] += static_cast<double>(sc[k]) * static_cast<double>(acc32[k][r]);
-          acc32[k][r] = 0.f;
-        }
+      for (int r = 0; r < 9; ++r) {
+        sm.acc64[0][r][tid] += static_cast<double>(sc[0]) * static_cast<double>(acc[r].x);
+        sm.acc64[1][r][tid] += static_cast<double>(sc[1]) * static_cast<double>(acc[r].y);
+        acc[r] = make_float2(0.f, 0.f);
+      }
       __syncthreads();
       for (int e = tid; e < nc * 3; e += THREADS) dO_row[c0 * 3 + e] += sm.dsum[e];
     }

@@ -50,7 +50,8 @@ threads) on a bounded sample of the same workload and prints the same metric.
 `--case NAME [--case-queries N]` runs one kernel on a small case twice and
 exits (the commands behind the ncu summaries in profiles/): fp64_c3 (streaming
 FP64 kernel), fp64_tiled_c3 (FP64 over the prepared mesh), mixed_c3, adjoint_c4
-(per-face mixed adjoint), closest_c3 (closest-point traversal), fwn_c3 (fast
+(per-face mixed adjoint on the gradient workload), adjoint_c3 (the same on the
+c3 workload), closest_c3 (closest-point traversal), fwn_c3 (fast
 winding number, beta = 2) and normals_s9 (area-weighted vertex normals of the
 subdivision-9 sphere).
 """
@@ -94,7 +95,7 @@ def parse_args():
     p.add_argument("--no-fast", action="store_true", help="skip the fast winding-number legs")
     p.add_argument("--no-normals", action="store_true", help="skip the vertex-normal workloads")
     p.add_argument("--case", choices=("fp64_c3", "fp64_tiled_c3", "mixed_c3", "adjoint_c4",
-                                      "closest_c3", "fwn_c3", "normals_s9"),
+                                      "closest_c3", "fwn_c3", "normals_s9", "adjoint_c3"),
                    help="run one kernel on a small case twice (for profiling) and exit")
     p.add_argument("--case-queries", type=int, default=None)
     p.add_argument("--autotune", action="store_true",
@@ -846,10 +847,12 @@ def run_case(args):
     handle = _lib.lib()
     default_nq = {"fp64_c3": 16384, "fp64_tiled_c3": 32768, "mixed_c3": 65536,
                   "adjoint_c4": 16384, "closest_c3": 1 << 20, "fwn_c3": 1 << 20,
-                  "normals_s9": 1}[args.case]
+                  "normals_s9": 1, "adjoint_c3": 65536}[args.case]
     nq = args.case_queries or default_nq
     V, F, O, _ = synthetic.workload("c4_grad" if args.case == "adjoint_c4" else "c3_mixed",
                                     n_queries=nq)
+    if args.case == "adjoint_c3":
+        args.case = "adjoint_c4"  # the same call on the c3 inputs
     Vt, Ft, Ot = (torch.from_numpy(x).cuda() for x in (V, F, O))
     sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     tri, ld, nf = wa.triangle_soa(Vt, Ft)

@@ -622,7 +622,7 @@ __device__ __forceinline__ void mixed_tile_pairs(const unsigned char* rec, const
 }
 
 template <int THREADS, int QPT, int STAGES>
-__global__ void __launch_bounds__(THREADS, 5) mixed_forward_kernel(const MixedArgs a) {
+__global__ void __launch_bounds__(THREADS, 4) mixed_forward_kernel(const MixedArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* ring = smem_raw;  // [STAGES][kTileBytes]
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + STAGES * kTileBytes);

@@ -788,6 +788,12 @@ def gpu_arm(args):
                "sample": f"{n} queries (50/50 box/near) x {nf} faces in {dt:.1f} s, oracle "
                          f"restatement of src/capi.mojo:205-294 over {cores} threads "
                          f"({cpu_model()})"}
+        # The reference's own fan-out caps its pool at four workers (python/igl/_lib.py:37).
+        w4 = min(4, cores)
+        rate4, n4, dt4 = oracle_rate(tri, O, w4, target_s=6.0)
+        cpu["reference_fanout"] = {"value": rate4, "unit": "pairs/s", "cores": w4,
+                                   "sample": f"{n4} queries in {dt4:.1f} s over {w4} threads, "
+                                             "the reference's MAX_WORKERS"}
 
     if rank == 0:
         line = {

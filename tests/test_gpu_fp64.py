@@ -148,3 +148,28 @@ def test_device_entry_rejects_bad_layout(gpu_required):
     handle = _lib.lib()
     assert handle.wn_forward_fp64_device(None, 3, None, None, 2, 1, 0, None) != 0  # odd ld
     assert "ld" in _lib.last_error()
+
+
+@pytest.mark.parametrize("mode", list(MODES))
+def test_translated_multiscale_soup_and_vertex_fans(gpu_required, oracle_mod, mode):
+    """The mixed path's adversarial inputs at the FP64 bar: a mesh 1e6 from the
+    origin, a self-intersecting soup with sizes over four decades, and queries
+    1e-9..1e-3 from vertices where faces fan out."""
+    rng = np.random.default_rng(11)
+    V, F = igl.synthetic.bumpy_icosphere(3, seed=6)
+    t = np.array([1e6, -7e5, 3e5])
+    O = igl.synthetic.mixed_queries(V, F, 256, seed=7, near_sigma=1e-4)
+    tri = igl._triangle_soa(V + t, F)
+    assert np.abs(gpu_host(tri, O + t, mode) - oracle_mod.winding_soa(tri, O + t)).max() <= TOL
+    nf = 3000
+    corners = (rng.uniform(-1, 1, size=(nf, 1, 3))
+               + 10.0 ** rng.uniform(-4, 0, size=(nf, 1, 1)) * rng.normal(size=(nf, 3, 3)))
+    tri = np.ascontiguousarray(corners.transpose(1, 2, 0).reshape(9, nf))
+    O = rng.uniform(-1.2, 1.2, size=(300, 3))
+    assert np.abs(gpu_host(tri, O, mode) - oracle_mod.winding_soa(tri, O)).max() <= TOL
+    vid = rng.integers(0, len(V), size=300)
+    d = rng.normal(size=(300, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    O = V[vid] + d * 10.0 ** rng.uniform(-9, -3, size=(300, 1))
+    tri = igl._triangle_soa(V, F)
+    assert np.abs(gpu_host(tri, O, mode) - oracle_mod.winding_soa(tri, O)).max() <= TOL

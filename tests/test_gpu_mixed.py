@@ -166,3 +166,49 @@ def test_deterministic_repeat(gpu_required):
     tri = igl._triangle_soa(V, F)
     a = mixed_host(tri, O)
     assert np.array_equal(mixed_host(tri, O), a)
+
+
+@pytest.mark.parametrize("offset", [1e2, 1e4, 1e6])
+def test_translated_far_from_origin(gpu_required, oracle_mod, offset):
+    """A unit-size mesh far from the origin: the FP32 frames are tile-local, so the
+    error must not grow with the offset (FP64 tile centres absorb it)."""
+    V, F = igl.synthetic.bumpy_icosphere(4, seed=6)
+    O = igl.synthetic.mixed_queries(V, F, 1024, seed=7, near_sigma=1e-4)
+    t = np.array([offset, -0.7 * offset, 0.3 * offset])
+    tri = igl._triangle_soa(V + t, F)
+    W = mixed_host(tri, O + t)
+    assert np.abs(W - oracle_mod.winding_soa(tri, O + t)).max() <= TOL
+
+
+def test_random_soup_multiscale(gpu_required, oracle_mod):
+    """Self-intersecting soup, triangle sizes log-uniform over four decades, queries
+    uniform in the cube and within 1e-5..1e-2 of random faces."""
+    rng = np.random.default_rng(8)
+    nf = 6000
+    centre = rng.uniform(-1, 1, size=(nf, 1, 3))
+    size = 10.0 ** rng.uniform(-4, 0, size=(nf, 1, 1))
+    corners = centre + size * rng.normal(size=(nf, 3, 3))
+    tri = np.ascontiguousarray(corners.transpose(1, 2, 0).reshape(9, nf))
+    box = rng.uniform(-1.2, 1.2, size=(1024, 3))
+    pick = rng.integers(0, nf, size=1024)
+    u = rng.dirichlet([1, 1, 1], size=1024)
+    on = (u[:, :, None] * corners[pick]).sum(1)
+    n = np.cross(corners[pick, 1] - corners[pick, 0], corners[pick, 2] - corners[pick, 0])
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    near = on + n * (10.0 ** rng.uniform(-5, -2, size=(1024, 1))) * rng.choice([-1, 1], (1024, 1))
+    O = np.concatenate([box, near])
+    W = mixed_host(tri, O)
+    assert np.abs(W - oracle_mod.winding_soa(tri, O)).max() <= TOL
+
+
+def test_queries_clustered_at_vertex_fans(gpu_required, oracle_mod):
+    """Queries 1e-9..1e-3 from vertices where five or six faces meet."""
+    V, F = igl.synthetic.bumpy_icosphere(3, seed=9)
+    rng = np.random.default_rng(10)
+    vid = rng.integers(0, len(V), size=600)
+    d = rng.normal(size=(600, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    O = V[vid] + d * 10.0 ** rng.uniform(-9, -3, size=(600, 1))
+    tri = igl._triangle_soa(V, F)
+    W = mixed_host(tri, O)
+    assert np.abs(W - oracle_mod.winding_soa(tri, O)).max() <= TOL

@@ -558,6 +558,21 @@ def gpu_arm(args):
                         "value": rate, "unit": "points/s", "cores": cores, "kind": "port",
                         "sample": f"first {n_s} points in {dt_s:.1f} s, oracle restatement of "
                                   f"src/capi.mojo:401-586 over {cores} threads"}
+            if key == "c3":
+                # Signed distance: traversal + winding-number sign, all on the device.
+                S_d = torch.empty(npc, dtype=torch.float64, device=dev)
+                W_d = torch.empty(npc, dtype=torch.float64, device=dev)
+                fwn_s = tree.fast_winding()
+
+                def signed_step():
+                    kernel_timed(lambda: check(handle.wn_signed_distance_fast_device(
+                        tree.tree, fwn_s._handle, 2.0, P_d.data_ptr(), npc, S_d.data_ptr(),
+                        i_d.data_ptr(), c_d.data_ptr(), W_d.data_ptr(), sp)))
+
+                t_s = timed(signed_step, max(args.steps, 5), 3)[0]
+                entry["signed_distance_fast"] = {
+                    "ms_per_step": t_s * 1e3, "points_per_s": world * npc / t_s,
+                    "note": "closest point + fast winding number (beta = 2) + sign, one stream"}
             closest[key] = entry
             tree.close()
         closest["note"] = ("reference's published AABB.squared_distance for the "

@@ -260,6 +260,14 @@ int wn_aabb_squared_distance_device(void* tree, const double* P, int64_t np, dou
 int wn_aabb_squared_distance_host(void* tree, const double* P, int64_t np, double* sqrd,
                                   int64_t* index, double* closest);
 
+/* The same with the fast winding number (wn_fast_create over the same faces,
+ * evaluated at `beta`) for the sign: the sign can differ from the exact one only
+ * where |W| lies within the approximation's error of 1/2 (points essentially
+ * on the surface of a closed mesh, or near the boundary of an open one). */
+int wn_signed_distance_fast_device(void* tree, void* fast, double beta, const double* P,
+                                   int64_t np, double* s, int64_t* index, double* closest,
+                                   double* w, void* stream);
+
 /* Diagnostic: closest point on one triangle (tri9 = A, B, C) from p on the
  * host; out4 = (squared distance, x, y, z), by the arithmetic the host
  * traversal and the GPU kernel share, bit-identical to src/capi.mojo:401-495.

@@ -1261,6 +1261,21 @@ int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_
   return collect_device_error(c, c->stream);
 }
 
+int wn_signed_distance_fast_device(void* tree, void* fast, double beta, const double* P,
+                                   int64_t np, double* s, int64_t* index, double* closest,
+                                   double* w, void* stream) {
+  if (int code = check_points(tree, np)) return code;
+  if (!fast) return fail(WN_EINVAL, "null fast winding-number handle");
+  if (np == 0) return WN_OK;
+  if (!w) return fail(WN_EINVAL, "null pointer");
+  if (int code = wn_aabb_squared_distance_device(tree, P, np, s, index, closest, stream))
+    return code;
+  if (int code = wn_fast_eval_device(fast, P, np, beta, w, stream)) return code;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  const cudaError_t e = signed_from_winding(w, s, np, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "signed-distance launch");
+}
+
 // src/capi.mojo:945-947: 1 on success, 0 on failure (the shim raises). Large
 // problems go through the prepared-mesh FP64 kernel (its ~2 ms preparation is
 // repaid above ~1e9 pairs), small ones through the streaming FP64 kernel; both

@@ -362,22 +362,30 @@ def point_mesh_squared_distance(P, V, Ele, device="cpu"):
     return tree.squared_distance(V, Ele, P, device=device)
 
 
-def signed_distance(P, V, F, device="cpu", *, precision="fp64"):
+def signed_distance(P, V, F, device="cpu", *, precision="fp64", beta=2.0):
     """Distance to the surface, negative where the winding number says inside.
 
     Returns (S, I, C): S[i] = -sqrt(sqrd) when |W(P_i)| > 1/2, else
     +sqrt(sqrd), with (sqrd, I, C) from ``point_mesh_squared_distance`` and W
-    from ``winding_number`` on the same device (``precision`` applies to the
-    GPU winding number). For a closed, consistently oriented surface this is
-    the usual inside-negative signed distance; open meshes get the sign of the
+    from ``winding_number`` on the same device (``precision`` "fp64" or
+    "mixed", the latter for the GPU) or, with ``precision="fast"``, from
+    ``fast_winding_number`` at ``beta``, whose error only matters where |W| is
+    that close to 1/2. For a closed, consistently oriented surface this is the
+    usual inside-negative signed distance; open meshes get the sign of the
     rounded winding number. With no faces S is +inf.
     """
     points = _float_array(P, "P")
     if points.ndim != 2 or points.shape[1] != 3:
         raise ValueError("P must have shape (p, 3)")
+    if precision not in PRECISIONS + ("fast",):
+        raise ValueError(f"precision must be one of {PRECISIONS + ('fast',)}")
     sqrd, indices, closest = point_mesh_squared_distance(points, V, F, device=device)
-    W = winding_number(V, F, points, device=device, precision=precision) if len(points) else \
-        np.empty(0)
+    if not len(points):
+        W = np.empty(0)
+    elif precision == "fast":
+        W = fast_winding_number(V, F, points, device=device, beta=beta)
+    else:
+        W = winding_number(V, F, points, device=device, precision=precision)
     distance = np.sqrt(sqrd)
     return np.where(np.abs(W) > 0.5, -distance, distance), indices, closest
 

@@ -5,8 +5,9 @@
 ``query(P)`` runs the sm_100a traversal kernel on device-resident points and
 returns (sqrd, index, closest) tensors, bit-identical to the reference's CPU
 query (src/capi.mojo:401-586). ``signed_distance(P)`` adds the winding number
-of the same faces (FP64 or mixed precision) and signs the distance by it, all
-on the device: negative where |W| > 1/2.
+of the same faces (FP64, mixed precision, or the fast hierarchical
+approximation) and signs the distance by it, all on the device: negative where
+|W| > 1/2.
 
 Tensors are plumbing here: the kernels run in libwn_b200 on the tensors'
 memory and the current stream.
@@ -44,6 +45,7 @@ class DeviceAABB:
                                           ctypes.byref(self.tree)))
         self.kappa = kappa
         self._mesh = None
+        self._fast = None
 
     def query(self, P: torch.Tensor):
         """(sqrd (n,), index (n,) int64, closest (n, 3)) of device points P (n, 3)."""
@@ -68,10 +70,22 @@ class DeviceAABB:
             self._mesh = PreparedMesh(tri, ld, nf, self.kappa)
         return self._mesh
 
-    def signed_distance(self, P: torch.Tensor, precision: str = "fp64"):
-        """(S, index, closest, W): S = -sqrt(sqrd) where |W| > 1/2, else +sqrt(sqrd)."""
-        if precision not in ("fp64", "mixed"):
-            raise ValueError("precision must be 'fp64' or 'mixed'")
+    def fast_winding(self):
+        if self._fast is None:
+            from . import FastWindingNumber
+
+            self._fast = FastWindingNumber(self.vertices, self.faces)
+        return self._fast
+
+    def signed_distance(self, P: torch.Tensor, precision: str = "fp64", beta: float = 2.0):
+        """(S, index, closest, W): S = -sqrt(sqrd) where |W| > 1/2, else +sqrt(sqrd).
+
+        precision "fp64" or "mixed": the exact winding number; "fast": the
+        hierarchical one at ``beta`` (its error only matters where |W| is that
+        close to 1/2).
+        """
+        if precision not in ("fp64", "mixed", "fast"):
+            raise ValueError("precision must be 'fp64', 'mixed' or 'fast'")
         p = P.to(torch.float64).contiguous()
         n = p.shape[0]
         s = torch.empty(n, dtype=torch.float64, device=p.device)
@@ -80,7 +94,11 @@ class DeviceAABB:
         w = torch.empty(n, dtype=torch.float64, device=p.device)
         if n and not self.nf:
             return s.fill_(float("inf")), index.fill_(-1), closest.zero_(), w.zero_()
-        if n:
+        if n and precision == "fast":
+            _check(self.handle.wn_signed_distance_fast_device(
+                self.tree, self.fast_winding()._handle, float(beta), p.data_ptr(), n,
+                s.data_ptr(), index.data_ptr(), closest.data_ptr(), w.data_ptr(), _stream()))
+        elif n:
             mesh = self.winding_mesh()
             _check(self.handle.wn_signed_distance_device(
                 self.tree, mesh.mesh, 0 if precision == "fp64" else 1, p.data_ptr(), n,
@@ -91,6 +109,10 @@ class DeviceAABB:
         if self._mesh is not None:
             self._mesh.close()
             self._mesh = None
+        if self._fast is not None:
+            torch.cuda.current_stream().synchronize()
+            self._fast.close()
+            self._fast = None
         if self.tree:
             torch.cuda.current_stream().synchronize()
             self.handle.wn_aabb_destroy(self.tree)

@@ -233,3 +233,15 @@ def test_closest_point_matches_oracle_bitwise(oracle_mod):
         assert out.tobytes() == expected.tobytes() or (
             np.isnan(out).any() and np.array_equal(np.isnan(out), np.isnan(expected))), (
             t, p, out, expected)
+
+
+def test_signed_distance_fast_sign_cpu():
+    """The hierarchical winding number gives the same signs away from |W| ~ 1/2."""
+    V, F = igl.synthetic.bumpy_icosphere(4, seed=12)
+    P = igl.synthetic.mixed_queries(V, F, 2000, seed=13, near_sigma=1e-3)
+    exact, _, _ = igl.signed_distance(P, V, F)
+    fast, _, _ = igl.signed_distance(P, V, F, precision="fast")
+    assert np.array_equal(np.abs(fast), np.abs(exact))
+    assert np.array_equal(np.sign(fast), np.sign(exact))
+    with pytest.raises(ValueError):
+        igl.signed_distance(P, V, F, precision="half")

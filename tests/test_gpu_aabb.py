@@ -156,3 +156,24 @@ def test_device_error_word_stays_clear(gpu_required):
     _device_query(V, F, igl.synthetic.mixed_queries(V, F, 30_000, seed=2))
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     assert igl.lib().wn_stream_check(stream) == 0
+
+
+def test_signed_distance_fast_device(gpu_required):
+    import torch
+
+    from igl import distance
+
+    V, F = igl.synthetic.bumpy_icosphere(5, seed=14)
+    P = igl.synthetic.mixed_queries(V, F, 50_000, seed=15, near_sigma=1e-3)
+    tree = distance.DeviceAABB(V, F)
+    Pt = torch.from_numpy(P).cuda()
+    S64, i64, c64, W64 = tree.signed_distance(Pt, precision="fp64")
+    Sf, i_f, c_f, Wf = tree.signed_distance(Pt, precision="fast")
+    torch.cuda.synchronize()
+    assert torch.equal(i64, i_f) and torch.equal(c64, c_f)
+    assert torch.equal(S64.abs(), Sf.abs())
+    assert (Wf - W64).abs().max().item() <= 1e-2
+    assert torch.equal(torch.sign(S64), torch.sign(Sf))
+    S_np, _, _ = igl.signed_distance(P, V, F, device="gpu", precision="fast")
+    assert np.array_equal(S_np, Sf.cpu().numpy())
+    tree.close()

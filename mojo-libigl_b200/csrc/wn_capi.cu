@@ -50,6 +50,19 @@ int cuda_fail(cudaError_t e, const char* what) {
               cudaGetErrorString(e), cudaGetErrorName(e));
 }
 
+// A handle's device memory belongs to the device it was made on: a call made
+// while another device is current would launch kernels on memory that device
+// cannot address, so it is refused.
+int check_device(int handle_device, const char* what) {
+  int dev = -1;
+  const cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev != handle_device)
+    return fail(WN_EINVAL, "%s lives on device %d, but device %d is current", what,
+                handle_device, dev);
+  return WN_OK;
+}
+
 struct Buffer {
   void* ptr = nullptr;
   size_t bytes = 0;
@@ -447,6 +460,7 @@ int wn_forward_mixed_device(void* mesh, const double* q, int64_t nq, double* w, 
   DeviceCtx* c = context(&code);
   if (!c) return code;
   const MeshHandle* h = static_cast<const MeshHandle*>(mesh);
+  if ((code = check_device(h->device, "mesh")) != WN_OK) return code;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t sb = mixed_forward_scratch_bytes(h->m.ntiles, nq, c->sms);
   void* scratch = nullptr;
@@ -467,6 +481,7 @@ int wn_forward_fp64_mesh_device(void* mesh, const double* q, int64_t nq, double*
   DeviceCtx* c = context(&code);
   if (!c) return code;
   const MeshHandle* h = static_cast<const MeshHandle*>(mesh);
+  if ((code = check_device(h->device, "mesh")) != WN_OK) return code;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const Fp64TiledPlan p = plan_fp64_tiled(h->m.ntiles, nq, c->sms);
   double* scratch = nullptr;
@@ -506,6 +521,7 @@ int wn_forward_mixed_sorted_device(void* mesh, const double* q, const uint32_t* 
   DeviceCtx* c = context(&code);
   if (!c) return code;
   const MeshHandle* h = static_cast<const MeshHandle*>(mesh);
+  if ((code = check_device(h->device, "mesh")) != WN_OK) return code;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const MixedSplit p = plan_mixed(h->m.ntiles, nq, c->sms);
   double* partial = nullptr;
@@ -528,6 +544,7 @@ int wn_mixed_mesh_update(void* mesh, const double* tri, int64_t ld, void* stream
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
   if (!context(&code)) return code;
+  if ((code = check_device(h->device, "mesh")) != WN_OK) return code;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t sb = mixed_sort_scratch_bytes(h->m.nf);
   void* scratch = nullptr;
@@ -584,6 +601,7 @@ int wn_backward_mixed_device(void* mesh, const double* q, int64_t nq, const doub
   int code = WN_OK;
   DeviceCtx* c = context(&code);
   if (!c) return code;
+  if ((code = check_device(h->device, "mesh")) != WN_OK) return code;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const AdjointPlan p = plan_adjoint_mixed(h->m.ntiles, nq, c->sms);
   const size_t perm_bytes = ((static_cast<size_t>(std::max<int64_t>(nq, 1)) * 4 + 255) / 256) * 256;
@@ -686,6 +704,8 @@ int wn_batch_forward(void* batch, const double* V, const double* q, double* w, v
   int code = WN_OK;
   DeviceCtx* c = context(&code);
   if (!c) return code;
+  if ((code = check_device(static_cast<const BatchState*>(batch)->device, "batch")) != WN_OK)
+    return code;
   cudaError_t e = batch_forward(static_cast<BatchState*>(batch), V, q, w, c->stats, c->err,
                                 static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "batched forward launch");
@@ -697,6 +717,8 @@ int wn_batch_backward(void* batch, const double* V, const double* q, const doubl
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
   if (!context(&code)) return code;
+  if ((code = check_device(static_cast<const BatchState*>(batch)->device, "batch")) != WN_OK)
+    return code;
   cudaError_t e = batch_backward(static_cast<BatchState*>(batch), V, q, gw, dq, dV,
                                  static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "batched adjoint launch");
@@ -848,6 +870,8 @@ int wn_aabb_squared_distance_device(void* tree, const double* P, int64_t np, dou
   int code = WN_OK;
   DeviceCtx* c = context(&code);
   if (!c) return code;
+  if ((code = check_device(static_cast<const AabbHandle*>(tree)->device, "tree")) != WN_OK)
+    return code;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t sb = aabb_sort_bytes(np);
   void* scratch = nullptr;
@@ -869,6 +893,8 @@ int wn_aabb_squared_distance_host(void* tree, const double* P, int64_t np, doubl
   int code = WN_OK;
   DeviceCtx* c = context(&code);
   if (!c) return code;
+  if ((code = check_device(static_cast<const AabbHandle*>(tree)->device, "tree")) != WN_OK)
+    return code;
   const size_t out_bytes = align256(sizeof(int64_t) * np) + align256(sizeof(double) * 3 * np);
   cudaError_t e;
   if ((e = c->q.ensure(sizeof(double) * 3 * np)) != cudaSuccess ||
@@ -1211,6 +1237,7 @@ int wn_vertex_normals_device(void* handle, const double* V, int weighting, doubl
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
   if (!context(&code)) return code;
+  if ((code = check_device(h->device, "normals topology")) != WN_OK) return code;
   const int mode = weighting == 3 ? 1 : weighting;
   if ((code = normals_contrib(h, mode)) != WN_OK) return code;
   const cudaError_t e = normals_eval(h->t, V, mode, N, static_cast<cudaStream_t>(stream));

@@ -30,6 +30,9 @@
 
 namespace wn {
 
+// Most faces in one leaf (the kernel's deferred face lists rely on it).
+constexpr int kFwnLeafFaces = 8;
+
 struct __align__(64) FwnNode {
   double p[3];  // area-weighted centre of the node's faces
   double r;     // radius about p holding every vertex of those faces

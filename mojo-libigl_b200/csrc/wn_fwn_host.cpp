@@ -16,8 +16,6 @@
 namespace wn {
 namespace {
 
-constexpr int64_t kLeafFaces = 8;
-
 // Moments of the faces in records [lo, hi) about their area-weighted centre.
 void node_moments(const AabbTriRec* tris, int64_t lo, int64_t hi, FwnNode& node,
                   FwnMoments& out) {
@@ -123,10 +121,10 @@ int fwn_build(const double* V, int64_t nv, const int64_t* F, int64_t nf, int thr
     *why = "more than 2^31-1 faces";
     return -1;
   }
-  const int64_t nn = aabb_node_count(nf, kLeafFaces);
+  const int64_t nn = aabb_node_count(nf, kFwnLeafFaces);
   std::vector<double> boxes(6 * nn);
   std::vector<int64_t> nodes(4 * nn), order(nf);
-  const int64_t stack = aabb_build(V, nv, F, nf, kLeafFaces, boxes.data(), nodes.data(),
+  const int64_t stack = aabb_build(V, nv, F, nf, kFwnLeafFaces, boxes.data(), nodes.data(),
                                    order.data(), threads, why);
   if (stack < 0) return -1;
   if (stack > kAabbStack) {

@@ -38,6 +38,9 @@ enum {
   WN_ENOMEM = 5    /* device allocation failed */
 };
 
+/* Fault kinds of wn_inject_fault. */
+enum { WN_FAULT_NONE = 0, WN_FAULT_ALLOC = 1 };
+
 /* FP64 accumulation modes of the plain kernel. */
 enum {
   WN_FP64_ARGPROD = 0, /* bit-exact pair terms, argument-of-product sum */
@@ -99,6 +102,16 @@ int wn_stream_check(void* stream);
 int wn_selftest_bounded_wait(int64_t polls);
 /* Number of kernels this library has launched since it was loaded. */
 int64_t wn_launch_count(void);
+/* Host-side fault injection, for tests of the out-of-memory paths on a real
+ * device: kind WN_FAULT_ALLOC makes the (after+1)-th device allocation of the
+ * library from now on report failure (WN_ENOMEM from the entry point) without
+ * allocating; WN_FAULT_NONE disarms. One-shot. Every entry point returns
+ * before launching work that needs the failed allocation, so nothing on the
+ * device runs differently. WN_INJECT_FAULT=alloc:N in the environment arms it
+ * when the library is loaded. */
+int wn_inject_fault(int kind, int64_t after);
+/* 1 while an injected fault is armed and has not fired, else 0. */
+int wn_fault_armed(void);
 /* Measured FMA-pipe peak of the current device in TFLOP/s (FMA = 2 flops),
  * bits = 64 or 32: the roofline denominator of these FP64/FP32-bound kernels. */
 int wn_probe_fma_tflops(int bits, double* tflops);

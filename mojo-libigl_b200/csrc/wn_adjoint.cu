@@ -1147,7 +1147,7 @@ cudaError_t batch_edges_create(BatchState* b, const int64_t* F) {
   auto up = [](auto** dst, const auto& src, size_t min_count) -> cudaError_t {
     using T = typename std::remove_reference<decltype(src)>::type::value_type;
     const size_t n = std::max(src.size(), min_count);
-    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(dst), sizeof(T) * std::max<size_t>(n, 1));
+    cudaError_t e = dev_malloc(reinterpret_cast<void**>(dst), sizeof(T) * std::max<size_t>(n, 1));
     if (e == cudaSuccess && !src.empty())
       e = cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice);
     return e;
@@ -1160,15 +1160,15 @@ cudaError_t batch_edges_create(BatchState* b, const int64_t* F) {
       (e = up(&E->meshes, meshes, 1)) != cudaSuccess ||
       (e = up(&E->query_mesh, query_mesh, 1)) != cudaSuccess ||
       (e = up(&E->edge_mesh, edge_mesh, 1)) != cudaSuccess ||
-      (e = cudaMalloc(reinterpret_cast<void**>(&E->edges), sizeof(double) * 7 * E->le)) !=
+      (e = dev_malloc(reinterpret_cast<void**>(&E->edges), sizeof(double) * 7 * E->le)) !=
           cudaSuccess ||
-      (e = cudaMalloc(reinterpret_cast<void**>(&E->dedge), sizeof(double) * 6 * E->le)) !=
+      (e = dev_malloc(reinterpret_cast<void**>(&E->dedge), sizeof(double) * 6 * E->le)) !=
           cudaSuccess ||
-      (e = cudaMalloc(reinterpret_cast<void**>(&E->counter), sizeof(unsigned int))) !=
+      (e = dev_malloc(reinterpret_cast<void**>(&E->counter), sizeof(unsigned int))) !=
           cudaSuccess ||
-      (e = cudaMalloc(reinterpret_cast<void**>(&E->dO_part),
+      (e = dev_malloc(reinterpret_cast<void**>(&E->dO_part),
                       sizeof(double) * std::max<int64_t>(E->do_doubles, 1))) != cudaSuccess ||
-      (e = cudaMalloc(reinterpret_cast<void**>(&E->dE_part),
+      (e = dev_malloc(reinterpret_cast<void**>(&E->dE_part),
                       sizeof(double) * std::max<int64_t>(E->de_doubles, 1))) != cudaSuccess)
     return e;
   int per_sm = 0;

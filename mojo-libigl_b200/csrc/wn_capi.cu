@@ -31,6 +31,49 @@ std::atomic<int64_t> g_launches{0};
 
 namespace {
 
+std::atomic<int> g_fault_kind{WN_FAULT_NONE};  // armed kind
+std::atomic<int64_t> g_fault_left{0};          // matching events to let through first
+
+// One-shot: true for the armed event that the countdown reaches.
+bool fault_fires(int kind) {
+  if (g_fault_kind.load(std::memory_order_acquire) != kind) return false;
+  if (g_fault_left.fetch_sub(1, std::memory_order_acq_rel) != 0) return false;
+  int armed = kind;
+  return g_fault_kind.compare_exchange_strong(armed, WN_FAULT_NONE);
+}
+
+// WN_INJECT_FAULT=alloc:N arms an allocation fault when the library is loaded.
+struct FaultFromEnv {
+  FaultFromEnv() {
+    const char* s = std::getenv("WN_INJECT_FAULT");
+    long long n = -1;
+    if (s && std::sscanf(s, "alloc:%lld", &n) == 1 && n >= 0) {
+      g_fault_left.store(n);
+      g_fault_kind.store(WN_FAULT_ALLOC);
+    }
+  }
+} g_fault_from_env;
+
+}  // namespace
+
+cudaError_t dev_malloc(void** p, size_t bytes) {
+  if (fault_fires(WN_FAULT_ALLOC)) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+
+cudaError_t dev_malloc_async(void** p, size_t bytes, cudaStream_t stream) {
+  if (fault_fires(WN_FAULT_ALLOC)) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMallocAsync(p, bytes, stream);
+}
+
+namespace {
+
 constexpr int kMaxDevices = 64;
 
 thread_local std::string t_last_error;
@@ -72,7 +115,7 @@ struct Buffer {
     ptr = nullptr;
     bytes = 0;
     size_t grow = need + need / 4;
-    cudaError_t e = cudaMalloc(&ptr, grow);
+    cudaError_t e = dev_malloc(&ptr, grow);
     if (e != cudaSuccess) {
       ptr = nullptr;
       return e;
@@ -108,10 +151,11 @@ DeviceCtx* context(int* code) {
   DeviceCtx& c = g_ctx[dev];
   if (c.ready) return &c;
   if ((e = cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
-      (e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking)) != cudaSuccess ||
-      (e = cudaMalloc(&c.err, sizeof(int))) != cudaSuccess ||
+      (!c.stream &&
+       (e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking)) != cudaSuccess) ||
+      (!c.err && (e = dev_malloc(&c.err, sizeof(int))) != cudaSuccess) ||
       (e = cudaMemset(c.err, 0, sizeof(int))) != cudaSuccess ||
-      (e = cudaMalloc(&c.stats, 2 * sizeof(unsigned long long))) != cudaSuccess ||
+      (!c.stats && (e = dev_malloc(&c.stats, 2 * sizeof(unsigned long long))) != cudaSuccess) ||
       (e = cudaMemset(c.stats, 0, 2 * sizeof(unsigned long long))) != cudaSuccess) {
     *code = cuda_fail(e, "device context setup");
     return nullptr;
@@ -297,6 +341,18 @@ int wn_version(void) { return 100; }
 
 int64_t wn_launch_count(void) { return g_launches.load(); }
 
+int wn_inject_fault(int kind, int64_t after) {
+  if (kind != WN_FAULT_NONE && kind != WN_FAULT_ALLOC)
+    return fail(WN_EINVAL, "unknown fault kind %d", kind);
+  if (after < 0) return fail(WN_EINVAL, "negative countdown");
+  g_fault_kind.store(WN_FAULT_NONE);
+  g_fault_left.store(after);
+  g_fault_kind.store(kind);
+  return WN_OK;
+}
+
+int wn_fault_armed(void) { return g_fault_kind.load() != WN_FAULT_NONE ? 1 : 0; }
+
 int wn_probe_fma_tflops(int bits, double* tflops) {
   if ((bits != 32 && bits != 64) || !tflops) return fail(WN_EINVAL, "bits must be 32 or 64");
   std::lock_guard<std::mutex> lock(g_mutex);
@@ -373,7 +429,7 @@ int wn_forward_fp64_device(const double* tri, int64_t ld, const double* q, doubl
   double* scratch = nullptr;
   cudaError_t e = cudaSuccess;
   if (plan.scratch_doubles > 0 &&
-      (e = cudaMallocAsync(reinterpret_cast<void**>(&scratch),
+      (e = dev_malloc_async(reinterpret_cast<void**>(&scratch),
                            sizeof(double) * plan.scratch_doubles, st)) != cudaSuccess)
     return cuda_fail(e, "device allocation");
   e = launch_fp64(plan, mode, tri, ld, nf, q, nq, w, scratch, c->err, st);
@@ -404,15 +460,15 @@ int wn_mixed_mesh_create(const double* tri, int64_t ld, int64_t nf, double kappa
   cudaError_t e;
   void* scratch = nullptr;
   const size_t sb = mixed_sort_scratch_bytes(nf);
-  if ((e = cudaMalloc(reinterpret_cast<void**>(&h->m.tiles), mixed_tiles_bytes(nf))) !=
+  if ((e = dev_malloc(reinterpret_cast<void**>(&h->m.tiles), mixed_tiles_bytes(nf))) !=
           cudaSuccess ||
-      (e = cudaMalloc(reinterpret_cast<void**>(&h->m.tri64), mixed_tri64_bytes(nf))) !=
+      (e = dev_malloc(reinterpret_cast<void**>(&h->m.tri64), mixed_tri64_bytes(nf))) !=
           cudaSuccess ||
-      (e = cudaMalloc(reinterpret_cast<void**>(&h->m.face_of), mixed_face_of_bytes(nf))) !=
+      (e = dev_malloc(reinterpret_cast<void**>(&h->m.face_of), mixed_face_of_bytes(nf))) !=
           cudaSuccess ||
-      (e = cudaMalloc(reinterpret_cast<void**>(&h->m.reuse), mixed_reuse_bytes(nf))) !=
+      (e = dev_malloc(reinterpret_cast<void**>(&h->m.reuse), mixed_reuse_bytes(nf))) !=
           cudaSuccess ||
-      (e = cudaMallocAsync(&scratch, sb, st)) != cudaSuccess) {
+      (e = dev_malloc_async(&scratch, sb, st)) != cudaSuccess) {
     cudaFree(h->m.tiles);
     cudaFree(h->m.tri64);
     cudaFree(h->m.face_of);
@@ -464,7 +520,7 @@ int wn_forward_mixed_device(void* mesh, const double* q, int64_t nq, double* w, 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t sb = mixed_forward_scratch_bytes(h->m.ntiles, nq, c->sms);
   void* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(&scratch, sb, st);
+  cudaError_t e = dev_malloc_async(&scratch, sb, st);
   if (e != cudaSuccess) return cuda_fail(e, "device allocation");
   e = mixed_forward(h->m, q, nq, w, scratch, sb, c->sms, c->stats, c->err, st);
   cudaFreeAsync(scratch, st);
@@ -487,7 +543,7 @@ int wn_forward_fp64_mesh_device(void* mesh, const double* q, int64_t nq, double*
   double* scratch = nullptr;
   cudaError_t e = cudaSuccess;
   if (p.scratch_doubles > 0 &&
-      (e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), sizeof(double) * p.scratch_doubles,
+      (e = dev_malloc_async(reinterpret_cast<void**>(&scratch), sizeof(double) * p.scratch_doubles,
                            st)) != cudaSuccess)
     return cuda_fail(e, "device allocation");
   e = launch_fp64_tiled(p, h->m, q, nq, w, scratch, c->err, st);
@@ -504,7 +560,7 @@ int wn_mixed_sort_queries(const double* q, int64_t nq, uint32_t* perm, void* str
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t sb = mixed_sort_scratch_bytes(nq);
   void* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(&scratch, sb, st);
+  cudaError_t e = dev_malloc_async(&scratch, sb, st);
   if (e != cudaSuccess) return cuda_fail(e, "device allocation");
   e = mixed_sort_queries(q, nq, perm, scratch, sb, st);
   cudaFreeAsync(scratch, st);
@@ -527,7 +583,7 @@ int wn_forward_mixed_sorted_device(void* mesh, const double* q, const uint32_t* 
   double* partial = nullptr;
   cudaError_t e = cudaSuccess;
   if (p.partial_doubles > 0 &&
-      (e = cudaMallocAsync(reinterpret_cast<void**>(&partial), sizeof(double) * p.partial_doubles,
+      (e = dev_malloc_async(reinterpret_cast<void**>(&partial), sizeof(double) * p.partial_doubles,
                            st)) != cudaSuccess)
     return cuda_fail(e, "device allocation");
   e = mixed_forward_sorted(h->m, q, perm, nq, w, p, partial, c->stats, c->err, st);
@@ -548,7 +604,7 @@ int wn_mixed_mesh_update(void* mesh, const double* tri, int64_t ld, void* stream
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t sb = mixed_sort_scratch_bytes(h->m.nf);
   void* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(&scratch, sb, st);
+  cudaError_t e = dev_malloc_async(&scratch, sb, st);
   if (e != cudaSuccess) return cuda_fail(e, "device allocation");
   e = mixed_prepare_mesh(tri, ld, h->m.nf, h->m.kappa, &h->m, scratch, sb, st);
   cudaFreeAsync(scratch, st);
@@ -583,7 +639,7 @@ int wn_backward_fp64_device(const double* tri, int64_t ld, int64_t nf, const dou
   const AdjointPlan p = plan_adjoint(nf, nq, c->sms);
   const size_t sb = adjoint_scratch_bytes(p, ld, nq);
   void* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(&scratch, sb, st);
+  cudaError_t e = dev_malloc_async(&scratch, sb, st);
   if (e != cudaSuccess) return cuda_fail(e, "device allocation");
   e = adjoint_fp64(p, tri, ld, nf, q, nq, gw, dq, dtri, scratch, sb, st);
   cudaFreeAsync(scratch, st);
@@ -608,7 +664,7 @@ int wn_backward_mixed_device(void* mesh, const double* q, int64_t nq, const doub
   const size_t sort_bytes = mixed_sort_scratch_bytes(nq);
   const size_t adj_bytes = adjoint_scratch_bytes(p, h->m.ld64, nq);
   unsigned char* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&scratch),
+  cudaError_t e = dev_malloc_async(reinterpret_cast<void**>(&scratch),
                                   perm_bytes + std::max(sort_bytes, adj_bytes), st);
   if (e != cudaSuccess) return cuda_fail(e, "device allocation");
   uint32_t* perm = reinterpret_cast<uint32_t*>(scratch);
@@ -634,7 +690,7 @@ int wn_backward_edges_device(const double* edges, int64_t le, int64_t ne, const 
   const AdjointPlan p = plan_adjoint_edges(ne, nq, c->sms);
   const size_t sb = adjoint_edges_scratch_bytes(p, le, nq);
   void* scratch = nullptr;
-  cudaError_t e = cudaMallocAsync(&scratch, sb, st);
+  cudaError_t e = dev_malloc_async(&scratch, sb, st);
   if (e != cudaSuccess) return cuda_fail(e, "device allocation");
   e = adjoint_edges(p, edges, le, ne, q, nq, gw, dq, dedge, scratch, sb, st);
   cudaFreeAsync(scratch, st);
@@ -831,8 +887,8 @@ int wn_aabb_create(const double* V, int64_t nv, const int64_t* F, int64_t nf,
   if (nnodes > 0) {
     for (int k = 0; k < 6; ++k) h->t.root[k] = boxes[k];
     cudaError_t e;
-    if ((e = cudaMalloc(&h->t.nodes, sizeof(AabbNodeRec) * nrec.size())) != cudaSuccess ||
-        (e = cudaMalloc(&h->t.tris, sizeof(AabbTriRec) * trec.size())) != cudaSuccess ||
+    if ((e = dev_malloc(&h->t.nodes, sizeof(AabbNodeRec) * nrec.size())) != cudaSuccess ||
+        (e = dev_malloc(&h->t.tris, sizeof(AabbTriRec) * trec.size())) != cudaSuccess ||
         (e = cudaMemcpy(h->t.nodes, nrec.data(), sizeof(AabbNodeRec) * nrec.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(h->t.tris, trec.data(), sizeof(AabbTriRec) * trec.size(),
@@ -876,7 +932,7 @@ int wn_aabb_squared_distance_device(void* tree, const double* P, int64_t np, dou
   const size_t sb = aabb_sort_bytes(np);
   void* scratch = nullptr;
   cudaError_t e = cudaSuccess;
-  if (sb && (e = cudaMallocAsync(&scratch, sb, st)) != cudaSuccess)
+  if (sb && (e = dev_malloc_async(&scratch, sb, st)) != cudaSuccess)
     return cuda_fail(e, "device allocation");
   e = aabb_run(static_cast<const AabbHandle*>(tree), P, np, sqrd, index, closest, scratch, c->err,
                st);
@@ -971,9 +1027,9 @@ int fwn_upload(FwnHandle* h) {
   d.depth = h->host.depth;
   if (d.nnodes > 0) {
     cudaError_t e;
-    if ((e = cudaMalloc(&d.nodes, sizeof(FwnNode) * d.nnodes)) != cudaSuccess ||
-        (e = cudaMalloc(&d.moments, sizeof(FwnMoments) * d.nnodes)) != cudaSuccess ||
-        (e = cudaMalloc(&d.tris, sizeof(AabbTriRec) * h->host.nf)) != cudaSuccess ||
+    if ((e = dev_malloc(&d.nodes, sizeof(FwnNode) * d.nnodes)) != cudaSuccess ||
+        (e = dev_malloc(&d.moments, sizeof(FwnMoments) * d.nnodes)) != cudaSuccess ||
+        (e = dev_malloc(&d.tris, sizeof(AabbTriRec) * h->host.nf)) != cudaSuccess ||
         (e = cudaMemcpy(d.nodes, h->host.nodes, sizeof(FwnNode) * d.nnodes,
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(d.moments, h->host.moments, sizeof(FwnMoments) * d.nnodes,
@@ -1073,7 +1129,7 @@ int wn_fast_eval_device(void* handle, const double* q, int64_t nq, double beta, 
   const size_t sb = aabb_sort_bytes(nq);
   void* scratch = nullptr;
   cudaError_t e = cudaSuccess;
-  if (sb && (e = cudaMallocAsync(&scratch, sb, st)) != cudaSuccess)
+  if (sb && (e = dev_malloc_async(&scratch, sb, st)) != cudaSuccess)
     return cuda_fail(e, "device allocation");
   e = fwn_run(h, q, nq, beta, w, scratch, c->err, st);
   if (scratch) cudaFreeAsync(scratch, st);
@@ -1146,9 +1202,9 @@ int normals_alloc(NormalsHandle* h, int64_t nf, int64_t nv) {
   h->t.nv = nv;
   cudaGetDevice(&h->device);
   cudaError_t e;
-  if ((e = cudaMalloc(&h->t.F, sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess ||
-      (e = cudaMalloc(&h->t.indptr, sizeof(int32_t) * (nv + 1))) != cudaSuccess ||
-      (e = cudaMalloc(&h->t.entries, sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess) {
+  if ((e = dev_malloc(&h->t.F, sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess ||
+      (e = dev_malloc(&h->t.indptr, sizeof(int32_t) * (nv + 1))) != cudaSuccess ||
+      (e = dev_malloc(&h->t.entries, sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess) {
     normals_release(h);
     return cuda_fail(e, "device allocation");
   }
@@ -1163,7 +1219,7 @@ int normals_prepare(const int64_t* F, int64_t nf, cudaStream_t st, NormalsHandle
   const size_t f64_bytes = ((sizeof(int64_t) * 3 * nf + 255) / 256) * 256;
   const size_t sb = f64_bytes + 256 + normals_scratch_bytes(nf);
   unsigned char* scratch = nullptr;
-  if ((e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), sb, st)) != cudaSuccess)
+  if ((e = dev_malloc_async(reinterpret_cast<void**>(&scratch), sb, st)) != cudaSuccess)
     return cuda_fail(e, "device allocation");
   int64_t* F64 = reinterpret_cast<int64_t*>(scratch);
   int* bad = reinterpret_cast<int*>(scratch + f64_bytes);
@@ -1188,7 +1244,7 @@ int normals_contrib(NormalsHandle* h, int mode) {
   cudaFree(h->t.contrib);
   h->t.contrib = nullptr;
   h->t.contrib_doubles = 0;
-  const cudaError_t e = cudaMalloc(&h->t.contrib, sizeof(double) * (need > 0 ? need : 1));
+  const cudaError_t e = dev_malloc(&h->t.contrib, sizeof(double) * (need > 0 ? need : 1));
   if (e != cudaSuccess) return cuda_fail(e, "device allocation");
   h->t.contrib_doubles = need;
   return WN_OK;

@@ -14,6 +14,22 @@ void record_error(const char* message);
 // Kernels launched by this library since load (wn_launch_count()).
 extern std::atomic<int64_t> g_launches;
 
+// Every device allocation of the library goes through these two. They behave
+// as cudaMalloc / cudaMallocAsync, except that an allocation fault armed by
+// wn_inject_fault (or WN_INJECT_FAULT=alloc:N in the environment) makes the
+// chosen allocation report cudaErrorMemoryAllocation without allocating, so
+// the tests can walk every out-of-memory path on a real device.
+cudaError_t dev_malloc(void** p, size_t bytes);
+cudaError_t dev_malloc_async(void** p, size_t bytes, cudaStream_t stream);
+template <class T>
+cudaError_t dev_malloc(T** p, size_t bytes) {
+  return dev_malloc(reinterpret_cast<void**>(p), bytes);
+}
+template <class T>
+cudaError_t dev_malloc_async(T** p, size_t bytes, cudaStream_t stream) {
+  return dev_malloc_async(reinterpret_cast<void**>(p), bytes, stream);
+}
+
 // Failure-path self-test (wn_probe.cu): one CTA waits on an mbarrier phase that no
 // copy will complete, with a `polls` limit; the wait runs out, the kernel sets the
 // timeout bit of `err` and returns.

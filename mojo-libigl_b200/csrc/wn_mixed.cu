@@ -1150,7 +1150,7 @@ int batch_grid(int sms, int ctas_per_sm) {
 
 template <typename T>
 cudaError_t dmalloc(T** p, size_t count) {
-  return cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * std::max<size_t>(count, 1));
+  return dev_malloc(reinterpret_cast<void**>(p), sizeof(T) * std::max<size_t>(count, 1));
 }
 
 }  // namespace
@@ -1271,7 +1271,7 @@ cudaError_t batch_create(BatchState* b, int64_t nmesh, const int64_t* nv, const 
       (e = dmalloc(&d->qkeys_out, b->total_nq)) != cudaSuccess ||
       (e = dmalloc(&d->qvals_in, b->total_nq)) != cudaSuccess ||
       (e = dmalloc(&d->perm, b->total_nq)) != cudaSuccess ||
-      (e = cudaMalloc(&d->sort_temp, std::max<size_t>(d->sort_temp_bytes, 16))) != cudaSuccess ||
+      (e = dev_malloc(&d->sort_temp, std::max<size_t>(d->sort_temp_bytes, 16))) != cudaSuccess ||
       (e = dmalloc(&d->mesh.tiles, static_cast<size_t>(std::max<int64_t>(b->total_tiles, 1)) *
                                        kTileBytes)) != cudaSuccess ||
       (e = dmalloc(&d->mesh.tri64, 9 * ld64)) != cudaSuccess ||

@@ -34,7 +34,7 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(T a, T b, int iters, T* 
 template <typename T>
 cudaError_t run_probe(int sms, int iters, cudaStream_t stream, float* ms) {
   T* sink = nullptr;
-  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&sink), sizeof(T), stream);
+  cudaError_t e = dev_malloc_async(reinterpret_cast<void**>(&sink), sizeof(T), stream);
   if (e != cudaSuccess) return e;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);

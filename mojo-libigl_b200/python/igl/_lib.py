@@ -55,6 +55,8 @@ _WN_SIGNATURES = {
     "wn_stream_check": ([P], C_INT),
     "wn_selftest_bounded_wait": ([I], C_INT),
     "wn_launch_count": ([], I),
+    "wn_inject_fault": ([C_INT, I], C_INT),
+    "wn_fault_armed": ([], C_INT),
     "wn_probe_fma_tflops": ([C_INT, ctypes.POINTER(ctypes.c_double)], C_INT),
     "wn_forward_fp64_host": ([P, P, P, I, I, C_INT], C_INT),
     "wn_forward_fp64_device": ([P, I, P, P, I, I, C_INT, P], C_INT),

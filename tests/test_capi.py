@@ -4,6 +4,8 @@ import ctypes
 import glob
 import os
 import re
+import subprocess
+import sys
 
 from igl import _lib
 from conftest import ROOT
@@ -42,3 +44,21 @@ def test_runtime_queries_do_not_need_a_gpu():
     handle = _lib.lib()
     assert handle.wn_version() >= 100
     assert handle.wn_device_count() >= 0
+
+
+def test_fault_injection_arming_does_not_need_a_gpu():
+    handle = _lib.lib()
+    assert handle.wn_inject_fault(7, 0) != 0  # unknown kind
+    assert handle.wn_inject_fault(1, -1) != 0  # negative countdown
+    assert handle.wn_inject_fault(1, 5) == 0 and handle.wn_fault_armed() == 1
+    assert handle.wn_inject_fault(0, 0) == 0 and handle.wn_fault_armed() == 0
+
+
+def test_fault_injection_from_the_environment():
+    code = "from igl import _lib; print(_lib.lib().wn_fault_armed())"
+    env = dict(os.environ, WN_INJECT_FAULT="alloc:2",
+               PYTHONPATH=os.path.join(ROOT, "mojo-libigl_b200", "python"))
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip().splitlines()[-1] == "1"

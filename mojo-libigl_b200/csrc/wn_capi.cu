@@ -354,6 +354,7 @@ int wn_inject_fault(int kind, int64_t after) {
 int wn_fault_armed(void) { return g_fault_kind.load() != WN_FAULT_NONE ? 1 : 0; }
 
 int wn_probe_fma_tflops(int bits, double* tflops) {
+  WN_NVTX_RANGE();
   if ((bits != 32 && bits != 64) || !tflops) return fail(WN_EINVAL, "bits must be 32 or 64");
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
@@ -387,6 +388,7 @@ int wn_device_memory(int64_t* free_bytes, int64_t* total_bytes) {
 }
 
 int wn_selftest_bounded_wait(int64_t polls) {
+  WN_NVTX_RANGE();
   if (polls < 1 || polls > (int64_t(1) << 24)) return fail(WN_EINVAL, "polls must be in [1, 2^24]");
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
@@ -407,11 +409,13 @@ int wn_stream_check(void* stream) {
 
 int wn_forward_fp64_host(const double* tri, const double* q, double* w, int64_t nf, int64_t nq,
                          int mode) {
+  WN_NVTX_RANGE();
   return forward_fp64_host(tri, q, w, nf, nq, mode);
 }
 
 int wn_forward_fp64_device(const double* tri, int64_t ld, const double* q, double* w, int64_t nf,
                            int64_t nq, int mode, void* stream) {
+  WN_NVTX_RANGE();
   if (nf < 0 || nq < 0 || (ld & 1) || ld < nf)
     return fail(WN_EINVAL, "bad sizes (nf=%lld, nq=%lld, ld=%lld; ld must be even and >= nf)",
                 (long long)nf, (long long)nq, (long long)ld);
@@ -439,11 +443,13 @@ int wn_forward_fp64_device(const double* tri, int64_t ld, const double* q, doubl
 
 int wn_forward_mixed_host(const double* tri, const double* q, double* w, int64_t nf, int64_t nq,
                           double kappa) {
+  WN_NVTX_RANGE();
   return forward_mixed_host(tri, q, w, nf, nq, kappa);
 }
 
 int wn_mixed_mesh_create(const double* tri, int64_t ld, int64_t nf, double kappa, void* stream,
                          void** mesh_out) {
+  WN_NVTX_RANGE();
   if (!mesh_out) return fail(WN_EINVAL, "null mesh_out");
   *mesh_out = nullptr;
   if (nf < 0 || nf > 0x7fffffffLL || (ld & 1) || ld < nf)
@@ -508,6 +514,7 @@ int wn_mixed_mesh_destroy(void* mesh) {
 }
 
 int wn_forward_mixed_device(void* mesh, const double* q, int64_t nq, double* w, void* stream) {
+  WN_NVTX_RANGE();
   if (!mesh) return fail(WN_EINVAL, "null mesh");
   if (nq < 0 || nq > 0x7fffffffLL) return fail(WN_EINVAL, "bad nq=%lld", (long long)nq);
   if (nq == 0) return WN_OK;
@@ -529,6 +536,7 @@ int wn_forward_mixed_device(void* mesh, const double* q, int64_t nq, double* w, 
 
 int wn_forward_fp64_mesh_device(void* mesh, const double* q, int64_t nq, double* w,
                                 void* stream) {
+  WN_NVTX_RANGE();
   if (!mesh) return fail(WN_EINVAL, "null mesh");
   if (nq < 0 || nq > 0x7fffffffLL) return fail(WN_EINVAL, "bad nq=%lld", (long long)nq);
   if (nq == 0) return WN_OK;
@@ -552,6 +560,7 @@ int wn_forward_fp64_mesh_device(void* mesh, const double* q, int64_t nq, double*
 }
 
 int wn_mixed_sort_queries(const double* q, int64_t nq, uint32_t* perm, void* stream) {
+  WN_NVTX_RANGE();
   if (nq < 0 || nq > 0x7fffffffLL) return fail(WN_EINVAL, "bad nq=%lld", (long long)nq);
   if (nq == 0) return WN_OK;
   std::lock_guard<std::mutex> lock(g_mutex);
@@ -569,6 +578,7 @@ int wn_mixed_sort_queries(const double* q, int64_t nq, uint32_t* perm, void* str
 
 int wn_forward_mixed_sorted_device(void* mesh, const double* q, const uint32_t* perm, int64_t nq,
                                    double* w, void* stream) {
+  WN_NVTX_RANGE();
   if (!mesh) return fail(WN_EINVAL, "null mesh");
   if (nq < 0 || nq > 0x7fffffffLL) return fail(WN_EINVAL, "bad nq=%lld", (long long)nq);
   if (nq == 0) return WN_OK;
@@ -592,6 +602,7 @@ int wn_forward_mixed_sorted_device(void* mesh, const double* q, const uint32_t* 
 }
 
 int wn_mixed_mesh_update(void* mesh, const double* tri, int64_t ld, void* stream) {
+  WN_NVTX_RANGE();
   if (!mesh) return fail(WN_EINVAL, "null mesh");
   MeshHandle* h = static_cast<MeshHandle*>(mesh);
   if ((ld & 1) || ld < h->m.nf)
@@ -628,6 +639,7 @@ int wn_mixed_stats(int64_t* refined_pairs, int64_t* careful_visits, int reset) {
 
 int wn_backward_fp64_device(const double* tri, int64_t ld, int64_t nf, const double* q,
                             int64_t nq, const double* gw, double* dq, double* dtri, void* stream) {
+  WN_NVTX_RANGE();
   if (nf < 0 || nq < 0 || (ld & 1) || ld < nf)
     return fail(WN_EINVAL, "bad sizes (nf=%lld, nq=%lld, ld=%lld; ld must be even and >= nf)",
                 (long long)nf, (long long)nq, (long long)ld);
@@ -648,6 +660,7 @@ int wn_backward_fp64_device(const double* tri, int64_t ld, int64_t nf, const dou
 
 int wn_backward_mixed_device(void* mesh, const double* q, int64_t nq, const double* gw,
                              double* dq, double* dtri, int64_t ld, void* stream) {
+  WN_NVTX_RANGE();
   if (!mesh) return fail(WN_EINVAL, "null mesh");
   const MeshHandle* h = static_cast<const MeshHandle*>(mesh);
   if (nq < 0 || nq > 0x7fffffffLL || (ld & 1) || ld < h->m.nf)
@@ -679,6 +692,7 @@ int wn_backward_mixed_device(void* mesh, const double* q, int64_t nq, const doub
 int wn_backward_edges_device(const double* edges, int64_t le, int64_t ne, const double* q,
                              int64_t nq, const double* gw, double* dq, double* dedge,
                              void* stream) {
+  WN_NVTX_RANGE();
   if (ne < 0 || nq < 0 || le < ne)
     return fail(WN_EINVAL, "bad sizes (ne=%lld, nq=%lld, le=%lld)", (long long)ne,
                 (long long)nq, (long long)le);
@@ -700,6 +714,7 @@ int wn_backward_edges_device(const double* edges, int64_t le, int64_t ne, const 
 int wn_gather_vertex_grad_device(const double* dtri, int64_t ld, int corners,
                                  const int64_t* indptr, const int64_t* entries, int64_t nv,
                                  double* dV, void* stream) {
+  WN_NVTX_RANGE();
   if (nv < 0 || (corners != 2 && corners != 3))
     return fail(WN_EINVAL, "bad nv=%lld or corners=%d", (long long)nv, corners);
   cudaError_t e = gather_vertex_grad(dtri, ld, corners, indptr, entries, nv, dV,
@@ -710,6 +725,7 @@ int wn_gather_vertex_grad_device(const double* dtri, int64_t ld, int corners,
 int wn_batch_create(int64_t nmesh, const int64_t* nv, const int64_t* nf, const int64_t* nq,
                     const int64_t* faces, double kappa, int qpt, int64_t target_pairs,
                     int ctas_per_sm, void** batch_out) {
+  WN_NVTX_RANGE();
   if (!batch_out) return fail(WN_EINVAL, "null batch_out");
   *batch_out = nullptr;
   if (nmesh <= 0 || nmesh > (1 << 20) || !nv || !nf || !nq)
@@ -755,6 +771,7 @@ int wn_batch_create(int64_t nmesh, const int64_t* nv, const int64_t* nf, const i
 }
 
 int wn_batch_forward(void* batch, const double* V, const double* q, double* w, void* stream) {
+  WN_NVTX_RANGE();
   if (!batch) return fail(WN_EINVAL, "null batch");
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
@@ -769,6 +786,7 @@ int wn_batch_forward(void* batch, const double* V, const double* q, double* w, v
 
 int wn_batch_backward(void* batch, const double* V, const double* q, const double* gw,
                       double* dq, double* dV, void* stream) {
+  WN_NVTX_RANGE();
   if (!batch) return fail(WN_EINVAL, "null batch");
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
@@ -863,6 +881,7 @@ int wn_aabb_build(const double* V, int64_t nv, const int64_t* F, int64_t nf, int
 int wn_aabb_create(const double* V, int64_t nv, const int64_t* F, int64_t nf,
                    const double* boxes, const int64_t* nodes, const int64_t* order,
                    int64_t nnodes, void** tree) {
+  WN_NVTX_RANGE();
   if (!tree) return fail(WN_EINVAL, "null output handle");
   *tree = nullptr;
   if (nv < 0 || nf < 0 || nnodes < 0) return fail(WN_EINVAL, "negative size");
@@ -919,6 +938,7 @@ int wn_aabb_destroy(void* tree) {
 
 int wn_aabb_squared_distance_device(void* tree, const double* P, int64_t np, double* sqrd,
                                     int64_t* index, double* closest, void* stream) {
+  WN_NVTX_RANGE();
   if (int code = check_points(tree, np)) return code;
   if (np == 0) return WN_OK;
   if (!P || !sqrd || !index || !closest) return fail(WN_EINVAL, "null pointer");
@@ -942,6 +962,7 @@ int wn_aabb_squared_distance_device(void* tree, const double* P, int64_t np, dou
 
 int wn_aabb_squared_distance_host(void* tree, const double* P, int64_t np, double* sqrd,
                                   int64_t* index, double* closest) {
+  WN_NVTX_RANGE();
   if (int code = check_points(tree, np)) return code;
   if (np == 0) return WN_OK;
   if (!P || !sqrd || !index || !closest) return fail(WN_EINVAL, "null pointer");
@@ -981,6 +1002,7 @@ int wn_aabb_squared_distance_host(void* tree, const double* P, int64_t np, doubl
 int wn_signed_distance_device(void* tree, void* mesh, int precision, const double* P,
                               int64_t np, double* s, int64_t* index, double* closest, double* w,
                               void* stream) {
+  WN_NVTX_RANGE();
   if (int code = check_points(tree, np)) return code;
   if (!mesh) return fail(WN_EINVAL, "null mesh");
   if (precision != 0 && precision != 1) return fail(WN_EINVAL, "bad precision %d", precision);
@@ -1114,6 +1136,7 @@ int wn_fast_eval_cpu(void* handle, const double* q, int64_t nq, double beta, dou
 
 int wn_fast_eval_device(void* handle, const double* q, int64_t nq, double beta, double* w,
                         void* stream) {
+  WN_NVTX_RANGE();
   if (!handle) return fail(WN_EINVAL, "null handle");
   if (int code = check_beta(beta)) return code;
   if (nq < 0 || nq > 0x7fffffffLL) return fail(WN_EINVAL, "bad nq=%lld", (long long)nq);
@@ -1137,6 +1160,7 @@ int wn_fast_eval_device(void* handle, const double* q, int64_t nq, double beta, 
 }
 
 int wn_fast_eval_host(void* handle, const double* q, int64_t nq, double beta, double* w) {
+  WN_NVTX_RANGE();
   if (!handle) return fail(WN_EINVAL, "null handle");
   if (int code = check_beta(beta)) return code;
   if (nq < 0 || nq > 0x7fffffffLL) return fail(WN_EINVAL, "bad nq=%lld", (long long)nq);
@@ -1253,6 +1277,7 @@ int normals_contrib(NormalsHandle* h, int mode) {
 }  // namespace
 
 int wn_normals_create(const int64_t* F, int64_t nf, int64_t nv, void* stream, void** out) {
+  WN_NVTX_RANGE();
   if (!out) return fail(WN_EINVAL, "null output handle");
   *out = nullptr;
   std::lock_guard<std::mutex> lock(g_mutex);
@@ -1285,6 +1310,7 @@ int wn_normals_destroy(void* handle) {
 
 int wn_vertex_normals_device(void* handle, const double* V, int weighting, double* N,
                              void* stream) {
+  WN_NVTX_RANGE();
   if (!handle) return fail(WN_EINVAL, "null handle");
   if (int code = check_weighting(weighting)) return code;
   NormalsHandle* h = static_cast<NormalsHandle*>(handle);
@@ -1302,6 +1328,7 @@ int wn_vertex_normals_device(void* handle, const double* V, int weighting, doubl
 
 int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_t nf,
                            int weighting, double* N) {
+  WN_NVTX_RANGE();
   if (int code = check_weighting(weighting)) return code;
   if (nv < 0 || nf < 0) return fail(WN_EINVAL, "negative size");
   if (nv == 0) return WN_OK;
@@ -1347,6 +1374,7 @@ int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_
 int wn_signed_distance_fast_device(void* tree, void* fast, double beta, const double* P,
                                    int64_t np, double* s, int64_t* index, double* closest,
                                    double* w, void* stream) {
+  WN_NVTX_RANGE();
   if (int code = check_points(tree, np)) return code;
   if (!fast) return fail(WN_EINVAL, "null fast winding-number handle");
   if (np == 0) return WN_OK;
@@ -1364,6 +1392,7 @@ int wn_signed_distance_fast_device(void* tree, void* fast, double beta, const do
 // repaid above ~1e9 pairs), small ones through the streaming FP64 kernel; both
 // give pair terms bit-identical to the reference.
 int64_t mli_winding_gpu(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t nq) {
+  WN_NVTX_RANGE();
   const bool large = nf >= 4096 && static_cast<double>(nf) * static_cast<double>(nq) >= 1e9 &&
                      nf <= 0x7fffffffLL;
   return forward_fp64_host(reinterpret_cast<const double*>(tri),

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <atomic>
 #include <cstdint>
@@ -10,6 +11,17 @@ namespace wn {
 
 // Stores `message` as the calling thread's wn_last_error().
 void record_error(const char* message);
+
+// An NVTX range named after a C-ABI entry point, so a profiler's timeline (and
+// `ncu --nvtx --nvtx-include`) shows which call launched what. Without a tool
+// attached it costs a branch.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+#define WN_NVTX_RANGE() const ::wn::NvtxRange wn_nvtx_range_(__func__)
 
 // Kernels launched by this library since load (wn_launch_count()).
 extern std::atomic<int64_t> g_launches;

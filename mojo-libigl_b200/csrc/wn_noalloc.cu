@@ -83,6 +83,7 @@ extern "C" {
 
 int wn_forward_fp64_device_noalloc(const double* tri, int64_t ld, const double* q, double* w,
                                    int64_t nf, int64_t nq, int mode, void* stream) {
+  WN_NVTX_RANGE();
   if (nf < 0 || nq < 0 || (ld & 1) || ld < nf)
     return noalloc_fail(WN_EINVAL, "bad sizes: need nf >= 0, nq >= 0, ld even and ld >= nf");
   if (nq > kNoAllocMaxQueries)

@@ -493,6 +493,55 @@ def gpu_arm(args):
               "ratio_fwdbwd_to_fwd": t_g / t_f}
         bt.close()
 
+    # The reference's own winding-number benchmark (bench/bench.py:96-112 there):
+    # grid(120) = 28,322 faces, 256 and then 1024 queries drawn from
+    # default_rng(0) in [0,119]^2 x [-2,2], each call timed as it does (wall
+    # clock, best of 3 after one warm-up) through the drop-in igl.winding_number.
+    refwn = None
+    if rank == 0:
+        import igl
+        from igl import synthetic
+
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        WV, WF = synthetic.terrain_grid(120)
+        rng_w = np.random.default_rng(0)
+        Q256 = rng_w.uniform([0, 0, -2], [119, 119, 2], size=(256, 3))
+        Q1024 = rng_w.uniform([0, 0, -2], [119, 119, 2], size=(1024, 3))
+
+        def best_of(fn, repeat=3):
+            fn()
+            best = float("inf")
+            for _ in range(repeat):
+                t0 = time.perf_counter()
+                fn()
+                best = min(best, time.perf_counter() - t0)
+            return best * 1e3
+
+        W_gpu = igl.winding_number(WV, WF, Q1024, device="gpu")
+        W_ref = oracle.winding_number(WV, WF, Q1024, workers=host_cores())
+        refwn = {
+            "workload": "grid(120) height field (14,400 V, 28,322 F); 256 and 1024 queries "
+                        "uniform in [0,119]^2 x [-2,2] from default_rng(0) (the reference's "
+                        "winding-number benchmark)",
+            "gpu_1024q_ms": best_of(lambda: igl.winding_number(WV, WF, Q1024, device="gpu")),
+            "published_gpu_1024q_ms": 53.47,
+            "cpu_256q_ms": best_of(lambda: igl.winding_number(WV, WF, Q256)),
+            "published_cpu_256q_ms": 60.66,
+            "cpu_1024q_ms": best_of(lambda: igl.winding_number(WV, WF, Q1024)),
+            "published_cpu_1024q_ms": 215.09,
+            "cpu_workers": igl.worker_count(len(Q1024), len(WF) * len(Q1024), "winding"),
+            "oracle_port_1024q_ms": best_of(
+                lambda: oracle.winding_number(WV, WF, Q1024, workers=min(4, host_cores()))),
+            "oracle_port_workers": min(4, host_cores()),
+            "max_abs_diff_gpu_vs_oracle": float(np.abs(W_gpu - W_ref).max()),
+            "note": "wall clock of the whole API call (validation, SoA repack, copies, launch); "
+                    "published figures from the reference's README.md:93-104 (Xeon E5-2697 v4 "
+                    "host, GPU model not stated); the CPU rows run this library's host path "
+                    "with the reference's worker policy on this machine's cores",
+        }
+
     # Closest points (the AABB query beside the winding number).
     closest = None
     if not args.no_closest:
@@ -830,6 +879,7 @@ def gpu_arm(args):
             "fwd_bwd": fwdbwd,
             "c4_fwd_bwd": c4,
             "c5_batched": c5,
+            "winding_reference_bench": refwn,
             "closest_point": closest,
             "fast_winding": fast,
             "vertex_normals": normals_out,

@@ -145,3 +145,17 @@ def test_worker_count_and_spans():
     assert 1 <= _lib.worker_count(1000, 10**6, "winding") <= _lib.MAX_WORKERS
     assert _lib.spans(10, 3) == [(0, 4), (4, 8), (8, 10)]
     assert _lib.spans(2, 4) == [(0, 1), (1, 2)]
+
+
+@pytest.mark.parametrize("nf", [0, 1, 7, 1280, 28322])
+def test_triangle_soa_matches_the_reference_layout(nf):
+    """The per-corner gather gives the bytes of the reference's repack
+    (python/igl/__init__.py:248-250 there: vertices[faces] transposed to
+    rows 3*corner+axis)."""
+    rng = np.random.default_rng(nf)
+    V = rng.normal(size=(max(3, nf // 2 + 3), 3))
+    F = rng.integers(0, len(V), size=(nf, 3))
+    expected = np.ascontiguousarray(V[F].transpose(1, 2, 0).reshape(9, nf))
+    got = igl._triangle_soa(*igl._mesh(V, F))
+    assert got.flags.c_contiguous and got.dtype == np.float64
+    assert got.shape == (9, nf) and np.array_equal(got, expected)

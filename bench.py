@@ -541,6 +541,23 @@ def gpu_arm(args):
                     "host, GPU model not stated); the CPU rows run this library's host path "
                     "with the reference's worker policy on this machine's cores",
         }
+        # The two plain-FP64 configurations through the drop-in, end to end (host
+        # arrays in, host W out): 1,280 F x 4,096 Q and 18,842 F x 2^20 Q.
+        for name in ("c1_cpu", "c2_open"):
+            Vd, Fd, Od, desc_d = synthetic.workload(name)
+            pairs_d = float(len(Fd)) * len(Od)
+            W_d = igl.winding_number(Vd, Fd, Od, device="gpu")
+            sub = np.random.default_rng(8).choice(len(Od), min(len(Od), 512), replace=False)
+            entry = {"workload": desc_d, "pairs": pairs_d,
+                     "gpu_ms": best_of(lambda: igl.winding_number(Vd, Fd, Od, device="gpu")),
+                     "max_abs_diff_vs_oracle_512q": float(np.abs(
+                         W_d[sub] - oracle.winding_number(Vd, Fd, Od[sub],
+                                                          workers=host_cores())).max())}
+            entry["gpu_pairs_per_s"] = pairs_d / (entry["gpu_ms"] * 1e-3)
+            if name == "c1_cpu":
+                entry["cpu_ms"] = best_of(lambda: igl.winding_number(Vd, Fd, Od))
+                entry["cpu_workers"] = igl.worker_count(len(Od), pairs_d, "winding")
+            refwn["drop_in_" + name] = entry
 
     # Closest points (the AABB query beside the winding number).
     closest = None

@@ -201,6 +201,68 @@ __device__ __forceinline__ Corner pick_corner(unsigned code, const Corner& c0, c
   return code == 0 ? c0 : (code == 1 ? c1 : c2);
 }
 
+// Corner `pos` of face j when its reuse code M is known at compile time: one of
+// the previous face's corners (M = 0..2) or a new one computed from the tile.
+template <unsigned M>
+__device__ __forceinline__ Corner corner_of(const Corner& p0, const Corner& p1, const Corner& p2,
+                                            double ox, double oy, double oz, const double* s,
+                                            int pos, int j) {
+  if constexpr (M == 3)
+    return corner_exact(ox, oy, oz, s[(3 * pos) * kTileFaces + j],
+                        s[(3 * pos + 1) * kTileFaces + j], s[(3 * pos + 2) * kTileFaces + j]);
+  else if constexpr (M == 0)
+    return p0;
+  else if constexpr (M == 1)
+    return p1;
+  else
+    return p2;
+}
+
+// The three corners of face j. The code is the same for every lane (all lanes
+// walk the same face), so a switch over it is a uniform branch, and each case
+// names its corners at compile time: no per-register selects. The cases are
+// the 28 codes whose reused corners are distinct with at most two of them (a
+// face that shares all three corners with the previous one is a duplicate and
+// takes the generic path).
+__device__ __forceinline__ void face_corners(unsigned code, const Corner& p0, const Corner& p1,
+                                             const Corner& p2, double ox, double oy, double oz,
+                                             const double* s, int j, Corner& c0, Corner& c1,
+                                             Corner& c2) {
+#define WN_FACE_CASE(A, B, C)                                 \
+  case (A) | ((B) << 2) | ((C) << 4):                         \
+    c0 = corner_of<A>(p0, p1, p2, ox, oy, oz, s, 0, j);       \
+    c1 = corner_of<B>(p0, p1, p2, ox, oy, oz, s, 1, j);       \
+    c2 = corner_of<C>(p0, p1, p2, ox, oy, oz, s, 2, j);       \
+    return;
+  switch (code) {
+    WN_FACE_CASE(3, 3, 3)
+    WN_FACE_CASE(0, 3, 3) WN_FACE_CASE(1, 3, 3) WN_FACE_CASE(2, 3, 3)
+    WN_FACE_CASE(3, 0, 3) WN_FACE_CASE(3, 1, 3) WN_FACE_CASE(3, 2, 3)
+    WN_FACE_CASE(3, 3, 0) WN_FACE_CASE(3, 3, 1) WN_FACE_CASE(3, 3, 2)
+    WN_FACE_CASE(3, 0, 1) WN_FACE_CASE(3, 0, 2) WN_FACE_CASE(3, 1, 0)
+    WN_FACE_CASE(3, 1, 2) WN_FACE_CASE(3, 2, 0) WN_FACE_CASE(3, 2, 1)
+    WN_FACE_CASE(0, 3, 1) WN_FACE_CASE(0, 3, 2) WN_FACE_CASE(1, 3, 0)
+    WN_FACE_CASE(1, 3, 2) WN_FACE_CASE(2, 3, 0) WN_FACE_CASE(2, 3, 1)
+    WN_FACE_CASE(0, 1, 3) WN_FACE_CASE(0, 2, 3) WN_FACE_CASE(1, 0, 3)
+    WN_FACE_CASE(1, 2, 3) WN_FACE_CASE(2, 0, 3) WN_FACE_CASE(2, 1, 3)
+    default:
+      break;
+  }
+#undef WN_FACE_CASE
+  Corner c[3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const unsigned cm = (code >> (2 * m)) & 3u;
+    c[m] = cm == 3u ? corner_exact(ox, oy, oz, s[(3 * m) * kTileFaces + j],
+                                   s[(3 * m + 1) * kTileFaces + j],
+                                   s[(3 * m + 2) * kTileFaces + j])
+                    : pick_corner(cm, p0, p1, p2);
+  }
+  c0 = c[0];
+  c1 = c[1];
+  c2 = c[2];
+}
+
 template <int THREADS, int QPT, int STAGES>
 __global__ void __launch_bounds__(THREADS) fp64_tiled_kernel(const Fp64TiledArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -266,22 +328,14 @@ __global__ void __launch_bounds__(THREADS) fp64_tiled_kernel(const Fp64TiledArgs
       if (code == 0xffu) break;  // padding: the rest of the tile is empty
 #pragma unroll
       for (int k = 0; k < QPT; ++k) {
-        Corner c[3];
-#pragma unroll
-        for (int m = 0; m < 3; ++m) {
-          const unsigned cm = (code >> (2 * m)) & 3u;
-          if (cm == 3u)
-            c[m] = corner_exact(ox[k], oy[k], oz[k], s[(3 * m) * kTileFaces + j],
-                                s[(3 * m + 1) * kTileFaces + j], s[(3 * m + 2) * kTileFaces + j]);
-          else
-            c[m] = pick_corner(cm, p0[k], p1[k], p2[k]);
-        }
+        Corner c0, c1, c2;
+        face_corners(code, p0[k], p1[k], p2[k], ox[k], oy[k], oz[k], s, j, c0, c1, c2);
         double det, denom;
-        face_exact(c[0], c[1], c[2], det, denom);
+        face_exact(c0, c1, c2, det, denom);
         argacc_push(acc[k], denom, det);
-        p0[k] = c[0];
-        p1[k] = c[1];
-        p2[k] = c[2];
+        p0[k] = c0;
+        p1[k] = c1;
+        p2[k] = c2;
       }
     }
   }

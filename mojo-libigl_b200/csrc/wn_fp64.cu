@@ -407,7 +407,7 @@ Fp64Plan plan_fp64(int64_t nf, int64_t nq, int sms, int force_nsplit) {
   return p;
 }
 
-constexpr int kTiledThreads = 128, kTiledQpt = 1, kTiledStages = 3;
+constexpr int kTiledThreads = 128, kTiledQpt = 1, kTiledStages = 4;
 
 Fp64TiledPlan plan_fp64_tiled(int64_t ntiles, int64_t nq, int sms) {
   Fp64TiledPlan p;

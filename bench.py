@@ -98,8 +98,9 @@ def parse_args():
                                       "closest_c3", "fwn_c3", "normals_s9", "adjoint_c3"),
                    help="run one kernel on a small case twice (for profiling) and exit")
     p.add_argument("--case-queries", type=int, default=None)
-    p.add_argument("--autotune", action="store_true",
-                   help="autotune the batched launch (cached per GPU and size bucket)")
+    p.add_argument("--no-autotune", dest="autotune", action="store_false",
+                   help="run the batched launch with the fixed default configuration instead "
+                        "of the autotuner's choice (cached per GPU and size bucket)")
     return p.parse_args()
 
 
@@ -477,20 +478,37 @@ def gpu_arm(args):
         work = synthetic.batched_workload(seed=51 + rank)
         meshes = [(Vm, Fm) for Vm, Fm, _ in work]
         queries = [Om for _, _, Om in work]
+        t_tune = time.perf_counter()
         tuned = autotune.tune(meshes, queries) if args.autotune else None
+        t_tune = time.perf_counter() - t_tune
         cfg = tuned["config"] if tuned else {"qpt": 2, "target_pairs": 1 << 21, "kappa": 4.0}
         bt = batched.Batch(meshes, queries, **cfg)
         bt.gW.normal_()
         t_f = timed(lambda: bt.forward(), args.steps, 2)[0]
+        # Accuracy of the chosen configuration: up to 128 queries of every mesh
+        # against the plain FP64 kernel.
+        W_b = bt.split(bt.forward().clone())
+        err_b = []
+        for (Vm, Fm), Om, wm in zip(meshes, queries, W_b):
+            sel = np.random.default_rng(len(Om)).choice(len(Om), min(len(Om), 128), replace=False)
+            tri_m, ld_m, nf_m = wa.triangle_soa(torch.from_numpy(Vm).to(dev),
+                                                torch.from_numpy(Fm).to(dev))
+            ref_m = wa.forward_fp64(tri_m, ld_m, nf_m, torch.from_numpy(Om[sel]).to(dev))
+            err_b.append(float((wm[torch.from_numpy(sel).to(dev)] - ref_m).abs().max()))
         bt.capture(backward=True)
         t_g, launches_g, _ = timed(bt.replay, args.steps, 2)
         c5 = {"workload": "64 bumpy icospheres, subdivision U{2..7}, 0-10% faces deleted, "
                           "queries log-uniform in [1024, 2^20], 50/50 box/near(1e-3)",
               "meshes": len(meshes), "pairs": bt.pairs, "config": cfg,
-              "autotuned": tuned is not None, "info": bt.info(),
+              "autotuned": tuned is not None,
+              "autotune": ({k: v for k, v in tuned.items() if k != "config"} | {"seconds": t_tune}
+                           if tuned else None),
+              "info": bt.info(),
               "fwd_ms": t_f * 1e3, "fwd_pairs_per_s": world * bt.pairs / t_f,
               "graph_fwdbwd_ms": t_g * 1e3, "graph_fwdbwd_pairs_per_s": world * bt.pairs / t_g,
-              "ratio_fwdbwd_to_fwd": t_g / t_f}
+              "ratio_fwdbwd_to_fwd": t_g / t_f,
+              "max_abs_err_vs_fp64": max(err_b),
+              "error_sample": "up to 128 queries of each mesh against the plain FP64 kernel"}
         bt.close()
 
     # The reference's own winding-number benchmark (bench/bench.py:96-112 there):

@@ -96,7 +96,7 @@ def tune(meshes, queries, space=None, backward: bool = True, sample_queries: int
     if use_cache:
         os.makedirs(os.path.dirname(path), exist_ok=True)
         cache[key] = result
-        tmp = path + ".tmp"
+        tmp = f"{path}.{os.getpid()}.tmp"  # one per process: ranks may tune at once
         with open(tmp, "w") as fh:
             json.dump(cache, fh, indent=1)
         os.replace(tmp, path)

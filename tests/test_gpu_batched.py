@@ -28,10 +28,12 @@ def _small_batch(n=7, seed=5, max_level=4, max_q=3000):
     return meshes, queries
 
 
-@pytest.mark.parametrize("qpt", [1, 2, 4])
-def test_batched_forward_matches_oracle(gpu_required, oracle_mod, qpt):
+@pytest.mark.parametrize("qpt,kappa", [(1, 4.0), (2, 4.0), (4, 4.0), (2, 3.0), (4, 3.0)])
+def test_batched_forward_matches_oracle(gpu_required, oracle_mod, qpt, kappa):
+    """Every configuration the autotuner may pick keeps the 1e-6 bound (kappa = 3
+    is the smallest refinement radius it is allowed)."""
     meshes, queries = _small_batch()
-    b = igl.batched.Batch(meshes, queries, qpt=qpt, target_pairs=1 << 16)
+    b = igl.batched.Batch(meshes, queries, qpt=qpt, target_pairs=1 << 16, kappa=kappa)
     try:
         W = b.split(b.forward().clone())
         assert b.info()["work_items"] > len(meshes)

@@ -133,7 +133,7 @@ struct DeviceCtx {
   unsigned long long* stats = nullptr;  // mixed-path counters (refined pairs, careful visits)
   Buffer tri, q, w, scratch;
   Buffer mesh_tiles, mesh_tri64, mesh_face_of, mesh_reuse;  // prepared mesh (host entry points)
-  Buffer nrm_f, nrm_indptr, nrm_entries, nrm_contrib;        // one-shot vertex normals
+  Buffer nrm_f, nrm_indptr, nrm_entries, nrm_order, nrm_contrib;  // one-shot vertex normals
 };
 
 std::mutex g_mutex;
@@ -1202,6 +1202,7 @@ void normals_release(NormalsHandle* h) {
   cudaFree(h->t.F);
   cudaFree(h->t.indptr);
   cudaFree(h->t.entries);
+  cudaFree(h->t.order);
   cudaFree(h->t.contrib);
   h->t = NormalsTopology{};
 }
@@ -1228,7 +1229,8 @@ int normals_alloc(NormalsHandle* h, int64_t nf, int64_t nv) {
   cudaError_t e;
   if ((e = dev_malloc(&h->t.F, sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess ||
       (e = dev_malloc(&h->t.indptr, sizeof(int32_t) * (nv + 1))) != cudaSuccess ||
-      (e = dev_malloc(&h->t.entries, sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess) {
+      (e = dev_malloc(&h->t.entries, sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess ||
+      (e = dev_malloc(&h->t.order, sizeof(int32_t) * (nv + 1))) != cudaSuccess) {
     normals_release(h);
     return cuda_fail(e, "device allocation");
   }
@@ -1241,7 +1243,7 @@ int normals_alloc(NormalsHandle* h, int64_t nf, int64_t nv) {
 int normals_prepare(const int64_t* F, int64_t nf, cudaStream_t st, NormalsHandle* h) {
   cudaError_t e = cudaSuccess;
   const size_t f64_bytes = ((sizeof(int64_t) * 3 * nf + 255) / 256) * 256;
-  const size_t sb = f64_bytes + 256 + normals_scratch_bytes(nf);
+  const size_t sb = f64_bytes + 256 + normals_scratch_bytes(nf, h->t.nv);
   unsigned char* scratch = nullptr;
   if ((e = dev_malloc_async(reinterpret_cast<void**>(&scratch), sb, st)) != cudaSuccess)
     return cuda_fail(e, "device allocation");
@@ -1250,7 +1252,8 @@ int normals_prepare(const int64_t* F, int64_t nf, cudaStream_t st, NormalsHandle
   if (nf > 0)
     e = cudaMemcpyAsync(F64, F, sizeof(int64_t) * 3 * nf, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
-    e = normals_build(h->t, F64, bad, scratch + f64_bytes + 256, normals_scratch_bytes(nf), st);
+    e = normals_build(h->t, F64, bad, scratch + f64_bytes + 256, normals_scratch_bytes(nf, h->t.nv),
+                      st);
   int bad_h = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&bad_h, bad, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaFreeAsync(scratch, st);
@@ -1346,6 +1349,7 @@ int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_
   if ((e = c->nrm_f.ensure(sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess ||
       (e = c->nrm_indptr.ensure(sizeof(int32_t) * (nv + 1))) != cudaSuccess ||
       (e = c->nrm_entries.ensure(sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess ||
+      (e = c->nrm_order.ensure(sizeof(int32_t) * (nv + 1))) != cudaSuccess ||
       (e = c->nrm_contrib.ensure(sizeof(double) * (ncontrib + 1))) != cudaSuccess ||
       (e = c->q.ensure(sizeof(double) * 3 * nv)) != cudaSuccess ||
       (e = c->w.ensure(sizeof(double) * 3 * nv)) != cudaSuccess)
@@ -1354,6 +1358,7 @@ int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_
   h.t.F = static_cast<int32_t*>(c->nrm_f.ptr);
   h.t.indptr = static_cast<int32_t*>(c->nrm_indptr.ptr);
   h.t.entries = static_cast<int32_t*>(c->nrm_entries.ptr);
+  h.t.order = static_cast<int32_t*>(c->nrm_order.ptr);
   h.t.contrib = static_cast<double*>(c->nrm_contrib.ptr);
   h.t.contrib_doubles = ncontrib;
   h.t.nf = nf;

@@ -1,8 +1,8 @@
 // Per-vertex normals on sm_100a in two coalesced passes (wn_normals.h):
 // face_contrib_kernel (one thread per face: the face normal and its corners'
-// contributions, written once) and vertex_gather_kernel (one thread per vertex:
-// its incidences' contributions added in face order, then the division by the
-// length). Nothing is scattered, so there are no atomics and no order
+// contributions, written once) and vertex_gather_kernel (one thread per vertex,
+// vertices taken by first incident face: its incidences' contributions added in
+// face order, then the division by the length). Nothing is scattered, so there are no atomics and no order
 // dependence: uniform and area normals are bit-identical to the reference's
 // serial loop (src/capi.mojo:146-202). Both passes stream their own arrays and
 // gather the other side's, so the work is bound by memory traffic.
@@ -88,12 +88,30 @@ __global__ void __launch_bounds__(kNormalThreads)
   }
 }
 
+// Sort keys of the visit order: a vertex's first incident face (nf for a
+// vertex on no face, so those come last).
+__global__ void vertex_keys_kernel(const int32_t* __restrict__ indptr,
+                                   const int32_t* __restrict__ entries, int64_t nv, int64_t nf,
+                                   uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const int32_t e0 = indptr[v];
+  keys[v] = e0 < indptr[v + 1] ? static_cast<uint32_t>(entries[e0] / 3)
+                               : static_cast<uint32_t>(nf);
+  vals[v] = static_cast<uint32_t>(v);
+}
+
+// Thread t finishes vertex order[t]. Visiting the vertices by first incident
+// face keeps the three readers of a face's contribution close together in time,
+// so the repeat reads hit L2 (in vertex-index order they can be a whole mesh
+// level apart). Each vertex's sum is unchanged: its incidences in face order.
 __global__ void __launch_bounds__(kNormalThreads)
     vertex_gather_kernel(const int32_t* __restrict__ indptr, const int32_t* __restrict__ entries,
-                         const double* __restrict__ contrib, int64_t nv, int mode,
-                         double* __restrict__ N) {
-  const int64_t v = static_cast<int64_t>(blockIdx.x) * kNormalThreads + threadIdx.x;
-  if (v >= nv) return;
+                         const int32_t* __restrict__ order, const double* __restrict__ contrib,
+                         int64_t nv, int mode, double* __restrict__ N) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * kNormalThreads + threadIdx.x;
+  if (t >= nv) return;
+  const int64_t v = __ldg(order + t);
   double acc[3] = {0.0, 0.0, 0.0};
   const int32_t e1 = indptr[v + 1];
   for (int32_t e = indptr[v]; e < e1; ++e) {
@@ -121,8 +139,8 @@ size_t round256(size_t n) { return ((n + 255) / 256) * 256; }
 
 }  // namespace
 
-size_t normals_scratch_bytes(int64_t nf) {
-  const int64_t n = 3 * nf;
+size_t normals_scratch_bytes(int64_t nf, int64_t nv) {
+  const int64_t n = 3 * nf > nv ? 3 * nf : nv;  // the incidence sort, then the vertex sort
   size_t temp = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, temp, static_cast<const uint32_t*>(nullptr),
                                   static_cast<uint32_t*>(nullptr),
@@ -136,25 +154,39 @@ cudaError_t normals_build(NormalsTopology& t, const int64_t* F64, int* bad, void
   const int64_t n = 3 * t.nf;
   cudaError_t e = cudaMemsetAsync(bad, 0, sizeof(int), stream);
   if (e != cudaSuccess) return e;
-  if (n == 0) return cudaMemsetAsync(t.indptr, 0, sizeof(int32_t) * (t.nv + 1), stream);
-  if (scratch_bytes < normals_scratch_bytes(t.nf)) return cudaErrorInvalidValue;
-  const size_t arr = round256(static_cast<size_t>(n) * 4);
+  if (scratch_bytes < normals_scratch_bytes(t.nf, t.nv)) return cudaErrorInvalidValue;
+  const size_t arr = round256(static_cast<size_t>(n > t.nv ? n : t.nv) * 4);
   unsigned char* s = static_cast<unsigned char*>(scratch);
   uint32_t* keys_in = reinterpret_cast<uint32_t*>(s);
   uint32_t* keys_out = reinterpret_cast<uint32_t*>(s + arr);
   uint32_t* vals_in = reinterpret_cast<uint32_t*>(s + 2 * arr);
   void* temp = s + 3 * arr;
   size_t temp_bytes = scratch_bytes - 3 * arr;
-  const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
-  faces_prepare_kernel<<<blocks, 256, 0, stream>>>(F64, n, t.nv, t.F, keys_in, vals_in, bad);
+  if (n == 0) {
+    e = cudaMemsetAsync(t.indptr, 0, sizeof(int32_t) * (t.nv + 1), stream);
+  } else {
+    const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
+    faces_prepare_kernel<<<blocks, 256, 0, stream>>>(F64, n, t.nv, t.F, keys_in, vals_in, bad);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    // Stable: equal vertex ids keep incidence order (face, then corner).
+    e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, vals_in,
+                                        reinterpret_cast<uint32_t*>(t.entries),
+                                        static_cast<int>(n), 0, key_bits(t.nv), stream);
+    if (e != cudaSuccess) return e;
+    csr_bounds_kernel<<<blocks, 256, 0, stream>>>(keys_out, n, t.nv, t.indptr);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+  }
+  if (e != cudaSuccess || t.nv == 0) return e;
+  // Visit order of the gather: vertices by first incident face (stable, so
+  // ties keep index order).
+  const unsigned vblocks = static_cast<unsigned>((t.nv + 255) / 256);
+  vertex_keys_kernel<<<vblocks, 256, 0, stream>>>(t.indptr, t.entries, t.nv, t.nf, keys_in,
+                                                  vals_in);
   g_launches.fetch_add(1, std::memory_order_relaxed);
-  // Stable: equal vertex ids keep incidence order (face, then corner).
   e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, vals_in,
-                                      reinterpret_cast<uint32_t*>(t.entries), static_cast<int>(n),
-                                      0, key_bits(t.nv), stream);
+                                      reinterpret_cast<uint32_t*>(t.order),
+                                      static_cast<int>(t.nv), 0, key_bits(t.nf), stream);
   if (e != cudaSuccess) return e;
-  csr_bounds_kernel<<<blocks, 256, 0, stream>>>(keys_out, n, t.nv, t.indptr);
-  g_launches.fetch_add(1, std::memory_order_relaxed);
   return cudaGetLastError();
 }
 
@@ -170,7 +202,7 @@ cudaError_t normals_eval(const NormalsTopology& t, const double* V, int mode, do
   }
   const int64_t vb = (t.nv + kNormalThreads - 1) / kNormalThreads;
   vertex_gather_kernel<<<static_cast<unsigned>(vb), kNormalThreads, 0, stream>>>(
-      t.indptr, t.entries, t.contrib, t.nv, mode, N);
+      t.indptr, t.entries, t.order, t.contrib, t.nv, mode, N);
   g_launches.fetch_add(1, std::memory_order_relaxed);
   return cudaGetLastError();
 }

@@ -6,7 +6,9 @@
 // one thread per face writes its contribution u * weight (per face for the
 // uniform and area weights, whose three corners share it; per corner for the
 // angle weight; a NaN marks a face the reference skips), then one thread per
-// vertex adds its incidences' contributions in CSR order and normalises. The
+// vertex adds its incidences' contributions in CSR order and normalises (the
+// vertices are visited by first incident face, an order set up with the lists,
+// so that a face's three readers come close together in time). The
 // additions are the reference's, operand for operand and in its order
 // (wn_normals.cuh), so positions can change between calls at no set-up cost.
 #pragma once
@@ -21,17 +23,18 @@ struct NormalsTopology {
   int32_t* F = nullptr;        // 3 nf
   int32_t* indptr = nullptr;   // nv + 1
   int32_t* entries = nullptr;  // 3 nf
+  int32_t* order = nullptr;    // nv: vertices by first incident face (the gather's visit order)
   double* contrib = nullptr;   // 9 nf (angle) or 3 nf doubles, grown on demand
   int64_t contrib_doubles = 0;
   int64_t nf = 0, nv = 0;
 };
 
-// Device bytes of scratch for preparing nf faces.
-size_t normals_scratch_bytes(int64_t nf);
+// Device bytes of scratch for preparing nf faces over nv vertices.
+size_t normals_scratch_bytes(int64_t nf, int64_t nv);
 
-// Prepares t.F and the incidence lists from F64 (device, 3 nf int64). Indices
-// outside [0, nv) are counted in *bad (device int, zeroed here) and kept out of
-// the lists; the caller checks *bad after the stream drains.
+// Prepares t.F, the incidence lists and the vertex visit order from F64 (device,
+// 3 nf int64). Indices outside [0, nv) are counted in *bad (device int, zeroed
+// here) and kept out of the lists; the caller checks *bad after the stream drains.
 cudaError_t normals_build(NormalsTopology& t, const int64_t* F64, int* bad, void* scratch,
                           size_t scratch_bytes, cudaStream_t stream);
 

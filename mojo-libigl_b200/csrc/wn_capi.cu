@@ -134,6 +134,10 @@ struct DeviceCtx {
   Buffer tri, q, w, scratch;
   Buffer mesh_tiles, mesh_tri64, mesh_face_of, mesh_reuse;  // prepared mesh (host entry points)
   Buffer nrm_f, nrm_indptr, nrm_entries, nrm_order, nrm_contrib;  // one-shot vertex normals
+  // Second stream and fork/join events for entry points that run two
+  // independent kernels side by side (created on first use).
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 std::mutex g_mutex;
@@ -1376,19 +1380,65 @@ int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_
   return collect_device_error(c, c->stream);
 }
 
+// The closest-point walk and the fast winding-number walk read only the points
+// and are both latency bound at low occupancy, so they run side by side: the
+// points are Morton-sorted once on the caller's stream, the closest-point
+// kernel follows there and the winding-number kernel runs on the context's
+// second stream (fork/join by events), then the sign is taken on the caller's
+// stream. Same results as running the two entry points one after the other.
 int wn_signed_distance_fast_device(void* tree, void* fast, double beta, const double* P,
                                    int64_t np, double* s, int64_t* index, double* closest,
                                    double* w, void* stream) {
   WN_NVTX_RANGE();
   if (int code = check_points(tree, np)) return code;
   if (!fast) return fail(WN_EINVAL, "null fast winding-number handle");
+  if (int code = check_beta(beta)) return code;
   if (np == 0) return WN_OK;
-  if (!w) return fail(WN_EINVAL, "null pointer");
-  if (int code = wn_aabb_squared_distance_device(tree, P, np, s, index, closest, stream))
-    return code;
-  if (int code = wn_fast_eval_device(fast, P, np, beta, w, stream)) return code;
+  if (!P || !s || !index || !closest || !w) return fail(WN_EINVAL, "null pointer");
   std::lock_guard<std::mutex> lock(g_mutex);
-  const cudaError_t e = signed_from_winding(w, s, np, static_cast<cudaStream_t>(stream));
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  const AabbHandle* ah = static_cast<const AabbHandle*>(tree);
+  if ((code = check_device(ah->device, "tree")) != WN_OK) return code;
+  FwnHandle* fh = static_cast<FwnHandle*>(fast);
+  if ((code = fwn_upload(fh)) != WN_OK) return code;
+  cudaError_t e = cudaSuccess;
+  if ((!c->side && (e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)) !=
+                       cudaSuccess) ||
+      (!c->fork && (e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming)) !=
+                       cudaSuccess) ||
+      (!c->join && (e = cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming)) !=
+                       cudaSuccess))
+    return cuda_fail(e, "second stream set-up");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t sb = aabb_sort_bytes(np);
+  void* scratch = nullptr;
+  if (sb && (e = dev_malloc_async(&scratch, sb, st)) != cudaSuccess)
+    return cuda_fail(e, "device allocation");
+  uint32_t* perm = nullptr;
+  if (np >= kAabbSortMin) {
+    perm = static_cast<uint32_t*>(scratch);
+    unsigned char* rest = static_cast<unsigned char*>(scratch) + align256(sizeof(uint32_t) * np);
+    e = mixed_sort_queries(P, np, perm, rest, mixed_sort_scratch_bytes(np), st);
+  }
+  bool forked = false;
+  if (e == cudaSuccess && (e = cudaEventRecord(c->fork, st)) == cudaSuccess &&
+      (e = cudaStreamWaitEvent(c->side, c->fork, 0)) == cudaSuccess) {
+    forked = true;
+    e = aabb_query(ah->t, P, np, perm, s, index, closest, c->err, st);
+    const cudaError_t e2 = fwn_eval_device(fh->dev, P, np, perm, beta, w, c->err, c->side);
+    if (e == cudaSuccess) e = e2;
+  }
+  // Join whatever was forked before anything else touches the scratch.
+  if (forked) {
+    const cudaError_t ej = cudaEventRecord(c->join, c->side) == cudaSuccess
+                               ? cudaStreamWaitEvent(st, c->join, 0)
+                               : cudaStreamSynchronize(c->side);
+    if (e == cudaSuccess) e = ej;
+  }
+  if (e == cudaSuccess) e = signed_from_winding(w, s, np, st);
+  if (scratch) cudaFreeAsync(scratch, st);
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "signed-distance launch");
 }
 

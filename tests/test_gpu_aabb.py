@@ -128,6 +128,30 @@ def test_signed_distance_device_matches_cpu(gpu_required):
     tree.close()
 
 
+@pytest.mark.parametrize("n", [1000, 20_000])  # below / above the Morton-sort threshold
+def test_fast_signed_distance_equals_its_two_parts(gpu_required, n):
+    """The fused entry (closest points and fast winding numbers on two streams
+    from one sorted order) gives exactly what the two separate calls give."""
+    import torch
+
+    from igl import distance
+
+    V, F = igl.synthetic.bumpy_icosphere(4, seed=9)
+    P = igl.synthetic.mixed_queries(V, F, n, seed=11, near_sigma=1e-3)
+    tree = distance.DeviceAABB(V, F)
+    Pt = torch.from_numpy(P).cuda()
+    sqrd, index, closest = (x.clone() for x in tree.query(Pt))
+    w_fast = tree.fast_winding().evaluate_torch(Pt, beta=2.0)
+    for _ in range(2):
+        S, I, C, W = tree.signed_distance(Pt, precision="fast", beta=2.0)
+        torch.cuda.synchronize()
+        assert torch.equal(I, index) and torch.equal(C, closest)
+        assert torch.equal(W, w_fast)
+        expected = torch.where(w_fast.abs() > 0.5, -sqrd.sqrt(), sqrd.sqrt())
+        assert torch.equal(S, expected)
+    tree.close()
+
+
 def test_empty_and_zero_points(gpu_required):
     import torch
 

@@ -656,7 +656,8 @@ def gpu_arm(args):
                 t_s = timed(signed_step, max(args.steps, 5), 3)[0]
                 entry["signed_distance_fast"] = {
                     "ms_per_step": t_s * 1e3, "points_per_s": world * npc / t_s,
-                    "note": "closest point + fast winding number (beta = 2) + sign, one stream"}
+                    "note": "closest point and fast winding number (beta = 2) side by side on two "
+                            "streams from one Morton order, then the sign"}
             closest[key] = entry
             tree.close()
         closest["note"] = ("reference's published AABB.squared_distance for the "

@@ -159,3 +159,23 @@ def test_triangle_soa_matches_the_reference_layout(nf):
     got = igl._triangle_soa(*igl._mesh(V, F))
     assert got.flags.c_contiguous and got.dtype == np.float64
     assert got.shape == (9, nf) and np.array_equal(got, expected)
+
+
+def test_vector_lanes_equal_the_scalar_path():
+    """mli_winding evaluates queries 8 (AVX-512) or 4 (AVX2) at a time; a span of
+    one query takes the scalar routine. Every query's result must be the same
+    bits either way, on-vertex and on-edge queries included."""
+    handle = _lib.lib()
+    V, F = igl.synthetic.bumpy_icosphere(2, seed=4)
+    rng = np.random.default_rng(6)
+    O = np.concatenate([V[:9], 0.5 * (V[F[:8, 0]] + V[F[:8, 1]]),
+                        rng.uniform(-1.5, 1.5, size=(20, 3))])  # 37: 8 + 8 + 8 + 8 + 4 + 1
+    tri = igl._triangle_soa(*igl._mesh(V, F))
+    whole = np.empty(len(O))
+    handle.mli_winding(tri.ctypes.data, O.ctypes.data, whole.ctypes.data, tri.shape[1], len(O),
+                       0, len(O))
+    single = np.empty(len(O))
+    for i in range(len(O)):
+        handle.mli_winding(tri.ctypes.data, O.ctypes.data, single.ctypes.data, tri.shape[1],
+                           len(O), i, i + 1)
+    assert np.array_equal(whole, single, equal_nan=True)

@@ -276,7 +276,10 @@ int wn_aabb_squared_distance_host(void* tree, const double* P, int64_t np, doubl
 /* The same with the fast winding number (wn_fast_create over the same faces,
  * evaluated at `beta`) for the sign: the sign can differ from the exact one only
  * where |W| lies within the approximation's error of 1/2 (points essentially
- * on the surface of a closed mesh, or near the boundary of an open one). */
+ * on the surface of a closed mesh, or near the boundary of an open one). The
+ * closest-point and winding-number walks run side by side, the second on a
+ * stream of the library's own that is forked from `stream` and joined back to
+ * it by events, so all results are ordered on `stream` as usual. */
 int wn_signed_distance_fast_device(void* tree, void* fast, double beta, const double* P,
                                    int64_t np, double* s, int64_t* index, double* closest,
                                    double* w, void* stream);

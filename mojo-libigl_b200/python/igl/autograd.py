@@ -63,6 +63,27 @@ def forward_fp64(tri: torch.Tensor, ld: int, nf: int, O: torch.Tensor) -> torch.
     return w
 
 
+def use_prepared_fp64(nf: int, nq: int) -> bool:
+    """The drop-in's rule (mli_winding_gpu): above 1e9 pairs the prepared-mesh
+    FP64 kernel, whose ~2 ms preparation its corner reuse repays."""
+    return 4096 <= nf <= 0x7FFFFFFF and float(nf) * nq >= 1e9
+
+
+def forward_fp64_prepared(tri: torch.Tensor, ld: int, nf: int, O: torch.Tensor) -> torch.Tensor:
+    """Plain FP64 W over a prepared mesh (Morton tiles, repeated corners reused):
+    the same bit-exact pair terms as forward_fp64, summed in tile order."""
+    q = O.to(torch.float64).contiguous()
+    w = torch.empty(q.shape[0], dtype=torch.float64, device=q.device)
+    if q.shape[0]:
+        mesh = PreparedMesh(tri, ld, nf)
+        try:
+            _check(mesh.handle.wn_forward_fp64_mesh_device(mesh.mesh, q.data_ptr(), q.shape[0],
+                                                           w.data_ptr(), _stream()))
+        finally:
+            mesh.close()
+    return w
+
+
 class PreparedMesh:
     """A mesh prepared for the mixed-precision kernels (Morton-ordered tiles)."""
 
@@ -197,6 +218,8 @@ class WindingNumberFunction(torch.autograd.Function):
                 ctx.mesh = mesh
             else:
                 mesh.close()
+        elif use_prepared_fp64(nf, O.shape[0]):
+            w = forward_fp64_prepared(tri, ld, nf, O)
         else:
             w = forward_fp64(tri, ld, nf, O)
         ctx.save_for_backward(V, F, O)

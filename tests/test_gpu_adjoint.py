@@ -205,3 +205,14 @@ def test_edge_and_face_adjoints_agree_on_nonmanifold_soup(gpu_required):
     for a, b in zip(res["faces"], res["edges"]):
         assert np.abs(a - b).max() <= 1e-9 * np.abs(a).max()
     del torch
+
+
+def test_large_fp64_forward_takes_the_prepared_mesh(gpu_required):
+    """Above 1e9 pairs the torch FP64 forward runs the prepared-mesh kernel, as
+    the drop-in does; it agrees with the streaming kernel within 1e-12."""
+    V, F, O, _ = igl.synthetic.workload("c2_open", n_queries=65536)  # 18,842 F: 1.2e9 pairs
+    Vt, Ft, Ot = _cuda(V), _cuda(F), _cuda(O)
+    assert wa.use_prepared_fp64(len(F), len(O))
+    W = wa.winding_number_torch(Vt, Ft, Ot, precision="fp64")
+    tri, ld, nf = wa.triangle_soa(Vt, Ft)
+    assert (W - wa.forward_fp64(tri, ld, nf, Ot)).abs().max().item() <= 1e-12

@@ -83,8 +83,11 @@ def gpu_forward(V, F, O, precision: str = "mixed"):
     from . import autograd as wa
 
     tri, ld, nf = wa.triangle_soa(V, F)
-    return wa.forward_mixed(tri, ld, nf, O) if precision == "mixed" else wa.forward_fp64(
-        tri, ld, nf, O)
+    if precision == "mixed":
+        return wa.forward_mixed(tri, ld, nf, O)
+    if wa.use_prepared_fp64(nf, O.shape[0]):
+        return wa.forward_fp64_prepared(tri, ld, nf, O)
+    return wa.forward_fp64(tri, ld, nf, O)
 
 
 def gpu_backward(V, F, O, gW):

@@ -195,27 +195,55 @@ void fwn_free(FwnHostTree* t) {
   *t = FwnHostTree{};
 }
 
+namespace {
+
+// One depth-first walk of query q (left child first): the far terms summed in
+// walk order into *far, and the leaf faces either multiplied into *acc (the
+// argument-of-product sum of wn_pair.cuh) or, when acc is null, their half
+// solid angles summed into *angle.
+void fwn_walk(const FwnHostTree& t, double qx, double qy, double qz, double beta, double* far,
+              ArgAcc* acc, double* angle) {
+  int32_t stack[kAabbStack];
+  int sp = 0;
+  if (t.nnodes > 0) stack[sp++] = 0;
+  while (sp > 0) {
+    const FwnNode& n = t.nodes[stack[--sp]];
+    const double y0 = n.p[0] - qx, y1 = n.p[1] - qy, y2 = n.p[2] - qz;
+    if (fwn_is_far(y0 * y0 + y1 * y1 + y2 * y2, beta, n.r)) {
+      if (far) *far += fwn_far_eval(t.moments[&n - t.nodes], y0, y1, y2);
+    } else if (n.count > 0) {
+      for (int32_t k = n.start; k < n.start + n.count; ++k) {
+        const AabbTriRec& r = t.tris[k];
+        if (acc) {
+          double det, denom;
+          pair_terms_exact(qx, qy, qz, r.a[0], r.a[1], r.a[2], r.b[0], r.b[1], r.b[2], r.c[0],
+                           r.c[1], r.c[2], det, denom);
+          argacc_push(*acc, denom, det);
+        } else {
+          *angle += fwn_face_angle(qx, qy, qz, r);
+        }
+      }
+    } else {
+      stack[sp++] = n.right;  // left child first
+      stack[sp++] = n.left;
+    }
+  }
+}
+
+}  // namespace
+
 void fwn_eval_host(const FwnHostTree& t, const double* q, int64_t q0, int64_t q1, double beta,
                    double* w) {
   for (int64_t qi = q0; qi < q1; ++qi) {
     const double qx = q[3 * qi], qy = q[3 * qi + 1], qz = q[3 * qi + 2];
     double far = 0.0, angle = 0.0;
-    int32_t stack[kAabbStack];
-    int sp = 0;
-    if (t.nnodes > 0) stack[sp++] = 0;
-    while (sp > 0) {
-      const FwnNode& n = t.nodes[stack[--sp]];
-      const double y0 = n.p[0] - qx, y1 = n.p[1] - qy, y2 = n.p[2] - qz;
-      if (fwn_is_far(y0 * y0 + y1 * y1 + y2 * y2, beta, n.r)) {
-        far += fwn_far_eval(t.moments[&n - t.nodes], y0, y1, y2);
-      } else if (n.count > 0) {
-        for (int32_t k = n.start; k < n.start + n.count; ++k)
-          angle += fwn_face_angle(qx, qy, qz, t.tris[k]);
-      } else {
-        stack[sp++] = n.right;  // left child first
-        stack[sp++] = n.left;
-      }
-    }
+    ArgAcc acc;
+    argacc_init(acc);
+    fwn_walk(t, qx, qy, qz, beta, &far, &acc, nullptr);
+    if (!acc.bad)
+      angle = std::atan2(acc.zi, acc.zr) + static_cast<double>(acc.k) * kTwoPi;
+    else  // the product degenerated: the per-face sum of the same faces
+      fwn_walk(t, qx, qy, qz, beta, nullptr, nullptr, &angle);
     w[qi] = far / (4.0 * kPi) + angle / (2.0 * kPi);
   }
 }

@@ -18,8 +18,10 @@
 // u_k = sum_i T2[i][k][i], v_i = sum_j T2[j][j][i] (the first three terms of
 // the expansion of (x - q) / |x - q|^3 about x = p, integrated over the faces).
 // Nearer nodes are opened; leaves add their faces' exact solid angles (the
-// bit-exact pair terms of the exact path and one atan2 per face). Each query
-// walks the tree depth first, left child first, so its sum has a fixed order.
+// bit-exact pair terms of the exact path, their angles summed through a running
+// complex product as there, the per-face atan2 sum when it degenerates). Each
+// query walks the tree depth first, left child first, so its sum has a fixed
+// order.
 #pragma once
 
 #include <cuda_runtime.h>

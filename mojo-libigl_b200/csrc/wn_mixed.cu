@@ -459,14 +459,33 @@ __device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t fir
     }
   } else {
     ++careful_tiles;
+    // Near pairs are only marked here (bit j of near[k]; a tile has at most 64
+    // faces) and refined below with the warp's lanes in step, each taking its
+    // own next near face, instead of the whole warp waiting on every face that
+    // any lane finds near. Each query still adds its refined angles in
+    // ascending face order, so the sums are unchanged.
+    static_assert(kTileFaces <= 64, "one bit per face of a tile");
+    unsigned long long near[QPT];
+#pragma unroll
+    for (int k = 0; k < QPT; ++k) near[k] = 0ull;
 #pragma unroll 1
     for (int j = 0; j < n; ++j) {
       const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2], r3 = fr[4 * j + 3];
 #pragma unroll
       for (int k = 0; k < QPT; ++k) {
         const PairSq p = pair_sq(r0, r1, r2, r3, lx[k], ly[k], lz[k]);
-        const bool near = fminf(p.aa, fminf(p.bb, p.cc)) < r3.w && qidx[k] >= 0;
-        if (near) {
+        if (fminf(p.aa, fminf(p.bb, p.cc)) < r3.w && qidx[k] >= 0)
+          near[k] |= 1ull << j;
+        else if (!skip[k])
+          pair_mul(p, zr[k], zi[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < QPT; ++k) {
+      while (__any_sync(0xffffffffu, near[k] != 0ull)) {
+        if (near[k] != 0ull) {
+          const int j = __ffsll(static_cast<long long>(near[k])) - 1;
+          near[k] &= near[k] - 1ull;
           const double* f64 = tri64 + first + j;
           const int64_t L = ld64;
           double det, denom;
@@ -475,8 +494,6 @@ __device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t fir
                            denom);
           s64[k] += atan2(det, denom);
           ++refined;
-        } else if (!skip[k]) {
-          pair_mul(p, zr[k], zi[k]);
         }
       }
     }

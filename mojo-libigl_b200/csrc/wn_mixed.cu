@@ -461,9 +461,8 @@ __device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t fir
     ++careful_tiles;
     // Near pairs are only marked here (bit j of near[k]; a tile has at most 64
     // faces) and refined below with the warp's lanes in step, each taking its
-    // own next near face, instead of the whole warp waiting on every face that
-    // any lane finds near. Each query still adds its refined angles in
-    // ascending face order, so the sums are unchanged.
+    // own next near face in ascending order, instead of the whole warp waiting
+    // on every face that any lane finds near.
     static_assert(kTileFaces <= 64, "one bit per face of a tile");
     unsigned long long near[QPT];
 #pragma unroll
@@ -480,8 +479,14 @@ __device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t fir
           pair_mul(p, zr[k], zi[k]);
       }
     }
+    // A query's refined pairs in this tile are multiplied into one FP64 running
+    // product (the argument-of-product sum of the FP64 kernels) whose argument
+    // is taken once; if it degenerates, the per-pair atan2 sum of the same faces.
 #pragma unroll
     for (int k = 0; k < QPT; ++k) {
+      const unsigned long long marked = near[k];
+      ArgAcc acc;
+      argacc_init(acc);
       while (__any_sync(0xffffffffu, near[k] != 0ull)) {
         if (near[k] != 0ull) {
           const int j = __ffsll(static_cast<long long>(near[k])) - 1;
@@ -492,8 +497,22 @@ __device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t fir
           pair_terms_exact(ox[k], oy[k], oz[k], f64[0], f64[L], f64[2 * L], f64[3 * L],
                            f64[4 * L], f64[5 * L], f64[6 * L], f64[7 * L], f64[8 * L], det,
                            denom);
-          s64[k] += atan2(det, denom);
+          argacc_push(acc, denom, det);
           ++refined;
+        }
+      }
+      if (marked == 0ull) continue;
+      if (!acc.bad) {
+        s64[k] += atan2(acc.zi, acc.zr) + static_cast<double>(acc.k) * kTwoPi;
+      } else {
+        for (unsigned long long m = marked; m != 0ull; m &= m - 1ull) {
+          const double* f64 = tri64 + first + (__ffsll(static_cast<long long>(m)) - 1);
+          const int64_t L = ld64;
+          double det, denom;
+          pair_terms_exact(ox[k], oy[k], oz[k], f64[0], f64[L], f64[2 * L], f64[3 * L],
+                           f64[4 * L], f64[5 * L], f64[6 * L], f64[7 * L], f64[8 * L], det,
+                           denom);
+          s64[k] += atan2(det, denom);
         }
       }
     }

@@ -5,7 +5,9 @@
 //
 // The reference creates a DeviceContext, four allocations and a synchronise on
 // every call (src/capi.mojo:366-398); here the context and buffers persist and
-// only grow.
+// only grow. Every device allocation goes through dev_malloc/dev_malloc_async
+// (host-side fault injection for the out-of-memory tests), every GPU entry point
+// opens an NVTX range, and handles refuse use on another device than their own.
 #include <cuda_runtime.h>
 
 #include <cstdarg>

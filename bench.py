@@ -52,8 +52,9 @@ exits (the commands behind the ncu summaries in profiles/): fp64_c3 (streaming
 FP64 kernel), fp64_tiled_c3 (FP64 over the prepared mesh), mixed_c3, adjoint_c4
 (per-face mixed adjoint on the gradient workload), adjoint_c3 (the same on the
 c3 workload), closest_c3 (closest-point traversal), fwn_c3 (fast
-winding number, beta = 2) and normals_s9 (area-weighted vertex normals of the
-subdivision-9 sphere).
+winding number, beta = 2), normals_s9 (area-weighted vertex normals of the
+subdivision-9 sphere) and batched_small (the batched persistent forward and
+edge adjoint on 16 uneven meshes with at most 65,536 queries each).
 """
 
 from __future__ import annotations
@@ -95,7 +96,8 @@ def parse_args():
     p.add_argument("--no-fast", action="store_true", help="skip the fast winding-number legs")
     p.add_argument("--no-normals", action="store_true", help="skip the vertex-normal workloads")
     p.add_argument("--case", choices=("fp64_c3", "fp64_tiled_c3", "mixed_c3", "adjoint_c4",
-                                      "closest_c3", "fwn_c3", "normals_s9", "adjoint_c3"),
+                                      "closest_c3", "fwn_c3", "normals_s9", "adjoint_c3",
+                                      "batched_small"),
                    help="run one kernel on a small case twice (for profiling) and exit")
     p.add_argument("--case-queries", type=int, default=None)
     p.add_argument("--no-autotune", dest="autotune", action="store_false",
@@ -934,6 +936,20 @@ def gpu_arm(args):
 def run_case(args):
     """One kernel, twice, on a reduced query batch of the c3 (or c4) workload."""
     import torch
+
+    if args.case == "batched_small":
+        from igl import batched, synthetic
+
+        work = synthetic.batched_workload(n_meshes=16, seed=51, max_queries=1 << 16, max_level=6)
+        bt = batched.Batch([(Vm, Fm) for Vm, Fm, _ in work], [Om for _, _, Om in work])
+        bt.gW.normal_()
+        for _ in range(2):
+            bt.forward()
+            bt.backward()
+        torch.cuda.synchronize()
+        print("ok", args.case, bt.info(), float(bt.W.abs().sum()))
+        bt.close()
+        return
 
     if args.case == "normals_s9":
         from igl import normals, synthetic

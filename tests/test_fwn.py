@@ -84,3 +84,34 @@ def test_contracts_and_edge_cases():
     assert igl.fast_winding_number(V, F, np.zeros((0, 3))).shape == (0,)
     w = igl.fast_winding_number(V, F, O[0])
     assert isinstance(w, float)
+
+
+def _degenerate_soup():
+    V, F = igl.synthetic.bumpy_icosphere(2, seed=21)
+    F = np.asarray(F)
+    zero = np.repeat(F[:6, :1], 3, axis=1)        # collapsed to a point
+    pinched = F[6:12][:, [0, 0, 1]]               # two equal corners
+    dup = F[12:40]                                # duplicated faces
+    flipped = F[40:60, ::-1]                      # reversed orientation
+    far_zero = np.full((9, 3), F[0, 0])           # a whole leaf of zero-area faces
+    Fs = np.ascontiguousarray(np.concatenate([F, zero, pinched, dup, flipped, far_zero]))
+    rng = np.random.default_rng(5)
+    O = np.concatenate([V[:30], 0.5 * (V[F[:20, 0]] + V[F[:20, 1]]),
+                        rng.uniform(-1.5, 1.5, size=(200, 3))])
+    return V, Fs, O
+
+
+@pytest.mark.parametrize("beta", [1.5, 2.0])
+def test_degenerate_soup_matches_oracle(oracle_mod, beta):
+    """Collapsed, pinched, duplicated and flipped faces, a leaf of zero-area
+    faces, queries on vertices and edges: the host evaluator against the
+    oracle's restatement (1e-12), and against the exact winding number when
+    beta is so large that nothing is expanded. (Not beta = 1: a node's radius
+    is the distance to its farthest vertex, so a query on that vertex sits
+    exactly on the far-test boundary, and two implementations that round the
+    node centre differently may expand the node or not.)"""
+    V, F, O = _degenerate_soup()
+    expected = oracle_mod.fast_winding_number(V, F, O, beta)
+    assert np.abs(igl.fast_winding_number(V, F, O, beta=beta) - expected).max() <= 1e-12
+    exact = oracle_mod.winding_number(V, F, O)
+    assert np.abs(igl.fast_winding_number(V, F, O, beta=1e9) - exact).max() <= 1e-12

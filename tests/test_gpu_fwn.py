@@ -65,3 +65,14 @@ def test_empty_inputs(gpu_required):
     assert igl.fast_winding_number(V, F, np.zeros((0, 3)), device="gpu").shape == (0,)
     w = igl.fast_winding_number(V, np.zeros((0, 3), np.int64), O, device="gpu")
     assert np.array_equal(w, np.zeros(10))
+
+
+def test_gpu_matches_host_on_a_degenerate_soup(gpu_required):
+    from test_fwn import _degenerate_soup
+
+    V, F, O = _degenerate_soup()
+    fwn = igl.FastWindingNumber(V, F)
+    for beta in (1.0, 2.0, 1e9):  # the same tree on both sides: beta = 1 included
+        assert np.abs(fwn.evaluate(O, device="gpu", beta=beta)
+                      - fwn.evaluate(O, beta=beta)).max() <= 1e-12
+    fwn.close()

@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kFwnThreads) fwn_kernel(const FwnArgs a) {
       const double2 p01 = ld2(n->p), p2r = ld2(n->p + 2);
       const int4 meta = __ldg(reinterpret_cast<const int4*>(&n->left));
       const double y0 = p01.x - qx, y1 = p01.y - qy, y2 = p2r.x - qz;
-      if (fwn_is_far(y0 * y0 + y1 * y1 + y2 * y2, a.beta, p2r.y)) {
+      if (fwn_is_far(fwn_dist2(y0, y1, y2), a.beta, p2r.y)) {
         lists.far[nfar++][tid] = node;
         node = -1;
       } else if (meta.w > 0) {

@@ -26,6 +26,13 @@ WN_HD double fwn_far_eval(const FwnMoments& m, double y0, double y1, double y2) 
   return a * i3 + b * i5 + c * i7;
 }
 
+// |y|^2 with every product and sum rounded separately (no contraction into
+// FMAs), so the GPU and the host classify every node the same way, also for a
+// query exactly on a node's sphere (a vertex at its radius).
+WN_HD double fwn_dist2(double y0, double y1, double y2) {
+  return dadd(dadd(dmul(y0, y0), dmul(y1, y1)), dmul(y2, y2));
+}
+
 // A node is replaced by its expansion when |q - p|^2 > (beta r)^2.
 WN_HD bool fwn_is_far(double d2, double beta, double r) {
   const double br = beta * r;

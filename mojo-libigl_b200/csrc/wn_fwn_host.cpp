@@ -209,7 +209,7 @@ void fwn_walk(const FwnHostTree& t, double qx, double qy, double qz, double beta
   while (sp > 0) {
     const FwnNode& n = t.nodes[stack[--sp]];
     const double y0 = n.p[0] - qx, y1 = n.p[1] - qy, y2 = n.p[2] - qz;
-    if (fwn_is_far(y0 * y0 + y1 * y1 + y2 * y2, beta, n.r)) {
+    if (fwn_is_far(fwn_dist2(y0, y1, y2), beta, n.r)) {
       if (far) *far += fwn_far_eval(t.moments[&n - t.nodes], y0, y1, y2);
     } else if (n.count > 0) {
       for (int32_t k = n.start; k < n.start + n.count; ++k) {

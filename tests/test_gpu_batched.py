@@ -106,3 +106,30 @@ def test_autotuner_picks_and_caches(gpu_required, tmp_path, monkeypatch):
     assert not first["cached"] and len(first["trials"]) == 2
     again = igl.autotune.tune(meshes, queries, space=space, reps=1)
     assert again["cached"] and again["config"] == first["config"]
+
+
+def test_meshes_without_faces_or_queries(gpu_required, oracle_mod):
+    """A mesh with no faces (W = 0 for its queries, no derivative), one with no
+    queries, and ordinary ones in the same batch, forward and backward."""
+    import torch
+
+    V1, F1 = igl.synthetic.bumpy_icosphere(2, seed=31)
+    V3, F3 = igl.synthetic.bumpy_icosphere(1, seed=32)
+    O1 = igl.synthetic.mixed_queries(V1, F1, 700, seed=33, near_sigma=1e-3)
+    O2 = np.random.default_rng(34).uniform(-1, 1, size=(300, 3))
+    O4 = igl.synthetic.mixed_queries(V3, F3, 200, seed=35, near_sigma=1e-3)
+    meshes = [(V1, F1), (V3, np.zeros((0, 3), np.int64)), (V3, F3), (V3, F3)]
+    queries = [O1, O2, np.zeros((0, 3)), O4]
+    b = igl.batched.Batch(meshes, queries, target_pairs=1 << 16)
+    try:
+        W = b.split(b.forward().clone())
+        assert np.abs(W[0].cpu().numpy() - oracle_mod.winding_number(V1, F1, O1)).max() <= 1e-6
+        assert torch.count_nonzero(W[1]) == 0 and W[2].numel() == 0
+        assert np.abs(W[3].cpu().numpy() - oracle_mod.winding_number(V3, F3, O4)).max() <= 1e-6
+        dV, dQ = b.backward(torch.ones_like(b.W))
+        torch.cuda.synchronize()
+        assert torch.isfinite(dV).all() and torch.isfinite(dQ).all()
+        assert torch.count_nonzero(b.split(dQ)[1]) == 0   # no faces: no derivative
+        assert torch.count_nonzero(b.split(dV, "v")[2]) == 0  # no queries: no derivative
+    finally:
+        b.close()

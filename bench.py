@@ -91,6 +91,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-c4", action="store_true", help="skip the gradient workload")
+    p.add_argument("--no-adjoint-workloads", action="store_true",
+                   help="skip fwd+bwd on the open c3 mesh and the c3 triangle soup")
     p.add_argument("--no-c5", action="store_true", help="skip the batched workload")
     p.add_argument("--no-closest", action="store_true", help="skip the closest-point workloads")
     p.add_argument("--no-fast", action="store_true", help="skip the fast winding-number legs")
@@ -469,6 +471,49 @@ def gpu_arm(args):
               "fwdbwd_faces_ms": t4["faces"] * 1e3, "fwdbwd_edges_ms": t4["edges"] * 1e3,
               "ratio_faces": t4["faces"] / t4["fwd"], "ratio_edges": t4["edges"] / t4["fwd"]}
         mesh4.close()
+
+    # fwd+bwd where the backward has work at the headline size: the c3 mesh with 8%
+    # of its faces deleted (about 72k boundary edges) and the c3 mesh as a triangle
+    # soup (every edge a boundary edge of the indexed mesh). Forward alone, then
+    # forward + each adjoint + the vertex gather, dL/dW ~ N(0, 1).
+    adj_work = None
+    if not args.no_adjoint_workloads:
+        from igl import synthetic
+
+        adj_work = {}
+        k_adj = min(args.steps, 3)
+        for wname in ("c3_open", "c3_soup"):
+            Va, Fa, Oa, desc_a = synthetic.workload(wname, n_queries=args.queries)
+            Vad, Fad = torch.from_numpy(Va).to(dev), torch.from_numpy(Fa).to(dev)
+            Oad = torch.from_numpy(Oa).to(dev)
+            gad = torch.from_numpy(np.random.default_rng(57).normal(size=len(Oa))).to(dev)
+            tria, lda, nfa = wa.triangle_soa(Vad, Fad)
+            mesha = wa.PreparedMesh(tria, lda, nfa)
+
+            def a_fwd():
+                check(handle.wn_mixed_mesh_update(mesha.mesh, tria.data_ptr(), lda, sp))
+                mesha.forward(Oad)
+
+            def a_faces():
+                a_fwd()
+                dqa, dta = mesha.backward(Oad, gad)
+                wa.gather_vertices(dta, lda, nfa, Fad, len(Va))
+
+            def a_edges():
+                a_fwd()
+                wa.backward_edges(Vad, Fad, Oad, gad)
+
+            ta = {k: timed(fn, k_adj, 1)[0] for k, fn in
+                  (("fwd", a_fwd), ("faces", a_faces), ("edges", a_edges))}
+            _, ne_a, _ = wa.boundary_edges(Vad, Fad)
+            adj_work[wname] = {
+                "workload": desc_a, "pairs": float(nfa) * len(Oa), "boundary_edges": ne_a,
+                "fwd_ms": ta["fwd"] * 1e3, "fwdbwd_faces_ms": ta["faces"] * 1e3,
+                "fwdbwd_edges_ms": ta["edges"] * 1e3,
+                "ratio_faces": ta["faces"] / ta["fwd"], "ratio_edges": ta["edges"] / ta["fwd"],
+                "steps": k_adj}
+            mesha.close()
+            del Vad, Fad, Oad, gad, tria
 
     # Batched workload: 64 bumpy icospheres (subdivision U{2..7}, 0-10% faces
     # deleted, queries log-uniform in [1024, 2^20]), forward and forward +
@@ -916,6 +961,7 @@ def gpu_arm(args):
                                 if "mixed" in results and "fp64" in results else None),
             "fwd_bwd": fwdbwd,
             "c4_fwd_bwd": c4,
+            "adjoint_workloads": adj_work,
             "c5_batched": c5,
             "winding_reference_bench": refwn,
             "closest_point": closest,

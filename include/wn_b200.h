@@ -136,8 +136,12 @@ int wn_forward_fp64_device(const double* tri, int64_t ld, const double* q, doubl
  * inside the library (held on every GPU that loads it until exit) instead of an
  * allocation. Limit: nq <= 524288 (2^19) queries, else WN_EINVAL. The first call
  * on each device looks up the array's device address and should come before
- * any stream capture. All calls share the array: calls that overlap on the GPU
- * race. Returns after the caller's stream has finished the work. */
+ * any stream capture. The stream must belong to the current device (else
+ * WN_EINVAL). All calls share the array: within one process a mutex held until
+ * the caller's stream has finished the work keeps calls from overlapping; calls
+ * that did overlap on the GPU would race. Returns after the caller's stream has
+ * finished the work, so a stream that is being captured is refused (WN_EINVAL)
+ * and left untouched. */
 int wn_forward_fp64_device_noalloc(const double* tri, int64_t ld, const double* q, double* w,
                                    int64_t nf, int64_t nq, int mode, void* stream);
 

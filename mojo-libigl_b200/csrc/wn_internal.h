@@ -72,6 +72,12 @@ struct Fp64Plan {
 // force_nsplit > 0 pins the number of face splits (tests use it).
 Fp64Plan plan_fp64(int64_t nf, int64_t nq, int sms, int force_nsplit = 0);
 
+// Plan of wn_forward_fp64_device_noalloc: plan_fp64 with the face splits capped
+// so that its nsplit * nq partial sums fit the fixed array of
+// kNoAllocScratchDoubles doubles (4 MiB) compiled into the library.
+constexpr int64_t kNoAllocScratchDoubles = int64_t(1) << 19;
+Fp64Plan noalloc_plan(int64_t nf, int64_t nq, int sms);
+
 // tri: 9 rows of `ld` doubles (row 3*corner+axis, ld even, ld >= nf), 16-byte
 // aligned; q: nq x 3; w: nq outputs (W, already divided by 2*pi); scratch:
 // plan.scratch_doubles doubles or null when that is 0; err: device error word.

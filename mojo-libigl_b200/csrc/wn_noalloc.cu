@@ -15,28 +15,35 @@
 // process exits. It holds the per-split partial angle sums of a face-split
 // launch, nsplit x nq doubles. The entry point accepts at most
 // kNoAllocMaxQueries queries and caps the number of face splits so that
-// nsplit * nq fits the array; larger query counts are rejected with WN_EINVAL.
+// nsplit * nq fits the array (noalloc_plan); larger query counts are rejected
+// with WN_EINVAL.
 //
 // Host code must not pass the array's name to a kernel: in host code the name
 // denotes a host-side stand-in, not a device address. On the first call on each
 // device (with that device current) the entry point asks the runtime for the
 // array's device address with cudaGetSymbolAddress, checks the result, and
 // caches it per device; that first call on a device should come before any
-// stream capture. Later calls reuse the cached address.
+// stream capture. Later calls reuse the cached address. The stream must belong
+// to the current device: the address is looked up for the current device, so a
+// stream of another device is refused with WN_EINVAL.
 //
 // Every call shares the one array and the one error word, and the array keeps
 // the last call's contents. Each call overwrites every partial sum it later
 // reads (one CTA writes each (split, query) entry before the summing kernel
-// reads it) and clears the error word, so nothing stale is read. Calls that
-// overlap on the GPU (for example on two streams at once) race on the array
-// and give wrong results: serialise them.
+// reads it) and clears the error word, so nothing stale is read. Within one
+// process calls do not overlap: each holds a mutex until its stream has
+// finished the work. That guarantee rests on those two alone; calls that did
+// overlap on the GPU would race on the array and give wrong results.
 //
 // The call is ordered on the caller's stream and returns after that stream has
 // finished the work, so that a kernel-reported error (a bounded wait that ran
-// out) can be returned. It calls no cudaMalloc, cudaFree or any allocating
-// library routine.
+// out) can be returned. Waiting for a stream that is being captured would end
+// the caller's capture with an error, so such a stream is refused up front
+// (WN_EINVAL) and left untouched. The call makes no cudaMalloc, cudaFree or
+// any allocating library routine.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <mutex>
 
@@ -46,7 +53,6 @@
 namespace wn {
 namespace {
 
-constexpr int64_t kNoAllocScratchDoubles = int64_t(1) << 19;  // 4 MiB of partial sums
 constexpr int64_t kNoAllocMaxQueries = kNoAllocScratchDoubles;
 constexpr int kNoAllocMaxDevices = 64;
 
@@ -75,6 +81,16 @@ int noalloc_fail(int code, const char* msg, cudaError_t e = cudaSuccess) {
 }
 
 }  // namespace
+
+Fp64Plan noalloc_plan(int64_t nf, int64_t nq, int sms) {
+  // wn_forward_fp64_device's plan, with the face splits capped so that the
+  // nsplit * nq partial sums fit the fixed array.
+  Fp64Plan plan = plan_fp64(nf, nq, sms);
+  const int64_t max_split = kNoAllocScratchDoubles / std::max<int64_t>(nq, 1);
+  if (plan.nsplit > max_split) plan = plan_fp64(nf, nq, sms, static_cast<int>(max_split));
+  return plan;
+}
+
 }  // namespace wn
 
 using namespace wn;
@@ -100,6 +116,21 @@ int wn_forward_fp64_device_noalloc(const double* tri, int64_t ld, const double* 
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
     return noalloc_fail(WN_ENODEV, "no usable CUDA device", e);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int stream_dev = dev;
+  if ((e = cudaStreamGetDevice(st, &stream_dev)) != cudaSuccess)
+    return noalloc_fail(WN_EINVAL, "cudaStreamGetDevice on the given stream", e);
+  if (stream_dev != dev)
+    return noalloc_fail(WN_EINVAL,
+                        "the stream belongs to another device than the current one: make the "
+                        "stream's device current before the call");
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if ((e = cudaStreamIsCapturing(st, &capture)) != cudaSuccess)
+    return noalloc_fail(WN_EINVAL, "cudaStreamIsCapturing on the given stream", e);
+  if (capture != cudaStreamCaptureStatusNone)
+    return noalloc_fail(WN_EINVAL,
+                        "the stream is being captured: this call waits for its stream before "
+                        "it returns, which would end the capture");
   NoAllocDevice& d = g_noalloc_dev[dev];
   if (!d.ready) {
     // Once per device, with that device current: device addresses of the
@@ -116,15 +147,10 @@ int wn_forward_fp64_device_noalloc(const double* tri, int64_t ld, const double* 
     d.ready = true;
   }
 
-  // Same launch plan as wn_forward_fp64_device, with the face splits capped so
-  // that nsplit * nq partial sums fit the fixed array.
-  Fp64Plan plan = plan_fp64(nf, nq, d.sms);
-  const int64_t max_split = kNoAllocScratchDoubles / nq;
-  if (plan.nsplit > max_split) plan = plan_fp64(nf, nq, d.sms, static_cast<int>(max_split));
+  const Fp64Plan plan = noalloc_plan(nf, nq, d.sms);
   if (plan.scratch_doubles > kNoAllocScratchDoubles)
     return noalloc_fail(WN_EINVAL, "face split does not fit the fixed scratch array");
 
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   if ((e = cudaMemsetAsync(d.err, 0, sizeof(int), st)) != cudaSuccess)
     return noalloc_fail(WN_ECUDA, "clearing the error word", e);
   if ((e = launch_fp64(plan, mode, tri, ld, nf, q, nq, w, d.partial, d.err, st)) != cudaSuccess)

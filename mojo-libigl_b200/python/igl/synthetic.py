@@ -151,6 +151,11 @@ def workload(name: str, n_queries: int | None = None):
               near offset N(0, 1e-3), box 1.2x.
     c3_mixed: s=7 closed (163,842 V, 327,680 F); 2^20 Q, 50/50, near N(0, 1e-4).
     c4_grad:  the c2 mesh; 262,144 near-surface Q, offset N(0, 1e-3).
+    c3_open:  the c3 mesh with 8% of its faces deleted (301,466 F, open: about
+              72k boundary edges); 2^20 Q, 50/50, near N(0, 1e-4).
+    c3_soup:  the c3 mesh as a triangle soup: every face has its own three
+              vertices (983,040 V, 327,680 F), so every edge is a boundary edge
+              of the indexed mesh; the c3 queries.
     """
     if name == "c1_cpu":
         V, F = bumpy_icosphere(3, seed=11)
@@ -174,7 +179,28 @@ def workload(name: str, n_queries: int | None = None):
         n = 262144 if n_queries is None else n_queries
         O = near_surface_points(V, F, n, seed=43, sigma=1e-3)
         return V, F, O, "c2 mesh (%d F) x %d near-surface Q (1e-3)" % (len(F), n)
+    if name == "c3_open":
+        V, F = bumpy_icosphere(7, seed=31)
+        F = delete_faces(F, 0.08, seed=32)
+        n = (1 << 20) if n_queries is None else n_queries
+        O = mixed_queries(V, F, n, seed=33, near_sigma=1e-4)
+        return V, F, O, ("bumpy icosphere s=7, 8%% faces deleted (%d F, open) x %d Q 50/50 "
+                         "box/near(1e-4)" % (len(F), n))
+    if name == "c3_soup":
+        V, F = bumpy_icosphere(7, seed=31)
+        n = (1 << 20) if n_queries is None else n_queries
+        O = mixed_queries(V, F, n, seed=33, near_sigma=1e-4)
+        Vs, Fs = unshare_vertices(V, F)
+        return Vs, Fs, O, ("c3 mesh as a triangle soup (%d V, %d F, every face its own "
+                           "vertices) x %d Q 50/50 box/near(1e-4)" % (len(Vs), len(Fs), n))
     raise ValueError(f"unknown workload {name!r}")
+
+
+def unshare_vertices(V: np.ndarray, F: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """The same triangles as a soup: face f gets vertices 3f, 3f+1, 3f+2."""
+    Vs = np.ascontiguousarray(V[F].reshape(-1, 3))
+    Fs = np.arange(3 * len(F), dtype=np.int64).reshape(-1, 3)
+    return Vs, Fs
 
 
 def batched_workload(n_meshes: int = 64, seed: int = 51, max_queries: int = 1 << 20,

@@ -4,6 +4,7 @@ import ctypes
 import glob
 import os
 import re
+import shutil
 import subprocess
 import sys
 
@@ -62,3 +63,23 @@ def test_fault_injection_from_the_environment():
                          timeout=300)
     assert out.returncode == 0, out.stderr
     assert out.stdout.strip().splitlines()[-1] == "1"
+
+
+def test_noalloc_plan_fits_its_fixed_array(tmp_path):
+    """The no-allocation entry point's face-split cap, on SM counts and query
+    counts where the uncapped plan would overflow its fixed array (host code)."""
+    lib_path = _lib.build()
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    cuda_inc = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(nvcc))), "include")
+    exe = tmp_path / "noalloc_plan_check"
+    build = subprocess.run(
+        ["g++", "-std=c++17", "-O1", "-I", cuda_inc,
+         "-I", os.path.join(ROOT, "mojo-libigl_b200", "csrc"),
+         os.path.join(ROOT, "tests", "noalloc_plan_check.cpp"), "-o", str(exe),
+         "-L", os.path.dirname(lib_path), "-lwn_b200",
+         "-Wl,-rpath," + os.path.dirname(lib_path)],
+        capture_output=True, text=True, timeout=300)
+    assert build.returncode == 0, build.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert run.returncode == 0, run.stdout + run.stderr
+    assert run.stdout.startswith("ok")

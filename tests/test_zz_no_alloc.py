@@ -6,8 +6,11 @@ face-split scratch in a fixed array inside the library. These tests call it
 through the C ABI, twice in a row on the same inputs, and compare each result
 with the allocating entry point wn_forward_fp64_device at the FP64 parity
 tolerance (1e-12); they also check that query counts beyond its limit
-(2^19) are refused. This file sorts last so a stop-at-first-failure run has
-already run every other test.
+(2^19) are refused, that a call succeeds while the library's next device
+allocation is set to fail (it makes none), and that a stream under capture is
+refused without ending the caller's capture (the call waits for its stream).
+This file sorts last so a stop-at-first-failure run has already run every
+other test.
 """
 
 import ctypes
@@ -78,3 +81,57 @@ def test_noalloc_refuses_more_than_its_limit(gpu_required):
     rc = noalloc(tri_d.data_ptr(), ld, q_d.data_ptr(), w_d.data_ptr(), nf, nq, 0, stream)
     assert rc != 0
     assert "524288" in _lib.last_error()
+
+
+def test_noalloc_makes_no_device_allocation(gpu_required):
+    """With the library's next device allocation armed to fail, the call still
+    succeeds and leaves the fault armed: it allocated nothing."""
+    import torch
+
+    handle = _lib.lib()
+    noalloc = _noalloc(handle)
+    V, F, O, _ = igl.synthetic.workload("c2_open", n_queries=3000)
+    tri_d, ld, nf = _device_soup(torch, V, F)
+    q_d = torch.from_numpy(O).cuda()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    expected = torch.empty(len(O), dtype=torch.float64, device="cuda")
+    assert handle.wn_forward_fp64_device(tri_d.data_ptr(), ld, q_d.data_ptr(),
+                                         expected.data_ptr(), nf, len(O), 0, stream) == 0
+    got = torch.empty_like(expected)
+    assert handle.wn_inject_fault(1, 0) == 0  # WN_FAULT_ALLOC: the next allocation fails
+    try:
+        rc = noalloc(tri_d.data_ptr(), ld, q_d.data_ptr(), got.data_ptr(), nf, len(O), 0, stream)
+        assert rc == 0, _lib.last_error()
+        assert handle.wn_fault_armed() == 1
+    finally:
+        handle.wn_inject_fault(0, 0)
+    assert float((got - expected).abs().max()) <= TOL
+
+
+def test_noalloc_refuses_a_capturing_stream(gpu_required):
+    """The call waits for its stream before returning, so on a stream under
+    capture it returns an error before touching the stream; the caller's capture
+    stays valid."""
+    import torch
+
+    handle = _lib.lib()
+    noalloc = _noalloc(handle)
+    V, F = igl.synthetic.bumpy_icosphere(1, seed=1)
+    tri_d, ld, nf = _device_soup(torch, V, F)
+    q_d = torch.zeros((16, 3), dtype=torch.float64, device="cuda")
+    w_d = torch.empty(16, dtype=torch.float64, device="cuda")
+    x = torch.zeros(8, device="cuda")
+    side = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(side):
+        graph.capture_begin()
+        x.add_(1.0)
+        rc = noalloc(tri_d.data_ptr(), ld, q_d.data_ptr(), w_d.data_ptr(), nf, 16, 0,
+                     ctypes.c_void_p(side.cuda_stream))
+        graph.capture_end()
+    assert rc != 0
+    assert "captured" in _lib.last_error()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert float(x.sum()) == 8.0

@@ -166,6 +166,13 @@ def oracle_rate(tri, O, cores: int, target_s: float):
     return nf * len(sample) / dt, len(sample), dt
 
 
+def oracle_isa() -> str:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    return oracle.isa()
+
+
 def oracle_aabb_rate(P, V, F, tree, cores: int, target_s: float):
     """Points/s of the oracle's closest-point query over `cores` threads on a
     prefix of P sized to take about target_s seconds."""
@@ -201,32 +208,49 @@ def closest_point_workloads(nq: int):
 
 
 def reference_arm(args):
+    """The reference's CPU path (the oracle port of its Mojo kernel, all host
+    threads) on a fixed query sample of the headline workload; every step times
+    the whole sample (wall clock), so ms_per_step is a measured step."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
     V, F, O, desc = make_inputs(args.subdivisions, args.queries, 0)
     tri = soa(V, F)
+    nf = len(F)
     cores = host_cores()
-    rates = []
-    samples = 0
+    rate, _, _ = oracle_rate(tri, O, cores, target_s=0.5)
+    n = int(min(len(O), max(cores, rate * 2.5 / nf)))  # about 2.5 s per step
+    half = len(O) // 2
+    sample = np.concatenate([O[: n // 2], O[half: half + n - n // 2]])
+    times = []
     for i in range(args.warmup + args.steps):
-        rate, n, dt = oracle_rate(tri, O, cores, target_s=4.0)
+        t0 = time.perf_counter()
+        oracle.winding_soa(tri, sample, workers=cores)
+        dt = time.perf_counter() - t0
         if i >= args.warmup:
-            rates.append(rate)
-            samples = n
-    value = float(np.median(rates))
-    ms = len(F) * args.queries / value * 1e3
+            times.append(dt)
+    dt = float(np.median(times))
+    value = nf * len(sample) / dt
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: " + desc,
-        "config": {"workload": "c3: " + desc, "precision": "fp64 (reference CPU path)"},
+        "config": {"workload": "c3: " + desc, "precision": "fp64 (reference CPU path)",
+                   "faces": nf, "queries_per_gpu": args.queries,
+                   "pairs_per_gpu_step": float(nf) * args.queries},
+        "sample": {"queries_per_step": len(sample), "pairs_per_step": float(nf) * len(sample),
+                   "step": "one pass of the reference CPU path over a fixed query sample of "
+                           "the workload (50/50 box/near) against all faces, wall clock; "
+                           "value = sample pairs / step time"},
         "cpu_baseline": {
             "value": value, "unit": "pairs/s", "cores": cores, "kind": "port",
-            "sample": f"{samples} queries (50/50 box/near) x {len(F)} faces per step, "
-                      f"oracle restatement of src/capi.mojo:205-294 over {cores} threads "
-                      f"({cpu_model()}); ms_per_step extrapolates to the full batch",
+            "sample": f"{len(sample)} queries (50/50 box/near) x {nf} faces per step, oracle "
+                      f"restatement of src/capi.mojo:205-294 over {cores} threads "
+                      f"({cpu_model()}, {oracle.isa()} clone)",
         },
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -934,7 +958,7 @@ def gpu_arm(args):
         cpu = {"value": rate, "unit": "pairs/s", "cores": cores, "kind": "port",
                "sample": f"{n} queries (50/50 box/near) x {nf} faces in {dt:.1f} s, oracle "
                          f"restatement of src/capi.mojo:205-294 over {cores} threads "
-                         f"({cpu_model()})"}
+                         f"({cpu_model()}, {oracle_isa()} clone)"}
         # The reference's own fan-out caps its pool at four workers (python/igl/_lib.py:37).
         w4 = min(4, cores)
         rate4, n4, dt4 = oracle_rate(tri, O, w4, target_s=6.0)

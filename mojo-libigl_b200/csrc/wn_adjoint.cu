@@ -26,6 +26,7 @@
 // touches. After the last chunk a block's face sums go to dF_part[g][corner][face]. Two
 // finishing kernels add the partials over r and over g in index order.
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 #include "wn_adjoint.h"
@@ -173,14 +174,28 @@ __global__ void __launch_bounds__(THREADS, 2) adjoint_fp64_kernel(const AdjointA
 // ---- mixed precision adjoint ---------------------------------------------
 // Same decomposition over the prepared mesh of the mixed forward (wn_mixed.cu):
 // 64-face tiles in Morton order with FP32 tile-local scaled coordinates, queries in
-// Morton order. A face block is 4 tiles; thread t keeps face (t mod 64) of tiles
-// 4b + (t/64) and 4b + 2 + (t/64), so each warp's 32 faces share one tile and a
-// query's far test against that tile is uniform over the warp. Far pairs are
-// evaluated in FP32 in the tile's scaled frame (derivatives scale as 1/length: the
-// tile's scale factor multiplies them back); a pair with a vertex closer than
-// kappa * h_face is evaluated in FP64 from the sorted FP64 soup. Per-face sums are
-// kept in FP32 within a query chunk and in FP64 across chunks; per-query sums over
-// faces are reduced in FP64 (large near-surface terms cancel there).
+// Morton order. A face block is 4 tiles and a CTA has 4 warps: warp w keeps tile
+// 4b + w, lane l its faces l and l + 32 as the two lanes of packed FP32x2
+// arithmetic (sm_100 add/mul/fma .f32x2), so a query's far test against the tile
+// is uniform over the warp. Far pairs are evaluated in FP32 in the tile's scaled
+// frame; the tile's scale factor (derivatives scale as 1/length) is folded into the
+// query's upstream gradient. A pair with a vertex closer than kappa * h_face is
+// evaluated in FP64 from the sorted FP64 soup. Per-face sums are kept in FP32 over
+// a few query chunks and in FP64 beyond; per-query sums over faces are reduced in a
+// fixed order, FP32 shares of far pairs and FP64 shares of refined pairs (large
+// near-surface terms cancel there) added in FP64.
+//
+// Per far pair, with a = A - o, e1 = B - A, e2 = C - A, n = e1 x e2 from the face
+// record and g the query's (scaled) upstream gradient:
+//   |a|^2, a.e1, a.e2 give |b|^2, |c|^2, a.b, b.c, c.a (as in the forward);
+//   la = |a|^2 rsqrt(|a|^2) ...; D_ab = la lb + a.b ...; 1/D by rcp;
+//   a x b = a x e1, c x a = e2 x a, b x c = n - a x b - c x a;
+//   k_A1 = g ra / D_ab, k_A2 = g ra / D_ca, k_B1 = g rb / D_ab, k_B2 = g rb / D_bc,
+//   k_C1 = g rc / D_bc, k_C2 = g rc / D_ca;
+//   -g dOmega/dA = k_A1 (a x b) + k_A2 (c x a), -g dOmega/dB = k_B1 (a x b) + k_B2 (b x c),
+//   -g dOmega/dC = k_C1 (b x c) + k_C2 (c x a),
+//   g dOmega/do = (k_A1 + k_B1)(a x b) + (k_B2 + k_C1)(b x c) + (k_C2 + k_A2)(c x a):
+// 83 FP32 operations (as 42 packed instructions per face pair) and 6 MUFU per pair.
 struct MixedAdjointArgs {
   const unsigned char* tiles;
   int64_t ntiles;
@@ -205,16 +220,24 @@ __global__ void gather_sorted_queries_kernel(const double* __restrict__ q,
   qs[s] = make_double4(q[3 * i], q[3 * i + 1], q[3 * i + 2], gw[i]);
 }
 
-// Shared-memory layout of adjoint_mixed_kernel (dynamic, QC queries per chunk).
-template <int THREADS, int QC>
-struct MixedAdjointSmem {
-  float dO32[QC][3][THREADS];         // per-thread FP32 dL/do shares of far pairs (transposed)
-  double acc64[2][9][THREADS];        // per-face FP64 sums across chunks (thread-private columns)
-  double red64[THREADS / 32][QC][3];  // per-warp FP64 shares of refined pairs
+// Shared-memory layout of adjoint_faces_kernel (dynamic, QC queries per chunk).
+constexpr int kFaThreads = 128;          // four warps, one 64-face tile each
+constexpr int kFaTiles = kFaThreads / 32;
+constexpr int kFaRow = kFaThreads + 4;   // padded row of per-thread dL/do shares
+constexpr int kFaQc = 16;                // queries per chunk (4 CTAs per SM fit the smem)
+constexpr int kFaFlushChunks = 4;        // FP32 face sums go to FP64 every 64 queries
+static_assert(kFaThreads == 2 * kTileFaces, "two faces per thread cover a tile per warp");
+
+template <int QC>
+struct FaceAdjSmem {
+  float dO32[QC * 3][kFaRow];         // per-thread FP32 dL/do shares, row 3*query + axis
+  double acc64[18][kFaThreads];       // per-face FP64 sums (thread-private columns)
+  double red64[kFaTiles][QC][3];      // per-warp FP64 shares of refined pairs
   double dsum[QC * 3];                // the chunk's dL/do sums before they go to global
-  double4 sq[QC];                     // FP64 query + g
-  float4 sl[QC][4];                   // local scaled query per tile, w = 1 if far
-  TileHeader th[4];
+  double4 q64[QC];                    // FP64 query and g (refinement)
+  float4 frame[QC][kFaTiles];         // query in the tile's scaled frame, w = g * scale
+  int flag[QC][kFaTiles];             // 0: far, 1: careful (near test), 2: skip
+  TileHeader th[kFaTiles];
 };
 
 // One refined (near) pair in FP64: g * dOmega into the face's FP64 sums in shared
@@ -234,118 +257,32 @@ __device__ __noinline__ void refine_pair_grad(const double* __restrict__ tri64, 
   for (int r = 0; r < 9; ++r) acc_col[r * stride] += gv[r];
 }
 
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
 // Lane k of a float2 (k a compile-time constant after unrolling).
-__device__ __forceinline__ float lane_of(const float2& v, int k) { return k == 0 ? v.x : v.y; }
 __device__ __forceinline__ float& lane_ref(float2& v, int k) { return k == 0 ? v.x : v.y; }
-
-// Far-pair gradient terms of one face (lane k) against one query, FP32: adds
-// the face's corner gradients (scaled by the tile's coordinate scale later) to
-// acc[r] lane k and its share of dL/do to dof[x] lane k.
-__device__ __forceinline__ void adj_far_lane(float g, float ax, float ay, float az,
-                                             const float2 (&fe1)[3], const float2 (&fe2)[3],
-                                             float aa, float bb, float cc, float ab, float bc,
-                                             float ca, float sck, int k, float2 (&acc)[9],
-                                             float2 (&dof)[3]) {
-  float ra, rb, rc, iab, ibc, ica;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(ra) : "f"(aa));
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rb) : "f"(bb));
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(cc));
-  const float rab = ra * rb, rbc = rb * rc, rca = rc * ra;
-  const float dab = fmaf(ab, rab, 1.f), dbc = fmaf(bc, rbc, 1.f), dca = fmaf(ca, rca, 1.f);
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(iab) : "f"(dab));
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ibc) : "f"(dbc));
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ica) : "f"(dca));
-  const float wab = g * rab * iab, wbc = g * rbc * ibc, wca = g * rca * ica;
-  const float bx = ax + lane_of(fe1[0], k), by = ay + lane_of(fe1[1], k), bz = az + lane_of(fe1[2], k);
-  const float cx = ax + lane_of(fe2[0], k), cy = ay + lane_of(fe2[1], k), cz = az + lane_of(fe2[2], k);
-  const float xab0 = ay * bz - az * by, xab1 = az * bx - ax * bz, xab2 = ax * by - ay * bx;
-  const float xbc0 = by * cz - bz * cy, xbc1 = bz * cx - bx * cz, xbc2 = bx * cy - by * cx;
-  const float xca0 = cy * az - cz * ay, xca1 = cz * ax - cx * az, xca2 = cx * ay - cy * ax;
-  // Negated coefficients: each of the 9 sums takes two FMAs.
-  const float nA1 = -ra * wab, nA2 = -ra * wca, nB1 = -rb * wab, nB2 = -rb * wbc;
-  const float nC1 = -rc * wbc, nC2 = -rc * wca;
-  lane_ref(acc[0], k) = fmaf(nA1, xab0, fmaf(nA2, xca0, lane_of(acc[0], k)));
-  lane_ref(acc[1], k) = fmaf(nA1, xab1, fmaf(nA2, xca1, lane_of(acc[1], k)));
-  lane_ref(acc[2], k) = fmaf(nA1, xab2, fmaf(nA2, xca2, lane_of(acc[2], k)));
-  lane_ref(acc[3], k) = fmaf(nB1, xab0, fmaf(nB2, xbc0, lane_of(acc[3], k)));
-  lane_ref(acc[4], k) = fmaf(nB1, xab1, fmaf(nB2, xbc1, lane_of(acc[4], k)));
-  lane_ref(acc[5], k) = fmaf(nB1, xab2, fmaf(nB2, xbc2, lane_of(acc[5], k)));
-  lane_ref(acc[6], k) = fmaf(nC1, xbc0, fmaf(nC2, xca0, lane_of(acc[6], k)));
-  lane_ref(acc[7], k) = fmaf(nC1, xbc1, fmaf(nC2, xca1, lane_of(acc[7], k)));
-  lane_ref(acc[8], k) = fmaf(nC1, xbc2, fmaf(nC2, xca2, lane_of(acc[8], k)));
-  const float sab = -(nA1 + nB1) * sck, sbc = -(nB2 + nC1) * sck, sca = -(nC2 + nA2) * sck;
-  lane_ref(dof[0], k) = fmaf(sab, xab0, fmaf(sbc, xbc0, fmaf(sca, xca0, lane_of(dof[0], k))));
-  lane_ref(dof[1], k) = fmaf(sab, xab1, fmaf(sbc, xbc1, fmaf(sca, xca1, lane_of(dof[1], k))));
-  lane_ref(dof[2], k) = fmaf(sab, xab2, fmaf(sbc, xbc2, fmaf(sca, xca2, lane_of(dof[2], k))));
+__device__ __forceinline__ float2 rsqrt2(float2 v) {
+  float2 r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r.x) : "f"(v.x));
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r.y) : "f"(v.y));
+  return r;
+}
+__device__ __forceinline__ float2 rcp2(float2 v) {
+  float2 r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.x) : "f"(v.x));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.y) : "f"(v.y));
+  return r;
+}
+// u x v component u1 v2 - u2 v1 as one multiply and one FMA (packed).
+__device__ __forceinline__ float2 cross_c(float2 u1, float2 v2, float2 u2, float2 v1) {
+  return __ffma2_rn(u1, v2, __fmul2_rn(make_float2(-u2.x, -u2.y), v1));
 }
 
-// adj_far_lane for both faces at once, packed; nsc = minus the two tiles' scales.
-__device__ __forceinline__ void adj_far_pair2(float g, float2 ax, float2 ay, float2 az,
-                                              const float2 (&fe1)[3], const float2 (&fe2)[3],
-                                              float2 aa, float2 bb, float2 cc, float2 ab,
-                                              float2 bc, float2 ca, float2 nsc,
-                                              float2 (&acc)[9], float2 (&dof)[3]) {
-  float2 ra, rb, rc, iab, ibc, ica;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(ra.x) : "f"(aa.x));
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(ra.y) : "f"(aa.y));
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rb.x) : "f"(bb.x));
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rb.y) : "f"(bb.y));
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rc.x) : "f"(cc.x));
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rc.y) : "f"(cc.y));
-  const float2 one = make_float2(1.f, 1.f);
-  const float2 rab = __fmul2_rn(ra, rb), rbc = __fmul2_rn(rb, rc), rca = __fmul2_rn(rc, ra);
-  const float2 dab = __ffma2_rn(ab, rab, one), dbc = __ffma2_rn(bc, rbc, one);
-  const float2 dca = __ffma2_rn(ca, rca, one);
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(iab.x) : "f"(dab.x));
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(iab.y) : "f"(dab.y));
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ibc.x) : "f"(dbc.x));
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ibc.y) : "f"(dbc.y));
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ica.x) : "f"(dca.x));
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ica.y) : "f"(dca.y));
-  const float2 g2 = make_float2(g, g);
-  const float2 wab = __fmul2_rn(__fmul2_rn(g2, rab), iab);
-  const float2 wbc = __fmul2_rn(__fmul2_rn(g2, rbc), ibc);
-  const float2 wca = __fmul2_rn(__fmul2_rn(g2, rca), ica);
-  const float2 bx = __fadd2_rn(ax, fe1[0]), by = __fadd2_rn(ay, fe1[1]), bz = __fadd2_rn(az, fe1[2]);
-  const float2 cx = __fadd2_rn(ax, fe2[0]), cy = __fadd2_rn(ay, fe2[1]), cz = __fadd2_rn(az, fe2[2]);
-  auto neg = [](float2 v) { return make_float2(-v.x, -v.y); };
-  // u x v component: u1 v2 - u2 v1 as one multiply and one FMA.
-  auto cross = [&](float2 u1, float2 v2, float2 u2, float2 v1) {
-    return __ffma2_rn(u1, v2, __fmul2_rn(neg(u2), v1));
-  };
-  const float2 xab0 = cross(ay, bz, az, by), xab1 = cross(az, bx, ax, bz), xab2 = cross(ax, by, ay, bx);
-  const float2 xbc0 = cross(by, cz, bz, cy), xbc1 = cross(bz, cx, bx, cz), xbc2 = cross(bx, cy, by, cx);
-  const float2 xca0 = cross(cy, az, cz, ay), xca1 = cross(cz, ax, cx, az), xca2 = cross(cx, ay, cy, ax);
-  const float2 nra = neg(ra), nrb = neg(rb), nrc = neg(rc);
-  const float2 nA1 = __fmul2_rn(nra, wab), nA2 = __fmul2_rn(nra, wca);
-  const float2 nB1 = __fmul2_rn(nrb, wab), nB2 = __fmul2_rn(nrb, wbc);
-  const float2 nC1 = __fmul2_rn(nrc, wbc), nC2 = __fmul2_rn(nrc, wca);
-  acc[0] = __ffma2_rn(nA1, xab0, __ffma2_rn(nA2, xca0, acc[0]));
-  acc[1] = __ffma2_rn(nA1, xab1, __ffma2_rn(nA2, xca1, acc[1]));
-  acc[2] = __ffma2_rn(nA1, xab2, __ffma2_rn(nA2, xca2, acc[2]));
-  acc[3] = __ffma2_rn(nB1, xab0, __ffma2_rn(nB2, xbc0, acc[3]));
-  acc[4] = __ffma2_rn(nB1, xab1, __ffma2_rn(nB2, xbc1, acc[4]));
-  acc[5] = __ffma2_rn(nB1, xab2, __ffma2_rn(nB2, xbc2, acc[5]));
-  acc[6] = __ffma2_rn(nC1, xbc0, __ffma2_rn(nC2, xca0, acc[6]));
-  acc[7] = __ffma2_rn(nC1, xbc1, __ffma2_rn(nC2, xca1, acc[7]));
-  acc[8] = __ffma2_rn(nC1, xbc2, __ffma2_rn(nC2, xca2, acc[8]));
-  const float2 sab = __fmul2_rn(__fadd2_rn(nA1, nB1), nsc);
-  const float2 sbc = __fmul2_rn(__fadd2_rn(nB2, nC1), nsc);
-  const float2 sca = __fmul2_rn(__fadd2_rn(nC2, nA2), nsc);
-  dof[0] = __ffma2_rn(sab, xab0, __ffma2_rn(sbc, xbc0, __ffma2_rn(sca, xca0, dof[0])));
-  dof[1] = __ffma2_rn(sab, xab1, __ffma2_rn(sbc, xbc1, __ffma2_rn(sca, xca1, dof[1])));
-  dof[2] = __ffma2_rn(sab, xab2, __ffma2_rn(sbc, xbc2, __ffma2_rn(sca, xca2, dof[2])));
-}
-
-template <int THREADS, int QC>
-__global__ void __launch_bounds__(THREADS, 3) adjoint_mixed_kernel(const MixedAdjointArgs a) {
-  static_assert(THREADS == 2 * kTileFaces, "one thread per face of two tiles");
-  constexpr int kTilesPerBlock = 4;
+template <int QC>
+__global__ void __launch_bounds__(kFaThreads, 4) adjoint_faces_kernel(const MixedAdjointArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  auto& sm = *reinterpret_cast<MixedAdjointSmem<THREADS, QC>*>(smem_raw);
+  auto& sm = *reinterpret_cast<FaceAdjSmem<QC>*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int j = tid & (kTileFaces - 1), half = tid >> 6;
-  const int64_t nblocks = (a.ntiles + kTilesPerBlock - 1) / kTilesPerBlock;
+  const int64_t nblocks = (a.ntiles + kFaTiles - 1) / kFaTiles;
   const int64_t range = blockIdx.x, group = blockIdx.y;
   const int64_t b_begin = range * a.blocks_per_range;
   const int64_t b_end = min(nblocks, b_begin + a.blocks_per_range);
@@ -355,153 +292,218 @@ __global__ void __launch_bounds__(THREADS, 3) adjoint_mixed_kernel(const MixedAd
 
   for (int64_t blk = b_begin; blk < b_end; ++blk) {
     __syncthreads();  // previous block's shared data fully consumed
-    if (tid < kTilesPerBlock) {
-      const int64_t t = blk * kTilesPerBlock + tid;
+    if (tid < kFaTiles) {
+      const int64_t t = blk * kFaTiles + tid;
       if (t < a.ntiles) {
         sm.th[tid] = *reinterpret_cast<const TileHeader*>(a.tiles + t * kTileBytes);
       } else {
         TileHeader empty{};
         empty.far_r2 = 0.0;  // every query is "far" from a missing tile
+        empty.scale = 1.0;
         sm.th[tid] = empty;
       }
     }
-    // Face records: A, e1 = B - A, e2 = C - A, |e1|^2, |e2|^2, e1.e2 and the
-    // refinement threshold (FaceRec layout), scaled tile-local FP32. The thread's
-    // two faces are the two lanes of every float2 (lane k = face k), so the far
-    // pairs of both run as packed FP32x2 arithmetic (sm_100 add/mul/fma .f32x2).
-    float2 fa[3], fe1[3], fe2[3], fg[3], acc[9];
-    float thr[2], sc[2];
-    int64_t slot[2];
-    bool valid[2];
+    // This warp's tile; lane k of every float2 is face lane + 32 k. Padding faces get
+    // a corner far away and zero edges: every term they give is exactly zero.
+    const int64_t t = blk * kFaTiles + warp;
+    const bool tile_ok = t < a.ntiles;
+    const unsigned char* rec = a.tiles + (tile_ok ? t : 0) * kTileBytes;
+    const int n = tile_ok ? reinterpret_cast<const TileHeader*>(rec)->n : 0;
+    float2 fa[3], fe1[3], fe2[3], fn[3], fg[3];
+    const float* thr_rec = reinterpret_cast<const float*>(rec + sizeof(TileHeader)) + 16 * lane + 15;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
-      const int64_t t = blk * kTilesPerBlock + 2 * k + half;
-      const bool tile_ok = t < a.ntiles;
-      const TileHeader* th =
-          reinterpret_cast<const TileHeader*>(a.tiles + (tile_ok ? t : 0) * kTileBytes);
-      valid[k] = tile_ok && j < th->n;
-      sc[k] = tile_ok ? static_cast<float>(th->scale) : 0.f;
-      slot[k] = (tile_ok ? t : 0) * kTileFaces + j;
-      const float* fr = reinterpret_cast<const float*>(a.tiles + (tile_ok ? t : 0) * kTileBytes +
-                                                       sizeof(TileHeader)) + 16 * j;
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        lane_ref(fa[r], k) = valid[k] ? fr[r] : 0.f;
-        lane_ref(fe1[r], k) = valid[k] ? fr[3 + r] : 0.f;
-        lane_ref(fe2[r], k) = valid[k] ? fr[6 + r] : 0.f;
-        lane_ref(fg[r], k) = valid[k] ? fr[12 + r] : 0.f;
+      const int j = lane + 32 * k;
+      const bool valid = j < n;
+      const float4* fr = reinterpret_cast<const float4*>(rec + sizeof(TileHeader)) + 4 * j;
+      float4 r0 = make_float4(1e18f, 1e18f, 1e18f, 0.f), r1 = make_float4(0.f, 0.f, 0.f, 0.f);
+      float4 r2 = r1, r3 = make_float4(0.f, 0.f, 0.f, -1.f);
+      if (valid) {
+        r0 = fr[0];
+        r1 = fr[1];
+        r2 = fr[2];
+        r3 = fr[3];
       }
-      thr[k] = valid[k] ? fr[15] : 0.f;
-#pragma unroll
-      for (int r = 0; r < 9; ++r) sm.acc64[k][r][tid] = 0.0;
+      lane_ref(fa[0], k) = r0.x;  lane_ref(fa[1], k) = r0.y;  lane_ref(fa[2], k) = r0.z;
+      lane_ref(fe1[0], k) = r0.w; lane_ref(fe1[1], k) = r1.x; lane_ref(fe1[2], k) = r1.y;
+      lane_ref(fe2[0], k) = r1.z; lane_ref(fe2[1], k) = r1.w; lane_ref(fe2[2], k) = r2.x;
+      lane_ref(fn[0], k) = r2.y;  lane_ref(fn[1], k) = r2.z;  lane_ref(fn[2], k) = r2.w;
+      lane_ref(fg[0], k) = r3.x;  lane_ref(fg[1], k) = r3.y;  lane_ref(fg[2], k) = r3.z;
     }
+    const int64_t slot0 = (tile_ok ? t : 0) * kTileFaces + lane;
 #pragma unroll
-    for (int r = 0; r < 9; ++r) acc[r] = make_float2(0.f, 0.f);
-    const float2 nsc = make_float2(-sc[0], -sc[1]);
-    const bool both_valid = valid[0] && valid[1];
+    for (int r = 0; r < 18; ++r) sm.acc64[r][tid] = 0.0;
+    float2 acc[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) acc[r] = f2(0.f);
+
+    int chunks = 0;
     for (int64_t c0 = q_begin; c0 < q_end; c0 += QC) {
       const int nc = static_cast<int>(q_end - c0 < QC ? q_end - c0 : QC);
-      __syncthreads();
-      for (int item = tid; item < nc * kTilesPerBlock; item += THREADS) {
-        const int jq = item / kTilesPerBlock, tt = item % kTilesPerBlock;
-        const double4 o = a.qs[c0 + jq];
-        const TileHeader& th = sm.th[tt];
-        const double dx = o.x - th.cx, dy = o.y - th.cy, dz = o.z - th.cz;
-        const double d2 = dx * dx + dy * dy + dz * dz;
-        sm.sl[jq][tt] = make_float4(static_cast<float>(dx * th.scale),
-                                    static_cast<float>(dy * th.scale),
-                                    static_cast<float>(dz * th.scale), d2 >= th.far_r2 ? 1.f : 0.f);
-        if (tt == 0) sm.sq[jq] = o;
+      __syncthreads();  // previous chunk's shared data fully consumed (and the headers landed)
+      for (int item = tid; item < QC * kFaTiles; item += kFaThreads) {
+        const int jq = item / kFaTiles, tt = item % kFaTiles;
+        if (jq < nc) {
+          const double4 o = a.qs[c0 + jq];
+          const TileHeader& th = sm.th[tt];
+          const double dx = o.x - th.cx, dy = o.y - th.cy, dz = o.z - th.cz;
+          const double d2 = dx * dx + dy * dy + dz * dz;
+          // Beyond 2^40 tile radii the tile's terms are below 2^-80 of a near one and
+          // squared FP32 distances could overflow: the tile is skipped for this query.
+          const bool skip = d2 * th.scale * th.scale > 1.2089258196146292e24;
+          sm.frame[jq][tt] = make_float4(static_cast<float>(dx * th.scale),
+                                         static_cast<float>(dy * th.scale),
+                                         static_cast<float>(dz * th.scale),
+                                         static_cast<float>(o.w * th.scale));
+          sm.flag[jq][tt] = skip ? 2 : (d2 >= th.far_r2 ? 0 : 1);
+          if (tt == 0) sm.q64[jq] = o;
+        }
       }
-      for (int e = tid; e < (THREADS / 32) * QC * 3; e += THREADS)
-        (&sm.red64[0][0][0])[e] = 0.0;
+      for (int e = tid; e < kFaTiles * QC * 3; e += kFaThreads) (&sm.red64[0][0][0])[e] = 0.0;
       __syncthreads();
+      static_assert(QC <= 32, "one mask bit per query of a chunk");
+      unsigned near0 = 0u, near1 = 0u;  // bit jq: the pair (query jq, face k) is refined
 #pragma unroll 1
       for (int jq = 0; jq < nc; ++jq) {
-        const float g = static_cast<float>(sm.sq[jq].w);
-        float2 dof[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-        double go[3] = {0.0, 0.0, 0.0};
-        bool refined = false;
-        const float4 l0 = sm.sl[jq][half], l1 = sm.sl[jq][2 + half];
-        const float2 ax = __fadd2_rn(fa[0], make_float2(-l0.x, -l1.x));
-        const float2 ay = __fadd2_rn(fa[1], make_float2(-l0.y, -l1.y));
-        const float2 az = __fadd2_rn(fa[2], make_float2(-l0.z, -l1.z));
-        const float2 aa = __ffma2_rn(ax, ax, __ffma2_rn(ay, ay, __fmul2_rn(az, az)));
-        const float2 s1 = __ffma2_rn(ax, fe1[0], __ffma2_rn(ay, fe1[1], __fmul2_rn(az, fe1[2])));
-        const float2 s2 = __ffma2_rn(ax, fe2[0], __ffma2_rn(ay, fe2[1], __fmul2_rn(az, fe2[2])));
-        const float2 ab = __fadd2_rn(aa, s1), ca = __fadd2_rn(aa, s2);
-        const float2 two = make_float2(2.f, 2.f);
-        const float2 bb = __ffma2_rn(two, s1, __fadd2_rn(aa, fg[0]));
-        const float2 cc = __ffma2_rn(two, s2, __fadd2_rn(aa, fg[1]));
-        const float2 bc = __fadd2_rn(ab, __fadd2_rn(s2, fg[2]));
-        const bool near0 = l0.w == 0.f && fminf(aa.x, fminf(bb.x, cc.x)) < thr[0];
-        const bool near1 = l1.w == 0.f && fminf(aa.y, fminf(bb.y, cc.y)) < thr[1];
-        if (!near0 && !near1 && both_valid) {
-          adj_far_pair2(g, ax, ay, az, fe1, fe2, aa, bb, cc, ab, bc, ca, nsc, acc, dof);
-        } else {
-#pragma unroll
-          for (int k = 0; k < 2; ++k) {
-            if (!valid[k]) continue;
-            if (k == 0 ? near0 : near1) {
-              refine_pair_grad(a.tri64, a.ld64, slot[k], sm.sq[jq], &sm.acc64[k][0][tid], THREADS,
-                               go);
-              refined = true;
-            } else {
-              adj_far_lane(g, lane_of(ax, k), lane_of(ay, k), lane_of(az, k), fe1, fe2, lane_of(aa, k),
-                           lane_of(bb, k), lane_of(cc, k), lane_of(ab, k), lane_of(bc, k), lane_of(ca, k),
-                           sc[k], k, acc, dof);
+        const float4 f = sm.frame[jq][warp];
+        const int flag = sm.flag[jq][warp];  // uniform over the warp
+        float2 d0 = f2(0.f), d1 = f2(0.f), d2 = f2(0.f);
+        if (flag != 2) {
+          const float2 ax = __fadd2_rn(fa[0], f2(-f.x));
+          const float2 ay = __fadd2_rn(fa[1], f2(-f.y));
+          const float2 az = __fadd2_rn(fa[2], f2(-f.z));
+          const float2 aa = __ffma2_rn(ax, ax, __ffma2_rn(ay, ay, __fmul2_rn(az, az)));
+          const float2 s1 = __ffma2_rn(ax, fe1[0], __ffma2_rn(ay, fe1[1], __fmul2_rn(az, fe1[2])));
+          const float2 s2 = __ffma2_rn(ax, fe2[0], __ffma2_rn(ay, fe2[1], __fmul2_rn(az, fe2[2])));
+          const float2 ab = __fadd2_rn(aa, s1), ca = __fadd2_rn(aa, s2);
+          const float2 bb = __ffma2_rn(f2(2.f), s1, __fadd2_rn(aa, fg[0]));
+          const float2 cc = __ffma2_rn(f2(2.f), s2, __fadd2_rn(aa, fg[1]));
+          const float2 bc = __fadd2_rn(ab, __fadd2_rn(s2, fg[2]));
+          const float2 ra = rsqrt2(aa), rb = rsqrt2(bb), rc = rsqrt2(cc);
+          const float2 la = __fmul2_rn(aa, ra), lb = __fmul2_rn(bb, rb), lc = __fmul2_rn(cc, rc);
+          const float2 iab = rcp2(__ffma2_rn(la, lb, ab));
+          const float2 ibc = rcp2(__ffma2_rn(lb, lc, bc));
+          const float2 ica = rcp2(__ffma2_rn(lc, la, ca));
+          const float2 g2 = f2(f.w);
+          const float2 gab = __fmul2_rn(g2, iab), gbc = __fmul2_rn(g2, ibc);
+          const float2 gca = __fmul2_rn(g2, ica);
+          float2 kA1 = __fmul2_rn(ra, gab), kA2 = __fmul2_rn(ra, gca);
+          float2 kB1 = __fmul2_rn(rb, gab), kB2 = __fmul2_rn(rb, gbc);
+          float2 kC1 = __fmul2_rn(rc, gbc), kC2 = __fmul2_rn(rc, gca);
+          if (flag == 1) {
+            // Careful visit: pairs with a vertex closer than kappa * h_face are
+            // refined in FP64 after the chunk; their FP32 terms are dropped here.
+            const float thr0 = lane < n ? __ldg(thr_rec) : -1.f;  // padding: never near
+            const float thr1 = lane + 32 < n ? __ldg(thr_rec + 16 * 32) : -1.f;
+            if (fminf(aa.x, fminf(bb.x, cc.x)) < thr0) {
+              near0 |= 1u << jq;
+              kA1.x = kA2.x = kB1.x = kB2.x = kC1.x = kC2.x = 0.f;
+            }
+            if (fminf(aa.y, fminf(bb.y, cc.y)) < thr1) {
+              near1 |= 1u << jq;
+              kA1.y = kA2.y = kB1.y = kB2.y = kC1.y = kC2.y = 0.f;
             }
           }
+          // a x b = a x e1, c x a = e2 x a, b x c = n - a x b - c x a.
+          const float2 xab0 = cross_c(ay, fe1[2], az, fe1[1]);
+          const float2 xab1 = cross_c(az, fe1[0], ax, fe1[2]);
+          const float2 xab2 = cross_c(ax, fe1[1], ay, fe1[0]);
+          const float2 xca0 = cross_c(fe2[1], az, fe2[2], ay);
+          const float2 xca1 = cross_c(fe2[2], ax, fe2[0], az);
+          const float2 xca2 = cross_c(fe2[0], ay, fe2[1], ax);
+          const float2 xbc0 = __fadd2_rn(__fadd2_rn(fn[0], make_float2(-xab0.x, -xab0.y)),
+                                         make_float2(-xca0.x, -xca0.y));
+          const float2 xbc1 = __fadd2_rn(__fadd2_rn(fn[1], make_float2(-xab1.x, -xab1.y)),
+                                         make_float2(-xca1.x, -xca1.y));
+          const float2 xbc2 = __fadd2_rn(__fadd2_rn(fn[2], make_float2(-xab2.x, -xab2.y)),
+                                         make_float2(-xca2.x, -xca2.y));
+          acc[0] = __ffma2_rn(kA1, xab0, __ffma2_rn(kA2, xca0, acc[0]));
+          acc[1] = __ffma2_rn(kA1, xab1, __ffma2_rn(kA2, xca1, acc[1]));
+          acc[2] = __ffma2_rn(kA1, xab2, __ffma2_rn(kA2, xca2, acc[2]));
+          acc[3] = __ffma2_rn(kB1, xab0, __ffma2_rn(kB2, xbc0, acc[3]));
+          acc[4] = __ffma2_rn(kB1, xab1, __ffma2_rn(kB2, xbc1, acc[4]));
+          acc[5] = __ffma2_rn(kB1, xab2, __ffma2_rn(kB2, xbc2, acc[5]));
+          acc[6] = __ffma2_rn(kC1, xbc0, __ffma2_rn(kC2, xca0, acc[6]));
+          acc[7] = __ffma2_rn(kC1, xbc1, __ffma2_rn(kC2, xca1, acc[7]));
+          acc[8] = __ffma2_rn(kC1, xbc2, __ffma2_rn(kC2, xca2, acc[8]));
+          const float2 sab = __fadd2_rn(kA1, kB1), sbc = __fadd2_rn(kB2, kC1);
+          const float2 sca = __fadd2_rn(kC2, kA2);
+          d0 = __ffma2_rn(sab, xab0, __ffma2_rn(sbc, xbc0, __fmul2_rn(sca, xca0)));
+          d1 = __ffma2_rn(sab, xab1, __ffma2_rn(sbc, xbc1, __fmul2_rn(sca, xca1)));
+          d2 = __ffma2_rn(sab, xab2, __ffma2_rn(sbc, xbc2, __fmul2_rn(sca, xca2)));
         }
-        const float dof0 = dof[0].x + dof[0].y, dof1 = dof[1].x + dof[1].y;
-        const float dof2 = dof[2].x + dof[2].y;
-        sm.dO32[jq][0][tid] = dof0;
-        sm.dO32[jq][1][tid] = dof1;
-        sm.dO32[jq][2][tid] = dof2;
-        // Refined pairs carry large, cancelling terms: reduce them in FP64.
-        if (__any_sync(0xffffffffu, refined)) {
-          for (int off = 16; off; off >>= 1) {
-            go[0] += __shfl_xor_sync(0xffffffffu, go[0], off);
-            go[1] += __shfl_xor_sync(0xffffffffu, go[1], off);
-            go[2] += __shfl_xor_sync(0xffffffffu, go[2], off);
-          }
-          if (lane == 0) {
-            sm.red64[warp][jq][0] = go[0];
-            sm.red64[warp][jq][1] = go[1];
-            sm.red64[warp][jq][2] = go[2];
-          }
+        sm.dO32[3 * jq][tid] = d0.x + d0.y;
+        sm.dO32[3 * jq + 1][tid] = d1.x + d1.y;
+        sm.dO32[3 * jq + 2][tid] = d2.x + d2.y;
+      }
+      // Near pairs in FP64, query by query with the warp's lanes in step; each
+      // query's FP64 dL/do shares are reduced over the warp in a fixed order.
+      for (unsigned pending = __reduce_or_sync(0xffffffffu, near0 | near1); pending;
+           pending &= pending - 1u) {
+        const int jq = __ffs(pending) - 1;
+        double go[3] = {0.0, 0.0, 0.0};
+        if ((near0 >> jq) & 1u)
+          refine_pair_grad(a.tri64, a.ld64, slot0, sm.q64[jq], &sm.acc64[0][tid], kFaThreads, go);
+        if ((near1 >> jq) & 1u)
+          refine_pair_grad(a.tri64, a.ld64, slot0 + 32, sm.q64[jq], &sm.acc64[9][tid],
+                           kFaThreads, go);
+        for (int off = 16; off; off >>= 1) {
+          go[0] += __shfl_xor_sync(0xffffffffu, go[0], off);
+          go[1] += __shfl_xor_sync(0xffffffffu, go[1], off);
+          go[2] += __shfl_xor_sync(0xffffffffu, go[2], off);
+        }
+        if (lane == 0) {
+          sm.red64[warp][jq][0] = go[0];
+          sm.red64[warp][jq][1] = go[1];
+          sm.red64[warp][jq][2] = go[2];
         }
       }
       __syncthreads();
-      // One warp per (query, component): FP32 shares summed in lane order, then the
-      // FP64 shares in warp order; then all threads add the sums into this CTA's row.
-      for (int e = warp; e < nc * 3; e += THREADS / 32) {
-        const int jq = e / 3, x = e % 3;
-        const float4 v4 = reinterpret_cast<const float4*>(&sm.dO32[jq][x][0])[lane];
-        float v = (v4.x + v4.y) + (v4.z + v4.w);
-        for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-        if (lane == 0) {
+      // Each (query, axis) row of 128 FP32 shares is summed by 4 lanes (32 shares each,
+      // in index order), the 4 partial sums by a fixed butterfly; the FP64 shares of
+      // refined pairs are added in warp order. Loop bounds are uniform per warp.
+      for (int base = 0; base + 8 * warp < QC * 3; base += kFaThreads / 4) {
+        const int row = base + (tid >> 2), part = tid & 3;
+        const float4* src = reinterpret_cast<const float4*>(&sm.dO32[row][32 * part]);
+        float4 s4 = src[0];
+#pragma unroll
+        for (int i = 1; i < 8; ++i) {
+          const float4 v = src[i];
+          s4.x += v.x;
+          s4.y += v.y;
+          s4.z += v.z;
+          s4.w += v.w;
+        }
+        float v = (s4.x + s4.y) + (s4.z + s4.w);
+        v += __shfl_xor_sync(0xffffffffu, v, 1);
+        v += __shfl_xor_sync(0xffffffffu, v, 2);
+        if (part == 0 && row < nc * 3) {
+          const int jq = row / 3, x = row % 3;
           double sum = static_cast<double>(v);
 #pragma unroll
-          for (int w = 0; w < THREADS / 32; ++w) sum += sm.red64[w][jq][x];
-          sm.dsum[e] = sum;
+          for (int w = 0; w < kFaTiles; ++w) sum += sm.red64[w][jq][x];
+          sm.dsum[row] = sum;
         }
       }
+      // FP32 face sums (minus g dOmega/dX, scale folded in) into FP64 every few chunks.
+      if (++chunks == kFaFlushChunks || c0 + QC >= q_end) {
+        chunks = 0;
 #pragma unroll
-      for (int r = 0; r < 9; ++r) {
-        sm.acc64[0][r][tid] += static_cast<double>(sc[0]) * static_cast<double>(acc[r].x);
-        sm.acc64[1][r][tid] += static_cast<double>(sc[1]) * static_cast<double>(acc[r].y);
-        acc[r] = make_float2(0.f, 0.f);
+        for (int r = 0; r < 9; ++r) {
+          sm.acc64[r][tid] -= static_cast<double>(acc[r].x);
+          sm.acc64[9 + r][tid] -= static_cast<double>(acc[r].y);
+          acc[r] = f2(0.f);
+        }
       }
       __syncthreads();
-      for (int e = tid; e < nc * 3; e += THREADS) dO_row[c0 * 3 + e] += sm.dsum[e];
+      for (int e = tid; e < nc * 3; e += kFaThreads) dO_row[c0 * 3 + e] += sm.dsum[e];
     }
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
-      if (!valid[k]) continue;
+      if (lane + 32 * k >= n) continue;
 #pragma unroll
       for (int r = 0; r < 9; ++r)
-        a.dF_part[(group * 9 + r) * a.ld64 + slot[k]] = sm.acc64[k][r][tid];
+        a.dF_part[(group * 9 + r) * a.ld64 + slot0 + 32 * k] = sm.acc64[9 * k + r][tid];
     }
   }
 }
@@ -700,7 +702,6 @@ __global__ void gather_vertex_kernel(const double* __restrict__ dtri, int64_t ld
 }
 
 constexpr int kAdjThreads = 128, kAdjFpt = 2, kAdjQc = 64;
-constexpr int kMixedAdjQc = 32;  // query chunk of the mixed adjoint (shared-memory budget)
 
 int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
@@ -721,6 +722,29 @@ AdjointPlan plan_waves(int64_t nblocks, int64_t nq, int64_t slots, int64_t qc) {
   const int64_t ngroups = std::max<int64_t>(1, std::min(max_groups, (2 * slots) / p.nranges));
   p.queries_per_group = cdiv(std::max<int64_t>(nq, 1), ngroups);
   p.ngroups = cdiv(std::max<int64_t>(nq, 1), p.queries_per_group);
+  return p;
+}
+
+// Like plan_waves, but the split between face ranges and query groups balances the
+// two partial arrays the split creates: nranges * nq * 3 doubles of dL/do partials
+// against ngroups * elem_doubles of per-element partials (elem_doubles = 9 * ld for
+// faces), for about two waves of `slots` resident CTAs.
+AdjointPlan plan_balanced(int64_t nblocks, int64_t nq, int64_t slots, int64_t qc,
+                          int64_t elem_doubles) {
+  AdjointPlan p;
+  nblocks = std::max<int64_t>(1, nblocks);
+  nq = std::max<int64_t>(1, nq);
+  const int64_t target = 2 * std::max<int64_t>(1, slots);
+  const double r = std::sqrt(static_cast<double>(target) * static_cast<double>(elem_doubles) /
+                             (3.0 * static_cast<double>(nq)));
+  const int64_t nranges =
+      std::max<int64_t>(1, std::min<int64_t>(std::min(nblocks, target), std::llround(r)));
+  p.blocks_per_range = cdiv(nblocks, nranges);
+  p.nranges = cdiv(nblocks, p.blocks_per_range);
+  const int64_t max_groups = std::max<int64_t>(1, std::min<int64_t>(cdiv(nq, qc), 65535));
+  const int64_t ngroups = std::max<int64_t>(1, std::min(max_groups, target / p.nranges));
+  p.queries_per_group = cdiv(nq, ngroups);
+  p.ngroups = cdiv(nq, p.queries_per_group);
   return p;
 }
 
@@ -814,11 +838,12 @@ cudaError_t adjoint_edges(const AdjointPlan& p, const double* edges, int64_t le,
 }
 
 AdjointPlan plan_adjoint_mixed(int64_t ntiles, int64_t nq, int sms) {
-  auto kernel = adjoint_mixed_kernel<2 * kTileFaces, kMixedAdjQc>;
-  const int smem = static_cast<int>(sizeof(MixedAdjointSmem<2 * kTileFaces, kMixedAdjQc>));
+  auto kernel = adjoint_faces_kernel<kFaQc>;
+  const int smem = static_cast<int>(sizeof(FaceAdjSmem<kFaQc>));
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  const int slots = resident_ctas(reinterpret_cast<const void*>(kernel), 2 * kTileFaces, smem, sms);
-  return plan_waves(cdiv(ntiles, 4), nq, slots, kMixedAdjQc);
+  const int slots = resident_ctas(reinterpret_cast<const void*>(kernel), kFaThreads, smem, sms);
+  return plan_balanced(cdiv(ntiles, kFaTiles), nq, slots, kFaQc,
+                       9 * std::max<int64_t>(ntiles, 1) * kTileFaces);
 }
 
 cudaError_t adjoint_mixed(const AdjointPlan& p, const MixedMesh& m, const double* q,
@@ -843,12 +868,12 @@ cudaError_t adjoint_mixed(const AdjointPlan& p, const MixedMesh& m, const double
       q, gw, perm, nq, qs);
   MixedAdjointArgs a{m.tiles, m.ntiles, m.tri64, m.ld64, qs, nq,
                      p.blocks_per_range, p.queries_per_group, dO_part, dF_part};
-  auto kernel = adjoint_mixed_kernel<2 * kTileFaces, kMixedAdjQc>;
-  const int smem = static_cast<int>(sizeof(MixedAdjointSmem<2 * kTileFaces, kMixedAdjQc>));
+  auto kernel = adjoint_faces_kernel<kFaQc>;
+  const int smem = static_cast<int>(sizeof(FaceAdjSmem<kFaQc>));
   e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  kernel<<<dim3(static_cast<unsigned>(p.nranges), static_cast<unsigned>(p.ngroups)),
-           2 * kTileFaces, smem, stream>>>(a);
+  kernel<<<dim3(static_cast<unsigned>(p.nranges), static_cast<unsigned>(p.ngroups)), kFaThreads,
+           smem, stream>>>(a);
   finish_dq_sorted_kernel<<<static_cast<unsigned>(cdiv(nq * 3, 256)), 256, 0, stream>>>(
       dO_part, p.nranges, nq, perm, dq);
   finish_dtri_sorted_kernel<<<static_cast<unsigned>(cdiv(9 * m.ld64, 256)), 256, 0, stream>>>(

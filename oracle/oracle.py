@@ -68,8 +68,15 @@ def lib() -> ctypes.CDLL:
         handle.mli_vertex_normals.restype = None
         handle.oracle_closest_point.argtypes = [ctypes.c_void_p] * 3
         handle.oracle_closest_point.restype = None
+        handle.oracle_isa.argtypes = []
+        handle.oracle_isa.restype = ctypes.c_int
         _handle = handle
     return _handle
+
+
+def isa() -> str:
+    """Vector ISA of the winding kernel's clone on this host (AVX-512 or AVX2)."""
+    return "AVX-512" if lib().oracle_isa() == 512 else "AVX2"
 
 
 def soa(V: np.ndarray, F: np.ndarray) -> np.ndarray:

@@ -68,21 +68,29 @@ inline double pair_angle(const double* tri, int64_t nf, int64_t fi, double ox, d
   return std::atan2(det, denom);
 }
 
-// capi.mojo:205-286
+// capi.mojo:205-286. Each W-wide group's (det, denom) terms are formed first and
+// their atan2 taken after, lane by lane: the same separately rounded operations as
+// one pair at a time, so every angle is the same, while the term loop can run as W
+// vector lanes. Multiversioned: the AVX-512 clone (W = 8 doubles per vector, the
+// reference's simd_width_of[float64] there) runs on hosts that have it, the build's
+// AVX2 baseline elsewhere; oracle_isa() says which one runs.
+__attribute__((target_clones("avx512f", "default")))
 double winding_one(const double* tri, double ox, double oy, double oz, int64_t nf) {
   double t[kL][kW];
   for (int l = 0; l < kL; ++l)
     for (int w = 0; w < kW; ++w) t[l][w] = 0.0;
+  double det[kW], den[kW];
+  auto group = [&](int64_t at, double* acc) {
+    for (int w = 0; w < kW; ++w) pair_terms(tri, nf, at + w, ox, oy, oz, &det[w], &den[w]);
+    for (int w = 0; w < kW; ++w) acc[w] += std::atan2(det[w], den[w]);
+  };
   int64_t fi = 0;
   while (fi + kL * kW <= nf) {  // capi.mojo:215-244
-    for (int l = 0; l < kL; ++l) {
-      const int64_t at = fi + l * kW;
-      for (int w = 0; w < kW; ++w) t[l][w] += pair_angle(tri, nf, at + w, ox, oy, oz);
-    }
+    for (int l = 0; l < kL; ++l) group(fi + l * kW, t[l]);
     fi += kL * kW;
   }
   while (fi + kW <= nf) {  // capi.mojo:245-264
-    for (int w = 0; w < kW; ++w) t[0][w] += pair_angle(tri, nf, fi + w, ox, oy, oz);
+    group(fi, t[0]);
     fi += kW;
   }
   // capi.mojo:265: ((totals + totals1) + (totals2 + totals3)).reduce_add()
@@ -130,6 +138,12 @@ void mli_arap_covariance_rims(int64_t, int64_t, int64_t, int64_t, int64_t, int64
 void mli_arap_rhs_rims(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t,
                        int64_t) {}
 void mli_arap_rotations(int64_t, int64_t, int64_t, int64_t, int64_t, int64_t) {}
+
+// Which clone of winding_one this host runs: 512 (AVX-512) or 256 (AVX2 baseline).
+int oracle_isa(void) {
+  __builtin_cpu_init();
+  return __builtin_cpu_supports("avx512f") ? 512 : 256;
+}
 
 // Oracle extras (no reference counterpart): per-pair term, exposed so tests can
 // compare single (det, denom, angle) triples bit-for-bit with the GPU kernel.

@@ -474,9 +474,12 @@ def gpu_arm(args):
         tri4, ld4, nf4 = wa.triangle_soa(V4d, F4d)
         mesh4 = wa.PreparedMesh(tri4, ld4, nf4)
 
-        def c4_fwd():
+        def c4_fwd_w():
             check(handle.wn_mixed_mesh_update(mesh4.mesh, tri4.data_ptr(), ld4, sp))
-            mesh4.forward(O4d)
+            return mesh4.forward(O4d)
+
+        def c4_fwd():
+            c4_fwd_w()
 
         def c4_faces():
             c4_fwd()
@@ -494,6 +497,38 @@ def gpu_arm(args):
               "fwd_ms": t4["fwd"] * 1e3,
               "fwdbwd_faces_ms": t4["faces"] * 1e3, "fwdbwd_edges_ms": t4["edges"] * 1e3,
               "ratio_faces": t4["faces"] / t4["fwd"], "ratio_edges": t4["edges"] / t4["fwd"]}
+        err4d = (c4_fwd_w() - wa.forward_fp64(tri4, ld4, nf4, O4d)).abs()
+        c4["max_abs_err_vs_fp64"] = float(err4d.max())
+        c4["p99_abs_err_vs_fp64"] = float(torch.quantile(err4d.float(), 0.99))
+        # The same queries as float32 (BASELINE's "float32 and float64 points"): the
+        # mixed forward and both adjoints take them as given; W's error is measured
+        # against the plain FP64 kernel at the rounded points, over every query.
+        O4f = O4d.to(torch.float32)
+        O4r = O4f.to(torch.float64)
+
+        def c4f_fwd():
+            check(handle.wn_mixed_mesh_update(mesh4.mesh, tri4.data_ptr(), ld4, sp))
+            return mesh4.forward(O4f)
+
+        def c4f_faces():
+            c4f_fwd()
+            dq4, dt4 = mesh4.backward(O4f, g4d)
+            wa.gather_vertices(dt4, ld4, nf4, F4d, len(V4))
+
+        def c4f_edges():
+            c4f_fwd()
+            wa.backward_edges(V4d, F4d, O4f, g4d)
+
+        t4f = {k: timed(fn, args.steps, 2)[0] for k, fn in
+               (("fwd", c4f_fwd), ("faces", c4f_faces), ("edges", c4f_edges))}
+        err4 = (c4f_fwd() - wa.forward_fp64(tri4, ld4, nf4, O4r)).abs()
+        c4["float32_queries"] = {
+            "fwd_ms": t4f["fwd"] * 1e3, "fwdbwd_faces_ms": t4f["faces"] * 1e3,
+            "fwdbwd_edges_ms": t4f["edges"] * 1e3,
+            "ratio_faces": t4f["faces"] / t4f["fwd"], "ratio_edges": t4f["edges"] / t4f["fwd"],
+            "max_abs_err_vs_fp64": float(err4.max()),
+            "p99_abs_err_vs_fp64": float(torch.quantile(err4.float(), 0.99)),
+            "queries_compared": len(O4)}
         mesh4.close()
 
     # fwd+bwd where the backward has work at the headline size: the c3 mesh with 8%

@@ -216,3 +216,31 @@ def test_large_fp64_forward_takes_the_prepared_mesh(gpu_required):
     W = wa.winding_number_torch(Vt, Ft, Ot, precision="fp64")
     tri, ld, nf = wa.triangle_soa(Vt, Ft)
     assert (W - wa.forward_fp64(tri, ld, nf, Ot)).abs().max().item() <= 1e-12
+
+
+def test_mixed_float32_queries_full_size_c4(gpu_required):
+    """Configuration 4 with float32 queries at full size (262,144 near-surface
+    points on the open 18,842-face mesh): the mixed forward against the plain FP64
+    kernel at the rounded points (<= 1e-6 over every query), and the mixed
+    per-face adjoint against the FP64 per-face adjoint there."""
+    import torch
+
+    V, F, O, _ = igl.synthetic.workload("c4_grad")
+    assert len(O) == 262144
+    g = np.random.default_rng(46).normal(size=len(O))
+    O32 = O.astype(np.float32)
+    Vt = _cuda(V).requires_grad_(True)
+    Ot = _cuda(O32).requires_grad_(True)
+    W = wa.winding_number_torch(Vt, _cuda(F), Ot, adjoint="faces")  # float32: mixed
+    assert W.dtype == torch.float32
+    (W * _cuda(g, torch.float32)).sum().backward()
+    Vr = _cuda(V).requires_grad_(True)
+    Or = _cuda(O32.astype(np.float64)).requires_grad_(True)
+    Wr = wa.winding_number_torch(Vr, _cuda(F), Or, precision="fp64", adjoint="faces")
+    (Wr * _cuda(g)).sum().backward()
+    assert float((W.double() - Wr).abs().max()) <= 1e-6
+    dV, dV64 = Vt.grad.cpu().numpy(), Vr.grad.cpu().numpy()
+    dO, dO64 = Ot.grad.double().cpu().numpy(), Or.grad.cpu().numpy()
+    assert np.isfinite(dV).all() and np.isfinite(dO).all()
+    assert np.abs(dV - dV64).max() <= 1e-4 * np.abs(dV64).max()
+    assert np.abs(dO - dO64).max() <= 1e-3 * np.abs(dO64).max()

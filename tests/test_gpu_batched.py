@@ -133,3 +133,55 @@ def test_meshes_without_faces_or_queries(gpu_required, oracle_mod):
         assert torch.count_nonzero(b.split(dV, "v")[2]) == 0  # no queries: no derivative
     finally:
         b.close()
+
+
+def _large_batch(seed=71, n=16, max_q=100_000):
+    """16 meshes including a subdivision-7 (327,680 F) and a subdivision-6 one,
+    0-10% faces deleted, queries log-uniform in [1024, 1e5], 50/50 box/near."""
+    rng = np.random.default_rng(seed)
+    levels = [7, 6] + [int(x) for x in rng.integers(2, 6, size=n - 2)]
+    meshes, queries = [], []
+    for i, level in enumerate(levels):
+        V, F = igl.synthetic.bumpy_icosphere(level, seed=700 + i)
+        F = igl.synthetic.delete_faces(F, float(rng.uniform(0, 0.1)), seed=800 + i)
+        nq = int(np.exp(rng.uniform(np.log(1024), np.log(max_q))))
+        meshes.append((V, F))
+        queries.append(igl.synthetic.mixed_queries(V, F, nq, seed=900 + i, near_sigma=1e-3))
+    return meshes, queries
+
+
+def test_full_scale_batch_forward_backward_graph(gpu_required):
+    """Configuration-5 scale: every query of every mesh against the plain FP64
+    kernel (<= 1e-6), the batched adjoint against the single-mesh boundary-edge
+    adjoint (<= 1e-12 relative), and a graph replay bit for bit equal to eager."""
+    import torch
+
+    meshes, queries = _large_batch()
+    assert max(len(F) for _, F in meshes) > 290_000
+    b = igl.batched.Batch(meshes, queries)
+    try:
+        b.gW.normal_(generator=torch.Generator(device="cuda").manual_seed(72))
+        b.step()
+        torch.cuda.synchronize()
+        eager = (b.W.clone(), b.dV.clone(), b.dQ.clone())
+        assert b.info()["work_items"] > len(meshes)
+        W = b.split(eager[0])
+        dVs, dQs, gs = b.split(eager[1], "v"), b.split(eager[2]), b.split(b.gW.clone())
+        for (V, F), O, w, dv, dq, g in zip(meshes, queries, W, dVs, dQs, gs):
+            Vt, Ft, Ot = (torch.from_numpy(x).cuda() for x in (V, F, O))
+            tri, ld, nf = wa.triangle_soa(Vt, Ft)
+            assert float((w - wa.forward_fp64(tri, ld, nf, Ot)).abs().max()) <= 1e-6
+            ref_v, ref_q = wa.backward_edges(Vt, Ft, Ot, g)
+            scale = max(float(ref_v.abs().max()), float(ref_q.abs().max()), 1e-30)
+            assert float((dv - ref_v).abs().max()) <= 1e-12 * scale
+            assert float((dq - ref_q).abs().max()) <= 1e-12 * scale
+        b.capture()
+        b.W.zero_()
+        b.dV.zero_()
+        b.dQ.zero_()
+        b.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(b.W, eager[0])
+        assert torch.equal(b.dV, eager[1]) and torch.equal(b.dQ, eager[2])
+    finally:
+        b.close()

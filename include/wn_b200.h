@@ -169,6 +169,10 @@ int wn_forward_mixed_device(void* mesh, const double* q, int64_t nq, double* w, 
 /* Re-prepare an existing mesh in place from new vertex positions (same face
  * count), e.g. once per step of a shape optimisation. */
 int wn_mixed_mesh_update(void* mesh, const double* tri, int64_t ld, void* stream);
+/* Faces per far test and angle product of the mixed forward on this mesh: 64
+ * (the default) or 32 (each half of a 64-face tile tested against its own ball
+ * and summed with its own product); same error bound either way. */
+int wn_mixed_mesh_set_tile_faces(void* mesh, int tile_faces);
 /* The two halves of wn_forward_mixed_device: Morton-order the queries into
  * perm (nq uint32, device), then evaluate the queries in that order. */
 int wn_mixed_sort_queries(const double* q, int64_t nq, uint32_t* perm, void* stream);
@@ -187,11 +191,13 @@ int wn_mixed_stats(int64_t* refined_pairs, int64_t* careful_visits, int reset);
  *   nv/nf/nq: host arrays of nmesh sizes; faces: host, total_nf x 3 int64,
  *   vertex indices local to each mesh (meshes concatenated in order).
  *   qpt: queries per thread (1, 2 or 4); target_pairs: pairs per work item;
- *   ctas_per_sm: persistent CTAs per SM (0 = as many as fit).
+ *   ctas_per_sm: persistent CTAs per SM (0 = as many as fit); tile_faces: faces
+ *   per far test and angle product, 64 or 32 (each half of a 64-face tile on its
+ *   own).
  *   V (total_nv x 3), q (total_nq x 3), w (total_nq): device, concatenated. */
 int wn_batch_create(int64_t nmesh, const int64_t* nv, const int64_t* nf, const int64_t* nq,
                     const int64_t* faces, double kappa, int qpt, int64_t target_pairs,
-                    int ctas_per_sm, void** batch_out);
+                    int ctas_per_sm, int tile_faces, void** batch_out);
 int wn_batch_forward(void* batch, const double* V, const double* q, double* w, void* stream);
 /* Adjoint of every mesh through its net boundary edges (FP64, persistent,
  * deterministic): gw (total_nq) -> dq (total_nq x 3), dV (total_nv x 3). Same
@@ -200,7 +206,7 @@ int wn_batch_backward(void* batch, const double* V, const double* q, const doubl
                       double* dq, double* dV, void* stream);
 /* out[0..n): nmesh, total_nv, total_nf, total_nq, total_tiles, work items,
  * persistent grid, partial sums, qpt, target_pairs, boundary edges, adjoint
- * work items. */
+ * work items, tile_faces. */
 int wn_batch_info(void* batch, int64_t* out, int64_t n);
 int wn_batch_destroy(void* batch);
 

@@ -310,12 +310,12 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_faces_kernel(const Mixe
     const unsigned char* rec = a.tiles + (tile_ok ? t : 0) * kTileBytes;
     const int n = tile_ok ? reinterpret_cast<const TileHeader*>(rec)->n : 0;
     float2 fa[3], fe1[3], fe2[3], fn[3], fg[3];
-    const float* thr_rec = reinterpret_cast<const float*>(rec + sizeof(TileHeader)) + 16 * lane + 15;
+    const float* thr_rec = reinterpret_cast<const float*>(rec + kTileHeaderBytes) + 16 * lane + 15;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int j = lane + 32 * k;
       const bool valid = j < n;
-      const float4* fr = reinterpret_cast<const float4*>(rec + sizeof(TileHeader)) + 4 * j;
+      const float4* fr = reinterpret_cast<const float4*>(rec + kTileHeaderBytes) + 4 * j;
       float4 r0 = make_float4(1e18f, 1e18f, 1e18f, 0.f), r1 = make_float4(0.f, 0.f, 0.f, 0.f);
       float4 r2 = r1, r3 = make_float4(0.f, 0.f, 0.f, -1.f);
       if (valid) {

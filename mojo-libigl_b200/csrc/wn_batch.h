@@ -32,6 +32,7 @@ struct BatchPlan {
   int64_t target_pairs = int64_t(1) << 23;  // pairs per work item
   int ctas_per_sm = 0;                      // 0 = as many as fit
   double kappa = 4.0;
+  int tile_faces = 64;                      // 64, or 32: far test and angle per half tile
 };
 
 struct BatchDevice;  // device buffers of the forward, defined in wn_mixed.cu

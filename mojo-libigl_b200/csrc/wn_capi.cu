@@ -628,6 +628,15 @@ int wn_mixed_mesh_update(void* mesh, const double* tri, int64_t ld, void* stream
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "mesh preparation");
 }
 
+int wn_mixed_mesh_set_tile_faces(void* mesh, int tile_faces) {
+  if (!mesh) return fail(WN_EINVAL, "null mesh");
+  if (tile_faces != kTileFaces && tile_faces != kHalfFaces)
+    return fail(WN_EINVAL, "tile_faces must be 64 or 32");
+  std::lock_guard<std::mutex> lock(g_mutex);
+  static_cast<MeshHandle*>(mesh)->m.tile_faces = tile_faces;
+  return WN_OK;
+}
+
 int wn_mixed_stats(int64_t* refined_pairs, int64_t* careful_visits, int reset) {
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
@@ -730,7 +739,7 @@ int wn_gather_vertex_grad_device(const double* dtri, int64_t ld, int corners,
 
 int wn_batch_create(int64_t nmesh, const int64_t* nv, const int64_t* nf, const int64_t* nq,
                     const int64_t* faces, double kappa, int qpt, int64_t target_pairs,
-                    int ctas_per_sm, void** batch_out) {
+                    int ctas_per_sm, int tile_faces, void** batch_out) {
   WN_NVTX_RANGE();
   if (!batch_out) return fail(WN_EINVAL, "null batch_out");
   *batch_out = nullptr;
@@ -754,11 +763,15 @@ int wn_batch_create(int64_t nmesh, const int64_t* nv, const int64_t* nf, const i
   if (int code = check_kappa(kappa)) return code;
   if (qpt != 1 && qpt != 2 && qpt != 4) return fail(WN_EINVAL, "qpt must be 1, 2 or 4");
   if (target_pairs < 1) return fail(WN_EINVAL, "target_pairs must be positive");
+  if (tile_faces != kTileFaces && tile_faces != kHalfFaces)
+    return fail(WN_EINVAL, "tile_faces must be 64 or 32");
+  if (ctas_per_sm < 0) return fail(WN_EINVAL, "ctas_per_sm must be >= 0");
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
   DeviceCtx* c = context(&code);
   if (!c) return code;
   BatchPlan plan;
+  plan.tile_faces = tile_faces;
   plan.qpt = qpt;
   plan.kappa = kappa;
   plan.target_pairs = target_pairs;
@@ -810,7 +823,7 @@ int wn_batch_info(void* batch, int64_t* out, int64_t n) {
   const int64_t vals[] = {b->nmesh,       b->total_nv,    b->total_nf, b->total_nq,
                           b->total_tiles, b->n_items,     b->grid,     b->total_partials,
                           b->plan.qpt,    b->plan.target_pairs,
-                          batch_boundary_edges(b), batch_edge_items(b)};
+                          batch_boundary_edges(b), batch_edge_items(b), b->plan.tile_faces};
   for (int64_t i = 0; i < n && i < static_cast<int64_t>(sizeof(vals) / sizeof(vals[0])); ++i)
     out[i] = vals[i];
   return WN_OK;

@@ -378,6 +378,36 @@ __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
   }
   const double h_face = valid ? sqrt(h2f) : 0.0;
 
+  // Half headers: warp w holds faces [32 w, 32 w + 32) of the sorted tile, i.e.
+  // half w. Centre of the half's vertex box, radius about it, longest edge.
+  static_assert(kHalfFaces == 32, "one warp per half tile");
+  {
+    double hlo[3], hhi[3], hc[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      hlo[x] = warp_min(valid ? fmin(v[x], fmin(v[3 + x], v[6 + x])) : INFINITY);
+      hhi[x] = warp_max(valid ? fmax(v[x], fmax(v[3 + x], v[6 + x])) : -INFINITY);
+      hc[x] = isfinite(hlo[x]) ? 0.5 * (hlo[x] + hhi[x]) : c[x];
+    }
+    double hr2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double dx = v[3 * k] - hc[0], dy = v[3 * k + 1] - hc[1], dz = v[3 * k + 2] - hc[2];
+      hr2 = fmax(hr2, dx * dx + dy * dy + dz * dz);
+    }
+    const double hr = warp_max(valid ? sqrt(hr2) : 0.0);
+    const double hh = warp_max(h_face);
+    if (lane == 0) {
+      HalfHeader* half = reinterpret_cast<HalfHeader*>(rec + sizeof(TileHeader));
+      const double far = ((hr + kappa * hh) * scale) * (1.0 + 1e-5) + 1e-5;
+      half->cx[warp] = static_cast<float>((hc[0] - c[0]) * scale);
+      half->cy[warp] = static_cast<float>((hc[1] - c[1]) * scale);
+      half->cz[warp] = static_cast<float>((hc[2] - c[2]) * scale);
+      half->far_r2[warp] = __double2float_ru(far * far);
+      for (int i = 0; i < 4; ++i) half->pad[4 * warp + i] = 0;
+    }
+  }
+
   FaceRec fr;
   const double ax = (v[0] - c[0]) * scale, ay = (v[1] - c[1]) * scale, az = (v[2] - c[2]) * scale;
   const double e1x = (v[3] - v[0]) * scale, e1y = (v[4] - v[1]) * scale,
@@ -403,7 +433,7 @@ __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
   // atan2(0, denom >= 0) = 0 exactly, and it never reaches rsqrt(0).
   const double thr = kappa * h_face * scale;
   fr.thr = (valid && h_face == 0.0) ? INFINITY : static_cast<float>(thr * thr);
-  reinterpret_cast<FaceRec*>(rec + sizeof(TileHeader))[j] = fr;
+  reinterpret_cast<FaceRec*>(rec + kTileHeaderBytes)[j] = fr;
 }
 
 struct MixedArgs {
@@ -455,101 +485,81 @@ __device__ __forceinline__ void pair_mul(const PairSq& p, float& zr, float& zi) 
   zi = ni;
 }
 
-// One 64-face tile against the QPT queries of this thread: FP32 argument-of-product
-// for far pairs, bit-exact FP64 terms + atan2 for near pairs, then the tile angle
-// added to the FP32 two-sum (hi, lo). `rec` is the tile record in shared memory,
-// `first` the tile's first slot in the sorted FP64 soup. Warp-collective (the fast
-// path is chosen by a vote over the warp), so every lane of the warp must call it.
+// Tile angle of one query, added with an FP32 two-sum (Knuth) into (hi, lo).
+__device__ __forceinline__ void add_tile_angle(float zr, float zi, float& hi, float& lo) {
+  const float ang = atan2f(zi, zr);
+  const float s = hi + ang;
+  const float bp = s - hi;
+  const float err = (hi - (s - bp)) + (ang - bp);
+  hi = s;
+  lo += err;
+}
+
+// Faces [j0, j1) of a tile against the QPT queries of this thread on the careful
+// path: FP32 argument-of-product for far pairs, bit-exact FP64 terms + atan2 for
+// near pairs, then the range's angle added to the FP32 two-sum (hi, lo). `fr` holds
+// the tile's face records, `first` is the tile's first slot in the sorted FP64
+// soup, (lx, ly, lz) the queries in the tile's frame, skip[k] marks a query for
+// which the tile is dropped (beyond 2^40 tile radii). Warp-collective.
 template <int QPT>
-__device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t first,
-                                           const double* __restrict__ tri64, int64_t ld64,
-                                           const double (&ox)[QPT], const double (&oy)[QPT],
-                                           const double (&oz)[QPT], const int64_t (&qidx)[QPT],
-                                           float (&hi)[QPT], float (&lo)[QPT],
-                                           double (&s64)[QPT], unsigned& refined,
-                                           unsigned& careful_tiles) {
-  const TileHeader& th = *reinterpret_cast<const TileHeader*>(rec);
-  const float4* fr = reinterpret_cast<const float4*>(rec + sizeof(TileHeader));
-  const int n = th.n;
-
-  float lx[QPT], ly[QPT], lz[QPT];
-  bool all_far = true;
-  bool skip[QPT];
-#pragma unroll
-  for (int k = 0; k < QPT; ++k) {
-    const double dx = ox[k] - th.cx, dy = oy[k] - th.cy, dz = oz[k] - th.cz;
-    const double d2 = dx * dx + dy * dy + dz * dz;
-    all_far &= (d2 >= th.far_r2) || qidx[k] < 0;
-    lx[k] = static_cast<float>(dx * th.scale);
-    ly[k] = static_cast<float>(dy * th.scale);
-    lz[k] = static_cast<float>(dz * th.scale);
-    // Beyond 2^40 tile radii the tile's solid angle is below 2^-80: it
-    // cannot change an FP32 sum, and squared distances could overflow.
-    skip[k] = d2 * th.scale * th.scale > 1.2089258196146292e24;
-    all_far &= !skip[k];
-  }
-  // The fast path: no lane has a near pair or a skipped tile.
-  all_far = __all_sync(0xffffffffu, all_far);
-
+__device__ __forceinline__ void careful_range(const float4* fr, int j0, int j1, int64_t first,
+                                              const double* __restrict__ tri64, int64_t ld64,
+                                              const double (&ox)[QPT], const double (&oy)[QPT],
+                                              const double (&oz)[QPT],
+                                              const int64_t (&qidx)[QPT],
+                                              const float (&lx)[QPT], const float (&ly)[QPT],
+                                              const float (&lz)[QPT], const bool (&skip)[QPT],
+                                              float (&hi)[QPT], float (&lo)[QPT],
+                                              double (&s64)[QPT], unsigned& refined) {
   float zr[QPT], zi[QPT];
 #pragma unroll
   for (int k = 0; k < QPT; ++k) {
     zr[k] = kZ0;
     zi[k] = 0.f;
   }
-
-  if (all_far) {
-#pragma unroll 2
-    for (int j = 0; j < n; ++j) {
-      const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2], r3 = fr[4 * j + 3];
+  // Near pairs are only marked here (bit j of near[k]; a tile has at most 64
+  // faces) and refined below with the warp's lanes in step, each taking its
+  // own next near face in ascending order, instead of the whole warp waiting
+  // on every face that any lane finds near.
+  static_assert(kTileFaces <= 64, "one bit per face of a tile");
+  unsigned long long near[QPT];
 #pragma unroll
-      for (int k = 0; k < QPT; ++k) pair_mul(pair_sq(r0, r1, r2, r3, lx[k], ly[k], lz[k]), zr[k], zi[k]);
-    }
-  } else {
-    ++careful_tiles;
-    // Near pairs are only marked here (bit j of near[k]; a tile has at most 64
-    // faces) and refined below with the warp's lanes in step, each taking its
-    // own next near face in ascending order, instead of the whole warp waiting
-    // on every face that any lane finds near.
-    static_assert(kTileFaces <= 64, "one bit per face of a tile");
-    unsigned long long near[QPT];
-#pragma unroll
-    for (int k = 0; k < QPT; ++k) near[k] = 0ull;
+  for (int k = 0; k < QPT; ++k) near[k] = 0ull;
 #pragma unroll 1
-    for (int j = 0; j < n; ++j) {
-      const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2], r3 = fr[4 * j + 3];
-#pragma unroll
-      for (int k = 0; k < QPT; ++k) {
-        const PairSq p = pair_sq(r0, r1, r2, r3, lx[k], ly[k], lz[k]);
-        if (fminf(p.aa, fminf(p.bb, p.cc)) < r3.w && qidx[k] >= 0)
-          near[k] |= 1ull << j;
-        else if (!skip[k])
-          pair_mul(p, zr[k], zi[k]);
-      }
-    }
-    // A query's refined pairs in this tile are multiplied into one FP64 running
-    // product (the argument-of-product sum of the FP64 kernels) whose argument
-    // is taken once; if it degenerates, the per-pair atan2 sum of the same faces.
+  for (int j = j0; j < j1; ++j) {
+    const float4 r0 = fr[4 * j], r1 = fr[4 * j + 1], r2 = fr[4 * j + 2], r3 = fr[4 * j + 3];
 #pragma unroll
     for (int k = 0; k < QPT; ++k) {
-      const unsigned long long marked = near[k];
-      ArgAcc acc;
-      argacc_init(acc);
-      while (__any_sync(0xffffffffu, near[k] != 0ull)) {
-        if (near[k] != 0ull) {
-          const int j = __ffsll(static_cast<long long>(near[k])) - 1;
-          near[k] &= near[k] - 1ull;
-          const double* f64 = tri64 + first + j;
-          const int64_t L = ld64;
-          double det, denom;
-          pair_terms_exact(ox[k], oy[k], oz[k], f64[0], f64[L], f64[2 * L], f64[3 * L],
-                           f64[4 * L], f64[5 * L], f64[6 * L], f64[7 * L], f64[8 * L], det,
-                           denom);
-          argacc_push(acc, denom, det);
-          ++refined;
-        }
+      const PairSq p = pair_sq(r0, r1, r2, r3, lx[k], ly[k], lz[k]);
+      if (fminf(p.aa, fminf(p.bb, p.cc)) < r3.w && qidx[k] >= 0)
+        near[k] |= 1ull << j;
+      else if (!skip[k])
+        pair_mul(p, zr[k], zi[k]);
+    }
+  }
+  // A query's refined pairs in this range are multiplied into one FP64 running
+  // product (the argument-of-product sum of the FP64 kernels) whose argument
+  // is taken once; if it degenerates, the per-pair atan2 sum of the same faces.
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    const unsigned long long marked = near[k];
+    ArgAcc acc;
+    argacc_init(acc);
+    while (__any_sync(0xffffffffu, near[k] != 0ull)) {
+      if (near[k] != 0ull) {
+        const int j = __ffsll(static_cast<long long>(near[k])) - 1;
+        near[k] &= near[k] - 1ull;
+        const double* f64 = tri64 + first + j;
+        const int64_t L = ld64;
+        double det, denom;
+        pair_terms_exact(ox[k], oy[k], oz[k], f64[0], f64[L], f64[2 * L], f64[3 * L],
+                         f64[4 * L], f64[5 * L], f64[6 * L], f64[7 * L], f64[8 * L], det,
+                         denom);
+        argacc_push(acc, denom, det);
+        ++refined;
       }
-      if (marked == 0ull) continue;
+    }
+    if (marked != 0ull) {
       if (!acc.bad) {
         s64[k] += atan2(acc.zi, acc.zr) + static_cast<double>(acc.k) * kTwoPi;
       } else {
@@ -564,16 +574,7 @@ __device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t fir
         }
       }
     }
-  }
-  // Tile angle, added with an FP32 two-sum (Knuth).
-#pragma unroll
-  for (int k = 0; k < QPT; ++k) {
-    const float ang = atan2f(zi[k], zr[k]);
-    const float s = hi[k] + ang;
-    const float bp = s - hi[k];
-    const float err = (hi[k] - (s - bp)) + (ang - bp);
-    hi[k] = s;
-    lo[k] += err;
+    add_tile_angle(zr[k], zi[k], hi[k], lo[k]);
   }
 }
 
@@ -584,10 +585,10 @@ __device__ __forceinline__ void mixed_tile(const unsigned char* rec, int64_t fir
 // transposed copy of the tile records supplies both faces' fields in adjacent
 // registers. Every per-face operation is the scalar path's, rounded the same
 // way per lane; each lane keeps its own running product (even faces, odd
-// faces), both started at 2^-50, and the two are multiplied once per tile.
+// faces), both started at 2^-50, and the two are multiplied once per range.
 // Each holds at most 32 factors of modulus in [3.8, 4.01], so both stay inside
 // [2^-50, 2^14.1] and their product inside [2^-100, 2^28.1], as the scalar
-// product does; the sum of the tile's angles is the same (< pi in magnitude).
+// product does; the sum of the range's angles is the same (< pi in magnitude).
 constexpr float kZ0Half = 8.8817841970012523e-16f;  // 2^-50
 constexpr int kPairFloats = 32;                     // one face pair, 16 fields x 2 lanes
 constexpr int kTileTransposedBytes = (kTileFaces / 2) * kPairFloats * 4;
@@ -595,7 +596,7 @@ constexpr int kTileTransposedBytes = (kTileFaces / 2) * kPairFloats * 4;
 // tbuf[32 p + 2 f + lane] = field f of face 2 p + lane, for the tile at `rec`.
 __device__ __forceinline__ void transpose_tile(const unsigned char* rec, float* tbuf, int tid,
                                                int threads) {
-  const float* src = reinterpret_cast<const float*>(rec + sizeof(TileHeader));
+  const float* src = reinterpret_cast<const float*>(rec + kTileHeaderBytes);
   for (int i = tid; i < kTileFaces * 16; i += threads) {
     const int j = i >> 4, f = i & 15;
     tbuf[kPairFloats * (j >> 1) + 2 * f + (j & 1)] = src[i];
@@ -640,35 +641,13 @@ __device__ __forceinline__ void pair2_mul(const float4* v, float2 nlx, float2 nl
   zi = ni;
 }
 
-// mixed_tile with the fast path on face pairs (tbuf: the transposed records
-// of the tile at `rec`); the careful path is mixed_tile's, on `rec`.
+// Faces [j0, j1) (j0 even) of a tile on the fast path: face pairs packed, an odd
+// last face on the scalar path, then the range's angle into (hi, lo).
 template <int QPT>
-__device__ __forceinline__ void mixed_tile_pairs(const unsigned char* rec, const float* tbuf,
-                                                 int64_t first, const double* __restrict__ tri64,
-                                                 int64_t ld64, const double (&ox)[QPT],
-                                                 const double (&oy)[QPT], const double (&oz)[QPT],
-                                                 const int64_t (&qidx)[QPT], float (&hi)[QPT],
-                                                 float (&lo)[QPT], double (&s64)[QPT],
-                                                 unsigned& refined, unsigned& careful_tiles) {
-  const TileHeader& th = *reinterpret_cast<const TileHeader*>(rec);
-  const int n = th.n;
-  bool all_far = true;
-  float lx[QPT], ly[QPT], lz[QPT];
-#pragma unroll
-  for (int k = 0; k < QPT; ++k) {
-    const double dx = ox[k] - th.cx, dy = oy[k] - th.cy, dz = oz[k] - th.cz;
-    const double d2 = dx * dx + dy * dy + dz * dz;
-    all_far &= (d2 >= th.far_r2) || qidx[k] < 0;
-    lx[k] = static_cast<float>(dx * th.scale);
-    ly[k] = static_cast<float>(dy * th.scale);
-    lz[k] = static_cast<float>(dz * th.scale);
-    all_far &= !(d2 * th.scale * th.scale > 1.2089258196146292e24);
-  }
-  if (!__all_sync(0xffffffffu, all_far)) {
-    mixed_tile<QPT>(rec, first, tri64, ld64, ox, oy, oz, qidx, hi, lo, s64, refined,
-                    careful_tiles);
-    return;
-  }
+__device__ __forceinline__ void packed_range(const float4* fr, const float* tbuf, int j0, int j1,
+                                             const float (&lx)[QPT], const float (&ly)[QPT],
+                                             const float (&lz)[QPT], float (&hi)[QPT],
+                                             float (&lo)[QPT]) {
   float2 zr2[QPT], zi2[QPT], nlx[QPT], nly[QPT], nlz[QPT];
 #pragma unroll
   for (int k = 0; k < QPT; ++k) {
@@ -678,34 +657,96 @@ __device__ __forceinline__ void mixed_tile_pairs(const unsigned char* rec, const
     nly[k] = make_float2(-ly[k], -ly[k]);
     nlz[k] = make_float2(-lz[k], -lz[k]);
   }
-  const int npairs = n >> 1;
+  const int p1 = j1 >> 1;
 #pragma unroll 2
-  for (int p = 0; p < npairs; ++p) {
+  for (int p = j0 >> 1; p < p1; ++p) {
     const float4* v = reinterpret_cast<const float4*>(tbuf + kPairFloats * p);
 #pragma unroll
     for (int k = 0; k < QPT; ++k) pair2_mul(v, nlx[k], nly[k], nlz[k], zr2[k], zi2[k]);
   }
-  const float4* fr = reinterpret_cast<const float4*>(rec + sizeof(TileHeader));
 #pragma unroll
   for (int k = 0; k < QPT; ++k) {
     float zr = zr2[k].x * zr2[k].y - zi2[k].x * zi2[k].y;
     float zi = zr2[k].x * zi2[k].y + zi2[k].x * zr2[k].y;
-    if (n & 1) {  // the odd last face, on the scalar path
-      const int j = n - 1;
+    if (j1 & 1) {  // the odd last face, on the scalar path
+      const int j = j1 - 1;
       pair_mul(pair_sq(fr[4 * j], fr[4 * j + 1], fr[4 * j + 2], fr[4 * j + 3], lx[k], ly[k],
                        lz[k]),
                zr, zi);
     }
-    const float ang = atan2f(zi, zr);
-    const float s = hi[k] + ang;
-    const float bp = s - hi[k];
-    const float err = (hi[k] - (s - bp)) + (ang - bp);
-    hi[k] = s;
-    lo[k] += err;
+    add_tile_angle(zr, zi, hi[k], lo[k]);
   }
 }
 
-template <int THREADS, int QPT, int STAGES>
+// One tile against the QPT queries of this thread (tbuf: the face-pair transposed
+// records of the tile at `rec`). Warps whose queries all lie outside the tile's
+// ball B(c, r + kappa h_tile) take the packed fast path over the whole tile;
+// otherwise, with HALF, each 32-face half is tested against its own ball and
+// takes the fast or the careful path on its own, and without HALF the whole
+// tile takes the careful path. One angle per (query, range) goes into (hi, lo).
+// Warp-collective: every lane of the warp must call it.
+template <int QPT, bool HALF>
+__device__ __forceinline__ void mixed_tile_pairs(const unsigned char* rec, const float* tbuf,
+                                                 int64_t first, const double* __restrict__ tri64,
+                                                 int64_t ld64, const double (&ox)[QPT],
+                                                 const double (&oy)[QPT], const double (&oz)[QPT],
+                                                 const int64_t (&qidx)[QPT], float (&hi)[QPT],
+                                                 float (&lo)[QPT], double (&s64)[QPT],
+                                                 unsigned& refined, unsigned& careful_tiles) {
+  const TileHeader& th = *reinterpret_cast<const TileHeader*>(rec);
+  const float4* fr = reinterpret_cast<const float4*>(rec + kTileHeaderBytes);
+  const int n = th.n;
+  bool all_far = true;
+  float lx[QPT], ly[QPT], lz[QPT];
+  bool skip[QPT];
+#pragma unroll
+  for (int k = 0; k < QPT; ++k) {
+    const double dx = ox[k] - th.cx, dy = oy[k] - th.cy, dz = oz[k] - th.cz;
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    all_far &= (d2 >= th.far_r2) || qidx[k] < 0;
+    lx[k] = static_cast<float>(dx * th.scale);
+    ly[k] = static_cast<float>(dy * th.scale);
+    lz[k] = static_cast<float>(dz * th.scale);
+    // Beyond 2^40 tile radii the tile's solid angle is below 2^-80: it
+    // cannot change an FP32 sum, and squared distances could overflow.
+    skip[k] = d2 * th.scale * th.scale > 1.2089258196146292e24;
+    all_far &= !skip[k];
+  }
+  if (__all_sync(0xffffffffu, all_far)) {
+    packed_range<QPT>(fr, tbuf, 0, n, lx, ly, lz, hi, lo);
+    return;
+  }
+  if constexpr (!HALF) {
+    ++careful_tiles;
+    careful_range<QPT>(fr, 0, n, first, tri64, ld64, ox, oy, oz, qidx, lx, ly, lz, skip, hi, lo,
+                       s64, refined);
+  } else {
+    const HalfHeader& hh = *reinterpret_cast<const HalfHeader*>(rec + sizeof(TileHeader));
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+      const int j0 = h * kHalfFaces, j1 = min(n, j0 + kHalfFaces);
+      if (j0 >= j1) break;
+      // Far test against the half's ball in the tile's FP32 frame; the stored
+      // radius is inflated beyond the frame's rounding, so "far" stays exact.
+      bool far_h = true;
+#pragma unroll
+      for (int k = 0; k < QPT; ++k) {
+        const float dx = lx[k] - hh.cx[h], dy = ly[k] - hh.cy[h], dz = lz[k] - hh.cz[h];
+        far_h &= (fmaf(dx, dx, fmaf(dy, dy, dz * dz)) >= hh.far_r2[h] && !skip[k]) ||
+                 qidx[k] < 0;
+      }
+      if (__all_sync(0xffffffffu, far_h)) {
+        packed_range<QPT>(fr, tbuf, j0, j1, lx, ly, lz, hi, lo);
+      } else {
+        ++careful_tiles;
+        careful_range<QPT>(fr, j0, j1, first, tri64, ld64, ox, oy, oz, qidx, lx, ly, lz, skip,
+                           hi, lo, s64, refined);
+      }
+    }
+  }
+}
+
+template <int THREADS, int QPT, int STAGES, bool HALF>
 __global__ void __launch_bounds__(THREADS, 4) mixed_forward_kernel(const MixedArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* ring = smem_raw;  // [STAGES][kTileBytes]
@@ -768,7 +809,7 @@ __global__ void __launch_bounds__(THREADS, 4) mixed_forward_kernel(const MixedAr
       break;
     }
     if (tid == 0 && t >= 1 && issued < ntiles) issue(issued++);
-    mixed_tile_pairs<QPT>(ring + slot * kTileBytes, tb, (t_begin + t) * kTileFaces, a.tri64,
+    mixed_tile_pairs<QPT, HALF>(ring + slot * kTileBytes, tb, (t_begin + t) * kTileFaces, a.tri64,
                           a.ld64, ox, oy, oz, qidx, hi, lo, s64, refined, careful_tiles);
   }
 
@@ -808,9 +849,9 @@ __global__ void sum_partials_kernel(const double* __restrict__ partial, int64_t 
 
 constexpr int kMixedThreads = 128, kMixedQpt = 2, kMixedStages = 4;
 
-template <int THREADS, int QPT, int STAGES>
+template <int THREADS, int QPT, int STAGES, bool HALF>
 cudaError_t launch_mixed_variant(const MixedArgs& a, int64_t nsplit, cudaStream_t stream) {
-  auto kernel = mixed_forward_kernel<THREADS, QPT, STAGES>;
+  auto kernel = mixed_forward_kernel<THREADS, QPT, STAGES, HALF>;
   const size_t smem = static_cast<size_t>(STAGES) * kTileBytes + sizeof(uint64_t) * STAGES +
                       2 * kTileTransposedBytes;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -921,7 +962,11 @@ cudaError_t mixed_forward_sorted(const MixedMesh& m, const double* q, const uint
   MixedArgs a{m.tiles, m.ntiles, m.tri64, m.ld64, q, perm, nq, w, partial,
               split.tiles_per_split, stats, err};
   cudaError_t e =
-      launch_mixed_variant<kMixedThreads, kMixedQpt, kMixedStages>(a, split.nsplit, stream);
+      m.tile_faces == kHalfFaces
+          ? launch_mixed_variant<kMixedThreads, kMixedQpt, kMixedStages, true>(a, split.nsplit,
+                                                                               stream)
+          : launch_mixed_variant<kMixedThreads, kMixedQpt, kMixedStages, false>(a, split.nsplit,
+                                                                                stream);
   if (e != cudaSuccess || split.nsplit == 1) return e;
   sum_partials_kernel<<<static_cast<unsigned>(blocks_for(nq, 256)), 256, 0, stream>>>(
       partial, split.nsplit, nq, w);
@@ -1093,7 +1138,7 @@ struct BatchArgs {
   int* err;
 };
 
-template <int THREADS, int QPT, int STAGES>
+template <int THREADS, int QPT, int STAGES, bool HALF>
 __global__ void __launch_bounds__(THREADS, QPT == 1 ? 6 : (QPT == 2 ? 4 : 3))
     batch_forward_kernel(const BatchArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1159,7 +1204,8 @@ __global__ void __launch_bounds__(THREADS, QPT == 1 ? 6 : (QPT == 2 ? 4 : 3))
         break;
       }
       if (tid == 0 && u >= 1 && issued < nt) issue(issued++);
-      mixed_tile_pairs<QPT>(ring + slot * kTileBytes, tb, (it.t_begin + u) * kTileFaces, a.tri64,
+      mixed_tile_pairs<QPT, HALF>(ring + slot * kTileBytes, tb, (it.t_begin + u) * kTileFaces,
+                                  a.tri64,
                             a.ld64, ox, oy, oz, qidx, hi, lo, s64, refined, careful_tiles);
     }
     if (failed) {
@@ -1204,10 +1250,10 @@ __global__ void batch_finish_kernel(const double* __restrict__ partial,
   w[perm[s]] = sum / kTwoPi;
 }
 
-template <int QPT>
+template <int QPT, bool HALF>
 cudaError_t launch_batch_variant(const BatchArgs& a, int grid, cudaStream_t stream) {
   constexpr int kThreads = 128, kStages = 4;
-  auto kernel = batch_forward_kernel<kThreads, QPT, kStages>;
+  auto kernel = batch_forward_kernel<kThreads, QPT, kStages, HALF>;
   const size_t smem = static_cast<size_t>(kStages) * kTileBytes + sizeof(uint64_t) * kStages +
                       2 * kTileTransposedBytes;
   cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1218,15 +1264,16 @@ cudaError_t launch_batch_variant(const BatchArgs& a, int grid, cudaStream_t stre
   return cudaGetLastError();
 }
 
-template <int QPT>
+template <int QPT, bool HALF>
 int batch_grid(int sms, int ctas_per_sm) {
   constexpr int kThreads = 128, kStages = 4;
   const size_t smem = static_cast<size_t>(kStages) * kTileBytes + sizeof(uint64_t) * kStages +
                       2 * kTileTransposedBytes;
   int per_sm = 0;
-  cudaFuncSetAttribute(batch_forward_kernel<kThreads, QPT, kStages>,
+  cudaFuncSetAttribute(batch_forward_kernel<kThreads, QPT, kStages, HALF>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_forward_kernel<kThreads, QPT, kStages>,
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
+                                                batch_forward_kernel<kThreads, QPT, kStages, HALF>,
                                                 kThreads, smem);
   if (ctas_per_sm > 0) per_sm = std::min(per_sm, ctas_per_sm);
   return std::max(1, per_sm) * std::max(1, sms);
@@ -1386,9 +1433,18 @@ cudaError_t batch_create(BatchState* b, int64_t nmesh, const int64_t* nv, const 
                       cudaMemcpyHostToDevice)) != cudaSuccess)
     return e;
   switch (plan.qpt) {
-    case 1: b->grid = batch_grid<1>(sms, plan.ctas_per_sm); break;
-    case 4: b->grid = batch_grid<4>(sms, plan.ctas_per_sm); break;
-    default: b->grid = batch_grid<2>(sms, plan.ctas_per_sm); break;
+    case 1:
+      b->grid = plan.tile_faces == kHalfFaces ? batch_grid<1, true>(sms, plan.ctas_per_sm)
+                                              : batch_grid<1, false>(sms, plan.ctas_per_sm);
+      break;
+    case 4:
+      b->grid = plan.tile_faces == kHalfFaces ? batch_grid<4, true>(sms, plan.ctas_per_sm)
+                                              : batch_grid<4, false>(sms, plan.ctas_per_sm);
+      break;
+    default:
+      b->grid = plan.tile_faces == kHalfFaces ? batch_grid<2, true>(sms, plan.ctas_per_sm)
+                                              : batch_grid<2, false>(sms, plan.ctas_per_sm);
+      break;
   }
   b->grid = static_cast<int>(std::min<int64_t>(b->grid, std::max<int64_t>(b->n_items, 1)));
   return cudaGetLastError();
@@ -1452,10 +1508,20 @@ cudaError_t batch_forward(BatchState* b, const double* V, const double* q, doubl
   BatchArgs a{d->mesh.tiles, d->mesh.tri64, d->mesh.ld64, q,     d->perm, d->items,
               b->n_items,    d->counter,    d->partial,   stats, err};
   if (b->n_items > 0) {
+    const bool half = b->plan.tile_faces == kHalfFaces;
     switch (b->plan.qpt) {
-      case 1: e = launch_batch_variant<1>(a, b->grid, stream); break;
-      case 4: e = launch_batch_variant<4>(a, b->grid, stream); break;
-      default: e = launch_batch_variant<2>(a, b->grid, stream); break;
+      case 1:
+        e = half ? launch_batch_variant<1, true>(a, b->grid, stream)
+                 : launch_batch_variant<1, false>(a, b->grid, stream);
+        break;
+      case 4:
+        e = half ? launch_batch_variant<4, true>(a, b->grid, stream)
+                 : launch_batch_variant<4, false>(a, b->grid, stream);
+        break;
+      default:
+        e = half ? launch_batch_variant<2, true>(a, b->grid, stream)
+                 : launch_batch_variant<2, false>(a, b->grid, stream);
+        break;
     }
     if (e != cudaSuccess) return e;
   }

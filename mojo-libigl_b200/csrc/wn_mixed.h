@@ -22,6 +22,22 @@ struct TileHeader {
 };
 static_assert(sizeof(TileHeader) == 64, "tile header is 64 bytes");
 
+// Second 64-byte header: the tile's two 32-face halves (faces [0, 32) and
+// [32, 64) of the tile), for kernels that test and sum each half on its own. In
+// the tile's scaled FP32 frame: the centre of each half's vertex bounding box
+// relative to the tile centre, and (r_half + kappa*h_half)^2 with the radius
+// inflated past the frame's FP32 rounding (relative 1e-5 plus 1e-5), so a
+// query tested "far" in FP32 has no near pair in that half.
+struct HalfHeader {
+  float cx[2], cy[2], cz[2];
+  float far_r2[2];
+  int32_t pad[8];
+};
+static_assert(sizeof(HalfHeader) == 64, "half header is 64 bytes");
+
+constexpr int kHalfFaces = kTileFaces / 2;
+constexpr int kTileHeaderBytes = static_cast<int>(sizeof(TileHeader) + sizeof(HalfHeader));
+
 // 64-byte face record, FP32 tile-local scaled coordinates. With a = A - o the
 // pair needs |a|^2, a.e1, a.e2 and a.n only: b = a + e1 and c = a + e2 give
 // |b|^2 = |a|^2 + 2 a.e1 + |e1|^2, a.b = |a|^2 + a.e1, b.c = a.b + a.e2 + e1.e2, ...
@@ -35,7 +51,7 @@ struct FaceRec {
 };
 static_assert(sizeof(FaceRec) == 64, "face record is 64 bytes");
 
-constexpr int kTileBytes = static_cast<int>(sizeof(TileHeader) + kTileFaces * sizeof(FaceRec));
+constexpr int kTileBytes = static_cast<int>(kTileHeaderBytes + kTileFaces * sizeof(FaceRec));
 static_assert(kTileBytes % 16 == 0, "bulk copies move multiples of 16 bytes");
 
 // A prepared mesh. All pointers are device memory owned by the caller.
@@ -45,6 +61,8 @@ struct MixedMesh {
   unsigned char* tiles = nullptr;  // ntiles * kTileBytes, 16-byte aligned
   double* tri64 = nullptr;         // 9 x ld64 sorted FP64 soup (ld64 = ntiles*kTileFaces)
   uint32_t* face_of = nullptr;     // ld64: sorted slot -> input face (0xffffffff = padding)
+  int tile_faces = 64;             // faces per far test and angle product of the mixed
+                                   // forward: 64, or 32 (each half tile on its own)
   uint8_t* reuse = nullptr;        // ld64: corner-slot code of the FP64 kernel per face
                                    // (s0 + 3 s1 + 9 s2 + 27 new-mask; 0xff = padding).
                                    // May be null.

@@ -63,6 +63,7 @@ _WN_SIGNATURES = {
     "wn_forward_mixed_host": ([P, P, P, I, I, ctypes.c_double], C_INT),
     "wn_mixed_mesh_create": ([P, I, I, ctypes.c_double, P, ctypes.POINTER(P)], C_INT),
     "wn_mixed_mesh_destroy": ([P], C_INT),
+    "wn_mixed_mesh_set_tile_faces": ([P, C_INT], C_INT),
     "wn_forward_fp64_mesh_device": ([P, P, I, P, P], C_INT),
     "wn_forward_mixed_device": ([P, P, I, P, P], C_INT),
     "wn_mixed_mesh_update": ([P, P, I, P], C_INT),
@@ -72,8 +73,8 @@ _WN_SIGNATURES = {
     "wn_backward_fp64_device": ([P, I, I, P, I, P, P, P, P], C_INT),
     "wn_gather_vertex_grad_device": ([P, I, C_INT, P, P, I, P, P], C_INT),
     "wn_backward_edges_device": ([P, I, I, P, I, P, P, P, P], C_INT),
-    "wn_batch_create": ([I, P, P, P, P, ctypes.c_double, C_INT, I, C_INT, ctypes.POINTER(P)],
-                        C_INT),
+    "wn_batch_create": ([I, P, P, P, P, ctypes.c_double, C_INT, I, C_INT, C_INT,
+                         ctypes.POINTER(P)], C_INT),
     "wn_batch_forward": ([P, P, P, P, P], C_INT),
     "wn_batch_backward": ([P, P, P, P, P, P, P], C_INT),
     "wn_batch_info": ([P, P, I], C_INT),

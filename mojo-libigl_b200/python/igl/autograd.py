@@ -7,10 +7,14 @@ dL/dO through the library's hand-written adjoints. Pair terms are recomputed
 adjoint="faces": per-face sums over the queries (``wn_backward_fp64_device`` or,
 for precision="mixed", ``wn_backward_mixed_device``), then dL/dV gathered from
 the per-corner face gradients through a vertex -> (face, corner) list.
-adjoint="edges" (default): the same derivative from the mesh's net boundary
-edges only (``wn_backward_edges_device``): the per-face terms of a directed side
-and of its reverse cancel at both endpoints, so interior edges contribute
-nothing (exactly zero for a closed, consistently oriented mesh).
+adjoint="edges": the same derivative from the mesh's net boundary edges only
+(``wn_backward_edges_device``): the per-face terms of a directed side and of its
+reverse cancel at both endpoints, so interior edges contribute nothing (exactly
+zero for a closed, consistently oriented mesh).
+adjoint="auto" (default): "edges", except for a mixed-precision forward on a
+mesh with more net boundary edges than EDGE_FACE_RATIO times its faces (a
+triangle soup has three per face), where the per-face mixed adjoint costs less
+than the FP64 boundary-edge one.
 
 Tensors are plumbing here: the forward and the adjoints run in libwn_b200's
 kernels on the tensors' memory and current stream.
@@ -23,6 +27,11 @@ import ctypes
 import torch
 
 from . import _lib
+
+
+# Above this many net boundary edges per face the per-face mixed adjoint is
+# cheaper than the FP64 boundary-edge adjoint.
+EDGE_FACE_RATIO = 1.0
 
 
 def _check(rc: int) -> None:
@@ -174,13 +183,14 @@ def boundary_edges(V: torch.Tensor, F: torch.Tensor):
     return edges, ne, ends
 
 
-def backward_edges(V, F, O, gW):
-    """(dL/dV, dL/dO) from the net boundary edges (FP64)."""
+def backward_edges(V, F, O, gW, edges=None):
+    """(dL/dV, dL/dO) from the net boundary edges (FP64); `edges` is
+    boundary_edges(V, F) when the caller has it already."""
     handle = _lib.lib()
     q = O.to(torch.float64).contiguous()
     gw = gW.to(torch.float64).contiguous()
     nq, nv = q.shape[0], V.shape[0]
-    edges, ne, ends = boundary_edges(V, F)
+    edges, ne, ends = edges if edges is not None else boundary_edges(V, F)
     le = edges.shape[1]
     dq = torch.empty((nq, 3), dtype=torch.float64, device=q.device)
     dedge = torch.zeros((6, le), dtype=torch.float64, device=q.device)
@@ -214,7 +224,7 @@ class WindingNumberFunction(torch.autograd.Function):
         if precision == "mixed":
             mesh = PreparedMesh(tri, ld, nf)
             w = mesh.forward(O)
-            if adjoint == "faces":
+            if adjoint in ("faces", "auto"):
                 ctx.mesh = mesh
             else:
                 mesh.close()
@@ -229,8 +239,17 @@ class WindingNumberFunction(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gW):
         V, F, O = ctx.saved_tensors
-        if ctx.adjoint == "edges":
-            dV, dq = backward_edges(V, F, O, gW)
+        adjoint = ctx.adjoint
+        edges = None
+        if adjoint == "auto":
+            edges = boundary_edges(V, F)
+            use_faces = ctx.mesh is not None and edges[1] > EDGE_FACE_RATIO * ctx.nf
+            adjoint = "faces" if use_faces else "edges"
+            if not use_faces and ctx.mesh is not None:
+                ctx.mesh.close()
+                ctx.mesh = None
+        if adjoint == "edges":
+            dV, dq = backward_edges(V, F, O, gW, edges)
         elif ctx.mesh is not None:
             dq, dtri = ctx.mesh.backward(O, gW)
             dV = gather_vertices(dtri, ctx.ld, ctx.nf, F, V.shape[0])
@@ -241,14 +260,16 @@ class WindingNumberFunction(torch.autograd.Function):
 
 
 def winding_number_torch(V: torch.Tensor, F: torch.Tensor, O: torch.Tensor,
-                         precision: str | None = None, adjoint: str = "edges") -> torch.Tensor:
+                         precision: str | None = None, adjoint: str = "auto") -> torch.Tensor:
     """Differentiable W for CUDA tensors V (nv,3), F (nf,3) int, O (nq,3).
 
     precision: "fp64" (plain FP64 forward and adjoint) or "mixed" (FP32 pairs with
     FP64 refinement of near-surface pairs, forward and adjoint); by default
     "mixed" for float32 queries and "fp64" otherwise. W has the dtype of O.
-    adjoint: "edges" (net boundary edges, FP64) or "faces" (per-face reduction,
-    in the forward's precision); both give the same derivative.
+    adjoint: "edges" (net boundary edges, FP64), "faces" (per-face reduction,
+    in the forward's precision) or "auto" (edges, or faces for a mixed forward on
+    a mesh with many boundary edges, e.g. a triangle soup); all give the same
+    derivative.
     """
     if precision is None:
         precision = "mixed" if O.dtype == torch.float32 else "fp64"
@@ -256,6 +277,6 @@ def winding_number_torch(V: torch.Tensor, F: torch.Tensor, O: torch.Tensor,
         raise RuntimeError("winding_number_torch needs CUDA tensors (no CPU fallback)")
     if precision not in ("fp64", "mixed"):
         raise ValueError("precision must be 'fp64' or 'mixed'")
-    if adjoint not in ("edges", "faces"):
-        raise ValueError("adjoint must be 'edges' or 'faces'")
+    if adjoint not in ("edges", "faces", "auto"):
+        raise ValueError("adjoint must be 'edges', 'faces' or 'auto'")
     return WindingNumberFunction.apply(V, F, O, precision, adjoint)

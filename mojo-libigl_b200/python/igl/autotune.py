@@ -1,14 +1,19 @@
-"""Autotuner for the batched launch: queries per thread, work-item size,
-persistent CTAs per SM and the refinement radius kappa.
+"""Autotuner for the batched launch: the tile shape (faces per tile, queries per
+thread), the work-item size, persistent CTAs per SM and the refinement radius
+kappa.
 
-``tune(meshes, queries)`` times every candidate on a query subsample of the
-batch (at most ``sample_queries`` per mesh, so a candidate costs tens of ms),
+``tune(meshes, queries)`` times candidates on a query subsample of the batch
+(at most ``sample_queries`` per mesh, so a candidate costs tens of ms),
 forward + backward by default, with CUDA events after a warm-up, and returns
-the fastest configuration. Results are cached in a JSON file keyed by GPU name,
-mesh count and size buckets: ``$WN_AUTOTUNE_CACHE`` or
-``~/.cache/wn_b200/autotune.json``. kappa only ranges over values whose error
-bound holds (>= 3; see wn_mixed.cu), so the choice trades speed, not accuracy
-beyond the tested bound.
+the fastest configuration. The search is a coordinate descent from the default
+configuration: each dimension in turn is swept with the others fixed at the
+best so far, and the sweep repeats until a full pass changes nothing (at most
+``passes`` times); ``search="grid"`` times the whole product instead. Results
+are cached in a JSON file keyed by GPU name, mesh count, size buckets and the
+search space: ``$WN_AUTOTUNE_CACHE`` or ``~/.cache/wn_b200/autotune.json``.
+kappa only ranges over values whose error bound holds (>= 3; see wn_mixed.cu),
+and 32- and 64-face tiles keep the same bound, so the choice trades speed, not
+accuracy beyond the tested bound.
 """
 
 from __future__ import annotations
@@ -24,11 +29,13 @@ import torch
 from .batched import Batch
 
 DEFAULT_SPACE = {
-    "qpt": (1, 2, 4),
-    "target_pairs": (1 << 21, 1 << 23),
-    "ctas_per_sm": (0,),
-    "kappa": (3.0, 4.0),
+    "tile_faces": (64, 32),
+    "qpt": (2, 1, 4),
+    "target_pairs": (1 << 23, 1 << 21),
+    "ctas_per_sm": (0, 2),
+    "kappa": (4.0, 3.0),
 }
+# The first value of each dimension is the starting point of the descent.
 
 
 def cache_path() -> str:
@@ -64,9 +71,14 @@ def _time(batch: Batch, backward: bool, reps: int) -> float:
 
 
 def tune(meshes, queries, space=None, backward: bool = True, sample_queries: int = 16384,
-         reps: int = 3, use_cache: bool = True, seed: int = 0) -> dict:
+         reps: int = 3, use_cache: bool = True, seed: int = 0, search: str = "descent",
+         passes: int = 2) -> dict:
     """Return {"config": {...}, "ms": ..., "trials": [...], "cached": bool}."""
-    key = cache_key(meshes, queries) + f"|bwd={int(backward)}"
+    if search not in ("descent", "grid"):
+        raise ValueError("search must be 'descent' or 'grid'")
+    space = space or DEFAULT_SPACE
+    key = (cache_key(meshes, queries) + f"|bwd={int(backward)}|{search}|" +
+           ",".join(f"{k}={list(v)}" for k, v in space.items()))
     path = cache_path()
     cache = {}
     if use_cache and os.path.exists(path):
@@ -80,19 +92,40 @@ def tune(meshes, queries, space=None, backward: bool = True, sample_queries: int
     sample = [O if len(O) <= sample_queries else O[rng.choice(len(O), sample_queries,
                                                                replace=False)]
               for O in queries]
-    space = space or DEFAULT_SPACE
     trials = []
-    for values in itertools.product(*space.values()):
-        cfg = dict(zip(space.keys(), values))
-        batch = Batch(meshes, sample, **cfg)
-        try:
-            batch.gW.normal_()
-            ms = _time(batch, backward, reps)
-        finally:
-            batch.close()
-        trials.append({"config": cfg, "ms": ms})
-    best = min(trials, key=lambda t: t["ms"])
-    result = {"config": best["config"], "ms": best["ms"], "trials": trials, "key": key}
+    timed = {}
+
+    def measure(cfg: dict) -> float:
+        k = tuple(sorted(cfg.items()))
+        if k not in timed:
+            batch = Batch(meshes, sample, **cfg)
+            try:
+                batch.gW.normal_()
+                timed[k] = _time(batch, backward, reps)
+            finally:
+                batch.close()
+            trials.append({"config": dict(cfg), "ms": timed[k]})
+        return timed[k]
+
+    if search == "grid":
+        for values in itertools.product(*space.values()):
+            measure(dict(zip(space.keys(), values)))
+    else:
+        cfg = {k: v[0] for k, v in space.items()}
+        best = measure(cfg)
+        for _ in range(max(1, passes)):
+            changed = False
+            for dim, values in space.items():
+                for v in values:
+                    cand = dict(cfg, **{dim: v})
+                    ms = measure(cand)
+                    if ms < best:
+                        best, cfg, changed = ms, cand, True
+            if not changed:
+                break
+    best_trial = min(trials, key=lambda t: t["ms"])
+    result = {"config": best_trial["config"], "ms": best_trial["ms"], "trials": trials,
+              "key": key, "search": search}
     if use_cache:
         os.makedirs(os.path.dirname(path), exist_ok=True)
         cache[key] = result

@@ -36,10 +36,11 @@ class Batch:
 
     INFO_FIELDS = ("nmesh", "total_nv", "total_nf", "total_nq", "total_tiles", "work_items",
                    "grid", "partial_sums", "qpt", "target_pairs", "boundary_edges",
-                   "adjoint_items")
+                   "adjoint_items", "tile_faces")
 
     def __init__(self, meshes, queries, kappa: float = 4.0, qpt: int = 2,
-                 target_pairs: int = 1 << 23, ctas_per_sm: int = 0, device="cuda"):
+                 target_pairs: int = 1 << 23, ctas_per_sm: int = 0, tile_faces: int = 64,
+                 device="cuda"):
         if len(meshes) != len(queries) or not meshes:
             raise ValueError("need one query set per mesh, and at least one mesh")
         self.handle = _lib.lib()
@@ -56,9 +57,9 @@ class Batch:
         _check(self.handle.wn_batch_create(len(meshes), self.nv.ctypes.data, self.nf.ctypes.data,
                                            self.nq.ctypes.data, faces.ctypes.data, float(kappa),
                                            int(qpt), int(target_pairs), int(ctas_per_sm),
-                                           ctypes.byref(self.batch)))
+                                           int(tile_faces), ctypes.byref(self.batch)))
         self.config = {"kappa": float(kappa), "qpt": int(qpt), "target_pairs": int(target_pairs),
-                       "ctas_per_sm": int(ctas_per_sm)}
+                       "ctas_per_sm": int(ctas_per_sm), "tile_faces": int(tile_faces)}
         dev = self.device
         self.V = torch.from_numpy(np.concatenate(Vs)).to(dev)
         self.Q = torch.from_numpy(np.concatenate(Qs)).to(dev)

@@ -244,3 +244,36 @@ def test_mixed_float32_queries_full_size_c4(gpu_required):
     assert np.isfinite(dV).all() and np.isfinite(dO).all()
     assert np.abs(dV - dV64).max() <= 1e-4 * np.abs(dV64).max()
     assert np.abs(dO - dO64).max() <= 1e-3 * np.abs(dO64).max()
+
+
+def test_auto_adjoint_picks_faces_on_a_soup_and_edges_on_a_mesh(gpu_required, monkeypatch):
+    """adjoint="auto": a mixed forward on a triangle soup (three boundary edges per
+    face) takes the per-face adjoint, one on an open indexed mesh the boundary-edge
+    adjoint; both give the FP64 adjoint's gradients."""
+    import torch
+
+    V, F = igl.synthetic.bumpy_icosphere(3, seed=81)
+    F = igl.synthetic.delete_faces(F, 0.05, seed=82)
+    O = igl.synthetic.mixed_queries(V, F, 2048, seed=83, near_sigma=1e-2)
+    g = np.random.default_rng(84).normal(size=len(O))
+    Vs, Fs = igl.synthetic.unshare_vertices(V, F)
+    calls = []
+    real_faces = wa.PreparedMesh.backward
+    real_edges = wa.backward_edges
+    monkeypatch.setattr(wa.PreparedMesh, "backward",
+                        lambda self, *a: calls.append("faces") or real_faces(self, *a))
+    monkeypatch.setattr(wa, "backward_edges",
+                        lambda *a, **k: calls.append("edges") or real_edges(*a, **k))
+    for (Vx, Fx), expect in (((Vs, Fs), "faces"), ((V, F), "edges")):
+        calls.clear()
+        grads = {}
+        for precision in ("mixed", "fp64"):
+            Vt = _cuda(Vx).requires_grad_(True)
+            Ot = _cuda(O).requires_grad_(True)
+            W = wa.winding_number_torch(Vt, _cuda(Fx), Ot, precision=precision)
+            (W * _cuda(g)).sum().backward()
+            grads[precision] = (Vt.grad.cpu().numpy(), Ot.grad.cpu().numpy())
+        assert calls[0] == expect, calls
+        for a, b in zip(grads["mixed"], grads["fp64"]):
+            assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max()
+    del torch

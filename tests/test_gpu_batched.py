@@ -28,12 +28,16 @@ def _small_batch(n=7, seed=5, max_level=4, max_q=3000):
     return meshes, queries
 
 
-@pytest.mark.parametrize("qpt,kappa", [(1, 4.0), (2, 4.0), (4, 4.0), (2, 3.0), (4, 3.0)])
-def test_batched_forward_matches_oracle(gpu_required, oracle_mod, qpt, kappa):
+@pytest.mark.parametrize("qpt,kappa,tile_faces", [
+    (1, 4.0, 64), (2, 4.0, 64), (4, 4.0, 64), (2, 3.0, 64), (4, 3.0, 64),
+    (1, 4.0, 32), (2, 4.0, 32), (4, 3.0, 32), (2, 3.0, 32)])
+def test_batched_forward_matches_oracle(gpu_required, oracle_mod, qpt, kappa, tile_faces):
     """Every configuration the autotuner may pick keeps the 1e-6 bound (kappa = 3
-    is the smallest refinement radius it is allowed)."""
+    is the smallest refinement radius it is allowed; 32-face tiles test and sum
+    each half of a tile on its own)."""
     meshes, queries = _small_batch()
-    b = igl.batched.Batch(meshes, queries, qpt=qpt, target_pairs=1 << 16, kappa=kappa)
+    b = igl.batched.Batch(meshes, queries, qpt=qpt, target_pairs=1 << 16, kappa=kappa,
+                          tile_faces=tile_faces)
     try:
         W = b.split(b.forward().clone())
         assert b.info()["work_items"] > len(meshes)
@@ -101,9 +105,12 @@ def test_graph_replay_matches_eager_and_is_deterministic(gpu_required):
 def test_autotuner_picks_and_caches(gpu_required, tmp_path, monkeypatch):
     monkeypatch.setenv("WN_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
     meshes, queries = _small_batch(n=4, seed=9)
-    space = {"qpt": (1, 2), "target_pairs": (1 << 16,), "ctas_per_sm": (0,), "kappa": (4.0,)}
+    space = {"qpt": (1, 2), "target_pairs": (1 << 16,), "ctas_per_sm": (0, 2),
+             "kappa": (4.0,), "tile_faces": (64, 32)}
     first = igl.autotune.tune(meshes, queries, space=space, reps=1)
-    assert not first["cached"] and len(first["trials"]) == 2
+    assert not first["cached"] and 4 <= len(first["trials"]) <= 8
+    assert {t["config"]["tile_faces"] for t in first["trials"]} == {64, 32}
+    assert {t["config"]["ctas_per_sm"] for t in first["trials"]} == {0, 2}
     again = igl.autotune.tune(meshes, queries, space=space, reps=1)
     assert again["cached"] and again["config"] == first["config"]
 

@@ -212,3 +212,48 @@ def test_queries_clustered_at_vertex_fans(gpu_required, oracle_mod):
     tri = igl._triangle_soa(V, F)
     W = mixed_host(tri, O)
     assert np.abs(W - oracle_mod.winding_soa(tri, O)).max() <= TOL
+
+
+@pytest.mark.parametrize("workload", ["c2_open", "c3_mixed", "soup"])
+def test_half_tiles_keep_the_bound(gpu_required, oracle_mod, workload):
+    """32 faces per far test and angle product (each half of a 64-face tile on its
+    own): the same 1e-6 bound as 64-face tiles, on an open mesh, on near-surface
+    queries of the c3 mesh, and on a multiscale soup whose halves' balls differ."""
+    import torch
+
+    if workload == "soup":
+        rng = np.random.default_rng(18)
+        nf = 3000
+        corners = rng.uniform(-1, 1, (nf, 1, 3)) + 10.0 ** rng.uniform(-3, 0, (nf, 1, 1)) * \
+            rng.normal(size=(nf, 3, 3))
+        tri = np.ascontiguousarray(corners.transpose(1, 2, 0).reshape(9, nf))
+        pick = rng.integers(0, nf, 1000)
+        O = np.concatenate([rng.uniform(-1.2, 1.2, (1000, 3)),
+                            corners[pick].mean(1) + 1e-4 * rng.normal(size=(1000, 3))])
+    else:
+        V, F, O, _ = igl.synthetic.workload(workload, n_queries=4096)
+        tri = igl._triangle_soa(V, F)
+    nf = tri.shape[1]
+    ld = nf + (nf & 1)
+    tri_d = torch.zeros((9, ld), dtype=torch.float64, device="cuda")
+    tri_d[:, :nf] = torch.from_numpy(tri)
+    q_d = torch.from_numpy(np.ascontiguousarray(O)).cuda()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    h = _lib.lib()
+    mesh = ctypes.c_void_p()
+    assert h.wn_mixed_mesh_create(tri_d.data_ptr(), ld, nf, 4.0, stream, ctypes.byref(mesh)) == 0
+    try:
+        out = {}
+        for tf in (64, 32):
+            assert h.wn_mixed_mesh_set_tile_faces(mesh, tf) == 0
+            w_d = torch.empty(len(O), dtype=torch.float64, device="cuda")
+            assert h.wn_forward_mixed_device(mesh, q_d.data_ptr(), len(O), w_d.data_ptr(),
+                                             stream) == 0, _lib.last_error()
+            assert h.wn_stream_check(stream) == 0
+            out[tf] = w_d.cpu().numpy()
+        assert h.wn_mixed_mesh_set_tile_faces(mesh, 48) != 0
+    finally:
+        h.wn_mixed_mesh_destroy(mesh)
+    ref = oracle_mod.winding_soa(tri, O, workers=8)
+    assert np.abs(out[64] - ref).max() <= TOL
+    assert np.abs(out[32] - ref).max() <= TOL

@@ -179,3 +179,40 @@ def test_vector_lanes_equal_the_scalar_path():
         handle.mli_winding(tri.ctypes.data, O.ctypes.data, single.ctypes.data, tri.shape[1],
                            len(O), i, i + 1)
     assert np.array_equal(whole, single, equal_nan=True)
+
+
+def test_autotune_coordinate_descent_without_a_gpu(monkeypatch):
+    """The tuner's search on a fake timing surface: it starts from the first value
+    of every dimension, sweeps one dimension at a time, keeps improvements, and
+    reports every configuration it timed (no GPU: Batch and timing are faked)."""
+    from igl import autotune
+
+    cost = {"tile_faces": {64: 0.0, 32: -1.0}, "qpt": {2: 0.0, 1: 2.0, 4: -0.5},
+            "ctas_per_sm": {0: 0.0, 2: 0.3}}
+
+    class FakeBatch:
+        def __init__(self, meshes, sample, **cfg):
+            self.cfg = cfg
+
+        def close(self):
+            pass
+
+        @property
+        def gW(self):
+            class G:
+                def normal_(self):
+                    pass
+            return G()
+
+    monkeypatch.setattr(autotune, "Batch", FakeBatch)
+    monkeypatch.setattr(autotune, "_time",
+                        lambda b, backward, reps: 10.0 + sum(cost[k][v] for k, v in b.cfg.items()))
+    monkeypatch.setattr(autotune, "cache_key", lambda m, q: "fake")
+    space = {"tile_faces": (64, 32), "qpt": (2, 1, 4), "ctas_per_sm": (0, 2)}
+    out = autotune.tune([None], [np.zeros((4, 3))], space=space, use_cache=False)
+    assert out["config"] == {"tile_faces": 32, "qpt": 4, "ctas_per_sm": 0}
+    assert out["ms"] == 8.5
+    assert out["trials"][0]["config"] == {"tile_faces": 64, "qpt": 2, "ctas_per_sm": 0}
+    assert len({tuple(sorted(t["config"].items())) for t in out["trials"]}) == len(out["trials"])
+    grid = autotune.tune([None], [np.zeros((4, 3))], space=space, use_cache=False, search="grid")
+    assert len(grid["trials"]) == 12 and grid["config"] == out["config"]

@@ -12,7 +12,9 @@ Legs, all on the same inputs:
     accumulation and FP64 refinement of near-surface pairs;
   * fp64:  the plain FP64 kernel, pair terms bit-identical to the reference;
   * fwdbwd_faces / fwdbwd_edges: mixed forward + the per-face mixed-precision
-    adjoint / the boundary-edge adjoint (both followed by the vertex gather);
+    adjoint / the mixed boundary-edge adjoint (both followed by the vertex gather);
+  * adjoint_workloads: the same on the c3 mesh with 8% of its faces deleted and
+    on the c3 mesh as a triangle soup (every edge a boundary edge);
   * c4: the gradient workload (subdivision-5 mesh, 8% faces deleted, 262,144
     near-surface queries): forward alone and forward + each adjoint;
   * c5: 64 uneven meshes in one persistent launch, forward alone and forward +
@@ -391,7 +393,7 @@ def gpu_arm(args):
 
     def fwdbwd_edges_step():
         mixed_step()
-        wa.backward_edges(V_d, F_d, q_d, gw_d)
+        wa.backward_edges(V_d, F_d, q_d, gw_d, precision="mixed")
 
     legs = {"mixed": mixed_step, "fp64": fp64_step, "fp64_stream": fp64_stream_step,
             "fwdbwd_faces": fwdbwd_faces_step, "fwdbwd_edges": fwdbwd_edges_step}
@@ -488,7 +490,7 @@ def gpu_arm(args):
 
         def c4_edges():
             c4_fwd()
-            wa.backward_edges(V4d, F4d, O4d, g4d)
+            wa.backward_edges(V4d, F4d, O4d, g4d, precision="mixed")
 
         t4 = {k: timed(fn, args.steps, 2)[0] for k, fn in
               (("fwd", c4_fwd), ("faces", c4_faces), ("edges", c4_edges))}
@@ -517,7 +519,7 @@ def gpu_arm(args):
 
         def c4f_edges():
             c4f_fwd()
-            wa.backward_edges(V4d, F4d, O4f, g4d)
+            wa.backward_edges(V4d, F4d, O4f, g4d, precision="mixed")
 
         t4f = {k: timed(fn, args.steps, 2)[0] for k, fn in
                (("fwd", c4f_fwd), ("faces", c4f_faces), ("edges", c4f_edges))}
@@ -560,17 +562,27 @@ def gpu_arm(args):
 
             def a_edges():
                 a_fwd()
+                wa.backward_edges(Vad, Fad, Oad, gad, precision="mixed")
+
+            def a_edges64():
+                a_fwd()
                 wa.backward_edges(Vad, Fad, Oad, gad)
 
-            ta = {k: timed(fn, k_adj, 1)[0] for k, fn in
-                  (("fwd", a_fwd), ("faces", a_faces), ("edges", a_edges))}
+            legs_a = [("fwd", a_fwd), ("faces", a_faces), ("edges", a_edges)]
+            if wname == "c3_open":
+                legs_a.append(("edges_fp64", a_edges64))
+            ta = {k: timed(fn, k_adj, 1)[0] for k, fn in legs_a}
             _, ne_a, _ = wa.boundary_edges(Vad, Fad)
             adj_work[wname] = {
                 "workload": desc_a, "pairs": float(nfa) * len(Oa), "boundary_edges": ne_a,
                 "fwd_ms": ta["fwd"] * 1e3, "fwdbwd_faces_ms": ta["faces"] * 1e3,
                 "fwdbwd_edges_ms": ta["edges"] * 1e3,
                 "ratio_faces": ta["faces"] / ta["fwd"], "ratio_edges": ta["edges"] / ta["fwd"],
-                "steps": k_adj}
+                "steps": k_adj,
+                "note": "faces: per-face mixed adjoint; edges: mixed boundary-edge adjoint"}
+            if "edges_fp64" in ta:
+                adj_work[wname]["fwdbwd_edges_fp64_ms"] = ta["edges_fp64"] * 1e3
+                adj_work[wname]["ratio_edges_fp64"] = ta["edges_fp64"] / ta["fwd"]
             mesha.close()
             del Vad, Fad, Oad, gad, tria
 

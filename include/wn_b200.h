@@ -234,6 +234,14 @@ int wn_backward_mixed_device(void* mesh, const double* q, int64_t nq, const doub
 int wn_backward_edges_device(const double* edges, int64_t le, int64_t ne, const double* q,
                              int64_t nq, const double* gw, double* dq, double* dedge,
                              void* stream);
+/* The boundary-edge adjoint in mixed precision: the same arguments and outputs,
+ * plus kappa (>= 3). Edges are Morton-ordered into 64-edge tiles inside the call;
+ * pairs with both endpoints at least kappa * |edge| from the query run in FP32 in
+ * the tile's scaled frame, the others in FP64; FP64 sums across query chunks and
+ * over edges. Deterministic. */
+int wn_backward_edges_mixed_device(const double* edges, int64_t le, int64_t ne, const double* q,
+                                   int64_t nq, const double* gw, double kappa, double* dq,
+                                   double* dedge, void* stream);
 
 /* dV (nv x 3) = sum of per-element corner gradients over each vertex's uses.
  * grad: rows 3*corner+axis with stride ld; corners = 3 (faces, dtri) or 2 (edges,

@@ -882,6 +882,496 @@ cudaError_t adjoint_mixed(const AdjointPlan& p, const MixedMesh& m, const double
   return cudaGetLastError();
 }
 
+namespace {
+
+// ---- mixed-precision boundary-edge adjoint -----------------------------------
+// The boundary-edge adjoint with the per-face mixed adjoint's precision split.
+// Edges are ordered along a Morton curve of their midpoints and cut into tiles of
+// 64; per tile an FP64 centre, a power-of-two scale ~ 1/radius and the squared
+// far radius (r + kappa h)^2 (h = the tile's longest edge); per edge, in the
+// tile's scaled FP32 frame, P, e = Q - P, |e|^2 and the multiplicity m. A pair
+// (query, edge) is near when an endpoint lies within kappa |e| of the query; near
+// pairs are evaluated in FP64 from the sorted FP64 edges, the rest in FP32: with
+// p = P - o, q = p + e, D = |p||q| + p.q (no cancellation at kappa >= 3: p and q
+// point the same way), k_P = g m r_p / D, k_Q = g m r_q / D, x = p x e (= p x q):
+//   -g m dOmega/dP += k_P x,  -g m dOmega/dQ += k_Q x,  g m dOmega/do += (k_P + k_Q) x,
+// 37 FP32 operations (as 19 packed instructions per edge pair) and 3 MUFU per
+// pair. Work split, fixed-order reductions and partial arrays as in the per-face
+// mixed adjoint; the outputs are those of adjoint_edges.
+struct EdgeRec {
+  float px, py, pz;  // endpoint P minus the tile centre, times the tile's scale
+  float ex, ey, ez;  // Q - P (formed in FP64, then rounded)
+  float ee;          // |Q - P|^2
+  float m;           // net multiplicity (0 for padding)
+};
+static_assert(sizeof(EdgeRec) == 32, "edge record is 32 bytes");
+constexpr int kEdgeTileBytes = static_cast<int>(sizeof(TileHeader) + kTileFaces * sizeof(EdgeRec));
+
+// AoS midpoints of the edges (7 x le SoA: P, Q, m), for the Morton sort.
+__global__ void edge_midpoints_kernel(const double* __restrict__ edges, int64_t le, int64_t ne,
+                                      double* __restrict__ mid) {
+  const int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+#pragma unroll
+  for (int x = 0; x < 3; ++x) mid[3 * e + x] = 0.5 * (edges[x * le + e] + edges[(3 + x) * le + e]);
+}
+
+__device__ __forceinline__ double warp_max_d(double v) {
+  for (int off = 16; off; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+  return v;
+}
+__device__ __forceinline__ double warp_min_d(double v) {
+  for (int off = 16; off; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off));
+  return v;
+}
+
+// One CTA of 64 threads per tile: edges order[64 t + j] in Morton order.
+__global__ void __launch_bounds__(kTileFaces) build_edge_tiles_kernel(
+    const double* __restrict__ edges, int64_t le, int64_t ne, const uint32_t* __restrict__ order,
+    double kappa, unsigned char* __restrict__ tiles, double* __restrict__ e64, int64_t ld64,
+    uint32_t* __restrict__ edge_of) {
+  __shared__ double red[8][kTileFaces / 32];
+  const int j = threadIdx.x, warp = j >> 5, lane = j & 31;
+  const int64_t tile = blockIdx.x;
+  const int64_t slot = tile * kTileFaces + j;
+  const bool valid = slot < ne;
+  const int64_t e = valid ? order[slot] : 0;
+  double v[7];
+#pragma unroll
+  for (int r = 0; r < 7; ++r) v[r] = valid ? edges[r * le + e] : 0.0;
+  double lo[3], hi[3];
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    lo[x] = warp_min_d(valid ? fmin(v[x], v[3 + x]) : INFINITY);
+    hi[x] = warp_max_d(valid ? fmax(v[x], v[3 + x]) : -INFINITY);
+  }
+  if (lane == 0)
+    for (int x = 0; x < 3; ++x) {
+      red[x][warp] = lo[x];
+      red[3 + x][warp] = hi[x];
+    }
+  __syncthreads();
+  double c[3];
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    const double l = fmin(red[x][0], red[x][1]), h = fmax(red[3 + x][0], red[3 + x][1]);
+    c[x] = isfinite(l) ? 0.5 * (l + h) : 0.0;
+  }
+  __syncthreads();
+  double r2 = 0.0, h2 = 0.0;
+  if (valid) {
+    for (int k = 0; k < 2; ++k) {
+      const double dx = v[3 * k] - c[0], dy = v[3 * k + 1] - c[1], dz = v[3 * k + 2] - c[2];
+      r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
+    }
+    const double ex = v[3] - v[0], ey = v[4] - v[1], ez = v[5] - v[2];
+    h2 = ex * ex + ey * ey + ez * ez;
+  }
+  double rt = warp_max_d(sqrt(r2)), ht = warp_max_d(sqrt(h2));
+  if (lane == 0) {
+    red[6][warp] = rt;
+    red[7][warp] = ht;
+  }
+  __syncthreads();
+  rt = fmax(red[6][0], red[6][1]);
+  ht = fmax(red[7][0], red[7][1]);
+  int ex2 = 0;
+  if (rt > 0.0) frexp(rt, &ex2);
+  const double scale = ldexp(1.0, -ex2);
+  unsigned char* rec = tiles + tile * kEdgeTileBytes;
+  if (j == 0) {
+    TileHeader th{};
+    th.cx = c[0];
+    th.cy = c[1];
+    th.cz = c[2];
+    const double far = rt + kappa * ht;
+    th.far_r2 = far * far;
+    th.scale = scale;
+    const int64_t left = ne - tile * kTileFaces;
+    th.n = static_cast<int32_t>(left < kTileFaces ? left : kTileFaces);
+    th.r = static_cast<float>(rt);
+    th.h = static_cast<float>(ht);
+    *reinterpret_cast<TileHeader*>(rec) = th;
+  }
+  EdgeRec er;
+  const double ex = (v[3] - v[0]) * scale, ey = (v[4] - v[1]) * scale, ez = (v[5] - v[2]) * scale;
+  er.px = valid ? static_cast<float>((v[0] - c[0]) * scale) : 1e18f;
+  er.py = valid ? static_cast<float>((v[1] - c[1]) * scale) : 1e18f;
+  er.pz = valid ? static_cast<float>((v[2] - c[2]) * scale) : 1e18f;
+  er.ex = static_cast<float>(ex);
+  er.ey = static_cast<float>(ey);
+  er.ez = static_cast<float>(ez);
+  er.ee = static_cast<float>(ex * ex + ey * ey + ez * ez);
+  er.m = static_cast<float>(v[6]);
+  reinterpret_cast<EdgeRec*>(rec + sizeof(TileHeader))[j] = er;
+#pragma unroll
+  for (int r = 0; r < 7; ++r) e64[r * ld64 + slot] = v[r];
+  edge_of[slot] = valid ? static_cast<uint32_t>(e) : 0xffffffffu;
+}
+
+// g m dOmega of one (query, edge) pair in FP64, the FP64 edge kernel's formula:
+// -g m dOmega/dP into gv[0..2], -g m dOmega/dQ into gv[3..5], g m dOmega/do into go.
+__device__ __noinline__ void refine_edge_grad(const double* __restrict__ e64, int64_t ld64,
+                                              int64_t slot, double4 o, double* acc_col,
+                                              int stride, double* go) {
+  double v[7];
+#pragma unroll
+  for (int r = 0; r < 7; ++r) v[r] = e64[r * ld64 + slot];
+  const double px = v[0] - o.x, py = v[1] - o.y, pz = v[2] - o.z;
+  const double qx = v[3] - o.x, qy = v[4] - o.y, qz = v[5] - o.z;
+  const double pp = px * px + py * py + pz * pz;
+  const double qq = qx * qx + qy * qy + qz * qz;
+  const double rp = rsqrt(pp), rq = rsqrt(qq);
+  const double rpq = rp * rq;
+  const double d = 1.0 + (px * qx + py * qy + pz * qz) * rpq;
+  const bool ok = v[6] != 0.0 && pp > 0.0 && qq > 0.0 && d > 0.0;
+  const double w = ok ? o.w * v[6] * rpq / d : 0.0;
+  const double cp = ok ? rp * w : 0.0, cq = ok ? rq * w : 0.0;
+  const double x0 = py * qz - pz * qy, x1 = pz * qx - px * qz, x2 = px * qy - py * qx;
+  acc_col[0] -= cp * x0;
+  acc_col[stride] -= cp * x1;
+  acc_col[2 * stride] -= cp * x2;
+  acc_col[3 * stride] -= cq * x0;
+  acc_col[4 * stride] -= cq * x1;
+  acc_col[5 * stride] -= cq * x2;
+  const double cs = cp + cq;
+  go[0] += cs * x0;
+  go[1] += cs * x1;
+  go[2] += cs * x2;
+}
+
+struct MixedEdgeArgs {
+  const unsigned char* tiles;  // ntiles * kEdgeTileBytes
+  int64_t ntiles;
+  const double* e64;  // sorted FP64 edges, 7 x ld64 (P, Q, m)
+  int64_t ld64;
+  const double4* qs;  // nq queries in Morton order: x, y, z, g
+  int64_t nq;
+  float kappa2;  // kappa^2: a pair is near when min(|p|^2, |q|^2) <= kappa^2 |e|^2
+  int64_t blocks_per_range, queries_per_group;
+  double* dO_part;  // [nranges][nq][3] by sorted position, zeroed before the launch
+  double* dE_part;  // [ngroups][6][ld64] by sorted slot
+};
+
+template <int QC>
+struct EdgeAdjSmem {
+  float dO32[QC * 3][kFaRow];   // per-thread FP32 dL/do shares, row 3*query + axis
+  double acc64[12][kFaThreads];  // per-edge FP64 sums (thread-private columns)
+  double red64[kFaTiles][QC][3];
+  double dsum[QC * 3];
+  double4 q64[QC];
+  float4 frame[QC][kFaTiles];
+  int flag[QC][kFaTiles];
+  TileHeader th[kFaTiles];
+};
+
+template <int QC>
+__global__ void __launch_bounds__(kFaThreads, 4) adjoint_edges_mixed_kernel(const MixedEdgeArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto& sm = *reinterpret_cast<EdgeAdjSmem<QC>*>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t nblocks = (a.ntiles + kFaTiles - 1) / kFaTiles;
+  const int64_t range = blockIdx.x, group = blockIdx.y;
+  const int64_t b_begin = range * a.blocks_per_range;
+  const int64_t b_end = min(nblocks, b_begin + a.blocks_per_range);
+  const int64_t q_begin = group * a.queries_per_group;
+  const int64_t q_end = min(a.nq, q_begin + a.queries_per_group);
+  double* dO_row = a.dO_part + range * a.nq * 3;
+
+  for (int64_t blk = b_begin; blk < b_end; ++blk) {
+    __syncthreads();  // previous block's shared data fully consumed
+    if (tid < kFaTiles) {
+      const int64_t t = blk * kFaTiles + tid;
+      if (t < a.ntiles) {
+        sm.th[tid] = *reinterpret_cast<const TileHeader*>(a.tiles + t * kEdgeTileBytes);
+      } else {
+        TileHeader empty{};
+        empty.far_r2 = 0.0;
+        empty.scale = 1.0;
+        sm.th[tid] = empty;
+      }
+    }
+    // This warp's tile; lane k of every float2 is edge lane + 32 k (padding edges
+    // carry a far corner, a zero edge and m = 0: every term they give is zero).
+    const int64_t t = blk * kFaTiles + warp;
+    const bool tile_ok = t < a.ntiles;
+    const unsigned char* rec = a.tiles + (tile_ok ? t : 0) * kEdgeTileBytes;
+    const int n = tile_ok ? reinterpret_cast<const TileHeader*>(rec)->n : 0;
+    float2 fp[3], fe[3], fee, fm;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int j = lane + 32 * k;
+      const float4* er = reinterpret_cast<const float4*>(rec + sizeof(TileHeader)) + 2 * j;
+      float4 r0 = make_float4(1e18f, 1e18f, 1e18f, 0.f), r1 = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (j < n) {
+        r0 = er[0];
+        r1 = er[1];
+      }
+      lane_ref(fp[0], k) = r0.x;  lane_ref(fp[1], k) = r0.y;  lane_ref(fp[2], k) = r0.z;
+      lane_ref(fe[0], k) = r0.w;  lane_ref(fe[1], k) = r1.x;  lane_ref(fe[2], k) = r1.y;
+      lane_ref(fee, k) = r1.z;    lane_ref(fm, k) = r1.w;
+    }
+    const int64_t slot0 = (tile_ok ? t : 0) * kTileFaces + lane;
+#pragma unroll
+    for (int r = 0; r < 12; ++r) sm.acc64[r][tid] = 0.0;
+    float2 acc[6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r) acc[r] = f2(0.f);
+    const float2 k2ee = __fmul2_rn(f2(a.kappa2), fee);
+
+    int chunks = 0;
+    for (int64_t c0 = q_begin; c0 < q_end; c0 += QC) {
+      const int nc = static_cast<int>(q_end - c0 < QC ? q_end - c0 : QC);
+      __syncthreads();
+      for (int item = tid; item < QC * kFaTiles; item += kFaThreads) {
+        const int jq = item / kFaTiles, tt = item % kFaTiles;
+        if (jq < nc) {
+          const double4 o = a.qs[c0 + jq];
+          const TileHeader& th = sm.th[tt];
+          const double dx = o.x - th.cx, dy = o.y - th.cy, dz = o.z - th.cz;
+          const double d2 = dx * dx + dy * dy + dz * dz;
+          const bool skip = d2 * th.scale * th.scale > 1.2089258196146292e24;
+          sm.frame[jq][tt] = make_float4(static_cast<float>(dx * th.scale),
+                                         static_cast<float>(dy * th.scale),
+                                         static_cast<float>(dz * th.scale),
+                                         static_cast<float>(o.w * th.scale));
+          sm.flag[jq][tt] = skip ? 2 : (d2 >= th.far_r2 ? 0 : 1);
+          if (tt == 0) sm.q64[jq] = o;
+        }
+      }
+      for (int e = tid; e < kFaTiles * QC * 3; e += kFaThreads) (&sm.red64[0][0][0])[e] = 0.0;
+      __syncthreads();
+      static_assert(QC <= 32, "one mask bit per query of a chunk");
+      unsigned near0 = 0u, near1 = 0u;
+#pragma unroll 1
+      for (int jq = 0; jq < nc; ++jq) {
+        const float4 f = sm.frame[jq][warp];
+        const int flag = sm.flag[jq][warp];
+        float2 d0 = f2(0.f), d1 = f2(0.f), d2 = f2(0.f);
+        if (flag != 2) {
+          const float2 px = __fadd2_rn(fp[0], f2(-f.x));
+          const float2 py = __fadd2_rn(fp[1], f2(-f.y));
+          const float2 pz = __fadd2_rn(fp[2], f2(-f.z));
+          const float2 pp = __ffma2_rn(px, px, __ffma2_rn(py, py, __fmul2_rn(pz, pz)));
+          const float2 s = __ffma2_rn(px, fe[0], __ffma2_rn(py, fe[1], __fmul2_rn(pz, fe[2])));
+          const float2 pq = __fadd2_rn(pp, s);
+          const float2 qq = __ffma2_rn(f2(2.f), s, __fadd2_rn(pp, fee));
+          const float2 rp = rsqrt2(pp), rq = rsqrt2(qq);
+          const float2 lp = __fmul2_rn(pp, rp), lq = __fmul2_rn(qq, rq);
+          const float2 iD = rcp2(__ffma2_rn(lp, lq, pq));
+          const float2 gD = __fmul2_rn(__fmul2_rn(f2(f.w), fm), iD);
+          float2 kp = __fmul2_rn(rp, gD), kq = __fmul2_rn(rq, gD);
+          if (flag == 1) {
+            // Careful visit: pairs with an endpoint within kappa |e| are refined in
+            // FP64 after the chunk; their FP32 terms are dropped here.
+            if (fminf(pp.x, qq.x) <= k2ee.x && lane < n) {
+              near0 |= 1u << jq;
+              kp.x = kq.x = 0.f;
+            }
+            if (fminf(pp.y, qq.y) <= k2ee.y && lane + 32 < n) {
+              near1 |= 1u << jq;
+              kp.y = kq.y = 0.f;
+            }
+          }
+          const float2 x0 = cross_c(py, fe[2], pz, fe[1]);
+          const float2 x1 = cross_c(pz, fe[0], px, fe[2]);
+          const float2 x2 = cross_c(px, fe[1], py, fe[0]);
+          acc[0] = __ffma2_rn(kp, x0, acc[0]);
+          acc[1] = __ffma2_rn(kp, x1, acc[1]);
+          acc[2] = __ffma2_rn(kp, x2, acc[2]);
+          acc[3] = __ffma2_rn(kq, x0, acc[3]);
+          acc[4] = __ffma2_rn(kq, x1, acc[4]);
+          acc[5] = __ffma2_rn(kq, x2, acc[5]);
+          const float2 cs = __fadd2_rn(kp, kq);
+          d0 = __fmul2_rn(cs, x0);
+          d1 = __fmul2_rn(cs, x1);
+          d2 = __fmul2_rn(cs, x2);
+        }
+        sm.dO32[3 * jq][tid] = d0.x + d0.y;
+        sm.dO32[3 * jq + 1][tid] = d1.x + d1.y;
+        sm.dO32[3 * jq + 2][tid] = d2.x + d2.y;
+      }
+      for (unsigned pending = __reduce_or_sync(0xffffffffu, near0 | near1); pending;
+           pending &= pending - 1u) {
+        const int jq = __ffs(pending) - 1;
+        double go[3] = {0.0, 0.0, 0.0};
+        if ((near0 >> jq) & 1u)
+          refine_edge_grad(a.e64, a.ld64, slot0, sm.q64[jq], &sm.acc64[0][tid], kFaThreads, go);
+        if ((near1 >> jq) & 1u)
+          refine_edge_grad(a.e64, a.ld64, slot0 + 32, sm.q64[jq], &sm.acc64[6][tid], kFaThreads,
+                           go);
+        for (int off = 16; off; off >>= 1) {
+          go[0] += __shfl_xor_sync(0xffffffffu, go[0], off);
+          go[1] += __shfl_xor_sync(0xffffffffu, go[1], off);
+          go[2] += __shfl_xor_sync(0xffffffffu, go[2], off);
+        }
+        if (lane == 0) {
+          sm.red64[warp][jq][0] = go[0];
+          sm.red64[warp][jq][1] = go[1];
+          sm.red64[warp][jq][2] = go[2];
+        }
+      }
+      __syncthreads();
+      for (int base = 0; base + 8 * warp < QC * 3; base += kFaThreads / 4) {
+        const int row = base + (tid >> 2), part = tid & 3;
+        const float4* src = reinterpret_cast<const float4*>(&sm.dO32[row][32 * part]);
+        float4 s4 = src[0];
+#pragma unroll
+        for (int i = 1; i < 8; ++i) {
+          const float4 v = src[i];
+          s4.x += v.x;
+          s4.y += v.y;
+          s4.z += v.z;
+          s4.w += v.w;
+        }
+        float v = (s4.x + s4.y) + (s4.z + s4.w);
+        v += __shfl_xor_sync(0xffffffffu, v, 1);
+        v += __shfl_xor_sync(0xffffffffu, v, 2);
+        if (part == 0 && row < nc * 3) {
+          const int jq = row / 3, x = row % 3;
+          double sum = static_cast<double>(v);
+#pragma unroll
+          for (int w = 0; w < kFaTiles; ++w) sum += sm.red64[w][jq][x];
+          sm.dsum[row] = sum;
+        }
+      }
+      if (++chunks == kFaFlushChunks || c0 + QC >= q_end) {
+        chunks = 0;
+#pragma unroll
+        for (int r = 0; r < 6; ++r) {
+          sm.acc64[r][tid] -= static_cast<double>(acc[r].x);
+          sm.acc64[6 + r][tid] -= static_cast<double>(acc[r].y);
+          acc[r] = f2(0.f);
+        }
+      }
+      __syncthreads();
+      for (int e = tid; e < nc * 3; e += kFaThreads) dO_row[c0 * 3 + e] += sm.dsum[e];
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      if (lane + 32 * k >= n) continue;
+#pragma unroll
+      for (int r = 0; r < 6; ++r)
+        a.dE_part[(group * 6 + r) * a.ld64 + slot0 + 32 * k] = sm.acc64[6 * k + r][tid];
+    }
+  }
+}
+
+// dedge[row][edge_of[slot]] = (1/4pi) sum_g dE_part[g][row][slot] (sorted slots to input edges).
+__global__ void finish_dedge_sorted_kernel(const double* __restrict__ part, int64_t ngroups,
+                                           int64_t ld64, const uint32_t* __restrict__ edge_of,
+                                           int64_t le, double* __restrict__ dedge) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= 6 * ld64) return;
+  const int64_t r = i / ld64, sl = i % ld64;
+  const uint32_t e = edge_of[sl];
+  if (e == 0xffffffffu) return;
+  double s = 0.0;
+  for (int64_t g = 0; g < ngroups; ++g) s += part[(g * 6 + r) * ld64 + sl];
+  dedge[r * le + e] = s * kInv4Pi;
+}
+
+constexpr int kEaQc = kFaQc;
+
+// Scratch layout of adjoint_edges_mixed (each piece 256-byte aligned).
+struct EdgeMixedLayout {
+  size_t mid, eperm, sort, tiles, e64, edge_of, qperm, qs, dO, dE, total;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+EdgeMixedLayout edge_mixed_layout(const AdjointPlan& p, int64_t ne, int64_t nq) {
+  const int64_t ntiles = std::max<int64_t>(1, cdiv(ne, kTileFaces));
+  const int64_t ld64 = ntiles * kTileFaces;
+  EdgeMixedLayout l{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += align256(std::max<size_t>(bytes, 1));
+    return at;
+  };
+  l.mid = take(sizeof(double) * 3 * static_cast<size_t>(ne));
+  l.eperm = take(sizeof(uint32_t) * static_cast<size_t>(ne));
+  l.sort = take(std::max(mixed_sort_scratch_bytes(ne), mixed_sort_scratch_bytes(nq)));
+  l.tiles = take(static_cast<size_t>(ntiles) * kEdgeTileBytes);
+  l.e64 = take(sizeof(double) * 7 * static_cast<size_t>(ld64));
+  l.edge_of = take(sizeof(uint32_t) * static_cast<size_t>(ld64));
+  l.qperm = take(sizeof(uint32_t) * static_cast<size_t>(nq));
+  l.qs = take(sizeof(double4) * static_cast<size_t>(nq));
+  l.dO = take(sizeof(double) * static_cast<size_t>(p.nranges) * nq * 3);
+  l.dE = take(sizeof(double) * static_cast<size_t>(p.ngroups) * 6 * ld64);
+  l.total = off;
+  return l;
+}
+
+}  // namespace
+
+AdjointPlan plan_adjoint_edges_mixed(int64_t ne, int64_t nq, int sms) {
+  auto kernel = adjoint_edges_mixed_kernel<kEaQc>;
+  const int smem = static_cast<int>(sizeof(EdgeAdjSmem<kEaQc>));
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const int slots = resident_ctas(reinterpret_cast<const void*>(kernel), kFaThreads, smem, sms);
+  const int64_t ntiles = std::max<int64_t>(1, cdiv(ne, kTileFaces));
+  return plan_balanced(cdiv(ntiles, kFaTiles), nq, slots, kEaQc, 6 * ntiles * kTileFaces);
+}
+
+size_t adjoint_edges_mixed_scratch_bytes(const AdjointPlan& p, int64_t ne, int64_t nq) {
+  return edge_mixed_layout(p, ne, nq).total;
+}
+
+cudaError_t adjoint_edges_mixed(const AdjointPlan& p, const double* edges, int64_t le, int64_t ne,
+                                const double* q, int64_t nq, const double* gw, double kappa,
+                                double* dq, double* dedge, void* scratch, size_t scratch_bytes,
+                                cudaStream_t stream) {
+  cudaError_t e = cudaSuccess;
+  if (nq > 0) e = cudaMemsetAsync(dq, 0, sizeof(double) * 3 * nq, stream);
+  if (e == cudaSuccess && ne > 0) e = cudaMemsetAsync(dedge, 0, sizeof(double) * 6 * le, stream);
+  if (e != cudaSuccess || nq <= 0 || ne <= 0) return e;
+  const EdgeMixedLayout l = edge_mixed_layout(p, ne, nq);
+  if (scratch_bytes < l.total) return cudaErrorInvalidValue;
+  unsigned char* s = static_cast<unsigned char*>(scratch);
+  double* mid = reinterpret_cast<double*>(s + l.mid);
+  uint32_t* eperm = reinterpret_cast<uint32_t*>(s + l.eperm);
+  unsigned char* tiles = s + l.tiles;
+  double* e64 = reinterpret_cast<double*>(s + l.e64);
+  uint32_t* edge_of = reinterpret_cast<uint32_t*>(s + l.edge_of);
+  uint32_t* qperm = reinterpret_cast<uint32_t*>(s + l.qperm);
+  double4* qs = reinterpret_cast<double4*>(s + l.qs);
+  double* dO_part = reinterpret_cast<double*>(s + l.dO);
+  double* dE_part = reinterpret_cast<double*>(s + l.dE);
+  const size_t sort_bytes = l.tiles - l.sort;
+  const int64_t ntiles = cdiv(ne, kTileFaces);
+  const int64_t ld64 = ntiles * kTileFaces;
+  edge_midpoints_kernel<<<static_cast<unsigned>(cdiv(ne, 256)), 256, 0, stream>>>(edges, le, ne,
+                                                                                mid);
+  if ((e = mixed_sort_queries(mid, ne, eperm, s + l.sort, sort_bytes, stream)) != cudaSuccess)
+    return e;
+  build_edge_tiles_kernel<<<static_cast<unsigned>(ntiles), kTileFaces, 0, stream>>>(
+      edges, le, ne, eperm, kappa, tiles, e64, ld64, edge_of);
+  if ((e = mixed_sort_queries(q, nq, qperm, s + l.sort, sort_bytes, stream)) != cudaSuccess)
+    return e;
+  gather_sorted_queries_kernel<<<static_cast<unsigned>(cdiv(nq, 256)), 256, 0, stream>>>(
+      q, gw, qperm, nq, qs);
+  if ((e = cudaMemsetAsync(dO_part, 0, sizeof(double) * static_cast<size_t>(p.nranges) * nq * 3,
+                           stream)) != cudaSuccess)
+    return e;
+  MixedEdgeArgs a{tiles, ntiles, e64, ld64, qs, nq, static_cast<float>(kappa * kappa),
+                  p.blocks_per_range, p.queries_per_group, dO_part, dE_part};
+  auto kernel = adjoint_edges_mixed_kernel<kEaQc>;
+  const int smem = static_cast<int>(sizeof(EdgeAdjSmem<kEaQc>));
+  if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
+      cudaSuccess)
+    return e;
+  kernel<<<dim3(static_cast<unsigned>(p.nranges), static_cast<unsigned>(p.ngroups)), kFaThreads,
+           smem, stream>>>(a);
+  finish_dq_sorted_kernel<<<static_cast<unsigned>(cdiv(nq * 3, 256)), 256, 0, stream>>>(
+      dO_part, p.nranges, nq, qperm, dq);
+  finish_dedge_sorted_kernel<<<static_cast<unsigned>(cdiv(6 * ld64, 256)), 256, 0, stream>>>(
+      dE_part, p.ngroups, ld64, edge_of, le, dedge);
+  g_launches.fetch_add(7, std::memory_order_relaxed);
+  return cudaGetLastError();
+}
+
 cudaError_t gather_vertex_grad(const double* dtri, int64_t ld, int corners,
                                const int64_t* indptr, const int64_t* entries, int64_t nv,
                                double* dV, cudaStream_t stream) {

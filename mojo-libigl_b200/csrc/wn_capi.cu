@@ -726,6 +726,29 @@ int wn_backward_edges_device(const double* edges, int64_t le, int64_t ne, const 
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "boundary-edge adjoint launch");
 }
 
+int wn_backward_edges_mixed_device(const double* edges, int64_t le, int64_t ne, const double* q,
+                                   int64_t nq, const double* gw, double kappa, double* dq,
+                                   double* dedge, void* stream) {
+  WN_NVTX_RANGE();
+  if (ne < 0 || nq < 0 || le < ne || nq > 0x7fffffffLL || ne > 0x7fffffffLL)
+    return fail(WN_EINVAL, "bad sizes (ne=%lld, nq=%lld, le=%lld)", (long long)ne,
+                (long long)nq, (long long)le);
+  if (int code = check_kappa(kappa)) return code;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  int code = WN_OK;
+  DeviceCtx* c = context(&code);
+  if (!c) return code;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const AdjointPlan p = plan_adjoint_edges_mixed(ne, nq, c->sms);
+  const size_t sb = adjoint_edges_mixed_scratch_bytes(p, ne, nq);
+  void* scratch = nullptr;
+  cudaError_t e = dev_malloc_async(&scratch, sb, st);
+  if (e != cudaSuccess) return cuda_fail(e, "device allocation");
+  e = adjoint_edges_mixed(p, edges, le, ne, q, nq, gw, kappa, dq, dedge, scratch, sb, st);
+  cudaFreeAsync(scratch, st);
+  return e == cudaSuccess ? WN_OK : cuda_fail(e, "mixed boundary-edge adjoint launch");
+}
+
 int wn_gather_vertex_grad_device(const double* dtri, int64_t ld, int corners,
                                  const int64_t* indptr, const int64_t* entries, int64_t nv,
                                  double* dV, void* stream) {

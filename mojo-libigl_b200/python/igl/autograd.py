@@ -8,13 +8,13 @@ adjoint="faces": per-face sums over the queries (``wn_backward_fp64_device`` or,
 for precision="mixed", ``wn_backward_mixed_device``), then dL/dV gathered from
 the per-corner face gradients through a vertex -> (face, corner) list.
 adjoint="edges": the same derivative from the mesh's net boundary edges only
-(``wn_backward_edges_device``): the per-face terms of a directed side and of its
-reverse cancel at both endpoints, so interior edges contribute nothing (exactly
-zero for a closed, consistently oriented mesh).
+(``wn_backward_edges_device``, or ``wn_backward_edges_mixed_device`` after a
+mixed forward): the per-face terms of a directed side and of its reverse cancel
+at both endpoints, so interior edges contribute nothing (exactly zero for a
+closed, consistently oriented mesh).
 adjoint="auto" (default): "edges", except for a mixed-precision forward on a
 mesh with more net boundary edges than EDGE_FACE_RATIO times its faces (a
-triangle soup has three per face), where the per-face mixed adjoint costs less
-than the FP64 boundary-edge one.
+triangle soup has three per face), where the per-face mixed adjoint costs less.
 
 Tensors are plumbing here: the forward and the adjoints run in libwn_b200's
 kernels on the tensors' memory and current stream.
@@ -30,8 +30,9 @@ from . import _lib
 
 
 # Above this many net boundary edges per face the per-face mixed adjoint is
-# cheaper than the FP64 boundary-edge adjoint.
-EDGE_FACE_RATIO = 1.0
+# cheaper than the mixed boundary-edge adjoint (an edge pair costs 37 FP32
+# operations, a face pair 83).
+EDGE_FACE_RATIO = 2.0
 
 
 def _check(rc: int) -> None:
@@ -183,9 +184,10 @@ def boundary_edges(V: torch.Tensor, F: torch.Tensor):
     return edges, ne, ends
 
 
-def backward_edges(V, F, O, gW, edges=None):
-    """(dL/dV, dL/dO) from the net boundary edges (FP64); `edges` is
-    boundary_edges(V, F) when the caller has it already."""
+def backward_edges(V, F, O, gW, edges=None, precision: str = "fp64", kappa: float = 4.0):
+    """(dL/dV, dL/dO) from the net boundary edges, in FP64 or (precision="mixed")
+    FP32 far pairs with FP64 near pairs; `edges` is boundary_edges(V, F) when the
+    caller has it already."""
     handle = _lib.lib()
     q = O.to(torch.float64).contiguous()
     gw = gW.to(torch.float64).contiguous()
@@ -194,9 +196,14 @@ def backward_edges(V, F, O, gW, edges=None):
     le = edges.shape[1]
     dq = torch.empty((nq, 3), dtype=torch.float64, device=q.device)
     dedge = torch.zeros((6, le), dtype=torch.float64, device=q.device)
-    _check(handle.wn_backward_edges_device(edges.data_ptr(), le, ne, q.data_ptr(), nq,
-                                           gw.data_ptr(), dq.data_ptr(), dedge.data_ptr(),
-                                           _stream()))
+    if precision == "mixed":
+        _check(handle.wn_backward_edges_mixed_device(edges.data_ptr(), le, ne, q.data_ptr(), nq,
+                                                     gw.data_ptr(), kappa, dq.data_ptr(),
+                                                     dedge.data_ptr(), _stream()))
+    else:
+        _check(handle.wn_backward_edges_device(edges.data_ptr(), le, ne, q.data_ptr(), nq,
+                                               gw.data_ptr(), dq.data_ptr(), dedge.data_ptr(),
+                                               _stream()))
     return gather_vertices(dedge, le, ne, ends, nv, corners=2), dq
 
 
@@ -234,6 +241,7 @@ class WindingNumberFunction(torch.autograd.Function):
             w = forward_fp64(tri, ld, nf, O)
         ctx.save_for_backward(V, F, O)
         ctx.tri, ctx.ld, ctx.nf, ctx.adjoint = tri, ld, nf, adjoint
+        ctx.precision = precision
         return w.to(O.dtype)
 
     @staticmethod
@@ -249,7 +257,7 @@ class WindingNumberFunction(torch.autograd.Function):
                 ctx.mesh.close()
                 ctx.mesh = None
         if adjoint == "edges":
-            dV, dq = backward_edges(V, F, O, gW, edges)
+            dV, dq = backward_edges(V, F, O, gW, edges, precision=ctx.precision)
         elif ctx.mesh is not None:
             dq, dtri = ctx.mesh.backward(O, gW)
             dV = gather_vertices(dtri, ctx.ld, ctx.nf, F, V.shape[0])
@@ -266,8 +274,8 @@ def winding_number_torch(V: torch.Tensor, F: torch.Tensor, O: torch.Tensor,
     precision: "fp64" (plain FP64 forward and adjoint) or "mixed" (FP32 pairs with
     FP64 refinement of near-surface pairs, forward and adjoint); by default
     "mixed" for float32 queries and "fp64" otherwise. W has the dtype of O.
-    adjoint: "edges" (net boundary edges, FP64), "faces" (per-face reduction,
-    in the forward's precision) or "auto" (edges, or faces for a mixed forward on
+    adjoint: "edges" (net boundary edges), "faces" (per-face reduction), both in
+    the forward's precision, or "auto" (edges, or faces for a mixed forward on
     a mesh with many boundary edges, e.g. a triangle soup); all give the same
     derivative.
     """

@@ -277,3 +277,35 @@ def test_auto_adjoint_picks_faces_on_a_soup_and_edges_on_a_mesh(gpu_required, mo
         for a, b in zip(grads["mixed"], grads["fp64"]):
             assert np.abs(a - b).max() <= 1e-4 * np.abs(b).max()
     del torch
+
+
+@pytest.mark.parametrize("case", ["c4", "open_c3_sample", "degenerate"])
+def test_mixed_edge_adjoint_matches_fp64_edge_adjoint(gpu_required, case):
+    """The mixed-precision boundary-edge adjoint (FP32 far pairs in Morton-ordered
+    64-edge tiles, FP64 pairs with an endpoint within kappa |e|) against the FP64
+    boundary-edge adjoint: within 1e-4 of the largest gradient, finite, and bit
+    for bit repeatable; queries on vertices and edge midpoints included."""
+    import torch
+
+    if case == "c4":
+        V, F, O, _ = igl.synthetic.workload("c4_grad", n_queries=16384)
+    elif case == "open_c3_sample":
+        V, F, O, _ = igl.synthetic.workload("c3_open", n_queries=4096)
+    else:
+        V, F = igl.synthetic.bumpy_icosphere(3, seed=91)
+        F = igl.synthetic.delete_faces(F, 0.2, seed=92).copy()
+        F[:9] = F[:9, [0, 2, 1]]
+        F = np.concatenate([F, F[30:33], [[4, 4, 17]]])
+        O = np.concatenate([V[:40], 0.5 * (V[F[:40, 0]] + V[F[:40, 1]]),
+                            igl.synthetic.mixed_queries(V, F, 2000, seed=93, near_sigma=1e-3)])
+    g = _cuda(np.random.default_rng(94).normal(size=len(O)))
+    Vt, Ft, Ot = _cuda(V), _cuda(F), _cuda(O)
+    edges = wa.boundary_edges(Vt, Ft)
+    assert edges[1] > 0
+    dV64, dO64 = wa.backward_edges(Vt, Ft, Ot, g, edges)
+    dVm, dOm = wa.backward_edges(Vt, Ft, Ot, g, edges, precision="mixed")
+    dVm2, dOm2 = wa.backward_edges(Vt, Ft, Ot, g, edges, precision="mixed")
+    assert torch.isfinite(dVm).all() and torch.isfinite(dOm).all()
+    assert torch.equal(dVm, dVm2) and torch.equal(dOm, dOm2)
+    assert float((dVm - dV64).abs().max()) <= 1e-4 * float(dV64.abs().max())
+    assert float((dOm - dO64).abs().max()) <= 1e-4 * float(dO64.abs().max())

@@ -53,7 +53,8 @@ threads) on a bounded sample of the same workload and prints the same metric.
 exits (the commands behind the ncu summaries in profiles/): fp64_c3 (streaming
 FP64 kernel), fp64_tiled_c3 (FP64 over the prepared mesh), mixed_c3, adjoint_c4
 (per-face mixed adjoint on the gradient workload), adjoint_c3 (the same on the
-c3 workload), closest_c3 (closest-point traversal), fwn_c3 (fast
+c3 workload), adjoint_soup (the same on the c3 triangle soup), edges_open_c3 (the
+mixed boundary-edge adjoint on the open c3 mesh), closest_c3 (closest-point traversal), fwn_c3 (fast
 winding number, beta = 2), normals_s9 (area-weighted vertex normals of the
 subdivision-9 sphere) and batched_small (the batched persistent forward and
 edge adjoint on 16 uneven meshes with at most 65,536 queries each).
@@ -101,7 +102,7 @@ def parse_args():
     p.add_argument("--no-normals", action="store_true", help="skip the vertex-normal workloads")
     p.add_argument("--case", choices=("fp64_c3", "fp64_tiled_c3", "mixed_c3", "adjoint_c4",
                                       "closest_c3", "fwn_c3", "normals_s9", "adjoint_c3",
-                                      "batched_small"),
+                                      "adjoint_soup", "edges_open_c3", "batched_small"),
                    help="run one kernel on a small case twice (for profiling) and exit")
     p.add_argument("--case-queries", type=int, default=None)
     p.add_argument("--no-autotune", dest="autotune", action="store_false",
@@ -1068,6 +1069,20 @@ def run_case(args):
         bt.close()
         return
 
+    if args.case == "edges_open_c3":
+        from igl import autograd as wa
+        from igl import synthetic
+
+        V, F, O, _ = synthetic.workload("c3_open", n_queries=args.case_queries or 65536)
+        Vt, Ft, Ot = (torch.from_numpy(x).cuda() for x in (V, F, O))
+        g = torch.from_numpy(np.random.default_rng(5).normal(size=len(O))).cuda()
+        edges = wa.boundary_edges(Vt, Ft)
+        for _ in range(2):
+            dV, dq = wa.backward_edges(Vt, Ft, Ot, g, edges, precision="mixed")
+        torch.cuda.synchronize()
+        print("ok", args.case, edges[1], len(O), float(dq.abs().sum()))
+        return
+
     if args.case == "normals_s9":
         from igl import normals, synthetic
 
@@ -1087,12 +1102,12 @@ def run_case(args):
     handle = _lib.lib()
     default_nq = {"fp64_c3": 16384, "fp64_tiled_c3": 32768, "mixed_c3": 65536,
                   "adjoint_c4": 16384, "closest_c3": 1 << 20, "fwn_c3": 1 << 20,
-                  "normals_s9": 1, "adjoint_c3": 65536}[args.case]
+                  "normals_s9": 1, "adjoint_c3": 65536, "adjoint_soup": 65536}[args.case]
     nq = args.case_queries or default_nq
-    V, F, O, _ = synthetic.workload("c4_grad" if args.case == "adjoint_c4" else "c3_mixed",
-                                    n_queries=nq)
-    if args.case == "adjoint_c3":
-        args.case = "adjoint_c4"  # the same call on the c3 inputs
+    wl = {"adjoint_c4": "c4_grad", "adjoint_soup": "c3_soup"}.get(args.case, "c3_mixed")
+    V, F, O, _ = synthetic.workload(wl, n_queries=nq)
+    if args.case in ("adjoint_c3", "adjoint_soup"):
+        args.case = "adjoint_c4"  # the same call on the c3 (or c3 soup) inputs
     Vt, Ft, Ot = (torch.from_numpy(x).cuda() for x in (V, F, O))
     sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     tri, ld, nf = wa.triangle_soa(Vt, Ft)

@@ -111,12 +111,22 @@ int wn_forward_fp64_device_noalloc(const double* tri, int64_t ld, const double* 
   if (mode != kFp64ArgProd && mode != kFp64Direct) return noalloc_fail(WN_EINVAL, "bad mode");
   if (nq == 0) return WN_OK;
 
+  // The capture state is asked first, before any other runtime call touches the
+  // stream: a refused call must leave the caller's capture intact.
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(st, &capture);
+  if (e != cudaSuccess)
+    return noalloc_fail(WN_EINVAL, "cudaStreamIsCapturing on the given stream", e);
+  if (capture != cudaStreamCaptureStatusNone)
+    return noalloc_fail(WN_EINVAL,
+                        "the stream is being captured: this call waits for its stream before "
+                        "it returns, which would end the capture");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
     return noalloc_fail(WN_ENODEV, "no usable CUDA device", e);
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   int stream_dev = dev;
   if ((e = cudaStreamGetDevice(st, &stream_dev)) != cudaSuccess)
     return noalloc_fail(WN_EINVAL, "cudaStreamGetDevice on the given stream", e);
@@ -124,13 +134,6 @@ int wn_forward_fp64_device_noalloc(const double* tri, int64_t ld, const double* 
     return noalloc_fail(WN_EINVAL,
                         "the stream belongs to another device than the current one: make the "
                         "stream's device current before the call");
-  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
-  if ((e = cudaStreamIsCapturing(st, &capture)) != cudaSuccess)
-    return noalloc_fail(WN_EINVAL, "cudaStreamIsCapturing on the given stream", e);
-  if (capture != cudaStreamCaptureStatusNone)
-    return noalloc_fail(WN_EINVAL,
-                        "the stream is being captured: this call waits for its stream before "
-                        "it returns, which would end the capture");
   NoAllocDevice& d = g_noalloc_dev[dev];
   if (!d.ready) {
     // Once per device, with that device current: device addresses of the

@@ -176,20 +176,15 @@ __global__ void sum_splits_kernel(const double* __restrict__ partial, int64_t ns
 // ---- FP64 over a prepared mesh, with corner reuse ---------------------------
 // Same bit-exact pair terms and argument-of-product sum, but the faces come from a
 // prepared mesh (wn_mixed.cu): Morton-ordered 64-face tiles whose faces are
-// ordered as strips. a = v - o and |a| (three subtractions, three products, two
-// sums and a correctly rounded sqrt) depend only on the vertex and the query, so
-// a corner shared with the previous face is not recomputed: the same bits, about
-// 40% fewer FP64 instructions per pair on a typical mesh.
-//
-// Each thread keeps three corner slots per query. A face's code (one byte,
-// s0 + 3 s1 + 9 s2 + 27 mask) names the slot holding each of its corners and
-// which of them are new; a new corner is computed straight into its slot (one the
-// face does not read otherwise), so nothing is copied between faces. The codes
-// are assigned per tile by the mesh preparation; 0xff marks padding.
+// ordered as strips, with a per-face code telling which corners equal a corner
+// of the previous face. a = v - o and |a| (three subtractions, three products,
+// two sums and a correctly rounded sqrt) depend only on the vertex and the
+// query, so a repeated corner is copied instead of recomputed: the same bits,
+// about 40% fewer FP64 instructions per pair on a typical mesh.
 struct Fp64TiledArgs {
   const double* tri64;  // 9 x ld64, tile-major sorted soup
   int64_t ld64;
-  const uint8_t* reuse;  // ld64 slot codes
+  const uint8_t* reuse;  // ld64 codes
   int64_t ntiles;
   const double* q;
   int64_t nq;
@@ -201,60 +196,75 @@ struct Fp64TiledArgs {
 
 constexpr int kFp64TileBytes = 9 * kTileFaces * 8 + kTileFaces;  // coordinates + codes
 
-template <int S>
-__device__ __forceinline__ Corner& slot_ref(Corner& s0, Corner& s1, Corner& s2) {
-  if constexpr (S == 0)
-    return s0;
-  else if constexpr (S == 1)
-    return s1;
+__device__ __forceinline__ Corner pick_corner(unsigned code, const Corner& c0, const Corner& c1,
+                                              const Corner& c2) {
+  return code == 0 ? c0 : (code == 1 ? c1 : c2);
+}
+
+// Corner `pos` of face j when its reuse code M is known at compile time: one of
+// the previous face's corners (M = 0..2) or a new one computed from the tile.
+template <unsigned M>
+__device__ __forceinline__ Corner corner_of(const Corner& p0, const Corner& p1, const Corner& p2,
+                                            double ox, double oy, double oz, const double* s,
+                                            int pos, int j) {
+  if constexpr (M == 3)
+    return corner_exact(ox, oy, oz, s[(3 * pos) * kTileFaces + j],
+                        s[(3 * pos + 1) * kTileFaces + j], s[(3 * pos + 2) * kTileFaces + j]);
+  else if constexpr (M == 0)
+    return p0;
+  else if constexpr (M == 1)
+    return p1;
   else
-    return s2;
+    return p2;
 }
 
-// Corner `pos` of face j from the tile in shared memory.
-__device__ __forceinline__ Corner tile_corner(const double* s, int pos, int j, double ox,
-                                              double oy, double oz) {
-  return corner_exact(ox, oy, oz, s[(3 * pos) * kTileFaces + j],
-                      s[(3 * pos + 1) * kTileFaces + j], s[(3 * pos + 2) * kTileFaces + j]);
-}
-
-// det and denom of face j for one query, its slots updated. The code is the same
-// for every lane (all lanes walk the same face), so the switch is a uniform branch;
-// each case names its slots at compile time. The preparation emits only these 28
-// codes (strip faces with one or two shared corners in distinct slots, and faces
-// whose corners are all computed anew, which is what any other face gets).
-__device__ __forceinline__ void face_from_slots(unsigned code, Corner& q0, Corner& q1, Corner& q2,
-                                                double ox, double oy, double oz,
-                                                const double* s, int j, double& det,
-                                                double& denom) {
-#define WN_SLOT_BODY(S0, S1, S2, M)                                                     \
-    if ((M) & 1) slot_ref<S0>(q0, q1, q2) = tile_corner(s, 0, j, ox, oy, oz);           \
-    if ((M) & 2) slot_ref<S1>(q0, q1, q2) = tile_corner(s, 1, j, ox, oy, oz);           \
-    if ((M) & 4) slot_ref<S2>(q0, q1, q2) = tile_corner(s, 2, j, ox, oy, oz);           \
-    face_exact(slot_ref<S0>(q0, q1, q2), slot_ref<S1>(q0, q1, q2), slot_ref<S2>(q0, q1, q2), \
-               det, denom);                                                             \
+// The three corners of face j. The code is the same for every lane (all lanes
+// walk the same face), so a switch over it is a uniform branch, and each case
+// names its corners at compile time: no per-register selects. The cases are
+// the 28 codes whose reused corners are distinct with at most two of them (a
+// face that shares all three corners with the previous one is a duplicate and
+// takes the generic path).
+__device__ __forceinline__ void face_corners(unsigned code, const Corner& p0, const Corner& p1,
+                                             const Corner& p2, double ox, double oy, double oz,
+                                             const double* s, int j, Corner& c0, Corner& c1,
+                                             Corner& c2) {
+#define WN_FACE_CASE(A, B, C)                                 \
+  case (A) | ((B) << 2) | ((C) << 4):                         \
+    c0 = corner_of<A>(p0, p1, p2, ox, oy, oz, s, 0, j);       \
+    c1 = corner_of<B>(p0, p1, p2, ox, oy, oz, s, 1, j);       \
+    c2 = corner_of<C>(p0, p1, p2, ox, oy, oz, s, 2, j);       \
     return;
-#define WN_SLOT_CASE(S0, S1, S2, M) \
-  case (S0) + 3 * (S1) + 9 * (S2) + 27 * (M): WN_SLOT_BODY(S0, S1, S2, M)
   switch (code) {
-    WN_SLOT_CASE(0, 1, 2, 1) WN_SLOT_CASE(0, 1, 2, 2) WN_SLOT_CASE(0, 1, 2, 4)
-    WN_SLOT_CASE(0, 2, 1, 1) WN_SLOT_CASE(0, 2, 1, 2) WN_SLOT_CASE(0, 2, 1, 4)
-    WN_SLOT_CASE(1, 0, 2, 1) WN_SLOT_CASE(1, 0, 2, 2) WN_SLOT_CASE(1, 0, 2, 4)
-    WN_SLOT_CASE(1, 2, 0, 1) WN_SLOT_CASE(1, 2, 0, 2) WN_SLOT_CASE(1, 2, 0, 4)
-    WN_SLOT_CASE(2, 0, 1, 1) WN_SLOT_CASE(2, 0, 1, 2) WN_SLOT_CASE(2, 0, 1, 4)
-    WN_SLOT_CASE(2, 1, 0, 1) WN_SLOT_CASE(2, 1, 0, 2) WN_SLOT_CASE(2, 1, 0, 4)
-    WN_SLOT_CASE(0, 1, 2, 3) WN_SLOT_CASE(0, 1, 2, 5) WN_SLOT_CASE(0, 1, 2, 6)
-    WN_SLOT_CASE(0, 2, 1, 3) WN_SLOT_CASE(0, 2, 1, 5) WN_SLOT_CASE(1, 0, 2, 5)
-    WN_SLOT_CASE(1, 0, 2, 6) WN_SLOT_CASE(1, 2, 0, 3) WN_SLOT_CASE(2, 0, 1, 6)
-    default:  // all three corners new: (0, 1, 2), mask 7
-      WN_SLOT_BODY(0, 1, 2, 7)
+    WN_FACE_CASE(3, 3, 3)
+    WN_FACE_CASE(0, 3, 3) WN_FACE_CASE(1, 3, 3) WN_FACE_CASE(2, 3, 3)
+    WN_FACE_CASE(3, 0, 3) WN_FACE_CASE(3, 1, 3) WN_FACE_CASE(3, 2, 3)
+    WN_FACE_CASE(3, 3, 0) WN_FACE_CASE(3, 3, 1) WN_FACE_CASE(3, 3, 2)
+    WN_FACE_CASE(3, 0, 1) WN_FACE_CASE(3, 0, 2) WN_FACE_CASE(3, 1, 0)
+    WN_FACE_CASE(3, 1, 2) WN_FACE_CASE(3, 2, 0) WN_FACE_CASE(3, 2, 1)
+    WN_FACE_CASE(0, 3, 1) WN_FACE_CASE(0, 3, 2) WN_FACE_CASE(1, 3, 0)
+    WN_FACE_CASE(1, 3, 2) WN_FACE_CASE(2, 3, 0) WN_FACE_CASE(2, 3, 1)
+    WN_FACE_CASE(0, 1, 3) WN_FACE_CASE(0, 2, 3) WN_FACE_CASE(1, 0, 3)
+    WN_FACE_CASE(1, 2, 3) WN_FACE_CASE(2, 0, 3) WN_FACE_CASE(2, 1, 3)
+    default:
+      break;
   }
-#undef WN_SLOT_CASE
-#undef WN_SLOT_BODY
+#undef WN_FACE_CASE
+  Corner c[3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const unsigned cm = (code >> (2 * m)) & 3u;
+    c[m] = cm == 3u ? corner_exact(ox, oy, oz, s[(3 * m) * kTileFaces + j],
+                                   s[(3 * m + 1) * kTileFaces + j],
+                                   s[(3 * m + 2) * kTileFaces + j])
+                    : pick_corner(cm, p0, p1, p2);
+  }
+  c0 = c[0];
+  c1 = c[1];
+  c2 = c[2];
 }
 
 template <int THREADS, int QPT, int STAGES>
-__global__ void __launch_bounds__(THREADS, 7) fp64_tiled_kernel(const Fp64TiledArgs a) {
+__global__ void __launch_bounds__(THREADS) fp64_tiled_kernel(const Fp64TiledArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* ring = smem_raw;  // [STAGES][kFp64TileBytes]
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + STAGES * kFp64TileBytes);
@@ -294,11 +304,11 @@ __global__ void __launch_bounds__(THREADS, 7) fp64_tiled_kernel(const Fp64TiledA
   if (tid == 0)
     for (; issued < min(STAGES, ntiles); ++issued) issue(issued);
   ArgAcc acc[QPT];
-  Corner q0[QPT], q1[QPT], q2[QPT];  // the three corner slots of each query
+  Corner p0[QPT], p1[QPT], p2[QPT];
 #pragma unroll
   for (int k = 0; k < QPT; ++k) {
     argacc_init(acc[k]);
-    q0[k] = q1[k] = q2[k] = Corner{0, 0, 0, 0};
+    p0[k] = p1[k] = p2[k] = Corner{0, 0, 0, 0};
   }
   bool failed = false;
   int t = 0;
@@ -318,9 +328,14 @@ __global__ void __launch_bounds__(THREADS, 7) fp64_tiled_kernel(const Fp64TiledA
       if (code == 0xffu) break;  // padding: the rest of the tile is empty
 #pragma unroll
       for (int k = 0; k < QPT; ++k) {
+        Corner c0, c1, c2;
+        face_corners(code, p0[k], p1[k], p2[k], ox[k], oy[k], oz[k], s, j, c0, c1, c2);
         double det, denom;
-        face_from_slots(code, q0[k], q1[k], q2[k], ox[k], oy[k], oz[k], s, j, det, denom);
+        face_exact(c0, c1, c2, det, denom);
         argacc_push(acc[k], denom, det);
+        p0[k] = c0;
+        p1[k] = c1;
+        p2[k] = c2;
       }
     }
   }

@@ -170,7 +170,6 @@ __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
   __shared__ int64_t sf[kTileFaces];
   __shared__ int sorder[kTileFaces];
   __shared__ int sbest[kTileFaces / 32];
-  __shared__ uint8_t sprev[kTileFaces];  // previous-face corner codes (reuse pass)
   const int j = threadIdx.x, warp = j >> 5, lane = j & 31;
   const int64_t tile = blockIdx.x;
   const int64_t first = tile_first ? tile_first[tile] : tile * kTileFaces;
@@ -263,7 +262,8 @@ __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
   // Order the tile's faces as strips: each next face is the unvisited one that
   // shares the most corners (bitwise-equal coordinates) with the current one.
   // Consecutive faces then share corners, whose (v - o, |v - o|) the FP64 kernel
-  // reuses through the slot codes in reuse[] (below).
+  // reuses; reuse[slot] says, per corner, which corner of the previous face it
+  // equals (0..2) or 3 for a new one (0xff marks padding).
 #pragma unroll
   for (int r = 0; r < 9; ++r) sv[j][r] = v[r];
   sf[j] = f;
@@ -306,7 +306,6 @@ __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
   for (int r = 0; r < 9; ++r) tri64[r * ld64 + slot] = valid ? v[r] : 0.0;
   face_of[slot] = valid ? static_cast<uint32_t>(f) : 0xffffffffu;
   if (reuse) {
-    // Per corner, the previous face's equal corner (0..2) or 3 for a new one ...
     unsigned code = 0;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -319,54 +318,7 @@ __global__ void __launch_bounds__(kTileFaces) build_tiles_kernel(
             match = static_cast<unsigned>(m);
       code |= match << (2 * k);
     }
-    sprev[j] = static_cast<uint8_t>(code);
-    __syncthreads();
-    // ... then, walking the tile in order, the corner slots of the FP64 kernel
-    // (wn_fp64.cu): a shared corner stays in the slot it had in the previous face,
-    // new corners take the free slots in increasing order. Code s0 + 3 s1 + 9 s2 +
-    // 27 mask (mask bit k: corner k is new), 0xff for padding.
-    if (j == 0) {
-      unsigned held[3] = {0u, 1u, 2u};  // slots of the previous face's corners
-      for (int i = 0; i < kTileFaces; ++i) {
-        if (i >= cnt) {
-          reuse[tile * kTileFaces + i] = 0xff;
-          continue;
-        }
-        const unsigned c = sprev[i];
-        unsigned sl[3] = {0u, 0u, 0u}, mask = 0u;
-        bool used[3] = {false, false, false};
-        for (int k = 0; k < 3; ++k) {
-          const unsigned m = (c >> (2 * k)) & 3u;
-          if (m < 3u && i > 0) {
-            sl[k] = held[m];
-            used[sl[k]] = true;
-          } else {
-            mask |= 1u << k;
-          }
-        }
-        unsigned next = 0u;
-        for (int k = 0; k < 3; ++k) {
-          if (!((mask >> k) & 1u)) continue;
-          while (used[next]) ++next;
-          sl[k] = next;
-          used[next] = true;
-        }
-        // The FP64 kernel names the slots of strip faces at compile time; a face
-        // whose shared corners would share a slot (repeated corners) or that has no
-        // new corner is computed anew in slots 0, 1, 2.
-        if (mask == 0u || sl[0] == sl[1] || sl[1] == sl[2] || sl[0] == sl[2]) {
-          mask = 7u;
-          sl[0] = 0u;
-          sl[1] = 1u;
-          sl[2] = 2u;
-        }
-        reuse[tile * kTileFaces + i] = static_cast<uint8_t>(sl[0] + 3u * sl[1] + 9u * sl[2] +
-                                                            27u * mask);
-        held[0] = sl[0];
-        held[1] = sl[1];
-        held[2] = sl[2];
-      }
-    }
+    reuse[slot] = valid ? static_cast<uint8_t>(code) : static_cast<uint8_t>(0xff);
   }
   double h2f = 0.0;
 #pragma unroll

@@ -63,9 +63,8 @@ struct MixedMesh {
   uint32_t* face_of = nullptr;     // ld64: sorted slot -> input face (0xffffffff = padding)
   int tile_faces = 64;             // faces per far test and angle product of the mixed
                                    // forward: 64, or 32 (each half tile on its own)
-  uint8_t* reuse = nullptr;        // ld64: corner-slot code of the FP64 kernel per face
-                                   // (s0 + 3 s1 + 9 s2 + 27 new-mask; 0xff = padding).
-                                   // May be null.
+  uint8_t* reuse = nullptr;        // ld64: per corner (2 bits) the previous face's equal corner
+                                   // (0..2) or 3 = new; 0xff = padding. May be null.
 };
 
 inline int64_t mixed_tiles(int64_t nf) { return nf > 0 ? (nf + kTileFaces - 1) / kTileFaces : 1; }

@@ -238,10 +238,14 @@ int wn_backward_edges_device(const double* edges, int64_t le, int64_t ne, const 
  * plus kappa (>= 3). Edges are Morton-ordered into 64-edge tiles inside the call;
  * pairs with both endpoints at least kappa * |edge| from the query run in FP32 in
  * the tile's scaled frame, the others in FP64; FP64 sums across query chunks and
- * over edges. Deterministic. */
+ * over edges. Deterministic. unit_weights = 0: the per-endpoint sums are weighted
+ * by m, as wn_backward_edges_device's. unit_weights = 1 (edges welded by position
+ * from a triangle soup, m = the net count of the soup's directed sides on the
+ * edge): dedge holds the unweighted sums -dL/dW dOmega/dP and -dL/dW dOmega/dQ of
+ * one side P -> Q, to be signed per soup side, while dq still uses m. */
 int wn_backward_edges_mixed_device(const double* edges, int64_t le, int64_t ne, const double* q,
-                                   int64_t nq, const double* gw, double kappa, double* dq,
-                                   double* dedge, void* stream);
+                                   int64_t nq, const double* gw, double kappa, int unit_weights,
+                                   double* dq, double* dedge, void* stream);
 
 /* dV (nv x 3) = sum of per-element corner gradients over each vertex's uses.
  * grad: rows 3*corner+axis with stride ld; corners = 3 (faces, dtri) or 2 (edges,

@@ -235,7 +235,10 @@ struct FaceAdjSmem {
   double red64[kFaTiles][QC][3];      // per-warp FP64 shares of refined pairs
   double dsum[QC * 3];                // the chunk's dL/do sums before they go to global
   double4 q64[QC];                    // FP64 query and g (refinement)
-  float4 frame[QC][kFaTiles];         // query in the tile's scaled frame, w = g * scale
+  // Per (query, tile), as ready-made FP32x2 operands (both lanes alike): minus the
+  // query in the tile's scaled frame, g * scale and its negation:
+  // (-x, -x, -y, -y), (-z, -z, gs, gs), (-gs, -gs, 0, 0).
+  float4 frame[QC][kFaTiles][3];
   int flag[QC][kFaTiles];             // 0: far, 1: careful (near test), 2: skip
   TileHeader th[kFaTiles];
 };
@@ -277,6 +280,82 @@ __device__ __forceinline__ float2 cross_c(float2 u1, float2 v2, float2 u2, float
   return __ffma2_rn(u1, v2, __fmul2_rn(make_float2(-u2.x, -u2.y), v1));
 }
 
+// One query against this thread's two faces (the two lanes of every float2): adds
+// -g dOmega/d(A, B, C) into acc and returns g dOmega/do in d. fr: the query's
+// frame operands (see FaceAdjSmem::frame); fnn = -n. Every operand is a whole
+// FP32x2 pair and no sign is flipped per pair: -a comes from one packed multiply,
+// -(b x c) = a x b + c x a - n, and the two coefficients of b x c are formed with
+// -g. With CAREFUL, a lane whose face has a vertex closer than sqrt(thr) takes
+// g = 0 (and unit squared lengths, so every term is finite and zero); bit k of
+// the result flags lane k.
+template <bool CAREFUL>
+__device__ __forceinline__ unsigned face_pair_terms(const float4 (&fr)[3], const float2 (&fa)[3],
+                                                    const float2 (&fe1)[3], const float2 (&fe2)[3],
+                                                    const float2 (&fnn)[3], const float2 (&fg)[3],
+                                                    float thr0, float thr1, float2 (&acc)[9],
+                                                    float2 (&d)[3]) {
+  const float4 f0 = fr[0], f1 = fr[1], f2v = fr[2];
+  const float2 ax = __fadd2_rn(fa[0], make_float2(f0.x, f0.y));
+  const float2 ay = __fadd2_rn(fa[1], make_float2(f0.z, f0.w));
+  const float2 az = __fadd2_rn(fa[2], make_float2(f1.x, f1.y));
+  float2 g2 = make_float2(f1.z, f1.w), ng2 = make_float2(f2v.x, f2v.y);
+  const float2 m1 = f2(-1.f), two = f2(2.f);
+  float2 aa = __ffma2_rn(ax, ax, __ffma2_rn(ay, ay, __fmul2_rn(az, az)));
+  const float2 s1 = __ffma2_rn(ax, fe1[0], __ffma2_rn(ay, fe1[1], __fmul2_rn(az, fe1[2])));
+  const float2 s2 = __ffma2_rn(ax, fe2[0], __ffma2_rn(ay, fe2[1], __fmul2_rn(az, fe2[2])));
+  const float2 ab = __fadd2_rn(aa, s1), ca = __fadd2_rn(aa, s2);
+  float2 bb = __ffma2_rn(two, s1, __fadd2_rn(aa, fg[0]));
+  float2 cc = __ffma2_rn(two, s2, __fadd2_rn(aa, fg[1]));
+  const float2 bc = __fadd2_rn(ab, __fadd2_rn(s2, fg[2]));
+  unsigned nb = 0u;
+  if constexpr (CAREFUL) {
+    const bool n0 = fminf(aa.x, fminf(bb.x, cc.x)) < thr0;
+    const bool n1 = fminf(aa.y, fminf(bb.y, cc.y)) < thr1;
+    nb = (n0 ? 1u : 0u) | (n1 ? 2u : 0u);
+    g2 = make_float2(n0 ? 0.f : g2.x, n1 ? 0.f : g2.y);
+    ng2 = make_float2(n0 ? 0.f : ng2.x, n1 ? 0.f : ng2.y);
+    aa = make_float2(n0 ? 1.f : aa.x, n1 ? 1.f : aa.y);
+    bb = make_float2(n0 ? 1.f : bb.x, n1 ? 1.f : bb.y);
+    cc = make_float2(n0 ? 1.f : cc.x, n1 ? 1.f : cc.y);
+  }
+  const float2 ra = rsqrt2(aa), rb = rsqrt2(bb), rc = rsqrt2(cc);
+  const float2 la = __fmul2_rn(aa, ra), lb = __fmul2_rn(bb, rb), lc = __fmul2_rn(cc, rc);
+  const float2 iab = rcp2(__ffma2_rn(la, lb, ab));
+  const float2 ibc = rcp2(__ffma2_rn(lb, lc, bc));
+  const float2 ica = rcp2(__ffma2_rn(lc, la, ca));
+  const float2 gab = __fmul2_rn(g2, iab), gca = __fmul2_rn(g2, ica);
+  const float2 ngbc = __fmul2_rn(ng2, ibc);
+  const float2 kA1 = __fmul2_rn(ra, gab), kA2 = __fmul2_rn(ra, gca);
+  const float2 kB1 = __fmul2_rn(rb, gab), nkB2 = __fmul2_rn(rb, ngbc);
+  const float2 nkC1 = __fmul2_rn(rc, ngbc), kC2 = __fmul2_rn(rc, gca);
+  // a x b = a x e1 and c x a = e2 x a with -a; -(b x c) = a x b + c x a - n.
+  const float2 nax = __fmul2_rn(ax, m1), nay = __fmul2_rn(ay, m1), naz = __fmul2_rn(az, m1);
+  const float2 xab0 = __ffma2_rn(ay, fe1[2], __fmul2_rn(naz, fe1[1]));
+  const float2 xab1 = __ffma2_rn(az, fe1[0], __fmul2_rn(nax, fe1[2]));
+  const float2 xab2 = __ffma2_rn(ax, fe1[1], __fmul2_rn(nay, fe1[0]));
+  const float2 xca0 = __ffma2_rn(fe2[1], az, __fmul2_rn(fe2[2], nay));
+  const float2 xca1 = __ffma2_rn(fe2[2], ax, __fmul2_rn(fe2[0], naz));
+  const float2 xca2 = __ffma2_rn(fe2[0], ay, __fmul2_rn(fe2[1], nax));
+  const float2 nxbc0 = __fadd2_rn(__fadd2_rn(xab0, xca0), fnn[0]);
+  const float2 nxbc1 = __fadd2_rn(__fadd2_rn(xab1, xca1), fnn[1]);
+  const float2 nxbc2 = __fadd2_rn(__fadd2_rn(xab2, xca2), fnn[2]);
+  acc[0] = __ffma2_rn(kA1, xab0, __ffma2_rn(kA2, xca0, acc[0]));
+  acc[1] = __ffma2_rn(kA1, xab1, __ffma2_rn(kA2, xca1, acc[1]));
+  acc[2] = __ffma2_rn(kA1, xab2, __ffma2_rn(kA2, xca2, acc[2]));
+  acc[3] = __ffma2_rn(kB1, xab0, __ffma2_rn(nkB2, nxbc0, acc[3]));
+  acc[4] = __ffma2_rn(kB1, xab1, __ffma2_rn(nkB2, nxbc1, acc[4]));
+  acc[5] = __ffma2_rn(kB1, xab2, __ffma2_rn(nkB2, nxbc2, acc[5]));
+  acc[6] = __ffma2_rn(nkC1, nxbc0, __ffma2_rn(kC2, xca0, acc[6]));
+  acc[7] = __ffma2_rn(nkC1, nxbc1, __ffma2_rn(kC2, xca1, acc[7]));
+  acc[8] = __ffma2_rn(nkC1, nxbc2, __ffma2_rn(kC2, xca2, acc[8]));
+  const float2 sab = __fadd2_rn(kA1, kB1), nsbc = __fadd2_rn(nkB2, nkC1);
+  const float2 sca = __fadd2_rn(kC2, kA2);
+  d[0] = __ffma2_rn(sab, xab0, __ffma2_rn(nsbc, nxbc0, __fmul2_rn(sca, xca0)));
+  d[1] = __ffma2_rn(sab, xab1, __ffma2_rn(nsbc, nxbc1, __fmul2_rn(sca, xca1)));
+  d[2] = __ffma2_rn(sab, xab2, __ffma2_rn(nsbc, nxbc2, __fmul2_rn(sca, xca2)));
+  return nb;
+}
+
 template <int QC>
 __global__ void __launch_bounds__(kFaThreads, 4) adjoint_faces_kernel(const MixedAdjointArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -309,7 +388,7 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_faces_kernel(const Mixe
     const bool tile_ok = t < a.ntiles;
     const unsigned char* rec = a.tiles + (tile_ok ? t : 0) * kTileBytes;
     const int n = tile_ok ? reinterpret_cast<const TileHeader*>(rec)->n : 0;
-    float2 fa[3], fe1[3], fe2[3], fn[3], fg[3];
+    float2 fa[3], fe1[3], fe2[3], fnn[3], fg[3];  // fnn = -n
     const float* thr_rec = reinterpret_cast<const float*>(rec + kTileHeaderBytes) + 16 * lane + 15;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
@@ -327,7 +406,7 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_faces_kernel(const Mixe
       lane_ref(fa[0], k) = r0.x;  lane_ref(fa[1], k) = r0.y;  lane_ref(fa[2], k) = r0.z;
       lane_ref(fe1[0], k) = r0.w; lane_ref(fe1[1], k) = r1.x; lane_ref(fe1[2], k) = r1.y;
       lane_ref(fe2[0], k) = r1.z; lane_ref(fe2[1], k) = r1.w; lane_ref(fe2[2], k) = r2.x;
-      lane_ref(fn[0], k) = r2.y;  lane_ref(fn[1], k) = r2.z;  lane_ref(fn[2], k) = r2.w;
+      lane_ref(fnn[0], k) = -r2.y; lane_ref(fnn[1], k) = -r2.z; lane_ref(fnn[2], k) = -r2.w;
       lane_ref(fg[0], k) = r3.x;  lane_ref(fg[1], k) = r3.y;  lane_ref(fg[2], k) = r3.z;
     }
     const int64_t slot0 = (tile_ok ? t : 0) * kTileFaces + lane;
@@ -351,10 +430,13 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_faces_kernel(const Mixe
           // Beyond 2^40 tile radii the tile's terms are below 2^-80 of a near one and
           // squared FP32 distances could overflow: the tile is skipped for this query.
           const bool skip = d2 * th.scale * th.scale > 1.2089258196146292e24;
-          sm.frame[jq][tt] = make_float4(static_cast<float>(dx * th.scale),
-                                         static_cast<float>(dy * th.scale),
-                                         static_cast<float>(dz * th.scale),
-                                         static_cast<float>(o.w * th.scale));
+          const float lx = static_cast<float>(dx * th.scale);
+          const float ly = static_cast<float>(dy * th.scale);
+          const float lz = static_cast<float>(dz * th.scale);
+          const float gs = static_cast<float>(o.w * th.scale);
+          sm.frame[jq][tt][0] = make_float4(-lx, -lx, -ly, -ly);
+          sm.frame[jq][tt][1] = make_float4(-lz, -lz, gs, gs);
+          sm.frame[jq][tt][2] = make_float4(-gs, -gs, 0.f, 0.f);
           sm.flag[jq][tt] = skip ? 2 : (d2 >= th.far_r2 ? 0 : 1);
           if (tt == 0) sm.q64[jq] = o;
         }
@@ -363,78 +445,44 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_faces_kernel(const Mixe
       __syncthreads();
       static_assert(QC <= 32, "one mask bit per query of a chunk");
       unsigned near0 = 0u, near1 = 0u;  // bit jq: the pair (query jq, face k) is refined
+      // This warp's far and careful queries of the chunk (flags of its tile), taken in
+      // two branch-free loops; skipped queries only store zero shares.
+      const int myflag = lane < nc ? sm.flag[lane][warp] : 2;
+      const unsigned far_q = __ballot_sync(0xffffffffu, myflag == 0);
+      const unsigned careful_q = __ballot_sync(0xffffffffu, myflag == 1);
+      const unsigned skip_q = __ballot_sync(0xffffffffu, myflag == 2 && lane < nc);
 #pragma unroll 1
-      for (int jq = 0; jq < nc; ++jq) {
-        const float4 f = sm.frame[jq][warp];
-        const int flag = sm.flag[jq][warp];  // uniform over the warp
-        float2 d0 = f2(0.f), d1 = f2(0.f), d2 = f2(0.f);
-        if (flag != 2) {
-          const float2 ax = __fadd2_rn(fa[0], f2(-f.x));
-          const float2 ay = __fadd2_rn(fa[1], f2(-f.y));
-          const float2 az = __fadd2_rn(fa[2], f2(-f.z));
-          const float2 aa = __ffma2_rn(ax, ax, __ffma2_rn(ay, ay, __fmul2_rn(az, az)));
-          const float2 s1 = __ffma2_rn(ax, fe1[0], __ffma2_rn(ay, fe1[1], __fmul2_rn(az, fe1[2])));
-          const float2 s2 = __ffma2_rn(ax, fe2[0], __ffma2_rn(ay, fe2[1], __fmul2_rn(az, fe2[2])));
-          const float2 ab = __fadd2_rn(aa, s1), ca = __fadd2_rn(aa, s2);
-          const float2 bb = __ffma2_rn(f2(2.f), s1, __fadd2_rn(aa, fg[0]));
-          const float2 cc = __ffma2_rn(f2(2.f), s2, __fadd2_rn(aa, fg[1]));
-          const float2 bc = __fadd2_rn(ab, __fadd2_rn(s2, fg[2]));
-          const float2 ra = rsqrt2(aa), rb = rsqrt2(bb), rc = rsqrt2(cc);
-          const float2 la = __fmul2_rn(aa, ra), lb = __fmul2_rn(bb, rb), lc = __fmul2_rn(cc, rc);
-          const float2 iab = rcp2(__ffma2_rn(la, lb, ab));
-          const float2 ibc = rcp2(__ffma2_rn(lb, lc, bc));
-          const float2 ica = rcp2(__ffma2_rn(lc, la, ca));
-          const float2 g2 = f2(f.w);
-          const float2 gab = __fmul2_rn(g2, iab), gbc = __fmul2_rn(g2, ibc);
-          const float2 gca = __fmul2_rn(g2, ica);
-          float2 kA1 = __fmul2_rn(ra, gab), kA2 = __fmul2_rn(ra, gca);
-          float2 kB1 = __fmul2_rn(rb, gab), kB2 = __fmul2_rn(rb, gbc);
-          float2 kC1 = __fmul2_rn(rc, gbc), kC2 = __fmul2_rn(rc, gca);
-          if (flag == 1) {
-            // Careful visit: pairs with a vertex closer than kappa * h_face are
-            // refined in FP64 after the chunk; their FP32 terms are dropped here.
-            const float thr0 = lane < n ? __ldg(thr_rec) : -1.f;  // padding: never near
-            const float thr1 = lane + 32 < n ? __ldg(thr_rec + 16 * 32) : -1.f;
-            if (fminf(aa.x, fminf(bb.x, cc.x)) < thr0) {
-              near0 |= 1u << jq;
-              kA1.x = kA2.x = kB1.x = kB2.x = kC1.x = kC2.x = 0.f;
-            }
-            if (fminf(aa.y, fminf(bb.y, cc.y)) < thr1) {
-              near1 |= 1u << jq;
-              kA1.y = kA2.y = kB1.y = kB2.y = kC1.y = kC2.y = 0.f;
-            }
-          }
-          // a x b = a x e1, c x a = e2 x a, b x c = n - a x b - c x a.
-          const float2 xab0 = cross_c(ay, fe1[2], az, fe1[1]);
-          const float2 xab1 = cross_c(az, fe1[0], ax, fe1[2]);
-          const float2 xab2 = cross_c(ax, fe1[1], ay, fe1[0]);
-          const float2 xca0 = cross_c(fe2[1], az, fe2[2], ay);
-          const float2 xca1 = cross_c(fe2[2], ax, fe2[0], az);
-          const float2 xca2 = cross_c(fe2[0], ay, fe2[1], ax);
-          const float2 xbc0 = __fadd2_rn(__fadd2_rn(fn[0], make_float2(-xab0.x, -xab0.y)),
-                                         make_float2(-xca0.x, -xca0.y));
-          const float2 xbc1 = __fadd2_rn(__fadd2_rn(fn[1], make_float2(-xab1.x, -xab1.y)),
-                                         make_float2(-xca1.x, -xca1.y));
-          const float2 xbc2 = __fadd2_rn(__fadd2_rn(fn[2], make_float2(-xab2.x, -xab2.y)),
-                                         make_float2(-xca2.x, -xca2.y));
-          acc[0] = __ffma2_rn(kA1, xab0, __ffma2_rn(kA2, xca0, acc[0]));
-          acc[1] = __ffma2_rn(kA1, xab1, __ffma2_rn(kA2, xca1, acc[1]));
-          acc[2] = __ffma2_rn(kA1, xab2, __ffma2_rn(kA2, xca2, acc[2]));
-          acc[3] = __ffma2_rn(kB1, xab0, __ffma2_rn(kB2, xbc0, acc[3]));
-          acc[4] = __ffma2_rn(kB1, xab1, __ffma2_rn(kB2, xbc1, acc[4]));
-          acc[5] = __ffma2_rn(kB1, xab2, __ffma2_rn(kB2, xbc2, acc[5]));
-          acc[6] = __ffma2_rn(kC1, xbc0, __ffma2_rn(kC2, xca0, acc[6]));
-          acc[7] = __ffma2_rn(kC1, xbc1, __ffma2_rn(kC2, xca1, acc[7]));
-          acc[8] = __ffma2_rn(kC1, xbc2, __ffma2_rn(kC2, xca2, acc[8]));
-          const float2 sab = __fadd2_rn(kA1, kB1), sbc = __fadd2_rn(kB2, kC1);
-          const float2 sca = __fadd2_rn(kC2, kA2);
-          d0 = __ffma2_rn(sab, xab0, __ffma2_rn(sbc, xbc0, __fmul2_rn(sca, xca0)));
-          d1 = __ffma2_rn(sab, xab1, __ffma2_rn(sbc, xbc1, __fmul2_rn(sca, xca1)));
-          d2 = __ffma2_rn(sab, xab2, __ffma2_rn(sbc, xbc2, __fmul2_rn(sca, xca2)));
+      for (unsigned m = far_q; m; m &= m - 1u) {
+        const int jq = __ffs(m) - 1;
+        float2 d[3];
+        face_pair_terms<false>(sm.frame[jq][warp], fa, fe1, fe2, fnn, fg, 0.f, 0.f, acc, d);
+        sm.dO32[3 * jq][tid] = d[0].x + d[0].y;
+        sm.dO32[3 * jq + 1][tid] = d[1].x + d[1].y;
+        sm.dO32[3 * jq + 2][tid] = d[2].x + d[2].y;
+      }
+      if (careful_q) {
+        // Careful visits: pairs with a vertex closer than kappa * h_face are refined
+        // in FP64 below; their FP32 terms come out as zero here.
+        const float thr0 = lane < n ? __ldg(thr_rec) : -1.f;  // padding: never near
+        const float thr1 = lane + 32 < n ? __ldg(thr_rec + 16 * 32) : -1.f;
+#pragma unroll 1
+        for (unsigned m = careful_q; m; m &= m - 1u) {
+          const int jq = __ffs(m) - 1;
+          float2 d[3];
+          const unsigned nb = face_pair_terms<true>(sm.frame[jq][warp], fa, fe1, fe2, fnn, fg,
+                                                    thr0, thr1, acc, d);
+          near0 |= (nb & 1u) << jq;
+          near1 |= (nb >> 1) << jq;
+          sm.dO32[3 * jq][tid] = d[0].x + d[0].y;
+          sm.dO32[3 * jq + 1][tid] = d[1].x + d[1].y;
+          sm.dO32[3 * jq + 2][tid] = d[2].x + d[2].y;
         }
-        sm.dO32[3 * jq][tid] = d0.x + d0.y;
-        sm.dO32[3 * jq + 1][tid] = d1.x + d1.y;
-        sm.dO32[3 * jq + 2][tid] = d2.x + d2.y;
+      }
+      for (unsigned m = skip_q; m; m &= m - 1u) {
+        const int jq = __ffs(m) - 1;
+        sm.dO32[3 * jq][tid] = 0.f;
+        sm.dO32[3 * jq + 1][tid] = 0.f;
+        sm.dO32[3 * jq + 2][tid] = 0.f;
       }
       // Near pairs in FP64, query by query with the warp's lanes in step; each
       // query's FP64 dL/do shares are reduced over the warp in a fixed order.
@@ -1010,10 +1058,12 @@ __global__ void __launch_bounds__(kTileFaces) build_edge_tiles_kernel(
 }
 
 // g m dOmega of one (query, edge) pair in FP64, the FP64 edge kernel's formula:
-// -g m dOmega/dP into gv[0..2], -g m dOmega/dQ into gv[3..5], g m dOmega/do into go.
+// -g w dOmega/dP into gv[0..2], -g w dOmega/dQ into gv[3..5], g m dOmega/do into go,
+// with w = m, or w = 1 when `unit` (edges welded by position: per-endpoint sums
+// unweighted, the multiplicity only in dOmega/do).
 __device__ __noinline__ void refine_edge_grad(const double* __restrict__ e64, int64_t ld64,
                                               int64_t slot, double4 o, double* acc_col,
-                                              int stride, double* go) {
+                                              int stride, double* go, bool unit) {
   double v[7];
 #pragma unroll
   for (int r = 0; r < 7; ++r) v[r] = e64[r * ld64 + slot];
@@ -1024,8 +1074,8 @@ __device__ __noinline__ void refine_edge_grad(const double* __restrict__ e64, in
   const double rp = rsqrt(pp), rq = rsqrt(qq);
   const double rpq = rp * rq;
   const double d = 1.0 + (px * qx + py * qy + pz * qz) * rpq;
-  const bool ok = v[6] != 0.0 && pp > 0.0 && qq > 0.0 && d > 0.0;
-  const double w = ok ? o.w * v[6] * rpq / d : 0.0;
+  const bool ok = (unit || v[6] != 0.0) && pp > 0.0 && qq > 0.0 && d > 0.0;
+  const double w = ok ? o.w * (unit ? 1.0 : v[6]) * rpq / d : 0.0;
   const double cp = ok ? rp * w : 0.0, cq = ok ? rq * w : 0.0;
   const double x0 = py * qz - pz * qy, x1 = pz * qx - px * qz, x2 = px * qy - py * qx;
   acc_col[0] -= cp * x0;
@@ -1034,7 +1084,7 @@ __device__ __noinline__ void refine_edge_grad(const double* __restrict__ e64, in
   acc_col[3 * stride] -= cq * x0;
   acc_col[4 * stride] -= cq * x1;
   acc_col[5 * stride] -= cq * x2;
-  const double cs = cp + cq;
+  const double cs = unit ? (cp + cq) * v[6] : cp + cq;
   go[0] += cs * x0;
   go[1] += cs * x1;
   go[2] += cs * x2;
@@ -1060,12 +1110,64 @@ struct EdgeAdjSmem {
   double red64[kFaTiles][QC][3];
   double dsum[QC * 3];
   double4 q64[QC];
-  float4 frame[QC][kFaTiles];
+  float4 frame[QC][kFaTiles][2];  // (-x, -x, -y, -y), (-z, -z, gs, gs) as FP32x2 operands
   int flag[QC][kFaTiles];
   TileHeader th[kFaTiles];
 };
 
-template <int QC>
+// One query against this thread's two edges (the two lanes of every float2): adds
+// -g m dOmega/dP and -g m dOmega/dQ into acc and returns g m dOmega/do in d, every
+// operand a whole FP32x2 pair, no per-pair sign flip (-p from one packed multiply).
+// With CAREFUL, a lane whose edge has an endpoint within kappa |e| (k2ee = kappa^2
+// |e|^2, valid = the lane holds an edge) takes g = 0 and unit squared lengths, so
+// its terms are finite and zero; bit k of the result flags lane k. With UNIT the
+// per-endpoint sums take weight 1 and only dOmega/do the multiplicity m.
+template <bool CAREFUL, bool UNIT>
+__device__ __forceinline__ unsigned edge_pair_terms(const float4 (&fr)[2], const float2 (&fp)[3],
+                                                    const float2 (&fe)[3], float2 fee, float2 fm,
+                                                    float2 k2ee, bool valid0, bool valid1,
+                                                    float2 (&acc)[6], float2 (&d)[3]) {
+  const float4 f0 = fr[0], f1 = fr[1];
+  const float2 px = __fadd2_rn(fp[0], make_float2(f0.x, f0.y));
+  const float2 py = __fadd2_rn(fp[1], make_float2(f0.z, f0.w));
+  const float2 pz = __fadd2_rn(fp[2], make_float2(f1.x, f1.y));
+  float2 gm = UNIT ? make_float2(f1.z, f1.w) : __fmul2_rn(make_float2(f1.z, f1.w), fm);
+  float2 pp = __ffma2_rn(px, px, __ffma2_rn(py, py, __fmul2_rn(pz, pz)));
+  const float2 s = __ffma2_rn(px, fe[0], __ffma2_rn(py, fe[1], __fmul2_rn(pz, fe[2])));
+  const float2 pq = __fadd2_rn(pp, s);
+  float2 qq = __ffma2_rn(f2(2.f), s, __fadd2_rn(pp, fee));
+  unsigned nb = 0u;
+  if constexpr (CAREFUL) {
+    const bool n0 = valid0 && fminf(pp.x, qq.x) <= k2ee.x;
+    const bool n1 = valid1 && fminf(pp.y, qq.y) <= k2ee.y;
+    nb = (n0 ? 1u : 0u) | (n1 ? 2u : 0u);
+    gm = make_float2(n0 ? 0.f : gm.x, n1 ? 0.f : gm.y);
+    pp = make_float2(n0 ? 1.f : pp.x, n1 ? 1.f : pp.y);
+    qq = make_float2(n0 ? 1.f : qq.x, n1 ? 1.f : qq.y);
+  }
+  const float2 rp = rsqrt2(pp), rq = rsqrt2(qq);
+  const float2 lp = __fmul2_rn(pp, rp), lq = __fmul2_rn(qq, rq);
+  const float2 gD = __fmul2_rn(gm, rcp2(__ffma2_rn(lp, lq, pq)));
+  const float2 kp = __fmul2_rn(rp, gD), kq = __fmul2_rn(rq, gD);
+  const float2 m1 = f2(-1.f);
+  const float2 npx = __fmul2_rn(px, m1), npy = __fmul2_rn(py, m1), npz = __fmul2_rn(pz, m1);
+  const float2 x0 = __ffma2_rn(py, fe[2], __fmul2_rn(npz, fe[1]));
+  const float2 x1 = __ffma2_rn(pz, fe[0], __fmul2_rn(npx, fe[2]));
+  const float2 x2 = __ffma2_rn(px, fe[1], __fmul2_rn(npy, fe[0]));
+  acc[0] = __ffma2_rn(kp, x0, acc[0]);
+  acc[1] = __ffma2_rn(kp, x1, acc[1]);
+  acc[2] = __ffma2_rn(kp, x2, acc[2]);
+  acc[3] = __ffma2_rn(kq, x0, acc[3]);
+  acc[4] = __ffma2_rn(kq, x1, acc[4]);
+  acc[5] = __ffma2_rn(kq, x2, acc[5]);
+  const float2 cs = UNIT ? __fmul2_rn(__fadd2_rn(kp, kq), fm) : __fadd2_rn(kp, kq);
+  d[0] = __fmul2_rn(cs, x0);
+  d[1] = __fmul2_rn(cs, x1);
+  d[2] = __fmul2_rn(cs, x2);
+  return nb;
+}
+
+template <int QC, bool UNIT>
 __global__ void __launch_bounds__(kFaThreads, 4) adjoint_edges_mixed_kernel(const MixedEdgeArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   auto& sm = *reinterpret_cast<EdgeAdjSmem<QC>*>(smem_raw);
@@ -1131,10 +1233,12 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_edges_mixed_kernel(cons
           const double dx = o.x - th.cx, dy = o.y - th.cy, dz = o.z - th.cz;
           const double d2 = dx * dx + dy * dy + dz * dz;
           const bool skip = d2 * th.scale * th.scale > 1.2089258196146292e24;
-          sm.frame[jq][tt] = make_float4(static_cast<float>(dx * th.scale),
-                                         static_cast<float>(dy * th.scale),
-                                         static_cast<float>(dz * th.scale),
-                                         static_cast<float>(o.w * th.scale));
+          const float lx = static_cast<float>(dx * th.scale);
+          const float ly = static_cast<float>(dy * th.scale);
+          const float lz = static_cast<float>(dz * th.scale);
+          const float gs = static_cast<float>(o.w * th.scale);
+          sm.frame[jq][tt][0] = make_float4(-lx, -lx, -ly, -ly);
+          sm.frame[jq][tt][1] = make_float4(-lz, -lz, gs, gs);
           sm.flag[jq][tt] = skip ? 2 : (d2 >= th.far_r2 ? 0 : 1);
           if (tt == 0) sm.q64[jq] = o;
         }
@@ -1143,63 +1247,50 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_edges_mixed_kernel(cons
       __syncthreads();
       static_assert(QC <= 32, "one mask bit per query of a chunk");
       unsigned near0 = 0u, near1 = 0u;
+      const int myflag = lane < nc ? sm.flag[lane][warp] : 2;
+      const unsigned far_q = __ballot_sync(0xffffffffu, myflag == 0);
+      const unsigned careful_q = __ballot_sync(0xffffffffu, myflag == 1);
+      const unsigned skip_q = __ballot_sync(0xffffffffu, myflag == 2 && lane < nc);
 #pragma unroll 1
-      for (int jq = 0; jq < nc; ++jq) {
-        const float4 f = sm.frame[jq][warp];
-        const int flag = sm.flag[jq][warp];
-        float2 d0 = f2(0.f), d1 = f2(0.f), d2 = f2(0.f);
-        if (flag != 2) {
-          const float2 px = __fadd2_rn(fp[0], f2(-f.x));
-          const float2 py = __fadd2_rn(fp[1], f2(-f.y));
-          const float2 pz = __fadd2_rn(fp[2], f2(-f.z));
-          const float2 pp = __ffma2_rn(px, px, __ffma2_rn(py, py, __fmul2_rn(pz, pz)));
-          const float2 s = __ffma2_rn(px, fe[0], __ffma2_rn(py, fe[1], __fmul2_rn(pz, fe[2])));
-          const float2 pq = __fadd2_rn(pp, s);
-          const float2 qq = __ffma2_rn(f2(2.f), s, __fadd2_rn(pp, fee));
-          const float2 rp = rsqrt2(pp), rq = rsqrt2(qq);
-          const float2 lp = __fmul2_rn(pp, rp), lq = __fmul2_rn(qq, rq);
-          const float2 iD = rcp2(__ffma2_rn(lp, lq, pq));
-          const float2 gD = __fmul2_rn(__fmul2_rn(f2(f.w), fm), iD);
-          float2 kp = __fmul2_rn(rp, gD), kq = __fmul2_rn(rq, gD);
-          if (flag == 1) {
-            // Careful visit: pairs with an endpoint within kappa |e| are refined in
-            // FP64 after the chunk; their FP32 terms are dropped here.
-            if (fminf(pp.x, qq.x) <= k2ee.x && lane < n) {
-              near0 |= 1u << jq;
-              kp.x = kq.x = 0.f;
-            }
-            if (fminf(pp.y, qq.y) <= k2ee.y && lane + 32 < n) {
-              near1 |= 1u << jq;
-              kp.y = kq.y = 0.f;
-            }
-          }
-          const float2 x0 = cross_c(py, fe[2], pz, fe[1]);
-          const float2 x1 = cross_c(pz, fe[0], px, fe[2]);
-          const float2 x2 = cross_c(px, fe[1], py, fe[0]);
-          acc[0] = __ffma2_rn(kp, x0, acc[0]);
-          acc[1] = __ffma2_rn(kp, x1, acc[1]);
-          acc[2] = __ffma2_rn(kp, x2, acc[2]);
-          acc[3] = __ffma2_rn(kq, x0, acc[3]);
-          acc[4] = __ffma2_rn(kq, x1, acc[4]);
-          acc[5] = __ffma2_rn(kq, x2, acc[5]);
-          const float2 cs = __fadd2_rn(kp, kq);
-          d0 = __fmul2_rn(cs, x0);
-          d1 = __fmul2_rn(cs, x1);
-          d2 = __fmul2_rn(cs, x2);
-        }
-        sm.dO32[3 * jq][tid] = d0.x + d0.y;
-        sm.dO32[3 * jq + 1][tid] = d1.x + d1.y;
-        sm.dO32[3 * jq + 2][tid] = d2.x + d2.y;
+      for (unsigned m = far_q; m; m &= m - 1u) {
+        const int jq = __ffs(m) - 1;
+        float2 d[3];
+        edge_pair_terms<false, UNIT>(sm.frame[jq][warp], fp, fe, fee, fm, k2ee, true, true, acc,
+                                     d);
+        sm.dO32[3 * jq][tid] = d[0].x + d[0].y;
+        sm.dO32[3 * jq + 1][tid] = d[1].x + d[1].y;
+        sm.dO32[3 * jq + 2][tid] = d[2].x + d[2].y;
+      }
+#pragma unroll 1
+      for (unsigned m = careful_q; m; m &= m - 1u) {
+        // Careful visits: pairs with an endpoint within kappa |e| are refined in FP64
+        // below; their FP32 terms come out as zero here.
+        const int jq = __ffs(m) - 1;
+        float2 d[3];
+        const unsigned nb = edge_pair_terms<true, UNIT>(sm.frame[jq][warp], fp, fe, fee, fm, k2ee,
+                                                  lane < n, lane + 32 < n, acc, d);
+        near0 |= (nb & 1u) << jq;
+        near1 |= (nb >> 1) << jq;
+        sm.dO32[3 * jq][tid] = d[0].x + d[0].y;
+        sm.dO32[3 * jq + 1][tid] = d[1].x + d[1].y;
+        sm.dO32[3 * jq + 2][tid] = d[2].x + d[2].y;
+      }
+      for (unsigned m = skip_q; m; m &= m - 1u) {
+        const int jq = __ffs(m) - 1;
+        sm.dO32[3 * jq][tid] = 0.f;
+        sm.dO32[3 * jq + 1][tid] = 0.f;
+        sm.dO32[3 * jq + 2][tid] = 0.f;
       }
       for (unsigned pending = __reduce_or_sync(0xffffffffu, near0 | near1); pending;
            pending &= pending - 1u) {
         const int jq = __ffs(pending) - 1;
         double go[3] = {0.0, 0.0, 0.0};
         if ((near0 >> jq) & 1u)
-          refine_edge_grad(a.e64, a.ld64, slot0, sm.q64[jq], &sm.acc64[0][tid], kFaThreads, go);
+          refine_edge_grad(a.e64, a.ld64, slot0, sm.q64[jq], &sm.acc64[0][tid], kFaThreads, go,
+                           UNIT);
         if ((near1 >> jq) & 1u)
           refine_edge_grad(a.e64, a.ld64, slot0 + 32, sm.q64[jq], &sm.acc64[6][tid], kFaThreads,
-                           go);
+                           go, UNIT);
         for (int off = 16; off; off >>= 1) {
           go[0] += __shfl_xor_sync(0xffffffffu, go[0], off);
           go[1] += __shfl_xor_sync(0xffffffffu, go[1], off);
@@ -1307,7 +1398,7 @@ EdgeMixedLayout edge_mixed_layout(const AdjointPlan& p, int64_t ne, int64_t nq) 
 }  // namespace
 
 AdjointPlan plan_adjoint_edges_mixed(int64_t ne, int64_t nq, int sms) {
-  auto kernel = adjoint_edges_mixed_kernel<kEaQc>;
+  auto kernel = adjoint_edges_mixed_kernel<kEaQc, false>;
   const int smem = static_cast<int>(sizeof(EdgeAdjSmem<kEaQc>));
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   const int slots = resident_ctas(reinterpret_cast<const void*>(kernel), kFaThreads, smem, sms);
@@ -1321,8 +1412,8 @@ size_t adjoint_edges_mixed_scratch_bytes(const AdjointPlan& p, int64_t ne, int64
 
 cudaError_t adjoint_edges_mixed(const AdjointPlan& p, const double* edges, int64_t le, int64_t ne,
                                 const double* q, int64_t nq, const double* gw, double kappa,
-                                double* dq, double* dedge, void* scratch, size_t scratch_bytes,
-                                cudaStream_t stream) {
+                                bool unit, double* dq, double* dedge, void* scratch,
+                                size_t scratch_bytes, cudaStream_t stream) {
   cudaError_t e = cudaSuccess;
   if (nq > 0) e = cudaMemsetAsync(dq, 0, sizeof(double) * 3 * nq, stream);
   if (e == cudaSuccess && ne > 0) e = cudaMemsetAsync(dedge, 0, sizeof(double) * 6 * le, stream);
@@ -1357,7 +1448,8 @@ cudaError_t adjoint_edges_mixed(const AdjointPlan& p, const double* edges, int64
     return e;
   MixedEdgeArgs a{tiles, ntiles, e64, ld64, qs, nq, static_cast<float>(kappa * kappa),
                   p.blocks_per_range, p.queries_per_group, dO_part, dE_part};
-  auto kernel = adjoint_edges_mixed_kernel<kEaQc>;
+  auto kernel = unit ? adjoint_edges_mixed_kernel<kEaQc, true>
+                     : adjoint_edges_mixed_kernel<kEaQc, false>;
   const int smem = static_cast<int>(sizeof(EdgeAdjSmem<kEaQc>));
   if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
       cudaSuccess)

@@ -45,13 +45,15 @@ cudaError_t adjoint_edges(const AdjointPlan& p, const double* edges, int64_t le,
 // Mixed-precision boundary-edge adjoint: the same inputs and outputs as
 // adjoint_edges, FP32 far pairs in Morton-ordered 64-edge tiles and FP64 pairs
 // with an endpoint within kappa |e| of the query (kappa >= 3). The edge and query
-// orders are built inside the call from `scratch`.
+// orders are built inside the call from `scratch`. With `unit` the per-endpoint sums
+// are unweighted and the multiplicity weights dL/do only (edges welded by position:
+// each edge stands for the soup's directed sides on it, signed per side afterwards).
 AdjointPlan plan_adjoint_edges_mixed(int64_t ne, int64_t nq, int sms);
 size_t adjoint_edges_mixed_scratch_bytes(const AdjointPlan& p, int64_t ne, int64_t nq);
 cudaError_t adjoint_edges_mixed(const AdjointPlan& p, const double* edges, int64_t le, int64_t ne,
                                 const double* q, int64_t nq, const double* gw, double kappa,
-                                double* dq, double* dedge, void* scratch, size_t scratch_bytes,
-                                cudaStream_t stream);
+                                bool unit, double* dq, double* dedge, void* scratch,
+                                size_t scratch_bytes, cudaStream_t stream);
 
 // dV (nv x 3) from per-element corner gradients (rows 3*corner+axis, stride ld) through the
 // vertex -> (corners*element + corner) list (CSR indptr, entries); corners = 3 (faces) or 2

@@ -727,8 +727,8 @@ int wn_backward_edges_device(const double* edges, int64_t le, int64_t ne, const 
 }
 
 int wn_backward_edges_mixed_device(const double* edges, int64_t le, int64_t ne, const double* q,
-                                   int64_t nq, const double* gw, double kappa, double* dq,
-                                   double* dedge, void* stream) {
+                                   int64_t nq, const double* gw, double kappa, int unit_weights,
+                                   double* dq, double* dedge, void* stream) {
   WN_NVTX_RANGE();
   if (ne < 0 || nq < 0 || le < ne || nq > 0x7fffffffLL || ne > 0x7fffffffLL)
     return fail(WN_EINVAL, "bad sizes (ne=%lld, nq=%lld, le=%lld)", (long long)ne,
@@ -744,7 +744,8 @@ int wn_backward_edges_mixed_device(const double* edges, int64_t le, int64_t ne, 
   void* scratch = nullptr;
   cudaError_t e = dev_malloc_async(&scratch, sb, st);
   if (e != cudaSuccess) return cuda_fail(e, "device allocation");
-  e = adjoint_edges_mixed(p, edges, le, ne, q, nq, gw, kappa, dq, dedge, scratch, sb, st);
+  e = adjoint_edges_mixed(p, edges, le, ne, q, nq, gw, kappa, unit_weights != 0, dq, dedge,
+                          scratch, sb, st);
   cudaFreeAsync(scratch, st);
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "mixed boundary-edge adjoint launch");
 }

@@ -73,7 +73,8 @@ _WN_SIGNATURES = {
     "wn_backward_fp64_device": ([P, I, I, P, I, P, P, P, P], C_INT),
     "wn_gather_vertex_grad_device": ([P, I, C_INT, P, P, I, P, P], C_INT),
     "wn_backward_edges_device": ([P, I, I, P, I, P, P, P, P], C_INT),
-    "wn_backward_edges_mixed_device": ([P, I, I, P, I, P, ctypes.c_double, P, P, P], C_INT),
+    "wn_backward_edges_mixed_device": ([P, I, I, P, I, P, ctypes.c_double, C_INT, P, P, P],
+                                       C_INT),
     "wn_batch_create": ([I, P, P, P, P, ctypes.c_double, C_INT, I, C_INT, C_INT,
                          ctypes.POINTER(P)], C_INT),
     "wn_batch_forward": ([P, P, P, P, P], C_INT),

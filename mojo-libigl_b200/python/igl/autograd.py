@@ -12,9 +12,14 @@ adjoint="edges": the same derivative from the mesh's net boundary edges only
 mixed forward): the per-face terms of a directed side and of its reverse cancel
 at both endpoints, so interior edges contribute nothing (exactly zero for a
 closed, consistently oriented mesh).
-adjoint="auto" (default): "edges", except for a mixed-precision forward on a
-mesh with more net boundary edges than EDGE_FACE_RATIO times its faces (a
-triangle soup has three per face), where the per-face mixed adjoint costs less.
+adjoint="welded" (mixed precision): for triangle soups, whose faces share
+positions but not indices, every side is welded to the edges of equal endpoint
+coordinates (``welded_edges``): one edge's terms serve all sides on it, each
+side taking them with its own sign, and dL/dO only sees the edges' net counts.
+adjoint="auto" (default): "edges", except after a mixed-precision forward on a
+mesh with more net boundary edges than FACE_COST times its faces (a triangle
+soup has three per face), where it takes "welded" or "faces", whichever has the
+lower count times cost.
 
 Tensors are plumbing here: the forward and the adjoints run in libwn_b200's
 kernels on the tensors' memory and current stream.
@@ -29,10 +34,10 @@ import torch
 from . import _lib
 
 
-# Above this many net boundary edges per face the per-face mixed adjoint is
-# cheaper than the mixed boundary-edge adjoint (an edge pair costs 37 FP32
-# operations, a face pair 83).
-EDGE_FACE_RATIO = 2.0
+# Cost of one mixed face pair in units of one mixed edge pair (measured on the
+# c3 workloads): "auto" takes the cheapest of the boundary edges, the edges
+# welded by position and the faces by count times cost.
+FACE_COST = 1.5
 
 
 def _check(rc: int) -> None:
@@ -198,13 +203,83 @@ def backward_edges(V, F, O, gW, edges=None, precision: str = "fp64", kappa: floa
     dedge = torch.zeros((6, le), dtype=torch.float64, device=q.device)
     if precision == "mixed":
         _check(handle.wn_backward_edges_mixed_device(edges.data_ptr(), le, ne, q.data_ptr(), nq,
-                                                     gw.data_ptr(), kappa, dq.data_ptr(),
+                                                     gw.data_ptr(), kappa, 0, dq.data_ptr(),
                                                      dedge.data_ptr(), _stream()))
     else:
         _check(handle.wn_backward_edges_device(edges.data_ptr(), le, ne, q.data_ptr(), nq,
                                                gw.data_ptr(), dq.data_ptr(), dedge.data_ptr(),
                                                _stream()))
     return gather_vertices(dedge, le, ne, ends, nv, corners=2), dq
+
+
+def welded_edges(V: torch.Tensor, F: torch.Tensor):
+    """The sides of the faces welded by vertex position (for triangle soups).
+
+    Every directed side a -> b of a face is keyed by its endpoints' coordinates,
+    ordered so that the first is lexicographically smaller (sigma = +1 when that
+    is a, -1 when it is b); sides on the same segment share one edge. Returns
+    (edges (7, le) float64 SoA: the two endpoints and m = the sum of the sides'
+    sigma; ng; side_edge (ns,) the edge of every kept side; sigma (ns,); ends
+    (ns, 2) the sides' vertex indices a, b). Zero-length sides are dropped.
+    """
+    a = torch.cat([F[:, 0], F[:, 1], F[:, 2]]).to(torch.int64)
+    b = torch.cat([F[:, 1], F[:, 2], F[:, 0]]).to(torch.int64)
+    Vd = V.to(torch.float64)
+    Pa, Pb = Vd[a], Vd[b]
+    diff = Pa != Pb
+    keep = diff.any(1)
+    a, b, Pa, Pb, diff = a[keep], b[keep], Pa[keep], Pb[keep], diff[keep]
+    first = diff.to(torch.int8).argmax(1, keepdim=True)
+    sigma = torch.where(Pa.gather(1, first)[:, 0] < Pb.gather(1, first)[:, 0], 1, -1)
+    lo = torch.where(sigma[:, None] > 0, Pa, Pb)
+    hi = torch.where(sigma[:, None] > 0, Pb, Pa)
+    ng, le = 0, 1
+    if a.numel():
+        uniq, side_edge = torch.unique(torch.cat([lo, hi], 1), dim=0, return_inverse=True)
+        ng = uniq.shape[0]
+        le = ng
+    else:
+        uniq = torch.zeros((0, 6), dtype=torch.float64, device=V.device)
+        side_edge = torch.zeros(0, dtype=torch.int64, device=V.device)
+    m = torch.zeros(max(ng, 1), dtype=torch.int64, device=V.device)
+    if ng:
+        m.scatter_add_(0, side_edge, sigma.to(torch.int64))
+    edges = torch.zeros((7, le), dtype=torch.float64, device=V.device)
+    if ng:
+        edges[0:3, :ng] = uniq[:, 0:3].T
+        edges[3:6, :ng] = uniq[:, 3:6].T
+        edges[6, :ng] = m[:ng].to(torch.float64)
+    return edges, ng, side_edge, sigma, torch.stack([a, b], 1)
+
+
+def backward_welded_edges(V, F, O, gW, welded=None, kappa: float = 4.0):
+    """(dL/dV, dL/dO) of a triangle soup from its sides welded by position.
+
+    One edge stands for every directed side on its segment: the mixed edge adjoint
+    sums each edge's unweighted endpoint terms once (dL/dO weighted by the net
+    count m of its sides, so sides that cancel add nothing there), and every side
+    a -> b takes them with its own sign: (da, db) = (dP, dQ) for sigma = +1 and
+    (-dQ, -dP) for sigma = -1. The per-vertex sums then run in a fixed order.
+    """
+    handle = _lib.lib()
+    q = O.to(torch.float64).contiguous()
+    gw = gW.to(torch.float64).contiguous()
+    nq, nv = q.shape[0], V.shape[0]
+    edges, ng, side_edge, sigma, ends = welded if welded is not None else welded_edges(V, F)
+    le = edges.shape[1]
+    dq = torch.empty((nq, 3), dtype=torch.float64, device=q.device)
+    dedge = torch.zeros((6, le), dtype=torch.float64, device=q.device)
+    _check(handle.wn_backward_edges_mixed_device(edges.data_ptr(), le, ng, q.data_ptr(), nq,
+                                                 gw.data_ptr(), kappa, 1, dq.data_ptr(),
+                                                 dedge.data_ptr(), _stream()))
+    ns = ends.shape[0]
+    dside = torch.zeros((6, max(ns, 1)), dtype=torch.float64, device=q.device)
+    if ns:
+        de = dedge[:, side_edge]
+        pos = (sigma > 0)[None, :]
+        dside[0:3, :ns] = torch.where(pos, de[0:3], -de[3:6])
+        dside[3:6, :ns] = torch.where(pos, de[3:6], -de[0:3])
+    return gather_vertices(dside, max(ns, 1), ns, ends, nv, corners=2), dq
 
 
 def backward_fp64(tri, ld, nf, O, gW, F, nv):
@@ -231,7 +306,7 @@ class WindingNumberFunction(torch.autograd.Function):
         if precision == "mixed":
             mesh = PreparedMesh(tri, ld, nf)
             w = mesh.forward(O)
-            if adjoint in ("faces", "auto"):
+            if adjoint in ("faces", "auto", "welded"):
                 ctx.mesh = mesh
             else:
                 mesh.close()
@@ -249,15 +324,23 @@ class WindingNumberFunction(torch.autograd.Function):
         V, F, O = ctx.saved_tensors
         adjoint = ctx.adjoint
         edges = None
+        welded = None
         if adjoint == "auto":
             edges = boundary_edges(V, F)
-            use_faces = ctx.mesh is not None and edges[1] > EDGE_FACE_RATIO * ctx.nf
-            adjoint = "faces" if use_faces else "edges"
-            if not use_faces and ctx.mesh is not None:
+            adjoint = "edges"
+            if ctx.mesh is not None and edges[1] > FACE_COST * ctx.nf:
+                welded = welded_edges(V, F)
+                adjoint = "welded" if welded[1] < FACE_COST * ctx.nf else "faces"
+            if adjoint != "faces" and ctx.mesh is not None:
                 ctx.mesh.close()
                 ctx.mesh = None
         if adjoint == "edges":
             dV, dq = backward_edges(V, F, O, gW, edges, precision=ctx.precision)
+        elif adjoint == "welded":
+            dV, dq = backward_welded_edges(V, F, O, gW, welded)
+            if ctx.mesh is not None:
+                ctx.mesh.close()
+                ctx.mesh = None
         elif ctx.mesh is not None:
             dq, dtri = ctx.mesh.backward(O, gW)
             dV = gather_vertices(dtri, ctx.ld, ctx.nf, F, V.shape[0])
@@ -275,9 +358,9 @@ def winding_number_torch(V: torch.Tensor, F: torch.Tensor, O: torch.Tensor,
     FP64 refinement of near-surface pairs, forward and adjoint); by default
     "mixed" for float32 queries and "fp64" otherwise. W has the dtype of O.
     adjoint: "edges" (net boundary edges), "faces" (per-face reduction), both in
-    the forward's precision, or "auto" (edges, or faces for a mixed forward on
-    a mesh with many boundary edges, e.g. a triangle soup); all give the same
-    derivative.
+    the forward's precision, "welded" (mixed only: the sides welded by position,
+    for triangle soups whose faces share coordinates but not indices) or "auto"
+    (the cheapest of these); all give the same derivative.
     """
     if precision is None:
         precision = "mixed" if O.dtype == torch.float32 else "fp64"
@@ -285,6 +368,8 @@ def winding_number_torch(V: torch.Tensor, F: torch.Tensor, O: torch.Tensor,
         raise RuntimeError("winding_number_torch needs CUDA tensors (no CPU fallback)")
     if precision not in ("fp64", "mixed"):
         raise ValueError("precision must be 'fp64' or 'mixed'")
-    if adjoint not in ("edges", "faces", "auto"):
-        raise ValueError("adjoint must be 'edges', 'faces' or 'auto'")
+    if adjoint not in ("edges", "faces", "welded", "auto"):
+        raise ValueError("adjoint must be 'edges', 'faces', 'welded' or 'auto'")
+    if adjoint == "welded" and precision != "mixed":
+        raise ValueError("adjoint='welded' runs in mixed precision only")
     return WindingNumberFunction.apply(V, F, O, precision, adjoint)

@@ -309,3 +309,38 @@ def test_mixed_edge_adjoint_matches_fp64_edge_adjoint(gpu_required, case):
     assert torch.equal(dVm, dVm2) and torch.equal(dOm, dOm2)
     assert float((dVm - dV64).abs().max()) <= 1e-4 * float(dV64.abs().max())
     assert float((dOm - dO64).abs().max()) <= 1e-4 * float(dO64.abs().max())
+
+
+@pytest.mark.parametrize("case", ["closed_soup", "open_soup", "random_soup"])
+def test_welded_edge_adjoint_on_soups(gpu_required, case):
+    """The soup adjoint through sides welded by position against the per-face
+    FP64 adjoint: within 1e-4 of the largest gradient, for a closed mesh and an
+    open one given as soups (every edge shared by two sides) and a random soup
+    (no shared sides); adjoint="auto" picks it where it is cheaper than faces."""
+    import torch
+
+    V, F = igl.synthetic.bumpy_icosphere(3, seed=101)
+    if case == "open_soup":
+        F = igl.synthetic.delete_faces(F, 0.1, seed=102)
+    if case == "random_soup":
+        rng = np.random.default_rng(103)
+        Vs = rng.normal(size=(3 * 900, 3))
+        Fs = np.arange(3 * 900).reshape(-1, 3)
+    else:
+        Vs, Fs = igl.synthetic.unshare_vertices(V, F)
+    O = igl.synthetic.mixed_queries(Vs, Fs, 3000, seed=104, near_sigma=1e-3)
+    g = _cuda(np.random.default_rng(105).normal(size=len(O)))
+    Vt, Ft, Ot = _cuda(Vs), _cuda(Fs), _cuda(O)
+    welded = wa.welded_edges(Vt, Ft)
+    dVw, dOw = wa.backward_welded_edges(Vt, Ft, Ot, g, welded)
+    ref = {}
+    Vr = _cuda(Vs).requires_grad_(True)
+    Orr = _cuda(O).requires_grad_(True)
+    W = wa.winding_number_torch(Vr, Ft, Orr, precision="fp64", adjoint="faces")
+    (W * g).sum().backward()
+    dV64, dO64 = Vr.grad, Orr.grad
+    assert torch.isfinite(dVw).all() and torch.isfinite(dOw).all()
+    assert float((dVw - dV64).abs().max()) <= 1e-4 * float(dV64.abs().max())
+    assert float((dOw - dO64).abs().max()) <= 1e-4 * float(dO64.abs().max()) + 1e-12
+    if case == "closed_soup":
+        assert welded[1] == 3 * len(Fs) // 2

@@ -216,3 +216,32 @@ def test_autotune_coordinate_descent_without_a_gpu(monkeypatch):
     assert len({tuple(sorted(t["config"].items())) for t in out["trials"]}) == len(out["trials"])
     grid = autotune.tune([None], [np.zeros((4, 3))], space=space, use_cache=False, search="grid")
     assert len(grid["trials"]) == 12 and grid["config"] == out["config"]
+
+
+def test_welded_edges_of_a_soup_without_a_gpu():
+    """Sides welded by position: a closed mesh as a soup gives every geometric
+    edge once (1.5 per face) with net count 0; an open one has count +-1 exactly
+    on its boundary; each side points to its edge with the sign of its direction."""
+    import torch
+
+    from igl import autograd as wa
+    from igl import synthetic
+
+    V, F = synthetic.bumpy_icosphere(2, seed=3)
+    Vs, Fs = synthetic.unshare_vertices(V, F)
+    edges, ng, side_edge, sigma, ends = wa.welded_edges(torch.from_numpy(Vs),
+                                                        torch.from_numpy(Fs))
+    assert ng == 3 * len(F) // 2
+    assert float(edges[6, :ng].abs().max()) == 0.0
+    P, Q = edges[0:3, side_edge].T.numpy(), edges[3:6, side_edge].T.numpy()
+    A, B = Vs[ends[:, 0].numpy()], Vs[ends[:, 1].numpy()]
+    fwd = sigma.numpy() > 0
+    assert np.array_equal(P[fwd], A[fwd]) and np.array_equal(Q[fwd], B[fwd])
+    assert np.array_equal(P[~fwd], B[~fwd]) and np.array_equal(Q[~fwd], A[~fwd])
+    Fo = synthetic.delete_faces(F, 0.1, seed=4)
+    Vo, Fo = synthetic.unshare_vertices(V, Fo)
+    e_open, ng_open, *_ = wa.welded_edges(torch.from_numpy(Vo), torch.from_numpy(Fo))
+    _, nb, _ = wa.boundary_edges(torch.from_numpy(V), torch.from_numpy(
+        synthetic.delete_faces(F, 0.1, seed=4)))
+    assert int((e_open[6, :ng_open] != 0).sum()) == nb
+    assert float(e_open[6, :ng_open].abs().max()) == 1.0

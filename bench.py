@@ -569,18 +569,29 @@ def gpu_arm(args):
                 a_fwd()
                 wa.backward_edges(Vad, Fad, Oad, gad)
 
-            legs_a = [("fwd", a_fwd), ("faces", a_faces), ("edges", a_edges)]
+            def a_welded():
+                a_fwd()
+                wa.backward_welded_edges(Vad, Fad, Oad, gad)
+
+            legs_a = [("fwd", a_fwd), ("faces", a_faces)]
             if wname == "c3_open":
-                legs_a.append(("edges_fp64", a_edges64))
+                legs_a += [("edges", a_edges), ("edges_fp64", a_edges64)]
+            else:
+                legs_a += [("welded", a_welded)]
             ta = {k: timed(fn, k_adj, 1)[0] for k, fn in legs_a}
             _, ne_a, _ = wa.boundary_edges(Vad, Fad)
             adj_work[wname] = {
                 "workload": desc_a, "pairs": float(nfa) * len(Oa), "boundary_edges": ne_a,
                 "fwd_ms": ta["fwd"] * 1e3, "fwdbwd_faces_ms": ta["faces"] * 1e3,
-                "fwdbwd_edges_ms": ta["edges"] * 1e3,
-                "ratio_faces": ta["faces"] / ta["fwd"], "ratio_edges": ta["edges"] / ta["fwd"],
+                "ratio_faces": ta["faces"] / ta["fwd"],
                 "steps": k_adj,
-                "note": "faces: per-face mixed adjoint; edges: mixed boundary-edge adjoint"}
+                "note": "faces: per-face mixed adjoint; edges: mixed boundary-edge adjoint; "
+                        "welded: the soup's sides welded by position, mixed edge adjoint "
+                        "(welding inside the step)"}
+            for leg in ("edges", "welded"):
+                if leg in ta:
+                    adj_work[wname][f"fwdbwd_{leg}_ms"] = ta[leg] * 1e3
+                    adj_work[wname][f"ratio_{leg}"] = ta[leg] / ta["fwd"]
             if "edges_fp64" in ta:
                 adj_work[wname]["fwdbwd_edges_fp64_ms"] = ta["edges_fp64"] * 1e3
                 adj_work[wname]["ratio_edges_fp64"] = ta["edges_fp64"] / ta["fwd"]

@@ -388,27 +388,34 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_faces_kernel(const Mixe
     const bool tile_ok = t < a.ntiles;
     const unsigned char* rec = a.tiles + (tile_ok ? t : 0) * kTileBytes;
     const int n = tile_ok ? reinterpret_cast<const TileHeader*>(rec)->n : 0;
-    float2 fa[3], fe1[3], fe2[3], fnn[3], fg[3];  // fnn = -n
     const float* thr_rec = reinterpret_cast<const float*>(rec + kTileHeaderBytes) + 16 * lane + 15;
+    float4 r[2][4];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int j = lane + 32 * k;
-      const bool valid = j < n;
       const float4* fr = reinterpret_cast<const float4*>(rec + kTileHeaderBytes) + 4 * j;
-      float4 r0 = make_float4(1e18f, 1e18f, 1e18f, 0.f), r1 = make_float4(0.f, 0.f, 0.f, 0.f);
-      float4 r2 = r1, r3 = make_float4(0.f, 0.f, 0.f, -1.f);
-      if (valid) {
-        r0 = fr[0];
-        r1 = fr[1];
-        r2 = fr[2];
-        r3 = fr[3];
+      r[k][0] = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+      r[k][1] = r[k][2] = make_float4(0.f, 0.f, 0.f, 0.f);
+      r[k][3] = make_float4(0.f, 0.f, 0.f, -1.f);
+      if (j < n) {
+        r[k][0] = fr[0];
+        r[k][1] = fr[1];
+        r[k][2] = fr[2];
+        r[k][3] = fr[3];
       }
-      lane_ref(fa[0], k) = r0.x;  lane_ref(fa[1], k) = r0.y;  lane_ref(fa[2], k) = r0.z;
-      lane_ref(fe1[0], k) = r0.w; lane_ref(fe1[1], k) = r1.x; lane_ref(fe1[2], k) = r1.y;
-      lane_ref(fe2[0], k) = r1.z; lane_ref(fe2[1], k) = r1.w; lane_ref(fe2[2], k) = r2.x;
-      lane_ref(fnn[0], k) = -r2.y; lane_ref(fnn[1], k) = -r2.z; lane_ref(fnn[2], k) = -r2.w;
-      lane_ref(fg[0], k) = r3.x;  lane_ref(fg[1], k) = r3.y;  lane_ref(fg[2], k) = r3.z;
     }
+    // Each field of the two faces as one FP32x2 value, built whole (fnn = -n).
+    auto pr = [&](float a, float b) { return make_float2(a, b); };
+    const float2 fa[3] = {pr(r[0][0].x, r[1][0].x), pr(r[0][0].y, r[1][0].y),
+                          pr(r[0][0].z, r[1][0].z)};
+    const float2 fe1[3] = {pr(r[0][0].w, r[1][0].w), pr(r[0][1].x, r[1][1].x),
+                           pr(r[0][1].y, r[1][1].y)};
+    const float2 fe2[3] = {pr(r[0][1].z, r[1][1].z), pr(r[0][1].w, r[1][1].w),
+                           pr(r[0][2].x, r[1][2].x)};
+    const float2 fnn[3] = {pr(-r[0][2].y, -r[1][2].y), pr(-r[0][2].z, -r[1][2].z),
+                           pr(-r[0][2].w, -r[1][2].w)};
+    const float2 fg[3] = {pr(r[0][3].x, r[1][3].x), pr(r[0][3].y, r[1][3].y),
+                          pr(r[0][3].z, r[1][3].z)};
     const int64_t slot0 = (tile_ok ? t : 0) * kTileFaces + lane;
 #pragma unroll
     for (int r = 0; r < 18; ++r) sm.acc64[r][tid] = 0.0;
@@ -1199,20 +1206,25 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_edges_mixed_kernel(cons
     const bool tile_ok = t < a.ntiles;
     const unsigned char* rec = a.tiles + (tile_ok ? t : 0) * kEdgeTileBytes;
     const int n = tile_ok ? reinterpret_cast<const TileHeader*>(rec)->n : 0;
-    float2 fp[3], fe[3], fee, fm;
+    float4 r[2][2];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int j = lane + 32 * k;
       const float4* er = reinterpret_cast<const float4*>(rec + sizeof(TileHeader)) + 2 * j;
-      float4 r0 = make_float4(1e18f, 1e18f, 1e18f, 0.f), r1 = make_float4(0.f, 0.f, 0.f, 0.f);
+      r[k][0] = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+      r[k][1] = make_float4(0.f, 0.f, 0.f, 0.f);
       if (j < n) {
-        r0 = er[0];
-        r1 = er[1];
+        r[k][0] = er[0];
+        r[k][1] = er[1];
       }
-      lane_ref(fp[0], k) = r0.x;  lane_ref(fp[1], k) = r0.y;  lane_ref(fp[2], k) = r0.z;
-      lane_ref(fe[0], k) = r0.w;  lane_ref(fe[1], k) = r1.x;  lane_ref(fe[2], k) = r1.y;
-      lane_ref(fee, k) = r1.z;    lane_ref(fm, k) = r1.w;
     }
+    // Each field of the two edges as one FP32x2 value, built whole.
+    const float2 fp[3] = {make_float2(r[0][0].x, r[1][0].x), make_float2(r[0][0].y, r[1][0].y),
+                          make_float2(r[0][0].z, r[1][0].z)};
+    const float2 fe[3] = {make_float2(r[0][0].w, r[1][0].w), make_float2(r[0][1].x, r[1][1].x),
+                          make_float2(r[0][1].y, r[1][1].y)};
+    const float2 fee = make_float2(r[0][1].z, r[1][1].z);
+    const float2 fm = make_float2(r[0][1].w, r[1][1].w);
     const int64_t slot0 = (tile_ok ? t : 0) * kTileFaces + lane;
 #pragma unroll
     for (int r = 0; r < 12; ++r) sm.acc64[r][tid] = 0.0;

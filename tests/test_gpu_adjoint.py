@@ -246,10 +246,11 @@ def test_mixed_float32_queries_full_size_c4(gpu_required):
     assert np.abs(dO - dO64).max() <= 1e-3 * np.abs(dO64).max()
 
 
-def test_auto_adjoint_picks_faces_on_a_soup_and_edges_on_a_mesh(gpu_required, monkeypatch):
+def test_auto_adjoint_picks_welded_edges_on_a_soup_and_edges_on_a_mesh(gpu_required,
+                                                                      monkeypatch):
     """adjoint="auto": a mixed forward on a triangle soup (three boundary edges per
-    face) takes the per-face adjoint, one on an open indexed mesh the boundary-edge
-    adjoint; both give the FP64 adjoint's gradients."""
+    face, 1.5 welded edges per face) takes the welded-edge adjoint, one on an open
+    indexed mesh the boundary-edge adjoint; both give the FP64 adjoint's gradients."""
     import torch
 
     V, F = igl.synthetic.bumpy_icosphere(3, seed=81)
@@ -260,11 +261,14 @@ def test_auto_adjoint_picks_faces_on_a_soup_and_edges_on_a_mesh(gpu_required, mo
     calls = []
     real_faces = wa.PreparedMesh.backward
     real_edges = wa.backward_edges
+    real_welded = wa.backward_welded_edges
     monkeypatch.setattr(wa.PreparedMesh, "backward",
                         lambda self, *a: calls.append("faces") or real_faces(self, *a))
     monkeypatch.setattr(wa, "backward_edges",
                         lambda *a, **k: calls.append("edges") or real_edges(*a, **k))
-    for (Vx, Fx), expect in (((Vs, Fs), "faces"), ((V, F), "edges")):
+    monkeypatch.setattr(wa, "backward_welded_edges",
+                        lambda *a, **k: calls.append("welded") or real_welded(*a, **k))
+    for (Vx, Fx), expect in (((Vs, Fs), "welded"), ((V, F), "edges")):
         calls.clear()
         grads = {}
         for precision in ("mixed", "fp64"):

@@ -54,7 +54,8 @@ exits (the commands behind the ncu summaries in profiles/): fp64_c3 (streaming
 FP64 kernel), fp64_tiled_c3 (FP64 over the prepared mesh), mixed_c3, adjoint_c4
 (per-face mixed adjoint on the gradient workload), adjoint_c3 (the same on the
 c3 workload), adjoint_soup (the same on the c3 triangle soup), edges_open_c3 (the
-mixed boundary-edge adjoint on the open c3 mesh), closest_c3 (closest-point traversal), fwn_c3 (fast
+mixed boundary-edge adjoint on the open c3 mesh), welded_soup (the mixed edge adjoint
+over the c3 soup's sides welded by position), closest_c3 (closest-point traversal), fwn_c3 (fast
 winding number, beta = 2), normals_s9 (area-weighted vertex normals of the
 subdivision-9 sphere) and batched_small (the batched persistent forward and
 edge adjoint on 16 uneven meshes with at most 65,536 queries each).
@@ -102,7 +103,8 @@ def parse_args():
     p.add_argument("--no-normals", action="store_true", help="skip the vertex-normal workloads")
     p.add_argument("--case", choices=("fp64_c3", "fp64_tiled_c3", "mixed_c3", "adjoint_c4",
                                       "closest_c3", "fwn_c3", "normals_s9", "adjoint_c3",
-                                      "adjoint_soup", "edges_open_c3", "batched_small"),
+                                      "adjoint_soup", "edges_open_c3", "welded_soup",
+                                      "batched_small"),
                    help="run one kernel on a small case twice (for profiling) and exit")
     p.add_argument("--case-queries", type=int, default=None)
     p.add_argument("--no-autotune", dest="autotune", action="store_false",
@@ -1092,6 +1094,20 @@ def run_case(args):
             dV, dq = wa.backward_edges(Vt, Ft, Ot, g, edges, precision="mixed")
         torch.cuda.synchronize()
         print("ok", args.case, edges[1], len(O), float(dq.abs().sum()))
+        return
+
+    if args.case == "welded_soup":
+        from igl import autograd as wa
+        from igl import synthetic
+
+        V, F, O, _ = synthetic.workload("c3_soup", n_queries=args.case_queries or 65536)
+        Vt, Ft, Ot = (torch.from_numpy(x).cuda() for x in (V, F, O))
+        g = torch.from_numpy(np.random.default_rng(5).normal(size=len(O))).cuda()
+        welded = wa.welded_edges(Vt, Ft)
+        for _ in range(2):
+            dV, dq = wa.backward_welded_edges(Vt, Ft, Ot, g, welded)
+        torch.cuda.synchronize()
+        print("ok", args.case, welded[1], len(O), float(dV.abs().sum()), float(dq.abs().sum()))
         return
 
     if args.case == "normals_s9":

@@ -242,7 +242,9 @@ int wn_backward_edges_device(const double* edges, int64_t le, int64_t ne, const 
  * by m, as wn_backward_edges_device's. unit_weights = 1 (edges welded by position
  * from a triangle soup, m = the net count of the soup's directed sides on the
  * edge): dedge holds the unweighted sums -dL/dW dOmega/dP and -dL/dW dOmega/dQ of
- * one side P -> Q, to be signed per soup side, while dq still uses m. */
+ * one side P -> Q, to be signed per soup side, while dq still uses m; there dq
+ * may be NULL, and dL/do is then not computed (a soup that is a closed surface has
+ * every m = 0, so its dL/do is exactly 0), which takes a leaner kernel. */
 int wn_backward_edges_mixed_device(const double* edges, int64_t le, int64_t ne, const double* q,
                                    int64_t nq, const double* gw, double kappa, int unit_weights,
                                    double* dq, double* dedge, void* stream);

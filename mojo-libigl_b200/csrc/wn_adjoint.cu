@@ -226,6 +226,7 @@ constexpr int kFaTiles = kFaThreads / 32;
 constexpr int kFaRow = kFaThreads + 4;   // padded row of per-thread dL/do shares
 constexpr int kFaQc = 16;                // queries per chunk (4 CTAs per SM fit the smem)
 constexpr int kFaFlushChunks = 4;        // FP32 face sums go to FP64 every 64 queries
+constexpr int kFaFlushQueries = kFaFlushChunks * kFaQc;
 static_assert(kFaThreads == 2 * kTileFaces, "two faces per thread cover a tile per warp");
 
 template <int QC>
@@ -1110,9 +1111,9 @@ struct MixedEdgeArgs {
   double* dE_part;  // [ngroups][6][ld64] by sorted slot
 };
 
-template <int QC>
+template <int QC, bool DQ = true>
 struct EdgeAdjSmem {
-  float dO32[QC * 3][kFaRow];   // per-thread FP32 dL/do shares, row 3*query + axis
+  float dO32[DQ ? QC * 3 : 1][kFaRow];  // per-thread FP32 dL/do shares, row 3*query + axis
   double acc64[12][kFaThreads];  // per-edge FP64 sums (thread-private columns)
   double red64[kFaTiles][QC][3];
   double dsum[QC * 3];
@@ -1128,10 +1129,13 @@ struct EdgeAdjSmem {
 // With CAREFUL, a lane whose edge has an endpoint within kappa |e| (k2ee = kappa^2
 // |e|^2, valid = the lane holds an edge) takes g = 0 and unit squared lengths, so
 // its terms are finite and zero; bit k of the result flags lane k. With UNIT the
-// per-endpoint sums take weight 1 and only dOmega/do the multiplicity m.
-template <bool CAREFUL, bool UNIT>
+// per-endpoint sums take weight 1 and only dOmega/do the multiplicity m; without DQ
+// (UNIT over edges whose m are all 0, so that every dOmega/do term is exactly 0) d is
+// left untouched.
+template <bool CAREFUL, bool UNIT, bool DQ = true>
 __device__ __forceinline__ unsigned edge_pair_terms(const float4 (&fr)[2], const float2 (&fp)[3],
-                                                    const float2 (&fe)[3], float2 fee, float2 fm,
+                                                    const float2 (&fe)[3],
+                                                    const float2 (&fne)[3], float2 fee, float2 fm,
                                                     float2 k2ee, bool valid0, bool valid1,
                                                     float2 (&acc)[6], float2 (&d)[3]) {
   const float4 f0 = fr[0], f1 = fr[1];
@@ -1156,28 +1160,36 @@ __device__ __forceinline__ unsigned edge_pair_terms(const float4 (&fr)[2], const
   const float2 lp = __fmul2_rn(pp, rp), lq = __fmul2_rn(qq, rq);
   const float2 gD = __fmul2_rn(gm, rcp2(__ffma2_rn(lp, lq, pq)));
   const float2 kp = __fmul2_rn(rp, gD), kq = __fmul2_rn(rq, gD);
-  const float2 m1 = f2(-1.f);
-  const float2 npx = __fmul2_rn(px, m1), npy = __fmul2_rn(py, m1), npz = __fmul2_rn(pz, m1);
-  const float2 x0 = __ffma2_rn(py, fe[2], __fmul2_rn(npz, fe[1]));
-  const float2 x1 = __ffma2_rn(pz, fe[0], __fmul2_rn(npx, fe[2]));
-  const float2 x2 = __ffma2_rn(px, fe[1], __fmul2_rn(npy, fe[0]));
+  // x = p x e with -e held per tile ((-a) b and a (-b) round alike): no negation per pair.
+  const float2 x0 = __ffma2_rn(py, fe[2], __fmul2_rn(pz, fne[1]));
+  const float2 x1 = __ffma2_rn(pz, fe[0], __fmul2_rn(px, fne[2]));
+  const float2 x2 = __ffma2_rn(px, fe[1], __fmul2_rn(py, fne[0]));
   acc[0] = __ffma2_rn(kp, x0, acc[0]);
   acc[1] = __ffma2_rn(kp, x1, acc[1]);
   acc[2] = __ffma2_rn(kp, x2, acc[2]);
   acc[3] = __ffma2_rn(kq, x0, acc[3]);
   acc[4] = __ffma2_rn(kq, x1, acc[4]);
   acc[5] = __ffma2_rn(kq, x2, acc[5]);
-  const float2 cs = UNIT ? __fmul2_rn(__fadd2_rn(kp, kq), fm) : __fadd2_rn(kp, kq);
-  d[0] = __fmul2_rn(cs, x0);
-  d[1] = __fmul2_rn(cs, x1);
-  d[2] = __fmul2_rn(cs, x2);
+  if constexpr (DQ) {
+    const float2 cs = UNIT ? __fmul2_rn(__fadd2_rn(kp, kq), fm) : __fadd2_rn(kp, kq);
+    d[0] = __fmul2_rn(cs, x0);
+    d[1] = __fmul2_rn(cs, x1);
+    d[2] = __fmul2_rn(cs, x2);
+  }
   return nb;
 }
 
-template <int QC, bool UNIT>
-__global__ void __launch_bounds__(kFaThreads, 4) adjoint_edges_mixed_kernel(const MixedEdgeArgs a) {
+__device__ __forceinline__ int jq_of(unsigned mask) { return __ffs(mask) - 1; }
+
+// NODQ (with UNIT, for callers that need no dL/do: every net multiplicity is 0)
+// compiles the dL/do path out, so that the per-query shares take no shared memory
+// and 96 registers fit five CTAs per SM.
+template <int QC, bool UNIT, bool NODQ = false>
+__global__ void __launch_bounds__(kFaThreads, NODQ ? 5 : 4)
+    adjoint_edges_mixed_kernel(const MixedEdgeArgs a) {
+  static_assert(UNIT || !NODQ, "dL/do is dropped only in the unit-weight mode");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  auto& sm = *reinterpret_cast<EdgeAdjSmem<QC>*>(smem_raw);
+  auto& sm = *reinterpret_cast<EdgeAdjSmem<QC, !NODQ>*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t nblocks = (a.ntiles + kFaTiles - 1) / kFaTiles;
   const int64_t range = blockIdx.x, group = blockIdx.y;
@@ -1223,8 +1235,13 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_edges_mixed_kernel(cons
                           make_float2(r[0][0].z, r[1][0].z)};
     const float2 fe[3] = {make_float2(r[0][0].w, r[1][0].w), make_float2(r[0][1].x, r[1][1].x),
                           make_float2(r[0][1].y, r[1][1].y)};
+    const float2 fne[3] = {__fmul2_rn(fe[0], f2(-1.f)), __fmul2_rn(fe[1], f2(-1.f)),
+                           __fmul2_rn(fe[2], f2(-1.f))};
     const float2 fee = make_float2(r[0][1].z, r[1][1].z);
     const float2 fm = make_float2(r[0][1].w, r[1][1].w);
+    // Welded sides whose net multiplicities are all 0 in this block (every side of a
+    // closed soup) give dOmega/do terms that are exactly 0: the block skips them.
+    const bool no_dq = NODQ || (UNIT && __syncthreads_and(fm.x == 0.f && fm.y == 0.f));
     const int64_t slot0 = (tile_ok ? t : 0) * kTileFaces + lane;
 #pragma unroll
     for (int r = 0; r < 12; ++r) sm.acc64[r][tid] = 0.0;
@@ -1255,7 +1272,8 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_edges_mixed_kernel(cons
           if (tt == 0) sm.q64[jq] = o;
         }
       }
-      for (int e = tid; e < kFaTiles * QC * 3; e += kFaThreads) (&sm.red64[0][0][0])[e] = 0.0;
+      if (!no_dq)
+        for (int e = tid; e < kFaTiles * QC * 3; e += kFaThreads) (&sm.red64[0][0][0])[e] = 0.0;
       __syncthreads();
       static_assert(QC <= 32, "one mask bit per query of a chunk");
       unsigned near0 = 0u, near1 = 0u;
@@ -1263,15 +1281,81 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_edges_mixed_kernel(cons
       const unsigned far_q = __ballot_sync(0xffffffffu, myflag == 0);
       const unsigned careful_q = __ballot_sync(0xffffffffu, myflag == 1);
       const unsigned skip_q = __ballot_sync(0xffffffffu, myflag == 2 && lane < nc);
+      if constexpr (UNIT) {
+        if (no_dq) {
+          float2 d[3];
+          // Two queries per pass (in increasing order, as one at a time would add
+          // them): the second's arithmetic overlaps the first's latencies.
 #pragma unroll 1
-      for (unsigned m = far_q; m; m &= m - 1u) {
-        const int jq = __ffs(m) - 1;
+          for (unsigned m = far_q; m;) {
+            const int j0 = jq_of(m);
+            m &= m - 1u;
+            if (m) {
+              const int j1 = jq_of(m);
+              m &= m - 1u;
+              edge_pair_terms<false, true, false>(sm.frame[j0][warp], fp, fe, fne, fee, fm, k2ee,
+                                                  true, true, acc, d);
+              edge_pair_terms<false, true, false>(sm.frame[j1][warp], fp, fe, fne, fee, fm, k2ee,
+                                                  true, true, acc, d);
+            } else {
+              edge_pair_terms<false, true, false>(sm.frame[j0][warp], fp, fe, fne, fee, fm, k2ee,
+                                                  true, true, acc, d);
+            }
+          }
+#pragma unroll 1
+          for (unsigned m = careful_q; m; m &= m - 1u) {
+            const int jq = jq_of(m);
+            const unsigned nb = edge_pair_terms<true, true, false>(
+                sm.frame[jq][warp], fp, fe, fne, fee, fm, k2ee, lane < n, lane + 32 < n, acc, d);
+            near0 |= (nb & 1u) << jq;
+            near1 |= (nb >> 1) << jq;
+          }
+          for (unsigned pending = __reduce_or_sync(0xffffffffu, near0 | near1); pending;
+               pending &= pending - 1u) {
+            const int jq = jq_of(pending);
+            double go[3] = {0.0, 0.0, 0.0};  // exactly 0 here: all m are 0
+            if ((near0 >> jq) & 1u)
+              refine_edge_grad(a.e64, a.ld64, slot0, sm.q64[jq], &sm.acc64[0][tid], kFaThreads,
+                               go, true);
+            if ((near1 >> jq) & 1u)
+              refine_edge_grad(a.e64, a.ld64, slot0 + 32, sm.q64[jq], &sm.acc64[6][tid],
+                               kFaThreads, go, true);
+          }
+          if (++chunks == kFaFlushQueries / QC || c0 + QC >= q_end) {
+            chunks = 0;
+#pragma unroll
+            for (int r = 0; r < 6; ++r) {
+              sm.acc64[r][tid] -= static_cast<double>(acc[r].x);
+              sm.acc64[6 + r][tid] -= static_cast<double>(acc[r].y);
+              acc[r] = f2(0.f);
+            }
+          }
+          continue;
+        }
+      }
+#pragma unroll 1
+      for (unsigned m = far_q; m;) {
+        const int j0 = jq_of(m);
+        m &= m - 1u;
         float2 d[3];
-        edge_pair_terms<false, UNIT>(sm.frame[jq][warp], fp, fe, fee, fm, k2ee, true, true, acc,
-                                     d);
-        sm.dO32[3 * jq][tid] = d[0].x + d[0].y;
-        sm.dO32[3 * jq + 1][tid] = d[1].x + d[1].y;
-        sm.dO32[3 * jq + 2][tid] = d[2].x + d[2].y;
+        if (m) {
+          const int j1 = jq_of(m);
+          m &= m - 1u;
+          float2 d1[3];
+          edge_pair_terms<false, UNIT>(sm.frame[j0][warp], fp, fe, fne, fee, fm, k2ee, true, true,
+                                       acc, d);
+          edge_pair_terms<false, UNIT>(sm.frame[j1][warp], fp, fe, fne, fee, fm, k2ee, true, true,
+                                       acc, d1);
+          sm.dO32[3 * j1][tid] = d1[0].x + d1[0].y;
+          sm.dO32[3 * j1 + 1][tid] = d1[1].x + d1[1].y;
+          sm.dO32[3 * j1 + 2][tid] = d1[2].x + d1[2].y;
+        } else {
+          edge_pair_terms<false, UNIT>(sm.frame[j0][warp], fp, fe, fne, fee, fm, k2ee, true, true,
+                                       acc, d);
+        }
+        sm.dO32[3 * j0][tid] = d[0].x + d[0].y;
+        sm.dO32[3 * j0 + 1][tid] = d[1].x + d[1].y;
+        sm.dO32[3 * j0 + 2][tid] = d[2].x + d[2].y;
       }
 #pragma unroll 1
       for (unsigned m = careful_q; m; m &= m - 1u) {
@@ -1279,8 +1363,8 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_edges_mixed_kernel(cons
         // below; their FP32 terms come out as zero here.
         const int jq = __ffs(m) - 1;
         float2 d[3];
-        const unsigned nb = edge_pair_terms<true, UNIT>(sm.frame[jq][warp], fp, fe, fee, fm, k2ee,
-                                                  lane < n, lane + 32 < n, acc, d);
+        const unsigned nb = edge_pair_terms<true, UNIT>(sm.frame[jq][warp], fp, fe, fne, fee, fm,
+                                                        k2ee, lane < n, lane + 32 < n, acc, d);
         near0 |= (nb & 1u) << jq;
         near1 |= (nb >> 1) << jq;
         sm.dO32[3 * jq][tid] = d[0].x + d[0].y;
@@ -1338,7 +1422,7 @@ __global__ void __launch_bounds__(kFaThreads, 4) adjoint_edges_mixed_kernel(cons
           sm.dsum[row] = sum;
         }
       }
-      if (++chunks == kFaFlushChunks || c0 + QC >= q_end) {
+      if (++chunks == kFaFlushQueries / QC || c0 + QC >= q_end) {
         chunks = 0;
 #pragma unroll
         for (int r = 0; r < 6; ++r) {
@@ -1375,6 +1459,7 @@ __global__ void finish_dedge_sorted_kernel(const double* __restrict__ part, int6
 }
 
 constexpr int kEaQc = kFaQc;
+constexpr int kEaQcNoDq = 32;  // without dL/do shares a 32-query chunk is cheap in shared memory
 
 // Scratch layout of adjoint_edges_mixed (each piece 256-byte aligned).
 struct EdgeMixedLayout {
@@ -1409,13 +1494,16 @@ EdgeMixedLayout edge_mixed_layout(const AdjointPlan& p, int64_t ne, int64_t nq) 
 
 }  // namespace
 
-AdjointPlan plan_adjoint_edges_mixed(int64_t ne, int64_t nq, int sms) {
-  auto kernel = adjoint_edges_mixed_kernel<kEaQc, false>;
-  const int smem = static_cast<int>(sizeof(EdgeAdjSmem<kEaQc>));
+AdjointPlan plan_adjoint_edges_mixed(int64_t ne, int64_t nq, int sms, bool no_dq) {
+  auto kernel = no_dq ? adjoint_edges_mixed_kernel<kEaQcNoDq, true, true>
+                      : adjoint_edges_mixed_kernel<kEaQc, false>;
+  const int smem = static_cast<int>(no_dq ? sizeof(EdgeAdjSmem<kEaQcNoDq, false>)
+                                          : sizeof(EdgeAdjSmem<kEaQc>));
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   const int slots = resident_ctas(reinterpret_cast<const void*>(kernel), kFaThreads, smem, sms);
   const int64_t ntiles = std::max<int64_t>(1, cdiv(ne, kTileFaces));
-  return plan_balanced(cdiv(ntiles, kFaTiles), nq, slots, kEaQc, 6 * ntiles * kTileFaces);
+  return plan_balanced(cdiv(ntiles, kFaTiles), nq, slots, no_dq ? kEaQcNoDq : kEaQc,
+                       6 * ntiles * kTileFaces);
 }
 
 size_t adjoint_edges_mixed_scratch_bytes(const AdjointPlan& p, int64_t ne, int64_t nq) {
@@ -1427,7 +1515,9 @@ cudaError_t adjoint_edges_mixed(const AdjointPlan& p, const double* edges, int64
                                 bool unit, double* dq, double* dedge, void* scratch,
                                 size_t scratch_bytes, cudaStream_t stream) {
   cudaError_t e = cudaSuccess;
-  if (nq > 0) e = cudaMemsetAsync(dq, 0, sizeof(double) * 3 * nq, stream);
+  const bool no_dq = dq == nullptr;  // unit weights only: dL/do not wanted
+  if (no_dq && !unit) return cudaErrorInvalidValue;
+  if (nq > 0 && !no_dq) e = cudaMemsetAsync(dq, 0, sizeof(double) * 3 * nq, stream);
   if (e == cudaSuccess && ne > 0) e = cudaMemsetAsync(dedge, 0, sizeof(double) * 6 * le, stream);
   if (e != cudaSuccess || nq <= 0 || ne <= 0) return e;
   const EdgeMixedLayout l = edge_mixed_layout(p, ne, nq);
@@ -1455,24 +1545,28 @@ cudaError_t adjoint_edges_mixed(const AdjointPlan& p, const double* edges, int64
     return e;
   gather_sorted_queries_kernel<<<static_cast<unsigned>(cdiv(nq, 256)), 256, 0, stream>>>(
       q, gw, qperm, nq, qs);
-  if ((e = cudaMemsetAsync(dO_part, 0, sizeof(double) * static_cast<size_t>(p.nranges) * nq * 3,
+  if (!no_dq &&
+      (e = cudaMemsetAsync(dO_part, 0, sizeof(double) * static_cast<size_t>(p.nranges) * nq * 3,
                            stream)) != cudaSuccess)
     return e;
   MixedEdgeArgs a{tiles, ntiles, e64, ld64, qs, nq, static_cast<float>(kappa * kappa),
                   p.blocks_per_range, p.queries_per_group, dO_part, dE_part};
-  auto kernel = unit ? adjoint_edges_mixed_kernel<kEaQc, true>
-                     : adjoint_edges_mixed_kernel<kEaQc, false>;
-  const int smem = static_cast<int>(sizeof(EdgeAdjSmem<kEaQc>));
+  auto kernel = no_dq ? adjoint_edges_mixed_kernel<kEaQcNoDq, true, true>
+                      : (unit ? adjoint_edges_mixed_kernel<kEaQc, true>
+                              : adjoint_edges_mixed_kernel<kEaQc, false>);
+  const int smem = static_cast<int>(no_dq ? sizeof(EdgeAdjSmem<kEaQcNoDq, false>)
+                                          : sizeof(EdgeAdjSmem<kEaQc>));
   if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
       cudaSuccess)
     return e;
   kernel<<<dim3(static_cast<unsigned>(p.nranges), static_cast<unsigned>(p.ngroups)), kFaThreads,
            smem, stream>>>(a);
-  finish_dq_sorted_kernel<<<static_cast<unsigned>(cdiv(nq * 3, 256)), 256, 0, stream>>>(
-      dO_part, p.nranges, nq, qperm, dq);
+  if (!no_dq)
+    finish_dq_sorted_kernel<<<static_cast<unsigned>(cdiv(nq * 3, 256)), 256, 0, stream>>>(
+        dO_part, p.nranges, nq, qperm, dq);
   finish_dedge_sorted_kernel<<<static_cast<unsigned>(cdiv(6 * ld64, 256)), 256, 0, stream>>>(
       dE_part, p.ngroups, ld64, edge_of, le, dedge);
-  g_launches.fetch_add(7, std::memory_order_relaxed);
+  g_launches.fetch_add(no_dq ? 6 : 7, std::memory_order_relaxed);
   return cudaGetLastError();
 }
 

@@ -48,7 +48,9 @@ cudaError_t adjoint_edges(const AdjointPlan& p, const double* edges, int64_t le,
 // orders are built inside the call from `scratch`. With `unit` the per-endpoint sums
 // are unweighted and the multiplicity weights dL/do only (edges welded by position:
 // each edge stands for the soup's directed sides on it, signed per side afterwards).
-AdjointPlan plan_adjoint_edges_mixed(int64_t ne, int64_t nq, int sms);
+// With `unit`, dq may be null: dL/do is not computed (no_dq in the plan; every m is 0
+// when the soup is a closed surface, so dL/do is exactly 0 there).
+AdjointPlan plan_adjoint_edges_mixed(int64_t ne, int64_t nq, int sms, bool no_dq = false);
 size_t adjoint_edges_mixed_scratch_bytes(const AdjointPlan& p, int64_t ne, int64_t nq);
 cudaError_t adjoint_edges_mixed(const AdjointPlan& p, const double* edges, int64_t le, int64_t ne,
                                 const double* q, int64_t nq, const double* gw, double kappa,

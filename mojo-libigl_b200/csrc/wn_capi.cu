@@ -734,12 +734,13 @@ int wn_backward_edges_mixed_device(const double* edges, int64_t le, int64_t ne, 
     return fail(WN_EINVAL, "bad sizes (ne=%lld, nq=%lld, le=%lld)", (long long)ne,
                 (long long)nq, (long long)le);
   if (int code = check_kappa(kappa)) return code;
+  if (!dq && !unit_weights) return fail(WN_EINVAL, "dq is required unless unit_weights = 1");
   std::lock_guard<std::mutex> lock(g_mutex);
   int code = WN_OK;
   DeviceCtx* c = context(&code);
   if (!c) return code;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const AdjointPlan p = plan_adjoint_edges_mixed(ne, nq, c->sms);
+  const AdjointPlan p = plan_adjoint_edges_mixed(ne, nq, c->sms, dq == nullptr);
   const size_t sb = adjoint_edges_mixed_scratch_bytes(p, ne, nq);
   void* scratch = nullptr;
   cudaError_t e = dev_malloc_async(&scratch, sb, st);

@@ -260,7 +260,9 @@ def backward_welded_edges(V, F, O, gW, welded=None, kappa: float = 4.0):
     sums each edge's unweighted endpoint terms once (dL/dO weighted by the net
     count m of its sides, so sides that cancel add nothing there), and every side
     a -> b takes them with its own sign: (da, db) = (dP, dQ) for sigma = +1 and
-    (-dQ, -dP) for sigma = -1. The per-vertex sums then run in a fixed order.
+    (-dQ, -dP) for sigma = -1. The per-vertex sums then run in a fixed order. A soup
+    that is a closed surface has every m = 0, so its dL/dO is exactly 0: the adjoint
+    is then called without dL/dO (a leaner kernel) and dL/dO returned as zeros.
     """
     handle = _lib.lib()
     q = O.to(torch.float64).contiguous()
@@ -268,10 +270,12 @@ def backward_welded_edges(V, F, O, gW, welded=None, kappa: float = 4.0):
     nq, nv = q.shape[0], V.shape[0]
     edges, ng, side_edge, sigma, ends = welded if welded is not None else welded_edges(V, F)
     le = edges.shape[1]
-    dq = torch.empty((nq, 3), dtype=torch.float64, device=q.device)
+    closed = ng == 0 or not bool(edges[6, :ng].any())
+    dq = (torch.zeros if closed else torch.empty)((nq, 3), dtype=torch.float64, device=q.device)
     dedge = torch.zeros((6, le), dtype=torch.float64, device=q.device)
     _check(handle.wn_backward_edges_mixed_device(edges.data_ptr(), le, ng, q.data_ptr(), nq,
-                                                 gw.data_ptr(), kappa, 1, dq.data_ptr(),
+                                                 gw.data_ptr(), kappa, 1,
+                                                 None if closed else dq.data_ptr(),
                                                  dedge.data_ptr(), _stream()))
     ns = ends.shape[0]
     dside = torch.zeros((6, max(ns, 1)), dtype=torch.float64, device=q.device)

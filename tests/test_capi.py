@@ -55,6 +55,16 @@ def test_fault_injection_arming_does_not_need_a_gpu():
     assert handle.wn_inject_fault(0, 0) == 0 and handle.wn_fault_armed() == 0
 
 
+def test_edge_adjoint_without_dq_needs_unit_weights():
+    """dq = NULL (dL/do not wanted) is accepted for the welded (unit-weight) edge
+    adjoint only; the argument check runs before any device work."""
+    handle = _lib.lib()
+    rc = handle.wn_backward_edges_mixed_device(None, 1, 1, None, 1, None, 4.0, 0, None, None,
+                                               None)
+    assert rc == 1  # WN_EINVAL
+    assert b"dq is required" in handle.wn_last_error()
+
+
 def test_fault_injection_from_the_environment():
     code = "from igl import _lib; print(_lib.lib().wn_fault_armed())"
     env = dict(os.environ, WN_INJECT_FAULT="alloc:2",

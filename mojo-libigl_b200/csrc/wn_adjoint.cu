@@ -1160,10 +1160,21 @@ __device__ __forceinline__ unsigned edge_pair_terms(const float4 (&fr)[2], const
   const float2 lp = __fmul2_rn(pp, rp), lq = __fmul2_rn(qq, rq);
   const float2 gD = __fmul2_rn(gm, rcp2(__ffma2_rn(lp, lq, pq)));
   const float2 kp = __fmul2_rn(rp, gD), kq = __fmul2_rn(rq, gD);
-  // x = p x e with -e held per tile ((-a) b and a (-b) round alike): no negation per pair.
-  const float2 x0 = __ffma2_rn(py, fe[2], __fmul2_rn(pz, fne[1]));
-  const float2 x1 = __ffma2_rn(pz, fe[0], __fmul2_rn(px, fne[2]));
-  const float2 x2 = __ffma2_rn(px, fe[1], __fmul2_rn(py, fne[0]));
+  // x = p x e. With dL/do the tile's -e saves negating p per pair ((-a) b and a (-b)
+  // round alike); without it the kernel's register budget is tighter than the three
+  // packed negations, which cost fewer instructions than the moves -e brings there.
+  float2 x0, x1, x2;
+  if constexpr (DQ) {
+    x0 = __ffma2_rn(py, fe[2], __fmul2_rn(pz, fne[1]));
+    x1 = __ffma2_rn(pz, fe[0], __fmul2_rn(px, fne[2]));
+    x2 = __ffma2_rn(px, fe[1], __fmul2_rn(py, fne[0]));
+  } else {
+    const float2 m1 = f2(-1.f);
+    const float2 npx = __fmul2_rn(px, m1), npy = __fmul2_rn(py, m1), npz = __fmul2_rn(pz, m1);
+    x0 = __ffma2_rn(py, fe[2], __fmul2_rn(npz, fe[1]));
+    x1 = __ffma2_rn(pz, fe[0], __fmul2_rn(npx, fe[2]));
+    x2 = __ffma2_rn(px, fe[1], __fmul2_rn(npy, fe[0]));
+  }
   acc[0] = __ffma2_rn(kp, x0, acc[0]);
   acc[1] = __ffma2_rn(kp, x1, acc[1]);
   acc[2] = __ffma2_rn(kp, x2, acc[2]);

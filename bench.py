@@ -629,6 +629,12 @@ def gpu_arm(args):
             err_b.append(float((wm[torch.from_numpy(sel).to(dev)] - ref_m).abs().max()))
         bt.capture(backward=True)
         t_g, launches_g, _ = timed(bt.replay, args.steps, 2)
+        # The same graph with the FP64 adjoint, for comparison.
+        bt.graph = None
+        torch.cuda.synchronize()
+        bt.handle.wn_batch_set_adjoint_fp64(bt.batch, 1)
+        bt.capture(backward=True)
+        t_g64 = timed(bt.replay, args.steps, 2)[0]
         c5 = {"workload": "64 bumpy icospheres, subdivision U{2..7}, 0-10% faces deleted, "
                           "queries log-uniform in [1024, 2^20], 50/50 box/near(1e-3)",
               "meshes": len(meshes), "pairs": bt.pairs, "config": cfg,
@@ -639,6 +645,9 @@ def gpu_arm(args):
               "fwd_ms": t_f * 1e3, "fwd_pairs_per_s": world * bt.pairs / t_f,
               "graph_fwdbwd_ms": t_g * 1e3, "graph_fwdbwd_pairs_per_s": world * bt.pairs / t_g,
               "ratio_fwdbwd_to_fwd": t_g / t_f,
+              "adjoint": "mixed (per-mesh Morton-ordered 64-edge tiles, FP64 near pairs)",
+              "graph_fwdbwd_fp64_adjoint_ms": t_g64 * 1e3,
+              "ratio_fwdbwd_fp64_adjoint": t_g64 / t_f,
               "max_abs_err_vs_fp64": max(err_b),
               "error_sample": "up to 128 queries of each mesh against the plain FP64 kernel"}
         bt.close()

@@ -199,14 +199,19 @@ int wn_batch_create(int64_t nmesh, const int64_t* nv, const int64_t* nf, const i
                     const int64_t* faces, double kappa, int qpt, int64_t target_pairs,
                     int ctas_per_sm, int tile_faces, void** batch_out);
 int wn_batch_forward(void* batch, const double* V, const double* q, double* w, void* stream);
-/* Adjoint of every mesh through its net boundary edges (FP64, persistent,
- * deterministic): gw (total_nq) -> dq (total_nq x 3), dV (total_nv x 3). Same
- * launch properties as wn_batch_forward. */
+/* Adjoint of every mesh through its net boundary edges (deterministic): gw
+ * (total_nq) -> dq (total_nq x 3), dV (total_nv x 3). Same launch properties as
+ * wn_batch_forward. Mixed precision by default, as the forward (each mesh's edges
+ * in their own Morton order, 64-edge tiles, FP32 pairs with FP64 pairs near an
+ * edge, as wn_backward_edges_mixed_device); FP64 after
+ * wn_batch_set_adjoint_fp64(batch, 1). Both paths' buffers come from
+ * wn_batch_create: switching allocates nothing. */
 int wn_batch_backward(void* batch, const double* V, const double* q, const double* gw,
                       double* dq, double* dV, void* stream);
+int wn_batch_set_adjoint_fp64(void* batch, int fp64);
 /* out[0..n): nmesh, total_nv, total_nf, total_nq, total_tiles, work items,
  * persistent grid, partial sums, qpt, target_pairs, boundary edges, adjoint
- * work items, tile_faces. */
+ * work items (of the selected precision), tile_faces, adjoint in FP64 (0/1). */
 int wn_batch_info(void* batch, int64_t* out, int64_t n);
 int wn_batch_destroy(void* batch);
 

@@ -981,17 +981,23 @@ __device__ __forceinline__ double warp_min_d(double v) {
   return v;
 }
 
-// One CTA of 64 threads per tile: edges order[64 t + j] in Morton order.
+// One CTA of 64 threads per tile: edges order[first + j], j < count, in Morton
+// order, with first = 64 t and count = min(64, ne - first), or (batched meshes,
+// whose tiles do not cross a mesh) both from tile_first / tile_count.
 __global__ void __launch_bounds__(kTileFaces) build_edge_tiles_kernel(
     const double* __restrict__ edges, int64_t le, int64_t ne, const uint32_t* __restrict__ order,
     double kappa, unsigned char* __restrict__ tiles, double* __restrict__ e64, int64_t ld64,
-    uint32_t* __restrict__ edge_of) {
+    uint32_t* __restrict__ edge_of, const int64_t* __restrict__ tile_first = nullptr,
+    const int32_t* __restrict__ tile_count = nullptr) {
   __shared__ double red[8][kTileFaces / 32];
   const int j = threadIdx.x, warp = j >> 5, lane = j & 31;
   const int64_t tile = blockIdx.x;
   const int64_t slot = tile * kTileFaces + j;
-  const bool valid = slot < ne;
-  const int64_t e = valid ? order[slot] : 0;
+  const int64_t first = tile_first ? tile_first[tile] : tile * kTileFaces;
+  const int64_t left = ne - first;
+  const int64_t count = tile_count ? tile_count[tile] : (left < kTileFaces ? left : kTileFaces);
+  const bool valid = j < count;
+  const int64_t e = valid ? order[first + j] : 0;
   double v[7];
 #pragma unroll
   for (int r = 0; r < 7; ++r) v[r] = valid ? edges[r * le + e] : 0.0;
@@ -1043,8 +1049,7 @@ __global__ void __launch_bounds__(kTileFaces) build_edge_tiles_kernel(
     const double far = rt + kappa * ht;
     th.far_r2 = far * far;
     th.scale = scale;
-    const int64_t left = ne - tile * kTileFaces;
-    th.n = static_cast<int32_t>(left < kTileFaces ? left : kTileFaces);
+    th.n = static_cast<int32_t>(count);
     th.r = static_cast<float>(rt);
     th.h = static_cast<float>(ht);
     *reinterpret_cast<TileHeader*>(rec) = th;
@@ -1192,23 +1197,33 @@ __device__ __forceinline__ unsigned edge_pair_terms(const float4 (&fr)[2], const
 
 __device__ __forceinline__ int jq_of(unsigned mask) { return __ffs(mask) - 1; }
 
+// The work of one CTA: blocks [b_begin, b_end) of kFaTiles edge tiles of one mesh
+// against its sorted queries [q_begin, q_end). Indices are local to the mesh: its
+// tiles, FP64 edge slots (row stride ld64) and sorted queries start at the pointers.
+struct EdgeWork {
+  const unsigned char* tiles;
+  int64_t ntiles;
+  const double* e64;
+  int64_t ld64;
+  const double4* qs;
+  float kappa2;
+  int64_t b_begin, b_end, q_begin, q_end;
+  double* dO_row;    // this edge range's dL/do partials, [sorted position][3], accumulated
+  double* dE_group;  // this query group's per-slot sums, [6][de_ld], written
+  int64_t de_ld;
+};
+
 // NODQ (with UNIT, for callers that need no dL/do: every net multiplicity is 0)
 // compiles the dL/do path out, so that the per-query shares take no shared memory
 // and 96 registers fit five CTAs per SM.
-template <int QC, bool UNIT, bool NODQ = false>
-__global__ void __launch_bounds__(kFaThreads, NODQ ? 5 : 4)
-    adjoint_edges_mixed_kernel(const MixedEdgeArgs a) {
+template <int QC, bool UNIT, bool NODQ>
+__device__ __forceinline__ void edge_adjoint_cta(const EdgeWork& a,
+                                                 EdgeAdjSmem<QC, !NODQ>& sm) {
   static_assert(UNIT || !NODQ, "dL/do is dropped only in the unit-weight mode");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  auto& sm = *reinterpret_cast<EdgeAdjSmem<QC, !NODQ>*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int64_t nblocks = (a.ntiles + kFaTiles - 1) / kFaTiles;
-  const int64_t range = blockIdx.x, group = blockIdx.y;
-  const int64_t b_begin = range * a.blocks_per_range;
-  const int64_t b_end = min(nblocks, b_begin + a.blocks_per_range);
-  const int64_t q_begin = group * a.queries_per_group;
-  const int64_t q_end = min(a.nq, q_begin + a.queries_per_group);
-  double* dO_row = a.dO_part + range * a.nq * 3;
+  const int64_t b_begin = a.b_begin, b_end = a.b_end;
+  const int64_t q_begin = a.q_begin, q_end = a.q_end;
+  double* dO_row = a.dO_row;
 
   for (int64_t blk = b_begin; blk < b_end; ++blk) {
     __syncthreads();  // previous block's shared data fully consumed
@@ -1450,9 +1465,33 @@ __global__ void __launch_bounds__(kFaThreads, NODQ ? 5 : 4)
       if (lane + 32 * k >= n) continue;
 #pragma unroll
       for (int r = 0; r < 6; ++r)
-        a.dE_part[(group * 6 + r) * a.ld64 + slot0 + 32 * k] = sm.acc64[6 * k + r][tid];
+        a.dE_group[r * a.de_ld + slot0 + 32 * k] = sm.acc64[6 * k + r][tid];
     }
   }
+}
+
+template <int QC, bool UNIT, bool NODQ = false>
+__global__ void __launch_bounds__(kFaThreads, NODQ ? 5 : 4)
+    adjoint_edges_mixed_kernel(const MixedEdgeArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto& sm = *reinterpret_cast<EdgeAdjSmem<QC, !NODQ>*>(smem_raw);
+  const int64_t nblocks = (a.ntiles + kFaTiles - 1) / kFaTiles;
+  const int64_t range = blockIdx.x, group = blockIdx.y;
+  EdgeWork w;
+  w.tiles = a.tiles;
+  w.ntiles = a.ntiles;
+  w.e64 = a.e64;
+  w.ld64 = a.ld64;
+  w.qs = a.qs;
+  w.kappa2 = a.kappa2;
+  w.b_begin = range * a.blocks_per_range;
+  w.b_end = min(nblocks, w.b_begin + a.blocks_per_range);
+  w.q_begin = group * a.queries_per_group;
+  w.q_end = min(a.nq, w.q_begin + a.queries_per_group);
+  w.dO_row = a.dO_part + range * a.nq * 3;
+  w.dE_group = a.dE_part + group * 6 * a.ld64;
+  w.de_ld = a.ld64;
+  edge_adjoint_cta<QC, UNIT, NODQ>(w, sm);
 }
 
 // dedge[row][edge_of[slot]] = (1/4pi) sum_g dE_part[g][row][slot] (sorted slots to input edges).
@@ -1609,6 +1648,22 @@ struct BatchEdgeMesh {
   int64_t e_off, ne, q_off, nq, nranges, ngroups, do_off, de_off;
 };
 
+// Mixed path: mesh m's edges fill tiles [tile_off, tile_off + ntile) (slots 64 per
+// tile, ld = 64 ntile per mesh) in its own Morton order; its sorted queries are
+// positions [q_off, q_off + nq) of the batch's.
+struct BatchMixedMesh {
+  int64_t tile_off, ntile, q_off, nq, nranges, ngroups, do_off, de_off;
+};
+
+// One CTA's work on the mixed path (the fields of EdgeWork, mesh-relative).
+struct BatchMixedItem {
+  int64_t tile_off, ntiles, q_off;
+  int64_t b_begin, b_end, q_begin, q_end;
+  int64_t do_row;   // dO offset of this range's row (mesh-local sorted positions)
+  int64_t de_base;  // dE offset of this group's [6][de_ld] block
+  int64_t de_ld;
+};
+
 struct BatchEdges {
   int64_t ne_total = 0, le = 1, n_items = 0, do_doubles = 0, de_doubles = 0;
   int grid = 0;
@@ -1625,6 +1680,29 @@ struct BatchEdges {
   unsigned int* counter = nullptr;
   double* dO_part = nullptr;
   double* dE_part = nullptr;
+  // Mixed path (the default).
+  bool fp64 = false;
+  int64_t nt = 0, m_items = 0, m_do = 0, m_de = 0;
+  int64_t* tile_first = nullptr;   // nt: sorted position of the tile's first edge
+  int32_t* tile_count = nullptr;   // nt
+  int32_t* tile_mesh = nullptr;    // nt
+  BatchMixedMesh* mmeshes = nullptr;
+  BatchMixedItem* mitems = nullptr;
+  double* mid = nullptr;           // ne_total x 3 edge midpoints
+  unsigned long long* box = nullptr;
+  uint64_t* keys_in = nullptr;
+  uint64_t* keys_out = nullptr;
+  uint32_t* vals_in = nullptr;
+  uint32_t* eperm = nullptr;       // ne_total
+  uint32_t* qperm = nullptr;       // total_nq
+  void* temp = nullptr;
+  size_t temp_bytes = 0;
+  unsigned char* tiles = nullptr;  // nt x kEdgeTileBytes
+  double* e64 = nullptr;           // 7 x 64 nt
+  uint32_t* edge_of = nullptr;     // 64 nt
+  double4* qs = nullptr;           // total_nq
+  double* mdO = nullptr;
+  double* mdE = nullptr;
 };
 
 namespace {
@@ -1782,6 +1860,81 @@ __global__ void batch_finish_dedge_kernel(const double* __restrict__ dE_part,
   dedge[r * le + e] = s * kInv4Pi;
 }
 
+constexpr int64_t kBatchMixedBlocks = 16;     // 4-tile blocks per range (4,096 edges)
+constexpr int64_t kBatchMixedQueries = 4096;  // sorted queries per group
+static_assert(kBatchMixedQueries % kFaFlushQueries == 0, "groups hold whole FP32 flushes");
+
+struct BatchMixedArgs {
+  const BatchMixedItem* items;
+  const unsigned char* tiles;
+  const double* e64;
+  int64_t ld64;
+  const double4* qs;
+  float kappa2;
+  double* dO;
+  double* dE;
+};
+
+// The mixed edge adjoint's CTA over work items: item blockIdx.x is one (mesh, edge
+// range, query group) of one mesh, whose sums go to the mesh's own partial rows.
+template <int QC>
+__global__ void __launch_bounds__(kFaThreads, 4) batch_edges_mixed_kernel(const BatchMixedArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  auto& sm = *reinterpret_cast<EdgeAdjSmem<QC, true>*>(smem_raw);
+  const BatchMixedItem it = a.items[blockIdx.x];
+  EdgeWork w;
+  w.tiles = a.tiles + it.tile_off * kEdgeTileBytes;
+  w.ntiles = it.ntiles;
+  w.e64 = a.e64 + it.tile_off * kTileFaces;
+  w.ld64 = a.ld64;
+  w.qs = a.qs + it.q_off;
+  w.kappa2 = a.kappa2;
+  w.b_begin = it.b_begin;
+  w.b_end = it.b_end;
+  w.q_begin = it.q_begin;
+  w.q_end = it.q_end;
+  w.dO_row = a.dO + it.do_row;
+  w.dE_group = a.dE + it.de_base;
+  w.de_ld = it.de_ld;
+  edge_adjoint_cta<QC, false, false>(w, sm);
+}
+
+// dq[qperm[s]] = (1/4pi) sum over the mesh's ranges of dO at sorted position s
+// (sorted positions are grouped by mesh as the input queries are).
+__global__ void batch_mixed_finish_dq_kernel(const double* __restrict__ dO,
+                                             const BatchMixedMesh* __restrict__ meshes,
+                                             const int32_t* __restrict__ query_mesh,
+                                             const uint32_t* __restrict__ qperm,
+                                             int64_t total_nq, double* __restrict__ dq) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= total_nq * 3) return;
+  const int64_t sp = i / 3, x = i % 3;
+  const BatchMixedMesh mm = meshes[query_mesh[sp]];
+  double s = 0.0;
+  for (int64_t r = 0; r < mm.nranges; ++r)
+    s += dO[mm.do_off + (r * mm.nq + (sp - mm.q_off)) * 3 + x];
+  dq[3 * static_cast<int64_t>(qperm[sp]) + x] = s * kInv4Pi;
+}
+
+// dedge[row][edge_of[slot]] = (1/4pi) sum over the mesh's groups of dE at the slot.
+__global__ void batch_mixed_finish_dedge_kernel(const double* __restrict__ dE,
+                                                const BatchMixedMesh* __restrict__ meshes,
+                                                const int32_t* __restrict__ tile_mesh,
+                                                const uint32_t* __restrict__ edge_of, int64_t nt,
+                                                int64_t le, double* __restrict__ dedge) {
+  const int64_t slots = nt * kTileFaces;
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= 6 * slots) return;
+  const int64_t r = i / slots, sl = i % slots;
+  const uint32_t e = edge_of[sl];
+  if (e == 0xffffffffu) return;
+  const BatchMixedMesh mm = meshes[tile_mesh[sl / kTileFaces]];
+  const int64_t ld = mm.ntile * kTileFaces, local = sl - mm.tile_off * kTileFaces;
+  double s = 0.0;
+  for (int64_t g = 0; g < mm.ngroups; ++g) s += dE[mm.de_off + (g * 6 + r) * ld + local];
+  dedge[r * le + e] = s * kInv4Pi;
+}
+
 }  // namespace
 
 cudaError_t batch_edges_create(BatchState* b, const int64_t* F) {
@@ -1895,6 +2048,103 @@ cudaError_t batch_edges_create(BatchState* b, const int64_t* F) {
       (e = dev_malloc(reinterpret_cast<void**>(&E->dE_part),
                       sizeof(double) * std::max<int64_t>(E->de_doubles, 1))) != cudaSuccess)
     return e;
+  // Mixed path: every mesh's edges in whole 64-edge tiles of their own, and (edge
+  // range, query group) items per mesh, largest first.
+  std::vector<BatchMixedMesh> mmeshes(b->nmesh);
+  std::vector<int64_t> tile_first;
+  std::vector<int32_t> tile_count, tile_mesh;
+  std::vector<BatchMixedItem> mitems;
+  {
+    int64_t mdo = 0, mde = 0, toff = 0;
+    for (int64_t m = 0; m < b->nmesh; ++m) {
+      const BatchEdgeMesh& em = meshes[m];
+      BatchMixedMesh& mm = mmeshes[m];
+      mm.tile_off = toff;
+      mm.ntile = cdiv(em.ne, kTileFaces);
+      mm.q_off = em.q_off;
+      mm.nq = em.nq;
+      for (int64_t t = 0; t < mm.ntile; ++t) {
+        tile_first.push_back(em.e_off + t * kTileFaces);
+        tile_count.push_back(static_cast<int32_t>(std::min<int64_t>(kTileFaces,
+                                                                    em.ne - t * kTileFaces)));
+        tile_mesh.push_back(static_cast<int32_t>(m));
+      }
+      toff += mm.ntile;
+      const bool work = em.ne > 0 && em.nq > 0;
+      const int64_t nblocks = cdiv(mm.ntile, kFaTiles), ld = mm.ntile * kTileFaces;
+      mm.nranges = work ? cdiv(nblocks, kBatchMixedBlocks) : 0;
+      mm.ngroups = work ? cdiv(em.nq, kBatchMixedQueries) : 0;
+      mm.do_off = mdo;
+      mm.de_off = mde;
+      for (int64_t r = 0; r < mm.nranges; ++r)
+        for (int64_t g = 0; g < mm.ngroups; ++g) {
+          BatchMixedItem it;
+          it.tile_off = mm.tile_off;
+          it.ntiles = mm.ntile;
+          it.q_off = mm.q_off;
+          it.b_begin = r * kBatchMixedBlocks;
+          it.b_end = std::min(nblocks, it.b_begin + kBatchMixedBlocks);
+          it.q_begin = g * kBatchMixedQueries;
+          it.q_end = std::min(em.nq, it.q_begin + kBatchMixedQueries);
+          it.do_row = mdo + r * em.nq * 3;
+          it.de_base = mde + g * 6 * ld;
+          it.de_ld = ld;
+          mitems.push_back(it);
+        }
+      mdo += mm.nranges * em.nq * 3;
+      mde += mm.ngroups * 6 * ld;
+    }
+    E->nt = toff;
+    E->m_do = mdo;
+    E->m_de = mde;
+  }
+  std::stable_sort(mitems.begin(), mitems.end(),
+                   [](const BatchMixedItem& x, const BatchMixedItem& y) {
+                     return (x.b_end - x.b_begin) * (x.q_end - x.q_begin) >
+                            (y.b_end - y.b_begin) * (y.q_end - y.q_begin);
+                   });
+  E->m_items = static_cast<int64_t>(mitems.size());
+  const int64_t nkeys = std::max<int64_t>({E->ne_total, b->total_nq, 1});
+  E->temp_bytes = batch_morton_temp_bytes(nkeys, b->mesh_bits);
+  const int64_t nt1 = std::max<int64_t>(E->nt, 1);
+  if ((e = up(&E->tile_first, tile_first, 1)) != cudaSuccess ||
+      (e = up(&E->tile_count, tile_count, 1)) != cudaSuccess ||
+      (e = up(&E->tile_mesh, tile_mesh, 1)) != cudaSuccess ||
+      (e = up(&E->mmeshes, mmeshes, 1)) != cudaSuccess ||
+      (e = up(&E->mitems, mitems, 1)) != cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->mid),
+                      sizeof(double) * 3 * std::max<int64_t>(E->ne_total, 1))) != cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->box),
+                      sizeof(unsigned long long) * 6 * std::max<int64_t>(b->nmesh, 1))) !=
+          cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->keys_in), sizeof(uint64_t) * nkeys)) !=
+          cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->keys_out), sizeof(uint64_t) * nkeys)) !=
+          cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->vals_in), sizeof(uint32_t) * nkeys)) !=
+          cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->eperm),
+                      sizeof(uint32_t) * std::max<int64_t>(E->ne_total, 1))) != cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->qperm),
+                      sizeof(uint32_t) * std::max<int64_t>(b->total_nq, 1))) != cudaSuccess ||
+      (e = dev_malloc(&E->temp, std::max<size_t>(E->temp_bytes, 16))) != cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->tiles),
+                      static_cast<size_t>(kEdgeTileBytes) * nt1)) != cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->e64),
+                      sizeof(double) * 7 * kTileFaces * nt1)) != cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->edge_of),
+                      sizeof(uint32_t) * kTileFaces * nt1)) != cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->qs),
+                      sizeof(double4) * std::max<int64_t>(b->total_nq, 1))) != cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->mdO),
+                      sizeof(double) * std::max<int64_t>(E->m_do, 1))) != cudaSuccess ||
+      (e = dev_malloc(reinterpret_cast<void**>(&E->mdE),
+                      sizeof(double) * std::max<int64_t>(E->m_de, 1))) != cudaSuccess)
+    return e;
+  if ((e = cudaFuncSetAttribute(batch_edges_mixed_kernel<kEaQc>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(sizeof(EdgeAdjSmem<kEaQc>)))) != cudaSuccess)
+    return e;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &per_sm, batch_edges_kernel<kAdjThreads, kAdjFpt, kAdjQc>, kAdjThreads, 0);
@@ -1904,14 +2154,24 @@ cudaError_t batch_edges_create(BatchState* b, const int64_t* F) {
 }
 
 int64_t batch_boundary_edges(const BatchState* b) { return b->edges ? b->edges->ne_total : 0; }
-int64_t batch_edge_items(const BatchState* b) { return b->edges ? b->edges->n_items : 0; }
+int64_t batch_edge_items(const BatchState* b) {
+  return b->edges ? (b->edges->fp64 ? b->edges->n_items : b->edges->m_items) : 0;
+}
+void batch_set_adjoint_fp64(BatchState* b, bool fp64) {
+  if (b->edges) b->edges->fp64 = fp64;
+}
+bool batch_adjoint_fp64(const BatchState* b) { return b->edges && b->edges->fp64; }
 
 void batch_edges_destroy(BatchState* b) {
   BatchEdges* E = b->edges;
   if (!E) return;
-  void* ptrs[] = {E->ends,   E->mult,       E->edges,     E->dedge,   E->indptr,
-                  E->entries, E->items,     E->meshes,    E->query_mesh, E->edge_mesh,
-                  E->counter, E->dO_part,   E->dE_part};
+  void* ptrs[] = {E->ends,     E->mult,       E->edges,     E->dedge,      E->indptr,
+                  E->entries,  E->items,      E->meshes,    E->query_mesh, E->edge_mesh,
+                  E->counter,  E->dO_part,    E->dE_part,   E->tile_first, E->tile_count,
+                  E->tile_mesh, E->mmeshes,   E->mitems,    E->mid,        E->box,
+                  E->keys_in,  E->keys_out,   E->vals_in,   E->eperm,      E->qperm,
+                  E->temp,     E->tiles,      E->e64,       E->edge_of,    E->qs,
+                  E->mdO,      E->mdE};
   for (void* p : ptrs) cudaFree(p);
   delete E;
   b->edges = nullptr;
@@ -1931,6 +2191,45 @@ cudaError_t batch_backward(BatchState* b, const double* V, const double* q, cons
   if (E->ne_total == 0 || b->total_nq == 0) return cudaSuccess;
   batch_edge_positions_kernel<<<static_cast<unsigned>(cdiv(E->ne_total, 256)), 256, 0, stream>>>(
       V, E->ends, E->mult, E->ne_total, E->le, E->edges);
+  if (!E->fp64) {
+    // Mixed: each mesh's edges and queries in their own Morton order, 64-edge tiles,
+    // then (range, group) items with fixed-order sums as the single-mesh path.
+    edge_midpoints_kernel<<<static_cast<unsigned>(cdiv(E->ne_total, 256)), 256, 0, stream>>>(
+        E->edges, E->le, E->ne_total, E->mid);
+    if ((e = batch_morton_order(E->mid, E->ne_total, E->edge_mesh, b->nmesh, b->mesh_bits,
+                                E->box, E->keys_in, E->keys_out, E->vals_in, E->eperm, E->temp,
+                                E->temp_bytes, stream)) != cudaSuccess)
+      return e;
+    build_edge_tiles_kernel<<<static_cast<unsigned>(E->nt), kTileFaces, 0, stream>>>(
+        E->edges, E->le, E->ne_total, E->eperm, b->plan.kappa, E->tiles, E->e64,
+        E->nt * kTileFaces, E->edge_of, E->tile_first, E->tile_count);
+    if ((e = batch_morton_order(q, b->total_nq, E->query_mesh, b->nmesh, b->mesh_bits, E->box,
+                                E->keys_in, E->keys_out, E->vals_in, E->qperm, E->temp,
+                                E->temp_bytes, stream)) != cudaSuccess)
+      return e;
+    gather_sorted_queries_kernel<<<static_cast<unsigned>(cdiv(b->total_nq, 256)), 256, 0,
+                                   stream>>>(q, gw, E->qperm, b->total_nq, E->qs);
+    if ((e = cudaMemsetAsync(E->mdO, 0, sizeof(double) * std::max<int64_t>(E->m_do, 1),
+                             stream)) != cudaSuccess)
+      return e;
+    const double kappa = b->plan.kappa;
+    BatchMixedArgs ma{E->mitems, E->tiles, E->e64, E->nt * kTileFaces, E->qs,
+                      static_cast<float>(kappa * kappa), E->mdO, E->mdE};
+    if (E->m_items > 0)
+      batch_edges_mixed_kernel<kEaQc>
+          <<<static_cast<unsigned>(E->m_items), kFaThreads,
+             static_cast<int>(sizeof(EdgeAdjSmem<kEaQc>)), stream>>>(ma);
+    batch_mixed_finish_dq_kernel<<<static_cast<unsigned>(cdiv(3 * b->total_nq, 256)), 256, 0,
+                                   stream>>>(E->mdO, E->mmeshes, E->query_mesh, E->qperm,
+                                             b->total_nq, dq);
+    batch_mixed_finish_dedge_kernel<<<static_cast<unsigned>(cdiv(6 * E->nt * kTileFaces, 256)),
+                                      256, 0, stream>>>(E->mdE, E->mmeshes, E->tile_mesh,
+                                                        E->edge_of, E->nt, E->le, E->dedge);
+    gather_vertex_kernel<<<static_cast<unsigned>(cdiv(b->total_nv, 256)), 256, 0, stream>>>(
+        E->dedge, E->le, 2, E->indptr, E->entries, b->total_nv, dV);
+    g_launches.fetch_add(E->m_items > 0 ? 7 : 6, std::memory_order_relaxed);
+    return cudaGetLastError();
+  }
   if ((e = cudaMemsetAsync(E->dO_part, 0, sizeof(double) * std::max<int64_t>(E->do_doubles, 1),
                            stream)) != cudaSuccess ||
       (e = cudaMemsetAsync(E->counter, 0, sizeof(unsigned int), stream)) != cudaSuccess)

@@ -72,4 +72,21 @@ int64_t batch_edge_items(const BatchState* b);
 cudaError_t batch_backward(BatchState* b, const double* V, const double* q, const double* gw,
                            double* dq, double* dV, cudaStream_t stream);
 
+// The adjoint's precision: mixed (FP32 edge pairs in per-mesh Morton-ordered 64-edge
+// tiles, FP64 near pairs; the default, as the forward) or FP64. Both paths' buffers
+// are allocated by batch_edges_create, so switching allocates nothing.
+void batch_set_adjoint_fp64(BatchState* b, bool fp64);
+bool batch_adjoint_fp64(const BatchState* b);
+
+// Morton order of n points (x, y, z rows) inside each mesh: keys mesh << 30 | the
+// 30-bit code against the mesh's own box (the single-mesh code for the same points),
+// one radix sort; perm[s] = the point at sorted position s, meshes in order. Buffers:
+// box nmesh x 6, keys and values n each, temp batch_morton_temp_bytes(n, mesh_bits).
+size_t batch_morton_temp_bytes(int64_t n, int mesh_bits);
+cudaError_t batch_morton_order(const double* pts, int64_t n, const int32_t* mesh_of,
+                               int64_t nmesh, int mesh_bits, unsigned long long* box,
+                               uint64_t* keys_in, uint64_t* keys_out, uint32_t* vals_in,
+                               uint32_t* perm, void* temp, size_t temp_bytes,
+                               cudaStream_t stream);
+
 }  // namespace wn

@@ -842,13 +842,22 @@ int wn_batch_backward(void* batch, const double* V, const double* q, const doubl
   return e == cudaSuccess ? WN_OK : cuda_fail(e, "batched adjoint launch");
 }
 
+int wn_batch_set_adjoint_fp64(void* batch, int fp64) {
+  if (!batch) return fail(WN_EINVAL, "null batch");
+  if (fp64 != 0 && fp64 != 1) return fail(WN_EINVAL, "fp64 must be 0 or 1, got %d", fp64);
+  std::lock_guard<std::mutex> lock(g_mutex);
+  batch_set_adjoint_fp64(static_cast<BatchState*>(batch), fp64 != 0);
+  return WN_OK;
+}
+
 int wn_batch_info(void* batch, int64_t* out, int64_t n) {
   if (!batch || !out) return fail(WN_EINVAL, "null argument");
   const BatchState* b = static_cast<const BatchState*>(batch);
   const int64_t vals[] = {b->nmesh,       b->total_nv,    b->total_nf, b->total_nq,
                           b->total_tiles, b->n_items,     b->grid,     b->total_partials,
                           b->plan.qpt,    b->plan.target_pairs,
-                          batch_boundary_edges(b), batch_edge_items(b), b->plan.tile_faces};
+                          batch_boundary_edges(b), batch_edge_items(b), b->plan.tile_faces,
+                          batch_adjoint_fp64(b) ? 1 : 0};
   for (int64_t i = 0; i < n && i < static_cast<int64_t>(sizeof(vals) / sizeof(vals[0])); ++i)
     out[i] = vals[i];
   return WN_OK;

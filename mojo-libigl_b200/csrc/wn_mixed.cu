@@ -1483,4 +1483,31 @@ cudaError_t batch_forward(BatchState* b, const double* V, const double* q, doubl
   return cudaGetLastError();
 }
 
+size_t batch_morton_temp_bytes(int64_t n, int mesh_bits) {
+  size_t bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, static_cast<uint64_t*>(nullptr),
+                                  static_cast<uint64_t*>(nullptr), static_cast<uint32_t*>(nullptr),
+                                  static_cast<uint32_t*>(nullptr),
+                                  static_cast<int>(std::max<int64_t>(n, 1)), 0, 30 + mesh_bits);
+  return bytes;
+}
+
+cudaError_t batch_morton_order(const double* pts, int64_t n, const int32_t* mesh_of,
+                               int64_t nmesh, int mesh_bits, unsigned long long* box,
+                               uint64_t* keys_in, uint64_t* keys_out, uint32_t* vals_in,
+                               uint32_t* perm, void* temp, size_t temp_bytes,
+                               cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  const int th = 256;
+  batch_bbox_init_kernel<<<static_cast<unsigned>(blocks_for(6 * nmesh, th)), th, 0, stream>>>(
+      box, nmesh);
+  batch_bbox_kernel<false><<<static_cast<unsigned>(blocks_for((n + 15) / 16, th)), th, 0,
+                             stream>>>(pts, 0, n, mesh_of, box);
+  batch_morton_kernel<false><<<static_cast<unsigned>(blocks_for(n, th)), th, 0, stream>>>(
+      pts, 0, n, mesh_of, box, keys_in, vals_in);
+  g_launches.fetch_add(3, std::memory_order_relaxed);
+  return cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, vals_in, perm,
+                                         static_cast<int>(n), 0, 30 + mesh_bits, stream);
+}
+
 }  // namespace wn

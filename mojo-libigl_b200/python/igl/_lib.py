@@ -78,6 +78,7 @@ _WN_SIGNATURES = {
     "wn_batch_create": ([I, P, P, P, P, ctypes.c_double, C_INT, I, C_INT, C_INT,
                          ctypes.POINTER(P)], C_INT),
     "wn_batch_forward": ([P, P, P, P, P], C_INT),
+    "wn_batch_set_adjoint_fp64": ([P, C_INT], C_INT),
     "wn_batch_backward": ([P, P, P, P, P, P, P], C_INT),
     "wn_batch_info": ([P, P, I], C_INT),
     "wn_batch_destroy": ([P], C_INT),

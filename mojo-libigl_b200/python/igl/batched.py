@@ -5,8 +5,9 @@ their query sets ``[O, ...]`` on the GPU and sets up libwn_b200's batched
 path: ``wn_batch_forward`` (mixed-precision forward of every mesh: one
 segmented Morton sort of faces, one of queries, one tile build, then a
 persistent kernel that takes (mesh, query block, tile range) work items from an
-atomic counter) and ``wn_batch_backward`` (boundary-edge adjoint of every mesh,
-also persistent). Both are allocation-free and never synchronise the host, so
+atomic counter) and ``wn_batch_backward`` (boundary-edge adjoint of every mesh:
+mixed precision by default, as the forward, or ``adjoint="fp64"``). Both are
+allocation-free and never synchronise the host, so
 ``capture()`` records forward + backward into a ``torch.cuda.CUDAGraph`` that
 ``replay()`` re-runs on whatever the static input tensors hold.
 """
@@ -36,11 +37,13 @@ class Batch:
 
     INFO_FIELDS = ("nmesh", "total_nv", "total_nf", "total_nq", "total_tiles", "work_items",
                    "grid", "partial_sums", "qpt", "target_pairs", "boundary_edges",
-                   "adjoint_items", "tile_faces")
+                   "adjoint_items", "tile_faces", "adjoint_fp64")
 
     def __init__(self, meshes, queries, kappa: float = 4.0, qpt: int = 2,
                  target_pairs: int = 1 << 23, ctas_per_sm: int = 0, tile_faces: int = 64,
-                 device="cuda"):
+                 adjoint: str = "mixed", device="cuda"):
+        if adjoint not in ("mixed", "fp64"):
+            raise ValueError(f"adjoint must be 'mixed' or 'fp64', got {adjoint!r}")
         if len(meshes) != len(queries) or not meshes:
             raise ValueError("need one query set per mesh, and at least one mesh")
         self.handle = _lib.lib()
@@ -58,8 +61,10 @@ class Batch:
                                            self.nq.ctypes.data, faces.ctypes.data, float(kappa),
                                            int(qpt), int(target_pairs), int(ctas_per_sm),
                                            int(tile_faces), ctypes.byref(self.batch)))
+        _check(self.handle.wn_batch_set_adjoint_fp64(self.batch, int(adjoint == "fp64")))
         self.config = {"kappa": float(kappa), "qpt": int(qpt), "target_pairs": int(target_pairs),
                        "ctas_per_sm": int(ctas_per_sm), "tile_faces": int(tile_faces)}
+        self.adjoint = adjoint
         dev = self.device
         self.V = torch.from_numpy(np.concatenate(Vs)).to(dev)
         self.Q = torch.from_numpy(np.concatenate(Qs)).to(dev)

@@ -65,6 +65,11 @@ def test_edge_adjoint_without_dq_needs_unit_weights():
     assert b"dq is required" in handle.wn_last_error()
 
 
+def test_batch_adjoint_precision_setter_checks_arguments():
+    handle = _lib.lib()
+    assert handle.wn_batch_set_adjoint_fp64(None, 1) == 1  # WN_EINVAL: null batch
+
+
 def test_fault_injection_from_the_environment():
     code = "from igl import _lib; print(_lib.lib().wn_fault_armed())"
     env = dict(os.environ, WN_INJECT_FAULT="alloc:2",

@@ -2,17 +2,23 @@
 
 The batched forward of every mesh must agree with the single-mesh mixed kernel
 and with the oracle (<= 1e-6), the batched adjoint with the single-mesh
-boundary-edge adjoint (<= 1e-12 relative), graph replays with eager runs
-bit for bit, and repeated runs with each other bit for bit.
+boundary-edge adjoint (FP64: <= 1e-12 relative; mixed: <= 1e-6 of the mixed one,
+<= 1e-4 of the FP64 one), graph replays with eager runs bit for bit, and
+repeated runs with each other bit for bit.
 """
 
 import numpy as np
 import pytest
 
 import igl
+from igl import _lib
 from igl import autograd as wa
 
 pytestmark = pytest.mark.gpu
+
+
+def _check_rc(rc):
+    assert rc == 0, _lib.last_error()
 
 
 def _small_batch(n=7, seed=5, max_level=4, max_q=3000):
@@ -48,23 +54,36 @@ def test_batched_forward_matches_oracle(gpu_required, oracle_mod, qpt, kappa, ti
         b.close()
 
 
-def test_batched_backward_matches_single_mesh_adjoint(gpu_required):
+@pytest.mark.parametrize("adjoint", ["fp64", "mixed"])
+def test_batched_backward_matches_single_mesh_adjoint(gpu_required, adjoint):
+    """FP64: the single-mesh FP64 edge adjoint within 1e-12 (relative to the
+    largest gradient). Mixed: the single-mesh mixed edge adjoint within 1e-6 (the
+    same tiles and pairs; only the FP32 flush points and the FP64 partial order
+    differ) and the FP64 one within 1e-4, as the single-mesh mixed path is."""
     import torch
 
     meshes, queries = _small_batch(seed=6)
-    b = igl.batched.Batch(meshes, queries, target_pairs=1 << 16)
+    b = igl.batched.Batch(meshes, queries, target_pairs=1 << 16, adjoint=adjoint)
     try:
+        assert b.info()["adjoint_fp64"] == (adjoint == "fp64")
         b.gW.copy_(torch.randn(b.gW.shape, dtype=torch.float64,
                                generator=torch.Generator().manual_seed(1)).cuda())
         b.forward()
         dV, dQ = b.backward()
         dVs, dQs, gs = b.split(dV.clone(), "v"), b.split(dQ.clone()), b.split(b.gW.clone())
+        dV2, dQ2 = b.backward()
+        assert torch.equal(dV2, dV) and torch.equal(dQ2, dQ)  # deterministic
         for (V, F), O, dv, dq, g in zip(meshes, queries, dVs, dQs, gs):
             Vt, Ft, Ot = (torch.from_numpy(x).cuda() for x in (V, F, O))
             ref_v, ref_q = wa.backward_edges(Vt, Ft, Ot, g)
             scale = max(float(ref_v.abs().max()), float(ref_q.abs().max()), 1e-30)
-            assert float((dv - ref_v).abs().max()) <= 1e-12 * scale
-            assert float((dq - ref_q).abs().max()) <= 1e-12 * scale
+            tol = 1e-12 if adjoint == "fp64" else 1e-4
+            assert float((dv - ref_v).abs().max()) <= tol * scale
+            assert float((dq - ref_q).abs().max()) <= tol * scale
+            if adjoint == "mixed":
+                mv, mq = wa.backward_edges(Vt, Ft, Ot, g, precision="mixed")
+                assert float((dv - mv).abs().max()) <= 1e-6 * scale
+                assert float((dq - mq).abs().max()) <= 1e-6 * scale
     finally:
         b.close()
 
@@ -159,13 +178,14 @@ def _large_batch(seed=71, n=16, max_q=100_000):
 
 def test_full_scale_batch_forward_backward_graph(gpu_required):
     """Configuration-5 scale: every query of every mesh against the plain FP64
-    kernel (<= 1e-6), the batched adjoint against the single-mesh boundary-edge
-    adjoint (<= 1e-12 relative), and a graph replay bit for bit equal to eager."""
+    kernel (<= 1e-6), the batched FP64 adjoint against the single-mesh FP64
+    boundary-edge adjoint (<= 1e-12 relative) and the mixed one against it within
+    1e-4, and graph replays bit for bit equal to eager (both precisions)."""
     import torch
 
     meshes, queries = _large_batch()
     assert max(len(F) for _, F in meshes) > 290_000
-    b = igl.batched.Batch(meshes, queries)
+    b = igl.batched.Batch(meshes, queries, adjoint="fp64")
     try:
         b.gW.normal_(generator=torch.Generator(device="cuda").manual_seed(72))
         b.step()
@@ -190,5 +210,22 @@ def test_full_scale_batch_forward_backward_graph(gpu_required):
         torch.cuda.synchronize()
         assert torch.equal(b.W, eager[0])
         assert torch.equal(b.dV, eager[1]) and torch.equal(b.dQ, eager[2])
+        # The mixed adjoint on the same batch: within 1e-4 of the FP64 one, and its
+        # graph replay bit for bit equal to its eager run.
+        b.graph = None
+        _check_rc(b.handle.wn_batch_set_adjoint_fp64(b.batch, 0))
+        b.step()
+        torch.cuda.synchronize()
+        mixed = (b.dV.clone(), b.dQ.clone())
+        for dv, dq, mv, mq in zip(dVs, dQs, b.split(mixed[0], "v"), b.split(mixed[1])):
+            scale = max(float(dv.abs().max()), float(dq.abs().max()), 1e-30)
+            assert float((mv - dv).abs().max()) <= 1e-4 * scale
+            assert float((mq - dq).abs().max()) <= 1e-4 * scale
+        b.capture()
+        b.dV.zero_()
+        b.dQ.zero_()
+        b.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(b.dV, mixed[0]) and torch.equal(b.dQ, mixed[1])
     finally:
         b.close()

@@ -629,6 +629,7 @@ def gpu_arm(args):
             err_b.append(float((wm[torch.from_numpy(sel).to(dev)] - ref_m).abs().max()))
         bt.capture(backward=True)
         t_g, launches_g, _ = timed(bt.replay, args.steps, 2)
+        info_b = bt.info()
         # The same graph with the FP64 adjoint, for comparison.
         bt.graph = None
         torch.cuda.synchronize()
@@ -641,7 +642,7 @@ def gpu_arm(args):
               "autotuned": tuned is not None,
               "autotune": ({k: v for k, v in tuned.items() if k != "config"} | {"seconds": t_tune}
                            if tuned else None),
-              "info": bt.info(),
+              "info": info_b,
               "fwd_ms": t_f * 1e3, "fwd_pairs_per_s": world * bt.pairs / t_f,
               "graph_fwdbwd_ms": t_g * 1e3, "graph_fwdbwd_pairs_per_s": world * bt.pairs / t_g,
               "ratio_fwdbwd_to_fwd": t_g / t_f,

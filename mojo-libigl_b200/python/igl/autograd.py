@@ -260,9 +260,10 @@ def backward_welded_edges(V, F, O, gW, welded=None, kappa: float = 4.0):
     sums each edge's unweighted endpoint terms once (dL/dO weighted by the net
     count m of its sides, so sides that cancel add nothing there), and every side
     a -> b takes them with its own sign: (da, db) = (dP, dQ) for sigma = +1 and
-    (-dQ, -dP) for sigma = -1. The per-vertex sums then run in a fixed order. A soup
-    that is a closed surface has every m = 0, so its dL/dO is exactly 0: the adjoint
-    is then called without dL/dO (a leaner kernel) and dL/dO returned as zeros.
+    (-dQ, -dP) for sigma = -1. The per-vertex sums then run in a fixed order. Edges
+    with m = 0 add exactly nothing to dL/dO, so they go through the adjoint without
+    dL/dO (a leaner kernel) and only the others (an open soup's boundary) through the
+    full one; a closed soup (every m = 0) gets dL/dO = 0 from one lean launch.
     """
     handle = _lib.lib()
     q = O.to(torch.float64).contiguous()
@@ -270,13 +271,28 @@ def backward_welded_edges(V, F, O, gW, welded=None, kappa: float = 4.0):
     nq, nv = q.shape[0], V.shape[0]
     edges, ng, side_edge, sigma, ends = welded if welded is not None else welded_edges(V, F)
     le = edges.shape[1]
-    closed = ng == 0 or not bool(edges[6, :ng].any())
-    dq = (torch.zeros if closed else torch.empty)((nq, 3), dtype=torch.float64, device=q.device)
+    dq = torch.zeros((nq, 3), dtype=torch.float64, device=q.device)
     dedge = torch.zeros((6, le), dtype=torch.float64, device=q.device)
-    _check(handle.wn_backward_edges_mixed_device(edges.data_ptr(), le, ng, q.data_ptr(), nq,
-                                                 gw.data_ptr(), kappa, 1,
-                                                 None if closed else dq.data_ptr(),
-                                                 dedge.data_ptr(), _stream()))
+    cancel = edges[6, :ng] == 0
+    n0 = int(cancel.sum()) if ng else 0
+
+    def run(sub, n, with_dq):
+        out = torch.zeros((6, max(sub.shape[1], 1)), dtype=torch.float64, device=q.device)
+        _check(handle.wn_backward_edges_mixed_device(sub.data_ptr(), sub.shape[1], n,
+                                                     q.data_ptr(), nq, gw.data_ptr(), kappa, 1,
+                                                     dq.data_ptr() if with_dq else None,
+                                                     out.data_ptr(), _stream()))
+        return out
+
+    if n0 in (0, ng):  # one kind of edge only: one launch
+        dedge = run(edges, ng, n0 == 0) if ng else dedge
+    else:
+        # Edges whose sides cancel (m = 0) contribute nothing to dL/dO: they take
+        # the kernel without it, the others (the soup's open boundary) the full one.
+        i0 = torch.nonzero(cancel).flatten()
+        i1 = torch.nonzero(~cancel).flatten()
+        dedge[:, i0] = run(edges[:, i0].contiguous(), n0, False)[:, :n0]
+        dedge[:, i1] = run(edges[:, i1].contiguous(), ng - n0, True)[:, :ng - n0]
     ns = ends.shape[0]
     dside = torch.zeros((6, max(ns, 1)), dtype=torch.float64, device=q.device)
     if ns:

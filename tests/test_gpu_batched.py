@@ -54,8 +54,8 @@ def test_batched_forward_matches_oracle(gpu_required, oracle_mod, qpt, kappa, ti
         b.close()
 
 
-@pytest.mark.parametrize("adjoint", ["fp64", "mixed"])
-def test_batched_backward_matches_single_mesh_adjoint(gpu_required, adjoint):
+@pytest.mark.parametrize("adjoint,kappa", [("fp64", 4.0), ("mixed", 4.0), ("mixed", 3.0)])
+def test_batched_backward_matches_single_mesh_adjoint(gpu_required, adjoint, kappa):
     """FP64: the single-mesh FP64 edge adjoint within 1e-12 (relative to the
     largest gradient). Mixed: the single-mesh mixed edge adjoint within 1e-6 (the
     same tiles and pairs; only the FP32 flush points and the FP64 partial order
@@ -63,7 +63,7 @@ def test_batched_backward_matches_single_mesh_adjoint(gpu_required, adjoint):
     import torch
 
     meshes, queries = _small_batch(seed=6)
-    b = igl.batched.Batch(meshes, queries, target_pairs=1 << 16, adjoint=adjoint)
+    b = igl.batched.Batch(meshes, queries, target_pairs=1 << 16, adjoint=adjoint, kappa=kappa)
     try:
         assert b.info()["adjoint_fp64"] == (adjoint == "fp64")
         b.gW.copy_(torch.randn(b.gW.shape, dtype=torch.float64,
@@ -81,7 +81,7 @@ def test_batched_backward_matches_single_mesh_adjoint(gpu_required, adjoint):
             assert float((dv - ref_v).abs().max()) <= tol * scale
             assert float((dq - ref_q).abs().max()) <= tol * scale
             if adjoint == "mixed":
-                mv, mq = wa.backward_edges(Vt, Ft, Ot, g, precision="mixed")
+                mv, mq = wa.backward_edges(Vt, Ft, Ot, g, precision="mixed", kappa=kappa)
                 assert float((dv - mv).abs().max()) <= 1e-6 * scale
                 assert float((dq - mq).abs().max()) <= 1e-6 * scale
     finally:

@@ -276,23 +276,35 @@ def backward_welded_edges(V, F, O, gW, welded=None, kappa: float = 4.0):
     cancel = edges[6, :ng] == 0
     n0 = int(cancel.sum()) if ng else 0
 
-    def run(sub, n, with_dq):
+    def run(sub, n, with_dq, stream):
         out = torch.zeros((6, max(sub.shape[1], 1)), dtype=torch.float64, device=q.device)
         _check(handle.wn_backward_edges_mixed_device(sub.data_ptr(), sub.shape[1], n,
                                                      q.data_ptr(), nq, gw.data_ptr(), kappa, 1,
                                                      dq.data_ptr() if with_dq else None,
-                                                     out.data_ptr(), _stream()))
+                                                     out.data_ptr(), stream))
         return out
 
     if n0 in (0, ng):  # one kind of edge only: one launch
-        dedge = run(edges, ng, n0 == 0) if ng else dedge
+        dedge = run(edges, ng, n0 == 0, _stream()) if ng else dedge
     else:
         # Edges whose sides cancel (m = 0) contribute nothing to dL/dO: they take
-        # the kernel without it, the others (the soup's open boundary) the full one.
+        # the kernel without it, the others (the soup's open boundary) the full one,
+        # on a second stream so that the two launches overlap (separate outputs).
         i0 = torch.nonzero(cancel).flatten()
         i1 = torch.nonzero(~cancel).flatten()
-        dedge[:, i0] = run(edges[:, i0].contiguous(), n0, False)[:, :n0]
-        dedge[:, i1] = run(edges[:, i1].contiguous(), ng - n0, True)[:, :ng - n0]
+        e0, e1 = edges[:, i0].contiguous(), edges[:, i1].contiguous()
+        main = torch.cuda.current_stream(q.device)
+        side = torch.cuda.Stream(q.device)
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            d1 = run(e1, ng - n0, True, ctypes.c_void_p(side.cuda_stream))
+        d0 = run(e0, n0, False, _stream())
+        main.wait_stream(side)
+        for t in (e1, dq, q, gw):  # made on the main stream, used on the side one
+            t.record_stream(side)
+        d1.record_stream(main)  # made on the side stream, read below on the main one
+        dedge[:, i0] = d0[:, :n0]
+        dedge[:, i1] = d1[:, :ng - n0]
     ns = ends.shape[0]
     dside = torch.zeros((6, max(ns, 1)), dtype=torch.float64, device=q.device)
     if ns:

@@ -1860,8 +1860,8 @@ __global__ void batch_finish_dedge_kernel(const double* __restrict__ dE_part,
   dedge[r * le + e] = s * kInv4Pi;
 }
 
-constexpr int64_t kBatchMixedBlocks = 16;     // 4-tile blocks per range (4,096 edges)
-constexpr int64_t kBatchMixedQueries = 4096;  // sorted queries per group
+constexpr int64_t kBatchMixedBlocks = 16;     // largest item: 4-tile blocks per range
+constexpr int64_t kBatchMixedQueries = 4096;  // (4,096 edges) and sorted queries per group
 static_assert(kBatchMixedQueries % kFaFlushQueries == 0, "groups hold whole FP32 flushes");
 
 struct BatchMixedArgs {
@@ -2055,6 +2055,23 @@ cudaError_t batch_edges_create(BatchState* b, const int64_t* F) {
   std::vector<int32_t> tile_count, tile_mesh;
   std::vector<BatchMixedItem> mitems;
   {
+    // Item size: the largest that still gives at least 8 items per SM (halving the
+    // longer side, edges or queries, down to one block or one FP32 flush of queries).
+    int64_t br = kBatchMixedBlocks, qg = kBatchMixedQueries;
+    auto items_for = [&](int64_t r, int64_t g) {
+      int64_t n = 0;
+      for (int64_t m = 0; m < b->nmesh; ++m)
+        if (meshes[m].ne > 0 && meshes[m].nq > 0)
+          n += cdiv(cdiv(cdiv(meshes[m].ne, kTileFaces), kFaTiles), r) * cdiv(meshes[m].nq, g);
+      return n;
+    };
+    const int64_t want = 8 * std::max(1, b->sms);
+    while (items_for(br, qg) < want && (br > 1 || qg > kFaFlushQueries)) {
+      if (qg > kFaFlushQueries && (qg >= br * kFaTiles * kTileFaces || br == 1))
+        qg /= 2;
+      else
+        br /= 2;
+    }
     int64_t mdo = 0, mde = 0, toff = 0;
     for (int64_t m = 0; m < b->nmesh; ++m) {
       const BatchEdgeMesh& em = meshes[m];
@@ -2072,8 +2089,8 @@ cudaError_t batch_edges_create(BatchState* b, const int64_t* F) {
       toff += mm.ntile;
       const bool work = em.ne > 0 && em.nq > 0;
       const int64_t nblocks = cdiv(mm.ntile, kFaTiles), ld = mm.ntile * kTileFaces;
-      mm.nranges = work ? cdiv(nblocks, kBatchMixedBlocks) : 0;
-      mm.ngroups = work ? cdiv(em.nq, kBatchMixedQueries) : 0;
+      mm.nranges = work ? cdiv(nblocks, br) : 0;
+      mm.ngroups = work ? cdiv(em.nq, qg) : 0;
       mm.do_off = mdo;
       mm.de_off = mde;
       for (int64_t r = 0; r < mm.nranges; ++r)
@@ -2082,10 +2099,10 @@ cudaError_t batch_edges_create(BatchState* b, const int64_t* F) {
           it.tile_off = mm.tile_off;
           it.ntiles = mm.ntile;
           it.q_off = mm.q_off;
-          it.b_begin = r * kBatchMixedBlocks;
-          it.b_end = std::min(nblocks, it.b_begin + kBatchMixedBlocks);
-          it.q_begin = g * kBatchMixedQueries;
-          it.q_end = std::min(em.nq, it.q_begin + kBatchMixedQueries);
+          it.b_begin = r * br;
+          it.b_end = std::min(nblocks, it.b_begin + br);
+          it.q_begin = g * qg;
+          it.q_end = std::min(em.nq, it.q_begin + qg);
           it.do_row = mdo + r * em.nq * 3;
           it.de_base = mde + g * 6 * ld;
           it.de_ld = ld;

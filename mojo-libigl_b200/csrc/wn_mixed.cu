@@ -535,47 +535,71 @@ __device__ __forceinline__ void careful_range(const float4* fr, int j0, int j1, 
 // fast path packs two FACES of a tile against one query: the query's
 // coordinates are the duplicated operand (set once per tile) and a face-pair
 // transposed copy of the tile records supplies both faces' fields in adjacent
-// registers. Every per-face operation is the scalar path's, rounded the same
-// way per lane; each lane keeps its own running product (even faces, odd
+// registers. The four query-dependent products are expanded about per-face
+// constants formed once per tile (in FP64 from the FP32 record, rounded once):
+// a.e1 = A.e1 - o.e1, a.e2, a.n likewise and |a|^2 = (|A|^2 + |o|^2) - 2A.o, 13
+// packed operations instead of 15 for a = A - o and its four products. On this
+// path every query is outside the tile's ball B(c, r + kappa h) while |A| <= r,
+// so |A| + |o| <= 3 |a| at worst and the expansion loses at most a few ulps more
+// than forming a first. The rest is the scalar path's arithmetic, rounded the
+// same way per lane; each lane keeps its own running product (even faces, odd
 // faces), both started at 2^-50, and the two are multiplied once per range.
 // Each holds at most 32 factors of modulus in [3.8, 4.01], so both stay inside
 // [2^-50, 2^14.1] and their product inside [2^-100, 2^28.1], as the scalar
 // product does; the sum of the range's angles is the same (< pi in magnitude).
 constexpr float kZ0Half = 8.8817841970012523e-16f;  // 2^-50
-constexpr int kPairFloats = 32;                     // one face pair, 16 fields x 2 lanes
+constexpr int kPairFields = 20;                     // per face: see transpose_tile
+constexpr int kPairFloats = 2 * kPairFields;        // one face pair, both lanes
 constexpr int kTileTransposedBytes = (kTileFaces / 2) * kPairFloats * 4;
 
-// tbuf[32 p + 2 f + lane] = field f of face 2 p + lane, for the tile at `rec`.
+// tbuf[40 p + 2 f + lane] = field f of face 2 p + lane, for the tile at `rec`: 2A
+// (0-2), e1 (3-5), e2 (6-8), n (9-11), |e1|^2, |e2|^2, e1.e2 (12-14), |A|^2, A.e1,
+// A.e2, A.n (15-18), 0 (19). One thread per face.
 __device__ __forceinline__ void transpose_tile(const unsigned char* rec, float* tbuf, int tid,
                                                int threads) {
-  const float* src = reinterpret_cast<const float*>(rec + kTileHeaderBytes);
-  for (int i = tid; i < kTileFaces * 16; i += threads) {
-    const int j = i >> 4, f = i & 15;
-    tbuf[kPairFloats * (j >> 1) + 2 * f + (j & 1)] = src[i];
+  const FaceRec* src = reinterpret_cast<const FaceRec*>(rec + kTileHeaderBytes);
+  for (int j = tid; j < kTileFaces; j += threads) {
+    const FaceRec r = src[j];
+    const double ax = r.ax, ay = r.ay, az = r.az;
+    const float f[kPairFields] = {
+        2.f * r.ax, 2.f * r.ay, 2.f * r.az, r.e1x, r.e1y, r.e1z, r.e2x, r.e2y, r.e2z, r.nx,
+        r.ny, r.nz, r.e11, r.e22, r.e12,
+        static_cast<float>(ax * ax + ay * ay + az * az),
+        static_cast<float>(ax * r.e1x + ay * r.e1y + az * r.e1z),
+        static_cast<float>(ax * r.e2x + ay * r.e2y + az * r.e2z),
+        static_cast<float>(ax * r.nx + ay * r.ny + az * r.nz), 0.f};
+    float* dst = tbuf + kPairFloats * (j >> 1) + (j & 1);
+#pragma unroll
+    for (int k = 0; k < kPairFields; ++k) dst[2 * k] = f[k];
   }
 }
 
 // pair_sq + pair_mul for two faces (lanes) against one query, (nlx, nly, nlz)
-// = minus the query's tile-local coordinates in both lanes.
+// = minus the query's tile-local coordinates and oo = their squared norm, in both
+// lanes; v = the face pair's fields as laid out by transpose_tile.
 __device__ __forceinline__ void pair2_mul(const float4* v, float2 nlx, float2 nly, float2 nlz,
-                                          float2& zr, float2& zi) {
-  const float4 v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3];
-  const float4 v4 = v[4], v5 = v[5], v6 = v[6];
-  const float2 e12 = make_float2(v[7].x, v[7].y);
+                                          float2 oo, float2& zr, float2& zi) {
+  const float4 v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3], v4 = v[4];
+  const float4 v5 = v[5], v6 = v[6], v7 = v[7], v8 = v[8], v9 = v[9];
+  const float2 e12 = make_float2(v7.x, v7.y);
   const float2 one = make_float2(1.f, 1.f), two = make_float2(2.f, 2.f);
-  const float2 ax = __fadd2_rn(make_float2(v0.x, v0.y), nlx);
-  const float2 ay = __fadd2_rn(make_float2(v0.z, v0.w), nly);
-  const float2 az = __fadd2_rn(make_float2(v1.x, v1.y), nlz);
-  const float2 aa = __ffma2_rn(ax, ax, __ffma2_rn(ay, ay, __fmul2_rn(az, az)));
-  const float2 s1 = __ffma2_rn(ax, make_float2(v1.z, v1.w),
-                               __ffma2_rn(ay, make_float2(v2.x, v2.y),
-                                          __fmul2_rn(az, make_float2(v2.z, v2.w))));
-  const float2 s2 = __ffma2_rn(ax, make_float2(v3.x, v3.y),
-                               __ffma2_rn(ay, make_float2(v3.z, v3.w),
-                                          __fmul2_rn(az, make_float2(v4.x, v4.y))));
-  const float2 det = __ffma2_rn(ax, make_float2(v4.z, v4.w),
-                                __ffma2_rn(ay, make_float2(v5.x, v5.y),
-                                           __fmul2_rn(az, make_float2(v5.z, v5.w))));
+  const float2 aa =
+      __ffma2_rn(nlx, make_float2(v0.x, v0.y),
+                 __ffma2_rn(nly, make_float2(v0.z, v0.w),
+                            __ffma2_rn(nlz, make_float2(v1.x, v1.y),
+                                       __fadd2_rn(make_float2(v7.z, v7.w), oo))));
+  const float2 s1 = __ffma2_rn(nlx, make_float2(v1.z, v1.w),
+                               __ffma2_rn(nly, make_float2(v2.x, v2.y),
+                                          __ffma2_rn(nlz, make_float2(v2.z, v2.w),
+                                                     make_float2(v8.x, v8.y))));
+  const float2 s2 = __ffma2_rn(nlx, make_float2(v3.x, v3.y),
+                               __ffma2_rn(nly, make_float2(v3.z, v3.w),
+                                          __ffma2_rn(nlz, make_float2(v4.x, v4.y),
+                                                     make_float2(v8.z, v8.w))));
+  const float2 det = __ffma2_rn(nlx, make_float2(v4.z, v4.w),
+                                __ffma2_rn(nly, make_float2(v5.x, v5.y),
+                                           __ffma2_rn(nlz, make_float2(v5.z, v5.w),
+                                                      make_float2(v9.x, v9.y))));
   const float2 ab = __fadd2_rn(aa, s1), ca = __fadd2_rn(aa, s2);
   const float2 bb = __ffma2_rn(two, s1, __fadd2_rn(aa, make_float2(v6.x, v6.y)));
   const float2 cc = __ffma2_rn(two, s2, __fadd2_rn(aa, make_float2(v6.z, v6.w)));
@@ -600,7 +624,7 @@ __device__ __forceinline__ void packed_range(const float4* fr, const float* tbuf
                                              const float (&lx)[QPT], const float (&ly)[QPT],
                                              const float (&lz)[QPT], float (&hi)[QPT],
                                              float (&lo)[QPT]) {
-  float2 zr2[QPT], zi2[QPT], nlx[QPT], nly[QPT], nlz[QPT];
+  float2 zr2[QPT], zi2[QPT], nlx[QPT], nly[QPT], nlz[QPT], oo[QPT];
 #pragma unroll
   for (int k = 0; k < QPT; ++k) {
     zr2[k] = make_float2(kZ0Half, kZ0Half);
@@ -608,13 +632,17 @@ __device__ __forceinline__ void packed_range(const float4* fr, const float* tbuf
     nlx[k] = make_float2(-lx[k], -lx[k]);
     nly[k] = make_float2(-ly[k], -ly[k]);
     nlz[k] = make_float2(-lz[k], -lz[k]);
+    const float o2 = fmaf(lx[k], lx[k], fmaf(ly[k], ly[k], lz[k] * lz[k]));
+    oo[k] = make_float2(o2, o2);
   }
   const int p1 = j1 >> 1;
-#pragma unroll 2
+  // Four face pairs per pass: with the shorter products this is what shows in time
+  // (either change alone measured no faster, the deeper unroll alone slower).
+#pragma unroll 4
   for (int p = j0 >> 1; p < p1; ++p) {
     const float4* v = reinterpret_cast<const float4*>(tbuf + kPairFloats * p);
 #pragma unroll
-    for (int k = 0; k < QPT; ++k) pair2_mul(v, nlx[k], nly[k], nlz[k], zr2[k], zi2[k]);
+    for (int k = 0; k < QPT; ++k) pair2_mul(v, nlx[k], nly[k], nlz[k], oo[k], zr2[k], zi2[k]);
   }
 #pragma unroll
   for (int k = 0; k < QPT; ++k) {

@@ -726,8 +726,11 @@ __device__ __forceinline__ void mixed_tile_pairs(const unsigned char* rec, const
   }
 }
 
+// Five CTAs per SM (at most 102 registers; it takes 94-96 without spills): the
+// extra warps hide more of the MUFU and packed-FMA latency than the four CTAs at
+// 122 registers did (c3 x 2^20: 430.2 -> 413.2 ms, the same results to the bit).
 template <int THREADS, int QPT, int STAGES, bool HALF>
-__global__ void __launch_bounds__(THREADS, 4) mixed_forward_kernel(const MixedArgs a) {
+__global__ void __launch_bounds__(THREADS, 5) mixed_forward_kernel(const MixedArgs a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* ring = smem_raw;  // [STAGES][kTileBytes]
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + STAGES * kTileBytes);

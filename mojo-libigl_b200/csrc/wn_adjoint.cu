@@ -1310,10 +1310,31 @@ __device__ __forceinline__ void edge_adjoint_cta(const EdgeWork& a,
       if constexpr (UNIT) {
         if (no_dq) {
           float2 d[3];
-          // Two queries per pass (in increasing order, as one at a time would add
-          // them): the second's arithmetic overlaps the first's latencies.
+          // Four, then two queries per pass (in increasing order, as one at a time
+          // would add them): the later ones' arithmetic overlaps the first's latencies.
+          unsigned rest = far_q;
 #pragma unroll 1
-          for (unsigned m = far_q; m;) {
+          for (unsigned m = rest; __popc(m) >= 4;) {
+            const int j0 = jq_of(m);
+            m &= m - 1u;
+            const int j1 = jq_of(m);
+            m &= m - 1u;
+            const int j2 = jq_of(m);
+            m &= m - 1u;
+            const int j3 = jq_of(m);
+            m &= m - 1u;
+            rest = m;
+            edge_pair_terms<false, true, false>(sm.frame[j0][warp], fp, fe, fne, fee, fm, k2ee,
+                                                true, true, acc, d);
+            edge_pair_terms<false, true, false>(sm.frame[j1][warp], fp, fe, fne, fee, fm, k2ee,
+                                                true, true, acc, d);
+            edge_pair_terms<false, true, false>(sm.frame[j2][warp], fp, fe, fne, fee, fm, k2ee,
+                                                true, true, acc, d);
+            edge_pair_terms<false, true, false>(sm.frame[j3][warp], fp, fe, fne, fee, fm, k2ee,
+                                                true, true, acc, d);
+          }
+#pragma unroll 1
+          for (unsigned m = rest; m;) {
             const int j0 = jq_of(m);
             m &= m - 1u;
             if (m) {

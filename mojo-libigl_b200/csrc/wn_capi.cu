@@ -1319,7 +1319,7 @@ int normals_prepare(const int64_t* F, int64_t nf, cudaStream_t st, NormalsHandle
 // Grows the per-face contribution buffer for `mode` (uniform/area: 3 doubles
 // per face, angle: 9).
 int normals_contrib(NormalsHandle* h, int mode) {
-  const int64_t need = (mode == 2 ? 9 : 3) * h->t.nf;
+  const int64_t need = normals_contrib_doubles(h->t.nf, mode);
   if (need <= h->t.contrib_doubles) return WN_OK;
   cudaFree(h->t.contrib);
   h->t.contrib = nullptr;
@@ -1397,7 +1397,7 @@ int wn_vertex_normals_host(const double* V, int64_t nv, const int64_t* F, int64_
   // The context's grow-only buffers hold the topology: no allocation per call
   // once they are large enough.
   const int mode = weighting == 3 ? 1 : weighting;
-  const int64_t ncontrib = (mode == 2 ? 9 : 3) * nf;
+  const int64_t ncontrib = normals_contrib_doubles(nf, mode);
   cudaError_t e;
   if ((e = c->nrm_f.ensure(sizeof(int32_t) * (3 * nf + 1))) != cudaSuccess ||
       (e = c->nrm_indptr.ensure(sizeof(int32_t) * (nv + 1))) != cudaSuccess ||

@@ -89,3 +89,34 @@ def test_out_of_range_faces_rejected_on_the_device(gpu_required):
     assert lib.wn_normals_create(bad.ctypes.data, len(bad), len(V), None, ctypes.byref(handle)) == 1
     # The library keeps working afterwards.
     assert igl.per_vertex_normals(V, F, device="gpu").tobytes() == igl.per_vertex_normals(V, F).tobytes()
+
+
+def test_unaligned_positions_and_long_incidence_lists(gpu_required):
+    """Positions that start 8 bytes past a 16-byte boundary (a tensor view), and a
+    vertex on 300 faces (its list spans several of the gather's chunks, and the
+    lists of the vertices around it start and end inside them)."""
+    import torch
+
+    from igl import normals
+
+    V, F = igl.synthetic.bumpy_icosphere(4, seed=8)
+    nv0 = len(V)
+    ring = 300
+    t = np.linspace(0.0, 2.0 * np.pi, ring, endpoint=False)
+    fan_v = np.concatenate([[[0.0, 0.0, 3.0]],
+                            np.stack([np.cos(t), np.sin(t), 3.0 + 0.1 * np.sin(3 * t)], 1)])
+    fan_f = np.stack([np.zeros(ring, np.int64), 1 + np.arange(ring),
+                      1 + (np.arange(ring) + 1) % ring], 1) + nv0
+    V = np.concatenate([V, fan_v])
+    F = np.concatenate([F[: len(F) // 2], fan_f, F[len(F) // 2:]])
+    nv = len(V)
+    buf = torch.zeros(3 * nv + 1, dtype=torch.float64, device="cuda")
+    view = buf[1:].view(nv, 3)
+    view.copy_(torch.from_numpy(V))
+    assert view.data_ptr() % 16 == 8
+    dn = normals.DeviceNormals(F, nv)
+    for weighting in (0, 1, 2):
+        got = dn.evaluate(view, weighting)
+        torch.cuda.synchronize()
+        assert _same(got.cpu().numpy(), igl.per_vertex_normals(V, F, weighting), weighting)
+    dn.close()

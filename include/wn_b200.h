@@ -333,10 +333,11 @@ int wn_signed_distance_device(void* tree, void* mesh, int precision, const doubl
  * The reference computes them only on the CPU (src/capi.mojo:146-202). Here the
  * topology F (nf x 3 int64, indices in [0, nv)) is prepared once per mesh (a
  * vertex -> (face, corner) list in face order, built on the device) and
- * wn_vertex_normals_device then evaluates N (nv x 3) from V (nv x 3) in one
- * launch, one thread per vertex, summing in the reference's order: uniform and
- * area normals bit-identical to mli_vertex_normals, angle normals through
- * CUDA's acos (within 1e-14). */
+ * wn_vertex_normals_device then evaluates N (nv x 3) from V (nv x 3, device
+ * doubles, any 8-byte-aligned address) in two launches (one thread per face
+ * writes its contribution, one thread per vertex adds its list), summing in the
+ * reference's order: uniform and area normals bit-identical to
+ * mli_vertex_normals, angle normals through CUDA's acos (within 1e-14). */
 int wn_normals_create(const int64_t* F, int64_t nf, int64_t nv, void* stream, void** handle);
 int wn_normals_destroy(void* handle);
 int wn_vertex_normals_device(void* handle, const double* V, int weighting, double* N,

@@ -2,8 +2,9 @@
 
 ``DeviceNormals(F, nv)`` prepares the topology once (the vertex -> (face,
 corner) lists, built on the device); ``evaluate(V, weighting)`` then computes
-the (nv, 3) normals of any vertex positions in one launch on the current
-stream, summing each vertex in the reference's order (src/capi.mojo:146-202).
+the (nv, 3) normals of any vertex positions in two launches on the current
+stream (the faces' contributions, then each vertex's sum), summing each vertex
+in the reference's order (src/capi.mojo:146-202).
 """
 
 from __future__ import annotations

@@ -11,6 +11,9 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
 
 #include "wn_pair.cuh"
 
@@ -257,6 +260,132 @@ WN_AVX512 void winding_query8(const double* tri, int64_t nf, const double* q, do
                        wn::kTwoPi;
 }
 
+// ---- corners shared between faces (AVX-512) ---------------------------------
+// A corner's a = v - o and |a| depend only on the vertex position and the
+// query, and a mesh gives most positions to several faces (about six in a
+// closed triangle mesh), while the soup repeats each position per face. The
+// faces are cut into chunks of consecutive faces; each chunk lists its distinct
+// corner positions (bitwise-equal coordinates) once, and for every block of
+// eight queries the chunk's lengths |a| are computed once per distinct position
+// and read by every face that uses it. They are the same square roots of the
+// same sums, so every bit of the result is unchanged, with a fraction of the
+// square roots (the slowest vector instruction of the pair). A mesh of up to
+// kWholeMeshFaces faces with at most kWholeMeshPositions positions is one chunk
+// (its lengths, 64 bytes per position, stay in L2); a larger one is cut into
+// chunks of kChunkFaces, which shares positions only where the face order
+// keeps neighbours together (a height field's rows, not every mesh).
+
+constexpr int64_t kChunkFaces = 2048;
+constexpr int64_t kWholeMeshFaces = 1 << 16;
+constexpr int64_t kWholeMeshPositions = 1 << 14;
+
+struct CornerChunks {
+  int64_t chunk_faces = 0;
+  std::vector<int64_t> start;  // first distinct position of each chunk (nchunks + 1)
+  std::vector<double> pos;     // distinct positions, 3 doubles each, chunk by chunk
+  std::vector<uint32_t> id;    // corner 3 * f + k -> its position's index within the chunk
+  int64_t max_positions = 0;   // the most distinct positions in one chunk
+};
+
+inline uint64_t word(double x) {
+  uint64_t u;
+  std::memcpy(&u, &x, 8);
+  return u;
+}
+
+// Chunk lists of the soup's corner positions, chunks of chunk_faces faces (an
+// open-addressing table at most half full, reset per chunk by a stamp).
+CornerChunks build_corner_chunks(const double* tri, int64_t nf, int64_t chunk_faces) {
+  CornerChunks cc;
+  cc.chunk_faces = chunk_faces;
+  const int64_t nchunks = (nf + chunk_faces - 1) / chunk_faces;
+  uint32_t slots = 64;
+  while (slots < 6 * chunk_faces) slots *= 2;
+  cc.start.resize(nchunks + 1);
+  cc.id.resize(3 * nf);
+  cc.pos.reserve(3 * static_cast<size_t>(nf));
+  std::vector<uint32_t> stamp(slots, 0), slot_id(slots);
+  int64_t npos = 0;
+  for (int64_t c = 0; c < nchunks; ++c) {
+    const uint32_t gen = static_cast<uint32_t>(c) + 1;
+    cc.start[c] = npos;
+    const int64_t f1 = (c + 1) * chunk_faces < nf ? (c + 1) * chunk_faces : nf;
+    for (int64_t f = c * chunk_faces; f < f1; ++f)
+      for (int k = 0; k < 3; ++k) {
+        const double x = tri[3 * k * nf + f], y = tri[(3 * k + 1) * nf + f],
+                     z = tri[(3 * k + 2) * nf + f];
+        const uint64_t bx = word(x), by = word(y), bz = word(z);
+        uint64_t h = bx * 0x9E3779B97F4A7C15ULL ^ by * 0xC2B2AE3D27D4EB4FULL ^
+                     bz * 0x165667B19E3779F9ULL;
+        h ^= h >> 29;
+        for (uint32_t slot = static_cast<uint32_t>(h) & (slots - 1);;
+             slot = (slot + 1) & (slots - 1)) {
+          if (stamp[slot] != gen) {  // a new position of this chunk
+            stamp[slot] = gen;
+            slot_id[slot] = static_cast<uint32_t>(npos - cc.start[c]);
+            cc.pos.push_back(x);
+            cc.pos.push_back(y);
+            cc.pos.push_back(z);
+            cc.id[3 * f + k] = slot_id[slot];
+            ++npos;
+            break;
+          }
+          const double* p = &cc.pos[3 * (cc.start[c] + slot_id[slot])];
+          if (word(p[0]) == bx && word(p[1]) == by && word(p[2]) == bz) {
+            cc.id[3 * f + k] = slot_id[slot];
+            break;
+          }
+        }
+      }
+    if (npos - cc.start[c] > cc.max_positions) cc.max_positions = npos - cc.start[c];
+  }
+  cc.start[nchunks] = npos;
+  return cc;
+}
+
+// winding_query8 with each chunk's corner lengths computed once per distinct
+// position into len (8 doubles per position, 64-byte aligned, cc.max_positions
+// of them) and read back by the faces.
+WN_AVX512 void winding_query8_shared(const double* tri, int64_t nf, const CornerChunks& cc,
+                                     double* len, const double* q, double* out) {
+  const __m512i idx = _mm512_set_epi64(21, 18, 15, 12, 9, 6, 3, 0);
+  const __m512d ox = _mm512_i64gather_pd(idx, q, 8);
+  const __m512d oy = _mm512_i64gather_pd(idx, q + 1, 8);
+  const __m512d oz = _mm512_i64gather_pd(idx, q + 2, 8);
+  Acc8 acc{_mm512_set1_pd(1.0), _mm512_setzero_pd(), _mm512_setzero_si512(), 0};
+  const int64_t nchunks = static_cast<int64_t>(cc.start.size()) - 1;
+  for (int64_t c = 0; c < nchunks; ++c) {
+    const double* p = &cc.pos[3 * cc.start[c]];
+    const int64_t np = cc.start[c + 1] - cc.start[c];
+    for (int64_t u = 0; u < np; ++u)
+      _mm512_store_pd(len + 8 * u, corner8(ox, oy, oz, p[3 * u], p[3 * u + 1], p[3 * u + 2]).l);
+    const int64_t cf = cc.chunk_faces;
+    const int64_t f1 = (c + 1) * cf < nf ? (c + 1) * cf : nf;
+    for (int64_t f = c * cf; f < f1; ++f) {
+      Corner8 v[3];
+      for (int k = 0; k < 3; ++k) {
+        v[k].x = _mm512_sub_pd(_mm512_set1_pd(tri[3 * k * nf + f]), ox);
+        v[k].y = _mm512_sub_pd(_mm512_set1_pd(tri[(3 * k + 1) * nf + f]), oy);
+        v[k].z = _mm512_sub_pd(_mm512_set1_pd(tri[(3 * k + 2) * nf + f]), oz);
+        v[k].l = _mm512_load_pd(len + 8 * static_cast<int64_t>(cc.id[3 * f + k]));
+      }
+      __m512d det, denom;
+      face8(v[0], v[1], v[2], det, denom);
+      push8(acc, denom, det);
+    }
+  }
+  alignas(64) double zr[8], zi[8];
+  alignas(64) int64_t k[8];
+  _mm512_store_pd(zr, acc.zr);
+  _mm512_store_pd(zi, acc.zi);
+  _mm512_store_si512(k, acc.k);
+  for (int j = 0; j < 8; ++j)
+    out[j] = ((acc.bad >> j) & 1)
+                 ? winding_query(tri, nf, q[3 * j], q[3 * j + 1], q[3 * j + 2])
+                 : (std::atan2(zi[j], zr[j]) + static_cast<double>(k[j]) * wn::kTwoPi) /
+                       wn::kTwoPi;
+}
+
 #undef WN_AVX512
 
 bool has_avx512() {
@@ -277,8 +406,25 @@ void mli_winding(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t nq, in
   const double* qq = reinterpret_cast<const double*>(q);
   double* d = reinterpret_cast<double*>(dst);
   int64_t qi = q0;
-  if (has_avx512())
+  if (has_avx512() && q1 - q0 >= 8 && nf > 0) {
+    // Shared corners pay when the chunks hold at most half as many distinct
+    // positions as corners (measured: at 0.67 per corner with lengths beyond L1
+    // they cost more than they save).
+    CornerChunks cc = build_corner_chunks(t, nf, kChunkFaces);
+    bool shared = 2 * cc.start.back() < 3 * nf;
+    if (!shared && nf <= kWholeMeshFaces) {
+      cc = build_corner_chunks(t, nf, nf);
+      shared = cc.max_positions <= kWholeMeshPositions && 2 * cc.start.back() < 3 * nf;
+    }
+    double* len = shared ? static_cast<double*>(std::aligned_alloc(
+                               64, 64 * static_cast<size_t>(cc.max_positions + 1)))
+                         : nullptr;
+    if (len) {
+      for (; qi + 8 <= q1; qi += 8) winding_query8_shared(t, nf, cc, len, qq + 3 * qi, d + qi);
+      std::free(len);
+    }
     for (; qi + 8 <= q1; qi += 8) winding_query8(t, nf, qq + 3 * qi, d + qi);
+  }
   for (; qi + 4 <= q1; qi += 4) winding_query4(t, nf, qq + 3 * qi, d + qi);
   for (; qi < q1; ++qi) d[qi] = winding_query(t, nf, qq[3 * qi], qq[3 * qi + 1], qq[3 * qi + 2]);
 }

@@ -245,3 +245,38 @@ def test_welded_edges_of_a_soup_without_a_gpu():
         synthetic.delete_faces(F, 0.1, seed=4)))
     assert int((e_open[6, :ng_open] != 0).sum()) == nb
     assert float(e_open[6, :ng_open].abs().max()) == 1.0
+
+
+def test_shared_corner_lengths_equal_the_scalar_path():
+    """With eight or more queries and a mesh whose faces share corner positions,
+    mli_winding computes each distinct position's |v - o| once per block of
+    queries, per chunk of 2,048 faces or for a whole small mesh. The results
+    must stay the scalar routine's bits: a grid cut into two chunks, a mesh above
+    the whole-mesh size, a soup whose faces share no position (plain path), and
+    no faces at all."""
+    handle = _lib.lib()
+    rng = np.random.default_rng(12)
+    Vg, Fg = igl.synthetic.terrain_grid(40)  # 3,042 faces: two chunks
+    Vb, Fb = igl.synthetic.bumpy_icosphere(6, seed=2)  # 81,920 faces
+    Vs, Fs = igl.synthetic.bumpy_icosphere(2, seed=5)
+    soup = Vs[Fs] + rng.normal(0.0, 1e-9, size=(len(Fs), 3, 3))  # no shared positions
+    cases = [(igl._triangle_soa(*igl._mesh(Vg, Fg)), Vg),
+             (igl._triangle_soa(*igl._mesh(Vb, Fb)), Vb),
+             (np.ascontiguousarray(soup.transpose(1, 2, 0).reshape(9, -1)), Vs)]
+    for tri, V in cases:
+        lo, hi = V.min(0), V.max(0)
+        O = np.ascontiguousarray(np.concatenate(
+            [V[:5], rng.uniform(lo, hi, size=(12, 3))]))  # 17: 8 + 8 + 1, on-vertex queries
+        whole = np.empty(len(O))
+        handle.mli_winding(tri.ctypes.data, O.ctypes.data, whole.ctypes.data, tri.shape[1],
+                           len(O), 0, len(O))
+        single = np.empty(len(O))
+        for i in range(len(O)):
+            handle.mli_winding(tri.ctypes.data, O.ctypes.data, single.ctypes.data,
+                               tri.shape[1], len(O), i, i + 1)
+        assert np.array_equal(whole, single, equal_nan=True)
+    empty = np.zeros((9, 0))
+    O = rng.uniform(-1.0, 1.0, size=(9, 3))
+    out = np.full(9, 7.0)
+    handle.mli_winding(empty.ctypes.data, O.ctypes.data, out.ctypes.data, 0, 9, 0, 9)
+    assert np.array_equal(out, np.zeros(9))

@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <new>
 #include <vector>
 
 #include "wn_pair.cuh"
@@ -264,27 +265,39 @@ WN_AVX512 void winding_query8(const double* tri, int64_t nf, const double* q, do
 // A corner's a = v - o and |a| depend only on the vertex position and the
 // query, and a mesh gives most positions to several faces (about six in a
 // closed triangle mesh), while the soup repeats each position per face. The
-// faces are cut into chunks of consecutive faces; each chunk lists its distinct
+// faces are taken in chunks of consecutive faces; each chunk lists its distinct
 // corner positions (bitwise-equal coordinates) once, and for every block of
 // eight queries the chunk's lengths |a| are computed once per distinct position
-// and read by every face that uses it. They are the same square roots of the
-// same sums, so every bit of the result is unchanged, with a fraction of the
+// and read back by every face that uses it. They are the same square roots of
+// the same sums, and each query still multiplies its faces' factors in face
+// order, so every bit of the result is unchanged, with a fraction of the
 // square roots (the slowest vector instruction of the pair). A mesh of up to
 // kWholeMeshFaces faces with at most kWholeMeshPositions positions is one chunk
 // (its lengths, 64 bytes per position, stay in L2); a larger one is cut into
-// chunks of kChunkFaces, which shares positions only where the face order
-// keeps neighbours together (a height field's rows, not every mesh).
+// chunks of kChunkFaces, which shares positions where the face order keeps
+// neighbours together (a height field's rows, not every mesh).
 
 constexpr int64_t kChunkFaces = 2048;
 constexpr int64_t kWholeMeshFaces = 1 << 16;
 constexpr int64_t kWholeMeshPositions = 1 << 14;
 
-struct CornerChunks {
-  int64_t chunk_faces = 0;
-  std::vector<int64_t> start;  // first distinct position of each chunk (nchunks + 1)
-  std::vector<double> pos;     // distinct positions, 3 doubles each, chunk by chunk
-  std::vector<uint32_t> id;    // corner 3 * f + k -> its position's index within the chunk
-  int64_t max_positions = 0;   // the most distinct positions in one chunk
+// Distinct corner positions of one chunk of faces. Sized once for the largest
+// chunk, so listing a chunk allocates nothing.
+struct ChunkPositions {
+  std::vector<double> pos;   // 3 doubles per distinct position
+  std::vector<uint32_t> id;  // corner 3 * (f - f0) + k -> its position's index
+  std::vector<uint32_t> stamp, slot_id;
+  uint32_t slots = 0, gen = 0;
+  int64_t count = 0;
+
+  explicit ChunkPositions(int64_t faces) {
+    slots = 64;
+    while (slots < 6 * faces) slots *= 2;  // an open-addressing table at most half full
+    pos.resize(9 * static_cast<size_t>(faces));
+    id.resize(3 * static_cast<size_t>(faces));
+    stamp.assign(slots, 0);
+    slot_id.resize(slots);
+  }
 };
 
 inline uint64_t word(double x) {
@@ -293,97 +306,142 @@ inline uint64_t word(double x) {
   return u;
 }
 
-// Chunk lists of the soup's corner positions, chunks of chunk_faces faces (an
-// open-addressing table at most half full, reset per chunk by a stamp).
-CornerChunks build_corner_chunks(const double* tri, int64_t nf, int64_t chunk_faces) {
-  CornerChunks cc;
-  cc.chunk_faces = chunk_faces;
-  const int64_t nchunks = (nf + chunk_faces - 1) / chunk_faces;
-  uint32_t slots = 64;
-  while (slots < 6 * chunk_faces) slots *= 2;
-  cc.start.resize(nchunks + 1);
-  cc.id.resize(3 * nf);
-  cc.pos.reserve(3 * static_cast<size_t>(nf));
-  std::vector<uint32_t> stamp(slots, 0), slot_id(slots);
-  int64_t npos = 0;
-  for (int64_t c = 0; c < nchunks; ++c) {
-    const uint32_t gen = static_cast<uint32_t>(c) + 1;
-    cc.start[c] = npos;
-    const int64_t f1 = (c + 1) * chunk_faces < nf ? (c + 1) * chunk_faces : nf;
-    for (int64_t f = c * chunk_faces; f < f1; ++f)
-      for (int k = 0; k < 3; ++k) {
-        const double x = tri[3 * k * nf + f], y = tri[(3 * k + 1) * nf + f],
-                     z = tri[(3 * k + 2) * nf + f];
-        const uint64_t bx = word(x), by = word(y), bz = word(z);
-        uint64_t h = bx * 0x9E3779B97F4A7C15ULL ^ by * 0xC2B2AE3D27D4EB4FULL ^
-                     bz * 0x165667B19E3779F9ULL;
-        h ^= h >> 29;
-        for (uint32_t slot = static_cast<uint32_t>(h) & (slots - 1);;
-             slot = (slot + 1) & (slots - 1)) {
-          if (stamp[slot] != gen) {  // a new position of this chunk
-            stamp[slot] = gen;
-            slot_id[slot] = static_cast<uint32_t>(npos - cc.start[c]);
-            cc.pos.push_back(x);
-            cc.pos.push_back(y);
-            cc.pos.push_back(z);
-            cc.id[3 * f + k] = slot_id[slot];
-            ++npos;
-            break;
-          }
-          const double* p = &cc.pos[3 * (cc.start[c] + slot_id[slot])];
-          if (word(p[0]) == bx && word(p[1]) == by && word(p[2]) == bz) {
-            cc.id[3 * f + k] = slot_id[slot];
-            break;
-          }
+// Lists the distinct corner positions of faces [f0, f1) into cp.
+void list_chunk(const double* tri, int64_t nf, int64_t f0, int64_t f1, ChunkPositions& cp) {
+  const uint32_t gen = ++cp.gen;  // invalidates the previous chunk's table entries
+  const uint32_t mask = cp.slots - 1;
+  int64_t n = 0;
+  for (int64_t f = f0; f < f1; ++f)
+    for (int k = 0; k < 3; ++k) {
+      const double x = tri[3 * k * nf + f], y = tri[(3 * k + 1) * nf + f],
+                   z = tri[(3 * k + 2) * nf + f];
+      const uint64_t bx = word(x), by = word(y), bz = word(z);
+      uint64_t h = bx * 0x9E3779B97F4A7C15ULL ^ by * 0xC2B2AE3D27D4EB4FULL ^
+                   bz * 0x165667B19E3779F9ULL;
+      h ^= h >> 29;
+      for (uint32_t slot = static_cast<uint32_t>(h) & mask;; slot = (slot + 1) & mask) {
+        if (cp.stamp[slot] != gen) {  // a new position of this chunk
+          cp.stamp[slot] = gen;
+          cp.slot_id[slot] = static_cast<uint32_t>(n);
+          cp.pos[3 * n] = x;
+          cp.pos[3 * n + 1] = y;
+          cp.pos[3 * n + 2] = z;
+          cp.id[3 * (f - f0) + k] = static_cast<uint32_t>(n);
+          ++n;
+          break;
+        }
+        const double* p = &cp.pos[3 * static_cast<int64_t>(cp.slot_id[slot])];
+        if (word(p[0]) == bx && word(p[1]) == by && word(p[2]) == bz) {
+          cp.id[3 * (f - f0) + k] = cp.slot_id[slot];
+          break;
         }
       }
-    if (npos - cc.start[c] > cc.max_positions) cc.max_positions = npos - cc.start[c];
-  }
-  cc.start[nchunks] = npos;
-  return cc;
+    }
+  cp.count = n;
 }
 
-// winding_query8 with each chunk's corner lengths computed once per distinct
-// position into len (8 doubles per position, 64-byte aligned, cc.max_positions
-// of them) and read back by the faces.
-WN_AVX512 void winding_query8_shared(const double* tri, int64_t nf, const CornerChunks& cc,
-                                     double* len, const double* q, double* out) {
-  const __m512i idx = _mm512_set_epi64(21, 18, 15, 12, 9, 6, 3, 0);
-  const __m512d ox = _mm512_i64gather_pd(idx, q, 8);
-  const __m512d oy = _mm512_i64gather_pd(idx, q + 1, 8);
-  const __m512d oz = _mm512_i64gather_pd(idx, q + 2, 8);
-  Acc8 acc{_mm512_set1_pd(1.0), _mm512_setzero_pd(), _mm512_setzero_si512(), 0};
-  const int64_t nchunks = static_cast<int64_t>(cc.start.size()) - 1;
-  for (int64_t c = 0; c < nchunks; ++c) {
-    const double* p = &cc.pos[3 * cc.start[c]];
-    const int64_t np = cc.start[c + 1] - cc.start[c];
-    for (int64_t u = 0; u < np; ++u)
-      _mm512_store_pd(len + 8 * u, corner8(ox, oy, oz, p[3 * u], p[3 * u + 1], p[3 * u + 2]).l);
-    const int64_t cf = cc.chunk_faces;
-    const int64_t f1 = (c + 1) * cf < nf ? (c + 1) * cf : nf;
-    for (int64_t f = c * cf; f < f1; ++f) {
-      Corner8 v[3];
-      for (int k = 0; k < 3; ++k) {
-        v[k].x = _mm512_sub_pd(_mm512_set1_pd(tri[3 * k * nf + f]), ox);
-        v[k].y = _mm512_sub_pd(_mm512_set1_pd(tri[(3 * k + 1) * nf + f]), oy);
-        v[k].z = _mm512_sub_pd(_mm512_set1_pd(tri[(3 * k + 2) * nf + f]), oz);
-        v[k].l = _mm512_load_pd(len + 8 * static_cast<int64_t>(cc.id[3 * f + k]));
-      }
-      __m512d det, denom;
-      face8(v[0], v[1], v[2], det, denom);
-      push8(acc, denom, det);
+// Faces [f0, f1) for the block of eight queries (ox, oy, oz) into acc: the
+// chunk's lengths into len (8 doubles per position, 64-byte aligned), then the
+// faces with their corners' lengths read back.
+WN_AVX512 void chunk8(const double* tri, int64_t nf, int64_t f0, int64_t f1,
+                      const ChunkPositions& cp, double* len, __m512d ox, __m512d oy, __m512d oz,
+                      Acc8& acc) {
+  const double* p = cp.pos.data();
+  for (int64_t u = 0; u < cp.count; ++u)
+    _mm512_store_pd(len + 8 * u, corner8(ox, oy, oz, p[3 * u], p[3 * u + 1], p[3 * u + 2]).l);
+  const uint32_t* id = cp.id.data();
+  for (int64_t f = f0; f < f1; ++f) {
+    Corner8 v[3];
+    for (int k = 0; k < 3; ++k) {
+      v[k].x = _mm512_sub_pd(_mm512_set1_pd(tri[3 * k * nf + f]), ox);
+      v[k].y = _mm512_sub_pd(_mm512_set1_pd(tri[(3 * k + 1) * nf + f]), oy);
+      v[k].z = _mm512_sub_pd(_mm512_set1_pd(tri[(3 * k + 2) * nf + f]), oz);
+      v[k].l = _mm512_load_pd(len + 8 * static_cast<int64_t>(id[3 * (f - f0) + k]));
     }
+    __m512d det, denom;
+    face8(v[0], v[1], v[2], det, denom);
+    push8(acc, denom, det);
   }
-  alignas(64) double zr[8], zi[8];
-  alignas(64) int64_t k[8];
-  _mm512_store_pd(zr, acc.zr);
-  _mm512_store_pd(zi, acc.zi);
-  _mm512_store_si512(k, acc.k);
-  for (int j = 0; j < 8; ++j)
-    out[j] = ((acc.bad >> j) & 1)
-                 ? winding_query(tri, nf, q[3 * j], q[3 * j + 1], q[3 * j + 2])
-                 : (std::atan2(zi[j], zr[j]) + static_cast<double>(k[j]) * wn::kTwoPi) /
-                       wn::kTwoPi;
+}
+
+// The blocks of eight queries q[0 .. 24 nb) against every face with shared
+// corner lengths, into out[0 .. 8 nb). Chunks outermost, so that each chunk is
+// listed once for all blocks. Returns false, having written nothing, when the
+// mesh shares too few positions or its buffers cannot be allocated.
+WN_AVX512 bool winding_blocks8_shared(const double* tri, int64_t nf, const double* q,
+                                      int64_t nb, double* out) {
+  const __m512i idx = _mm512_set_epi64(21, 18, 15, 12, 9, 6, 3, 0);
+  try {
+    // Shared corners pay when the chunks hold fewer than 1.5 distinct positions
+    // per face, half the corners (measured: at 0.67 per corner, with lengths
+    // beyond L1, they cost more than they save).
+    int64_t cf = nf < kChunkFaces ? nf : kChunkFaces;
+    ChunkPositions cp(cf);  // its table sized for the chunk, so that it stays in cache
+    list_chunk(tri, nf, 0, cf, cp);
+    bool shared = 2 * cp.count < 3 * cf;
+    if (!shared && cf < nf && nf <= kWholeMeshFaces) {
+      cf = nf;
+      cp = ChunkPositions(nf);
+      list_chunk(tri, nf, 0, nf, cp);
+      shared = cp.count <= kWholeMeshPositions && 2 * cp.count < 3 * nf;
+    }
+    if (!shared) return false;
+    // Each block's accumulator between chunks: zr, zi, k and the bad mask as 32
+    // 8-byte words (a plain aligned buffer: no vector of AVX-512 types in code
+    // built for the baseline ISA).
+    double* state = static_cast<double*>(std::aligned_alloc(64, 256 * static_cast<size_t>(nb)));
+    double* len = static_cast<double*>(
+        std::aligned_alloc(64, 64 * (3 * static_cast<size_t>(cf) + 1)));
+    if (!state || !len) {
+      std::free(state);
+      std::free(len);
+      return false;
+    }
+    for (int64_t b = 0; b < nb; ++b) {
+      _mm512_store_pd(state + 32 * b, _mm512_set1_pd(1.0));
+      _mm512_store_pd(state + 32 * b + 8, _mm512_setzero_pd());
+      _mm512_store_si512(state + 32 * b + 16, _mm512_setzero_si512());
+      state[32 * b + 24] = 0.0;  // bad mask, as the low byte of the word's bits
+    }
+    for (int64_t f0 = 0; f0 < nf; f0 += cf) {
+      const int64_t f1 = f0 + cf < nf ? f0 + cf : nf;
+      if (f0 > 0) list_chunk(tri, nf, f0, f1, cp);
+      for (int64_t b = 0; b < nb; ++b) {
+        const double* qb = q + 24 * b;
+        double* sb = state + 32 * b;
+        uint64_t bad_word;
+        std::memcpy(&bad_word, sb + 24, 8);
+        Acc8 acc{_mm512_load_pd(sb), _mm512_load_pd(sb + 8), _mm512_load_si512(sb + 16),
+                 static_cast<__mmask8>(bad_word)};
+        chunk8(tri, nf, f0, f1, cp, len, _mm512_i64gather_pd(idx, qb, 8),
+               _mm512_i64gather_pd(idx, qb + 1, 8), _mm512_i64gather_pd(idx, qb + 2, 8), acc);
+        _mm512_store_pd(sb, acc.zr);
+        _mm512_store_pd(sb + 8, acc.zi);
+        _mm512_store_si512(sb + 16, acc.k);
+        bad_word = acc.bad;
+        std::memcpy(sb + 24, &bad_word, 8);
+      }
+    }
+    std::free(len);
+    for (int64_t b = 0; b < nb; ++b) {
+      const double* qb = q + 24 * b;
+      const double* sb = state + 32 * b;
+      int64_t k[8];
+      uint64_t bad_word;
+      std::memcpy(k, sb + 16, 64);
+      std::memcpy(&bad_word, sb + 24, 8);
+      for (int j = 0; j < 8; ++j)
+        out[8 * b + j] =
+            ((bad_word >> j) & 1)
+                ? winding_query(tri, nf, qb[3 * j], qb[3 * j + 1], qb[3 * j + 2])
+                : (std::atan2(sb[8 + j], sb[j]) + static_cast<double>(k[j]) * wn::kTwoPi) /
+                      wn::kTwoPi;
+    }
+    std::free(state);
+    return true;
+  } catch (const std::bad_alloc&) {
+    return false;
+  }
 }
 
 #undef WN_AVX512
@@ -406,23 +464,9 @@ void mli_winding(int64_t tri, int64_t q, int64_t dst, int64_t nf, int64_t nq, in
   const double* qq = reinterpret_cast<const double*>(q);
   double* d = reinterpret_cast<double*>(dst);
   int64_t qi = q0;
-  if (has_avx512() && q1 - q0 >= 8 && nf > 0) {
-    // Shared corners pay when the chunks hold at most half as many distinct
-    // positions as corners (measured: at 0.67 per corner with lengths beyond L1
-    // they cost more than they save).
-    CornerChunks cc = build_corner_chunks(t, nf, kChunkFaces);
-    bool shared = 2 * cc.start.back() < 3 * nf;
-    if (!shared && nf <= kWholeMeshFaces) {
-      cc = build_corner_chunks(t, nf, nf);
-      shared = cc.max_positions <= kWholeMeshPositions && 2 * cc.start.back() < 3 * nf;
-    }
-    double* len = shared ? static_cast<double*>(std::aligned_alloc(
-                               64, 64 * static_cast<size_t>(cc.max_positions + 1)))
-                         : nullptr;
-    if (len) {
-      for (; qi + 8 <= q1; qi += 8) winding_query8_shared(t, nf, cc, len, qq + 3 * qi, d + qi);
-      std::free(len);
-    }
+  if (has_avx512()) {
+    const int64_t nb = (q1 - q0) / 8;
+    if (nb > 0 && nf > 0 && winding_blocks8_shared(t, nf, qq + 3 * qi, nb, d + qi)) qi += 8 * nb;
     for (; qi + 8 <= q1; qi += 8) winding_query8(t, nf, qq + 3 * qi, d + qi);
   }
   for (; qi + 4 <= q1; qi += 4) winding_query4(t, nf, qq + 3 * qi, d + qi);

@@ -319,6 +319,14 @@ int wn_signed_distance_fast_device(void* tree, void* fast, double beta, const do
  * Returns 0, or 1 for a null argument. No reference counterpart. */
 int wn_closest_point(const double* p, const double* tri9, double* out4);
 
+/* Diagnostic: the eight-lane form of wn_closest_point that the host traversal
+ * uses for a leaf's faces (AVX-512), on eight triangles at once: tri72 = rows
+ * Ax, Ay, Az, Bx, By, Bz, Cx, Cy, Cz of eight doubles (one triangle per
+ * column); out32 = rows squared distance, x, y, z of eight. Every lane is the
+ * scalar function's bits. Returns 0, 1 for a null argument, 2 when the CPU has
+ * no AVX-512. No reference counterpart. */
+int wn_closest_point8(const double* p, const double* tri72, double* out32);
+
 /* Signed distance by the winding-number sign (no reference counterpart):
  * s[i] = -sqrt(sqrd) where |W(P_i)| > 1/2, else +sqrt(sqrd); W comes from the
  * winding-number mesh `mesh` (wn_mixed_mesh_create over the same faces) with

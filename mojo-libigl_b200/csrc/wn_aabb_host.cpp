@@ -19,6 +19,8 @@
 // before the right one, so a node with n faces owns the next count(n) indices,
 // count(n) = 1 for n <= leaf and 1 + count(n / 2) + count(n - n / 2) above.
 // That fixed numbering lets two subtrees be built at the same time.
+#include <immintrin.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -379,10 +381,121 @@ int64_t aabb_pack(const double* V, int64_t nv, const int64_t* F, int64_t nf, con
 
 namespace {
 
+// ---- a leaf's faces eight at a time (AVX-512) -------------------------------
+// closest_on_triangle on eight faces at once, one per 64-bit lane: every
+// quantity of every region (the Voronoi walk's vertex, edge and interior
+// cases) is computed in all lanes with the scalar code's IEEE operations in the
+// same order (this file is built without FMA contraction; vector add, multiply
+// and divide round like their scalar forms), and each lane keeps the region the
+// scalar code would enter, decided by the same comparisons (ordered: false on
+// NaN, like C's). A lane whose triangle is degenerate (|denom| <= 1e-30 in the
+// interior case) is redone by the scalar function. So every lane's squared
+// distance and closest point are the scalar bits, and the caller still takes
+// the faces one by one in leaf order with the strict `<` update.
+
+#define WN_AVX512 __attribute__((target("avx512f,avx512dq")))
+
+struct Vec3x8 {
+  __m512d x, y, z;
+};
+
+WN_AVX512 inline Vec3x8 sub3(const Vec3x8& a, const Vec3x8& b) {
+  return {_mm512_sub_pd(a.x, b.x), _mm512_sub_pd(a.y, b.y), _mm512_sub_pd(a.z, b.z)};
+}
+
+WN_AVX512 inline __m512d dot3x8(const Vec3x8& a, const Vec3x8& b) {
+  return _mm512_add_pd(_mm512_add_pd(_mm512_mul_pd(a.x, b.x), _mm512_mul_pd(a.y, b.y)),
+                       _mm512_mul_pd(a.z, b.z));
+}
+
+// o + t * e, per component as the scalar dadd(o, dmul(t, e)).
+WN_AVX512 inline Vec3x8 along(const Vec3x8& o, __m512d t, const Vec3x8& e) {
+  return {_mm512_add_pd(o.x, _mm512_mul_pd(t, e.x)), _mm512_add_pd(o.y, _mm512_mul_pd(t, e.y)),
+          _mm512_add_pd(o.z, _mm512_mul_pd(t, e.z))};
+}
+
+// a <= b and a >= b per lane, false on NaN (C's relational operators).
+WN_AVX512 inline __mmask8 le(__m512d a, __m512d b) { return _mm512_cmp_pd_mask(a, b, _CMP_LE_OQ); }
+WN_AVX512 inline __mmask8 ge(__m512d a, __m512d b) { return _mm512_cmp_pd_mask(a, b, _CMP_GE_OQ); }
+
+WN_AVX512 inline Vec3x8 pick(__mmask8 m, const Vec3x8& a, const Vec3x8& b) {  // m ? b : a
+  return {_mm512_mask_blend_pd(m, a.x, b.x), _mm512_mask_blend_pd(m, a.y, b.y),
+          _mm512_mask_blend_pd(m, a.z, b.z)};
+}
+
+// tri: 9 x 8 doubles (A xyz, B xyz, C xyz rows, one face per column).
+// out: d2, x, y, z rows of 8. Lanes not in `live` are computed but unused.
+WN_AVX512 void closest8(double px, double py, double pz, const double* tri, double* out) {
+  const Vec3x8 P{_mm512_set1_pd(px), _mm512_set1_pd(py), _mm512_set1_pd(pz)};
+  const Vec3x8 A{_mm512_load_pd(tri), _mm512_load_pd(tri + 8), _mm512_load_pd(tri + 16)};
+  const Vec3x8 B{_mm512_load_pd(tri + 24), _mm512_load_pd(tri + 32), _mm512_load_pd(tri + 40)};
+  const Vec3x8 C{_mm512_load_pd(tri + 48), _mm512_load_pd(tri + 56), _mm512_load_pd(tri + 64)};
+  const __m512d zero = _mm512_setzero_pd();
+  const Vec3x8 ab = sub3(B, A), ac = sub3(C, A), ap = sub3(P, A);
+  const __m512d d1 = dot3x8(ab, ap), d2 = dot3x8(ac, ap);
+  const Vec3x8 bp = sub3(P, B);
+  const __m512d d3 = dot3x8(ab, bp), d4 = dot3x8(ac, bp);
+  const __m512d vc = _mm512_sub_pd(_mm512_mul_pd(d1, d4), _mm512_mul_pd(d3, d2));
+  const Vec3x8 cp = sub3(P, C);
+  const __m512d d5 = dot3x8(ab, cp), d6 = dot3x8(ac, cp);
+  const __m512d vb = _mm512_sub_pd(_mm512_mul_pd(d5, d2), _mm512_mul_pd(d1, d6));
+  const __m512d va = _mm512_sub_pd(_mm512_mul_pd(d3, d6), _mm512_mul_pd(d5, d4));
+  const __m512d u43 = _mm512_sub_pd(d4, d3), u56 = _mm512_sub_pd(d5, d6);
+  const __m512d denom = _mm512_add_pd(_mm512_add_pd(va, vb), vc);
+  // The scalar code's regions, first match wins.
+  const __mmask8 r0 = le(d1, zero) & le(d2, zero);                 // vertex A
+  const __mmask8 r1 = ge(d3, zero) & le(d4, d3);                   // vertex B
+  const __mmask8 r2 = le(vc, zero) & ge(d1, zero) & le(d3, zero);  // edge AB
+  const __mmask8 r3 = ge(d6, zero) & le(d5, d6);                   // vertex C
+  const __mmask8 r4 = le(vb, zero) & ge(d2, zero) & le(d6, zero);  // edge AC
+  const __mmask8 r5 = le(va, zero) & ge(u43, zero) & ge(u56, zero);  // edge BC
+  const __mmask8 rd =
+      _mm512_cmp_pd_mask(_mm512_abs_pd(denom), _mm512_set1_pd(1.0e-30), _CMP_LE_OQ);
+  const __m512d inv = _mm512_div_pd(_mm512_set1_pd(1.0), denom);
+  const __m512d v = _mm512_mul_pd(vb, inv), w = _mm512_mul_pd(vc, inv);
+  Vec3x8 q{_mm512_add_pd(_mm512_add_pd(A.x, _mm512_mul_pd(ab.x, v)), _mm512_mul_pd(ac.x, w)),
+           _mm512_add_pd(_mm512_add_pd(A.y, _mm512_mul_pd(ab.y, v)), _mm512_mul_pd(ac.y, w)),
+           _mm512_add_pd(_mm512_add_pd(A.z, _mm512_mul_pd(ab.z, v)), _mm512_mul_pd(ac.z, w))};
+  // Apply the regions from the last to the first, so the first match is what stays.
+  const Vec3x8 bc = sub3(C, B);
+  q = pick(r5, q, along(B, _mm512_div_pd(u43, _mm512_add_pd(u43, u56)), bc));
+  q = pick(r4, q, along(A, _mm512_div_pd(d2, _mm512_sub_pd(d2, d6)), ac));
+  q = pick(r3, q, C);
+  q = pick(r2, q, along(A, _mm512_div_pd(d1, _mm512_sub_pd(d1, d3)), ab));
+  q = pick(r1, q, B);
+  q = pick(r0, q, A);
+  const Vec3x8 dq = sub3(P, q);
+  _mm512_store_pd(out, dot3x8(dq, dq));
+  _mm512_store_pd(out + 8, q.x);
+  _mm512_store_pd(out + 16, q.y);
+  _mm512_store_pd(out + 24, q.z);
+  // Degenerate triangles (interior case with |denom| <= 1e-30): the scalar walk.
+  __mmask8 redo = static_cast<__mmask8>(rd & ~(r0 | r1 | r2 | r3 | r4 | r5));
+  while (redo) {
+    const int j = __builtin_ctz(redo);
+    redo = static_cast<__mmask8>(redo & (redo - 1));
+    const wn::ClosestHit h = wn::closest_on_triangle(
+        px, py, pz, tri[j], tri[8 + j], tri[16 + j], tri[24 + j], tri[32 + j], tri[40 + j],
+        tri[48 + j], tri[56 + j], tri[64 + j]);
+    out[j] = h.d2;
+    out[8 + j] = h.x;
+    out[16 + j] = h.y;
+    out[24 + j] = h.z;
+  }
+}
+
+#undef WN_AVX512
+
+bool has_avx512() {
+  static const bool yes = __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("avx512dq");
+  return yes;
+}
+
 // capi.mojo:522-586 for one query.
 void query_one(const double* p, const double* v, const int64_t* f, const double* boxes,
                const int64_t* nodes, const int64_t* order, double* sqrd, int64_t* index,
-               double* closest, int64_t* stack, int64_t nnodes, int64_t qi) {
+               double* closest, int64_t* stack, double* stack_d2, int64_t nnodes, int64_t qi,
+               bool vector8) {
   const double px = p[3 * qi], py = p[3 * qi + 1], pz = p[3 * qi + 2];
   auto box = [&](int64_t n) {
     const double* b = boxes + 6 * n;
@@ -392,11 +505,39 @@ void query_one(const double* p, const double* v, const int64_t* f, const double*
   int64_t best_face = -1;
   int64_t sp = 1;
   stack[0] = 0;
+  // Each entry keeps the box distance computed when it was pushed: the
+  // reference recomputes it at the pop from the same box and point, which is
+  // the same double, so the pop test is unchanged.
+  stack_d2[0] = nnodes > 0 ? box(0) : 0.0;
   while (sp > 0) {
     const int64_t node = stack[--sp];
-    if (node < 0 || node >= nnodes || box(node) > best) continue;
+    if (node < 0 || node >= nnodes || stack_d2[sp] > best) continue;
     const int64_t* nd = nodes + 4 * node;
-    if (nd[3] > 0) {
+    if (nd[3] > 0 && vector8) {
+      // Eight faces at a time through closest8, then taken one by one in order.
+      alignas(64) double tri[72], hit[32];
+      for (int64_t k0 = nd[2]; k0 < nd[2] + nd[3]; k0 += 8) {
+        const int n = static_cast<int>(std::min<int64_t>(8, nd[2] + nd[3] - k0));
+        for (int j = 0; j < 8; ++j) {
+          const int64_t fi = order[k0 + (j < n ? j : 0)];
+          for (int c = 0; c < 3; ++c) {
+            const double* X = v + 3 * f[3 * fi + c];
+            tri[24 * c + j] = X[0];
+            tri[24 * c + 8 + j] = X[1];
+            tri[24 * c + 16 + j] = X[2];
+          }
+        }
+        closest8(px, py, pz, tri, hit);
+        for (int j = 0; j < n; ++j)
+          if (hit[j] < best) {
+            best = hit[j];
+            best_face = order[k0 + j];
+            bx = hit[8 + j];
+            by = hit[16 + j];
+            bz = hit[24 + j];
+          }
+      }
+    } else if (nd[3] > 0) {
       for (int64_t k = nd[2]; k < nd[2] + nd[3]; ++k) {
         const int64_t fi = order[k];
         const double* A = v + 3 * f[3 * fi];
@@ -417,8 +558,14 @@ void query_one(const double* p, const double* v, const int64_t* f, const double*
       const double dl = box(nd[0]), dr = box(nd[1]);
       const bool left_near = dl < dr;
       const int64_t first = left_near ? nd[1] : nd[0], second = left_near ? nd[0] : nd[1];
-      if ((left_near ? dr : dl) <= best) stack[sp++] = first;
-      if ((left_near ? dl : dr) <= best) stack[sp++] = second;
+      if ((left_near ? dr : dl) <= best) {
+        stack_d2[sp] = left_near ? dr : dl;
+        stack[sp++] = first;
+      }
+      if ((left_near ? dl : dr) <= best) {
+        stack_d2[sp] = left_near ? dl : dr;
+        stack[sp++] = second;
+      }
     }
   }
   sqrd[qi] = best;
@@ -441,13 +588,17 @@ void mli_aabb_squared_distance(int64_t p, int64_t v, int64_t f, int64_t boxes, i
                                int64_t stack, int64_t np, int64_t nnodes, int64_t q0,
                                int64_t q1) {
   (void)np;
+  const bool vector8 = has_avx512();
+  // Distances beside the caller's stack: a node is pushed at most once per
+  // query, so nnodes + 1 entries always suffice.
+  std::vector<double> stack_d2(static_cast<size_t>(nnodes > 0 ? nnodes : 0) + 1);
   for (int64_t qi = q0; qi < q1; ++qi)
     query_one(reinterpret_cast<const double*>(p), reinterpret_cast<const double*>(v),
               reinterpret_cast<const int64_t*>(f), reinterpret_cast<const double*>(boxes),
               reinterpret_cast<const int64_t*>(nodes), reinterpret_cast<const int64_t*>(order),
               reinterpret_cast<double*>(sqrd), reinterpret_cast<int64_t*>(indices),
-              reinterpret_cast<double*>(closest), reinterpret_cast<int64_t*>(stack), nnodes,
-              qi);
+              reinterpret_cast<double*>(closest), reinterpret_cast<int64_t*>(stack),
+              stack_d2.data(), nnodes, qi, vector8);
 }
 
 // Diagnostic (no reference counterpart): the closest point on one triangle
@@ -463,6 +614,21 @@ int wn_closest_point(const double* p, const double* tri9, double* out4) {
   out4[1] = h.x;
   out4[2] = h.y;
   out4[3] = h.z;
+  return 0;
+}
+
+// Diagnostic (no reference counterpart): closest8, the eight-lane form the
+// host traversal uses for leaf faces, on eight triangles (tri72: rows Ax, Ay,
+// Az, Bx, ..., Cz of eight doubles) from p; out32 = rows d2, x, y, z of eight.
+// Lets tests pin every lane against the scalar arithmetic. Returns 0, 1 for a
+// null argument, 2 when the CPU has no AVX-512.
+int wn_closest_point8(const double* p, const double* tri72, double* out32) {
+  if (!p || !tri72 || !out32) return 1;
+  if (!has_avx512()) return 2;
+  alignas(64) double tri[72], hit[32];
+  std::copy(tri72, tri72 + 72, tri);
+  closest8(p[0], p[1], p[2], tri, hit);
+  std::copy(hit, hit + 32, out32);
   return 0;
 }
 

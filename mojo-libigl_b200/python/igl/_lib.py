@@ -91,6 +91,7 @@ _WN_SIGNATURES = {
     "wn_aabb_squared_distance_host": ([P, P, I, P, P, P], C_INT),
     "wn_signed_distance_device": ([P, P, C_INT, P, I, P, P, P, P, P], C_INT),
     "wn_closest_point": ([P, P, P], C_INT),
+    "wn_closest_point8": ([P, P, P], C_INT),
     "wn_signed_distance_fast_device": ([P, P, ctypes.c_double, P, I, P, P, P, P, P], C_INT),
     "wn_normals_create": ([P, I, I, P, ctypes.POINTER(P)], C_INT),
     "wn_normals_destroy": ([P], C_INT),

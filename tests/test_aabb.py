@@ -245,3 +245,30 @@ def test_signed_distance_fast_sign_cpu():
     assert np.array_equal(np.sign(fast), np.sign(exact))
     with pytest.raises(ValueError):
         igl.signed_distance(P, V, F, precision="half")
+
+
+def test_closest_point_eight_lanes_match_oracle_bitwise(oracle_mod):
+    """The host traversal takes a leaf's faces eight at a time (AVX-512): every
+    lane must give the scalar arithmetic's bits, for the point of each of the
+    eight adversarial triangles in turn (slivers, collinear and repeated corners,
+    points, scales, and points on vertices, edges and faces)."""
+    lib = igl.lib()
+    rng = np.random.default_rng(101)
+    tris, pts = _adversarial_triangles(rng, 4000)
+    tri72 = np.empty(72)
+    out = np.empty(32)
+    for g in range(0, len(tris), 8):
+        group = tris[g:g + 8]  # (8, 9): A xyz, B xyz, C xyz per triangle
+        tri72[:] = group.T.ravel()
+        for p in pts[g:g + 8]:
+            p = np.ascontiguousarray(p)
+            rc = lib.wn_closest_point8(p.ctypes.data, tri72.ctypes.data, out.ctypes.data)
+            if rc == 2:
+                pytest.skip("no AVX-512 on this CPU")
+            assert rc == 0
+            got = out.reshape(4, 8).T  # (8, 4): d2, x, y, z per lane
+            for t, lane in zip(group, got):
+                expected = np.array(oracle_mod.closest_point(p, t))
+                assert lane.tobytes() == expected.tobytes() or (
+                    np.isnan(lane).any() and np.array_equal(np.isnan(lane), np.isnan(expected))), (
+                    t, p, lane, expected)

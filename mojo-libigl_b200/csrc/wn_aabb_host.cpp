@@ -25,6 +25,8 @@
 #include <atomic>
 #include <cmath>
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <thread>
 #include <unordered_map>
 #include <utility>
@@ -508,10 +510,10 @@ void query_one(const double* p, const double* v, const int64_t* f, const double*
   // Each entry keeps the box distance computed when it was pushed: the
   // reference recomputes it at the pop from the same box and point, which is
   // the same double, so the pop test is unchanged.
-  stack_d2[0] = nnodes > 0 ? box(0) : 0.0;
+  if (stack_d2) stack_d2[0] = nnodes > 0 ? box(0) : 0.0;
   while (sp > 0) {
     const int64_t node = stack[--sp];
-    if (node < 0 || node >= nnodes || stack_d2[sp] > best) continue;
+    if (node < 0 || node >= nnodes || (stack_d2 ? stack_d2[sp] : box(node)) > best) continue;
     const int64_t* nd = nodes + 4 * node;
     if (nd[3] > 0 && vector8) {
       // Eight faces at a time through closest8, then taken one by one in order.
@@ -559,11 +561,11 @@ void query_one(const double* p, const double* v, const int64_t* f, const double*
       const bool left_near = dl < dr;
       const int64_t first = left_near ? nd[1] : nd[0], second = left_near ? nd[0] : nd[1];
       if ((left_near ? dr : dl) <= best) {
-        stack_d2[sp] = left_near ? dr : dl;
+        if (stack_d2) stack_d2[sp] = left_near ? dr : dl;
         stack[sp++] = first;
       }
       if ((left_near ? dl : dr) <= best) {
-        stack_d2[sp] = left_near ? dl : dr;
+        if (stack_d2) stack_d2[sp] = left_near ? dl : dr;
         stack[sp++] = second;
       }
     }
@@ -590,15 +592,17 @@ void mli_aabb_squared_distance(int64_t p, int64_t v, int64_t f, int64_t boxes, i
   (void)np;
   const bool vector8 = has_avx512();
   // Distances beside the caller's stack: a node is pushed at most once per
-  // query, so nnodes + 1 entries always suffice.
-  std::vector<double> stack_d2(static_cast<size_t>(nnodes > 0 ? nnodes : 0) + 1);
+  // query, so nnodes + 1 entries always suffice. Without the memory the pop
+  // recomputes the distance, as the reference does.
+  std::unique_ptr<double[]> stack_d2(
+      new (std::nothrow) double[static_cast<size_t>(nnodes > 0 ? nnodes : 0) + 1]);
   for (int64_t qi = q0; qi < q1; ++qi)
     query_one(reinterpret_cast<const double*>(p), reinterpret_cast<const double*>(v),
               reinterpret_cast<const int64_t*>(f), reinterpret_cast<const double*>(boxes),
               reinterpret_cast<const int64_t*>(nodes), reinterpret_cast<const int64_t*>(order),
               reinterpret_cast<double*>(sqrd), reinterpret_cast<int64_t*>(indices),
               reinterpret_cast<double*>(closest), reinterpret_cast<int64_t*>(stack),
-              stack_d2.data(), nnodes, qi, vector8);
+              stack_d2.get(), nnodes, qi, vector8);
 }
 
 // Diagnostic (no reference counterpart): the closest point on one triangle

@@ -272,3 +272,30 @@ def test_closest_point_eight_lanes_match_oracle_bitwise(oracle_mod):
                 assert lane.tobytes() == expected.tobytes() or (
                     np.isnan(lane).any() and np.array_equal(np.isnan(lane), np.isnan(expected))), (
                     t, p, lane, expected)
+
+
+@pytest.mark.parametrize("leaf", [1, 5, 16, 37])
+def test_host_query_on_other_leaf_sizes_matches_oracle(oracle_mod, leaf):
+    """Trees whose leaves hold more or fewer than eight faces: the host query
+    takes a leaf's faces in groups of eight lanes (a partial last group
+    included) and must still match the oracle's scalar walk bit for bit, ties
+    and duplicated faces included."""
+    V, F = _flat_grid_with_duplicates()
+    P = np.concatenate([np.column_stack([np.arange(30.0), np.arange(30.0), np.zeros(30)]),
+                        np.random.default_rng(leaf).uniform([-3, -3, -2], [32, 32, 2], (500, 3))])
+    boxes, nodes, order, stack_size = oracle_mod.build_aabb(V, F, leaf_size=leaf)
+    expected = oracle_mod.aabb_squared_distance(P, V, F, tree=(boxes, nodes, order, stack_size))
+    n = len(P)
+    sqrd = np.empty(n)
+    index = np.empty(n, dtype=np.int64)
+    closest = np.empty((n, 3))
+    stack = np.empty(stack_size, dtype=np.int64)
+    Pc = np.ascontiguousarray(P)
+    Vc = np.ascontiguousarray(V, dtype=np.float64)
+    Fc = np.ascontiguousarray(F, dtype=np.int64)
+    igl.lib().mli_aabb_squared_distance(
+        Pc.ctypes.data, Vc.ctypes.data, Fc.ctypes.data, boxes.ctypes.data, nodes.ctypes.data,
+        order.ctypes.data, sqrd.ctypes.data, index.ctypes.data, closest.ctypes.data,
+        stack.ctypes.data, n, len(nodes), 0, n)
+    for a, b in zip((sqrd, index, closest), expected):
+        assert np.array_equal(a, b)

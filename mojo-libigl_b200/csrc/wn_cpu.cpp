@@ -390,8 +390,10 @@ WN_AVX512 bool winding_blocks8_shared(const double* tri, int64_t nf, const doubl
     // 8-byte words (a plain aligned buffer: no vector of AVX-512 types in code
     // built for the baseline ISA).
     double* state = static_cast<double*>(std::aligned_alloc(64, 256 * static_cast<size_t>(nb)));
-    double* len = static_cast<double*>(
-        std::aligned_alloc(64, 64 * (3 * static_cast<size_t>(cf) + 1)));
+    // Lengths of one chunk's positions: at most three per face, or the whole
+    // mesh's count when it is one chunk.
+    const size_t npos = cf == nf ? static_cast<size_t>(cp.count) : 3 * static_cast<size_t>(cf);
+    double* len = static_cast<double*>(std::aligned_alloc(64, 64 * (npos + 1)));
     if (!state || !len) {
       std::free(state);
       std::free(len);

@@ -340,6 +340,22 @@ void list_chunk(const double* tri, int64_t nf, int64_t f0, int64_t f1, ChunkPosi
   cp.count = n;
 }
 
+// Chooses the chunks of the shared-corner path: cf faces per chunk, the first
+// chunk listed in cp. Shared corners pay when the chunks hold fewer than 1.5
+// distinct positions per face, half the corners (measured: at 0.67 per corner,
+// with lengths beyond L1, they cost more than they save); false otherwise.
+bool plan_shared(const double* tri, int64_t nf, ChunkPositions& cp, int64_t& cf) {
+  cf = nf < kChunkFaces ? nf : kChunkFaces;
+  cp = ChunkPositions(cf);  // its table sized for the chunk, so that it stays in cache
+  list_chunk(tri, nf, 0, cf, cp);
+  if (2 * cp.count < 3 * cf) return true;
+  if (cf == nf || nf > kWholeMeshFaces) return false;
+  cf = nf;
+  cp = ChunkPositions(nf);
+  list_chunk(tri, nf, 0, nf, cp);
+  return cp.count <= kWholeMeshPositions && 2 * cp.count < 3 * nf;
+}
+
 // Faces [f0, f1) for the block of eight queries (ox, oy, oz) into acc: the
 // chunk's lengths into len (8 doubles per position, 64-byte aligned), then the
 // faces with their corners' lengths read back.
@@ -372,20 +388,9 @@ WN_AVX512 bool winding_blocks8_shared(const double* tri, int64_t nf, const doubl
                                       int64_t nb, double* out) {
   const __m512i idx = _mm512_set_epi64(21, 18, 15, 12, 9, 6, 3, 0);
   try {
-    // Shared corners pay when the chunks hold fewer than 1.5 distinct positions
-    // per face, half the corners (measured: at 0.67 per corner, with lengths
-    // beyond L1, they cost more than they save).
-    int64_t cf = nf < kChunkFaces ? nf : kChunkFaces;
-    ChunkPositions cp(cf);  // its table sized for the chunk, so that it stays in cache
-    list_chunk(tri, nf, 0, cf, cp);
-    bool shared = 2 * cp.count < 3 * cf;
-    if (!shared && cf < nf && nf <= kWholeMeshFaces) {
-      cf = nf;
-      cp = ChunkPositions(nf);
-      list_chunk(tri, nf, 0, nf, cp);
-      shared = cp.count <= kWholeMeshPositions && 2 * cp.count < 3 * nf;
-    }
-    if (!shared) return false;
+    ChunkPositions cp(0);
+    int64_t cf = 0;
+    if (!plan_shared(tri, nf, cp, cf)) return false;
     // Each block's accumulator between chunks: zr, zi, k and the bad mask as 32
     // 8-byte words (a plain aligned buffer: no vector of AVX-512 types in code
     // built for the baseline ISA).

@@ -275,6 +275,12 @@ def test_shared_corner_lengths_equal_the_scalar_path():
             handle.mli_winding(tri.ctypes.data, O.ctypes.data, single.ctypes.data,
                                tri.shape[1], len(O), i, i + 1)
         assert np.array_equal(whole, single, equal_nan=True)
+        # A span that starts off a block boundary and leaves the rest untouched.
+        part = np.full(len(O), 7.0)
+        handle.mli_winding(tri.ctypes.data, O.ctypes.data, part.ctypes.data, tri.shape[1],
+                           len(O), 3, len(O) - 1)
+        assert np.array_equal(part[3:-1], single[3:-1], equal_nan=True)
+        assert np.all(part[:3] == 7.0) and part[-1] == 7.0
     empty = np.zeros((9, 0))
     O = rng.uniform(-1.0, 1.0, size=(9, 3))
     out = np.full(9, 7.0)

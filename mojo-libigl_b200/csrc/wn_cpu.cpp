@@ -7,6 +7,9 @@
 // the shared bit-exact ones (wn_pair.cuh; this file is built with
 // -ffp-contract=off) and the angles are summed with the argument-of-product
 // accumulator, with plain atan2 as the recovery path for a bad accumulator.
+// Queries go 8 (AVX-512) or 4 (AVX2) per vector; on meshes the AVX-512 path
+// computes each distinct corner position's |v - o| once per block of queries
+// (see "corners shared between faces"). Every result is the scalar routine's.
 #include <immintrin.h>
 
 #include <cmath>
